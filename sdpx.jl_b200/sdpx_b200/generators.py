@@ -1,0 +1,154 @@
+"""Seeded synthetic SDP instances.
+
+* `gate_closed_form`, `gate_dense`: the reference's deterministic gate problems
+  (benchmark/gates.jl:96-199), rebuilt from the same written-out 64-bit LCG so
+  they are bit-identical to the ones SDPX records baselines for.
+* `toy_t1`: the 2×2 toy problem of test/correctness.jl:65-80 (optimum 2√6).
+* `sdpa_dense`: strictly feasible dense SDPs in SDPA primal-dual form, mapped to
+  SDPX's core form.  With `blocks=[50], lp=0, m=100` this is the n=50/m=100
+  workload; with `blocks=[400, 200], lp=500, m=2000` it is the two-block plus
+  500-nonnegatives workload at m=2000.
+
+SDPA form:  max bᵀy  s.t.  Z = C − Σ yᵢAᵢ ⪰ 0  (dual of min ⟨C,X⟩, ⟨Aᵢ,X⟩ = bᵢ).
+SDPX form:  min cᵀx  s.t.  X = Σ xᵢÂᵢ − Ĉ ⪰ 0  with x ≡ y, Âᵢ = −Aᵢ, Ĉ = −C,
+c = −b (src/ir/lower_sdp.jl objective sign at :497-501).  SDPX's slack X is
+SDPA's Z and SDPX's dual Y is SDPA's X; objectives change sign.
+"""
+from __future__ import annotations
+
+from typing import List, Sequence
+
+import numpy as np
+
+from .problem import SDPProblem, ingest
+
+_MASK64 = (1 << 64) - 1
+
+
+class GateStream:
+    """The reference's reproducible LCG (benchmark/gates.jl:96-113)."""
+
+    def __init__(self, seed: int):
+        self.state = seed & _MASK64
+
+    def uniform(self) -> float:
+        self.state = (0x5851F42D4C957F2D * self.state + 0x14057B7EF767814F) & _MASK64
+        return float(self.state >> 11) / float(1 << 53)
+
+    def signed(self) -> float:
+        return 2.0 * self.uniform() - 1.0
+
+
+def gate_closed_form() -> SDPProblem:
+    """`closed_form_sdp` (benchmark/gates.jl:118-140); optimum 2√6."""
+    A = np.zeros((2, 2, 2))
+    A[0, 0, 0] = 1.0
+    A[1, 1, 1] = 1.0
+    return ingest([2.0, 3.0], [A], [np.array([[0.0, 1.0], [1.0, 0.0]])])
+
+
+def toy_t1() -> SDPProblem:
+    """T1 of test/correctness.jl:65-80: min 2x₁+3x₂ s.t. [[x₁,−1],[−1,x₂]] ⪰ 0."""
+    A = np.zeros((2, 2, 2))
+    A[0, 0, 0] = 1.0
+    A[1, 1, 1] = 1.0
+    C = np.array([[0.0, 1.0], [1.0, 0.0]])
+    return ingest([2.0, 3.0], [A], [C])
+
+
+def gate_dense(variables: int = 180, side: int = 8, blocks: int = 3, seed: int = 5) -> SDPProblem:
+    """`dense_sdp` (benchmark/gates.jl:151-199).  Julia comprehensions fill
+    column-major, so the side×side draw is filled column by column."""
+    s = GateStream(seed)
+    coef = [np.zeros((variables, side, side)) for _ in range(blocks)]
+    for blk in range(blocks):
+        for var in range(variables):
+            entry = np.empty((side, side))
+            for col in range(side):
+                for row in range(side):
+                    entry[row, col] = s.signed()
+            coef[blk][var] = entry + entry.T
+    interior = np.array([s.signed() for _ in range(variables)])
+    constants = []
+    objective = np.zeros(variables)
+    for blk in range(blocks):
+        combination = np.zeros((side, side))
+        for var in range(variables):
+            combination += interior[var] * coef[blk][var]
+        constants.append(combination - np.eye(side))
+        factor = np.empty((side, side))
+        for col in range(side):
+            for row in range(side):
+                factor[row, col] = s.signed()
+        dual = factor @ factor.T + side * np.eye(side)
+        for var in range(variables):
+            objective[var] += float(np.sum(coef[blk][var] * dual))
+    return ingest(objective, coef, constants)
+
+
+def sdpa_dense(m: int, blocks: Sequence[int], lp: int = 0, seed: int = 0,
+               dtype=np.float64) -> SDPProblem:
+    """Strictly feasible dense SDP (SDPA primal-dual form) in SDPX core form.
+
+    Draw order from `numpy.random.default_rng(seed)`, per PSD block of order n:
+    G (m×n×n, N(0,1)) with Aᵢ = (G+Gᵀ)/2, then W (n×n, N(0,1)) with
+    X0 = I + 0.1·WWᵀ/n; for the LP block (`lp` nonnegatives): aᵢ (m×lp,
+    N(0,1)) then x0 ~ U(0.5,1.5).  Then y0 ~ N(0,1)^m; then per PSD block
+    V (n×n) with Z0 = I + 0.1·VVᵀ/n; then the LP slack s0 ~ U(0.5,1.5).
+    b_i = Σ_l ⟨A_i^l, X0_l⟩ + a_iᵀx0,  C_l = Σ y0_i A_i^l + Z0_l,
+    c_lp = Σ y0_i a_i + s0.  The LP block becomes `lp` 1×1 PSD blocks.
+    """
+    rng = np.random.default_rng(seed)
+    As: List[np.ndarray] = []
+    X0s: List[np.ndarray] = []
+    for n in blocks:
+        G = rng.standard_normal((m, n, n))
+        A = G + np.transpose(G, (0, 2, 1))
+        A *= 0.5
+        del G
+        W = rng.standard_normal((n, n))
+        As.append(A)
+        X0s.append(np.eye(n) + 0.1 * (W @ W.T) / n)
+    if lp > 0:
+        a_lp = rng.standard_normal((m, lp))
+        x0_lp = rng.uniform(0.5, 1.5, lp)
+    b = np.zeros(m)
+    for A, X0 in zip(As, X0s):
+        b += A.reshape(m, -1) @ X0.reshape(-1)
+    if lp > 0:
+        b += a_lp @ x0_lp
+    y0 = rng.standard_normal(m)
+    Cs = []
+    for A, n in zip(As, blocks):
+        V = rng.standard_normal((n, n))
+        Z0 = np.eye(n) + 0.1 * (V @ V.T) / n
+        Cs.append((y0 @ A.reshape(m, -1)).reshape(n, n) + Z0)
+    if lp > 0:
+        s0 = rng.uniform(0.5, 1.5, lp)
+        c_lp = y0 @ a_lp + s0
+    # Map to SDPX: Âᵢ = −Aᵢ, Ĉ = −C, c = −b.
+    A_sdpx = [-A for A in As]
+    C_sdpx = [-C for C in Cs]
+    if lp > 0:
+        A_sdpx.append(-a_lp.reshape(m, lp, 1, 1))
+        C_sdpx.append(-c_lp)
+    return _assemble(-b, A_sdpx, C_sdpx, list(blocks), lp)
+
+
+def _assemble(c, A_sdpx, C_sdpx, blocks, lp) -> SDPProblem:
+    """Build the container without the O(m k²) symmetry re-checks of `ingest`
+    (the generator symmetrises by construction)."""
+    m = c.shape[0]
+    ks, Av, Cs = [], [], []
+    for A, C, n in zip(A_sdpx[:len(blocks)], C_sdpx[:len(blocks)], blocks):
+        ks.append(n)
+        Av.append(np.ascontiguousarray(A.reshape(m, n * n)))
+        Cs.append(np.ascontiguousarray(C))
+    if lp > 0:
+        a = A_sdpx[-1].reshape(m, lp)
+        cvec = C_sdpx[-1]
+        for j in range(lp):
+            ks.append(1)
+            Av.append(np.ascontiguousarray(a[:, j:j + 1]))
+            Cs.append(np.array([[cvec[j]]]))
+    return SDPProblem(np.ascontiguousarray(c), ks, Av, Cs, np.zeros((m, 0)), np.zeros(0))

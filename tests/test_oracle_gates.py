@@ -1,0 +1,76 @@
+"""Pin the CPU oracle (shared host driver + NumPy restatement of the Float64
+kernels) against the reference's own golden solves.
+
+The gate comparison rules are the reference's (benchmark/gates.jl:58-77,
+287-330): same status, iterations within ±1, objective within 1e-9 relative,
+residuals and gap no worse than 10× the recorded baseline (absolute floor
+1e-10).  T1 follows test/correctness.jl:65-95,236-254 (fixed policy, 19 ± 2
+iterations, objective within 1e-8 of 2√6).
+"""
+import json
+import math
+import os
+
+import pytest
+
+from sdpx_b200 import SolverOptions, generators as G
+from oracle.sdpx_oracle import oracle_solve
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "gates.json")))
+
+
+def _measure(result):
+    # benchmark/gates.jl:205-228 uses |p − d| / max(1, |p|)
+    return dict(status=result.status.value, iterations=result.iterations, objective=result.pObj,
+                relative_gap=abs(result.pObj - result.dObj) / max(1.0, abs(result.pObj)),
+                primal_residual=result.p_res, dual_residual=result.d_res)
+
+
+def _compare(name, measured):
+    base = GOLD[name]
+    rules = GOLD["compare"]
+    assert measured["status"] == base["status"]
+    assert abs(measured["iterations"] - base["iterations"]) <= rules["iterations"]
+    scale = max(1.0, abs(base["objective"]))
+    assert abs(measured["objective"] - base["objective"]) / scale <= rules["objective_rel"]
+    for key in ("relative_gap", "primal_residual", "dual_residual"):
+        limit = max(rules["residual_factor"] * base[key], rules["absolute_floor"])
+        assert measured[key] <= limit, (key, measured[key], limit)
+
+
+@pytest.mark.parametrize("name,build", [("sdp_closed_form", G.gate_closed_form),
+                                        ("sdp_dense", G.gate_dense)])
+def test_gate(name, build):
+    opts = SolverOptions().with_tolerance(GOLD[name]["tolerance"])
+    _compare(name, _measure(oracle_solve(build(), opts)))
+
+
+def test_closed_form_matches_analytic_optimum():
+    r = oracle_solve(G.gate_closed_form(), SolverOptions().with_tolerance(1e-10))
+    assert abs(r.pObj - 2 * math.sqrt(6)) / (2 * math.sqrt(6)) < 1e-10
+
+
+def test_t1_fixed_policy_iterations():
+    pin = GOLD["T1_fixed_policy"]
+    r = oracle_solve(G.toy_t1(), SolverOptions(parameter_policy="fixed",
+                                               parameter_strategy="fixed", scaling="none"))
+    assert r.status.value == "Optimal"
+    assert abs(r.iterations - pin["iterations"]) <= pin["iteration_slack"]
+    assert abs(r.pObj - 2 * math.sqrt(6)) < pin["objective_abs"]
+    assert abs(r.pObj - r.dObj) < pin["objective_abs"]
+
+
+def test_gate_stream_is_the_reference_lcg():
+    s = G.GateStream(5)
+    first = [s.state]
+    s.uniform()
+    # state ← 0x5851f42d4c957f2d·state + 0x14057b7ef767814f (mod 2^64)
+    expect = (0x5851F42D4C957F2D * 5 + 0x14057B7EF767814F) % (1 << 64)
+    assert s.state == expect and first[0] == 5
+
+
+def test_sdpa_generator_is_strictly_feasible():
+    prob = G.sdpa_dense(m=20, blocks=[6], lp=3, seed=1)
+    r = oracle_solve(prob)
+    assert r.status.value == "Optimal"
+    assert r.relative_gap <= 1e-8
