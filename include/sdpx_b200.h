@@ -1,0 +1,169 @@
+/*
+ * SDPX-B200 C ABI — the boundary between SDPX's Julia host code and the B200
+ * dense-SDP interior-point core (libsdpx_b200.so, sm_100a).
+ *
+ * Every function returns an int status: 0 = ok, > 0 = numerical outcome the
+ * caller must interpret (documented per call), < 0 = usage or CUDA error with a
+ * message available from sdpx_b200_last_error().  Nothing throws or aborts
+ * across the boundary.  Host arrays are only read/written during the call.
+ *
+ * Data conventions (SDPX's DenseCons, src/types/constraints.jl:12-27):
+ *   - block l has order k_l; A^(l) is a k_l²×m column-major matrix whose
+ *     column i is vec(A_i^(l)) (column-major vec); every A_i^(l) is symmetric;
+ *   - "stacked" host matrices (X, Y, dX, dY, C) concatenate the k_l×k_l
+ *     column-major blocks in block order: Σ_l k_l² doubles;
+ *   - the core solves SDPX's form min cᵀx s.t. X_l = Σ_i x_i A_i^(l) − C_l ⪰ 0
+ *     with no equality rows (n = 0).
+ *
+ * One handle = one solve = one CUDA stream.  A handle is not reentrant; use
+ * one handle per concurrent solve (SDPX: "Concurrent factorization must use
+ * distinct solver/provider workspaces", docs/src/providers.md).
+ */
+#ifndef SDPX_B200_H
+#define SDPX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDPX_B200_ABI_VERSION 1
+
+typedef struct sdpx_b200_handle sdpx_b200_handle;
+
+typedef struct {
+  int64_t m;                  /* number of variables x_i                       */
+  int32_t nblocks;            /* L                                             */
+  const int32_t* block_order; /* k_l, length L                                 */
+  const double* const* Av;    /* per block: k_l²·m doubles (column i = vec A_i) */
+  const double* const* C;     /* per block: k_l² doubles                       */
+  const double* c;            /* m                                             */
+} sdpx_b200_problem;
+
+/* Precision modes of the Newton system. */
+#define SDPX_B200_FP64 0  /* plain FP64 Schur assembly and Cholesky                */
+#define SDPX_B200_MIXED 1 /* split-BF16 Schur assembly, FP32 Cholesky, FP64 refine  */
+
+int sdpx_b200_abi_version(void);
+/* Message of the last failed sdpx_b200_create on this thread. */
+const char* sdpx_b200_create_error(void);
+
+/* Problem upload and workspace allocation.  Replaces the provider
+ * instantiation SDPX performs through `instantiate_la_backend`
+ * (src/la_backend.jl:508-570) and `Workspace(prob)` (src/workspace.jl:779). */
+int sdpx_b200_create(const sdpx_b200_problem* problem, int device, sdpx_b200_handle** out);
+void sdpx_b200_destroy(sdpx_b200_handle* h);
+const char* sdpx_b200_last_error(const sdpx_b200_handle* h);
+int sdpx_b200_set_precision(sdpx_b200_handle* h, int mode);
+
+/* Ruiz + per-variable + objective scaling of the resident data in place
+ * (`equilibrate`, src/ingest.jl:1431-1519).  Outputs: E (Σ k_l, per block
+ * congruence factors), s (m), objective scale, passes (L).  The original data
+ * is retained for sdpx_b200_rebuild_slack / sdpx_b200_original_residuals. */
+int sdpx_b200_equilibrate(sdpx_b200_handle* h, double* E, double* s, double* objective_scale,
+                          int32_t* passes);
+/* max_l ‖C_l‖∞ and ‖c‖∞ of the working (scaled) data. */
+int sdpx_b200_data_norms(sdpx_b200_handle* h, double* max_C, double* c_norm);
+
+/* Iterate I/O (stacked layout). */
+int sdpx_b200_set_iterate(sdpx_b200_handle* h, const double* x, const double* X, const double* Y);
+int sdpx_b200_get_iterate(sdpx_b200_handle* h, double* x, double* X, double* Y);
+int sdpx_b200_get_direction(sdpx_b200_handle* h, double* dx, double* dX, double* dY);
+int sdpx_b200_get_rhs(sdpx_b200_handle* h, double* r);
+/* x = 0, X = ω_p I, Y = ω_d I (fixed-policy start, src/solver/interior_point.jl:1600-1612). */
+int sdpx_b200_fixed_start(sdpx_b200_handle* h, double omega_p, double omega_d);
+
+/* Residuals P_l, d, R_l and (factor != 0) the block Cholesky factors of X, Y
+ * (`threaded_compute_residuals!`, src/kernels/threaded.jl:423-506).
+ * blocks_ok = 0 when a block factorization failed.  mu: L targets. */
+int sdpx_b200_residuals(sdpx_b200_handle* h, const double* mu, int use_affine, int factor,
+                        double* p_res, double* d_res, int* blocks_ok);
+/* max_l ‖P_l‖∞ of the last residual evaluation (src/step.jl:74-80). */
+int sdpx_b200_block_primal_residual(sdpx_b200_handle* h, double* value);
+/* min/max diagonal ratios of the X and Y factors (src/step.jl:273-281). */
+int sdpx_b200_block_margins(sdpx_b200_handle* h, double* primal, double* dual);
+
+/* Schur complement S_ij = tr(A_i X⁻¹ A_j Y) from the current block factors
+ * (`schur_build!` DenseCons, src/schur.jl:511-562).  identity != 0 uses X = Y = I
+ * (KKT cold start, src/solver/interior_point.jl:709-723). */
+int sdpx_b200_schur_build(sdpx_b200_handle* h, int identity);
+int sdpx_b200_get_schur(sdpx_b200_handle* h, double* S /* m×m, full symmetric */);
+
+/* Cholesky of S with ≤ 6 relative diagonal regularisation retries
+ * (`_factor_dense_kkt_native!`, src/kkt.jl:1404-1445).  Returns 0 and ok = 0
+ * when S stays indefinite.  quality = min/max |L_ii|. */
+int sdpx_b200_factorize(sdpx_b200_handle* h, int* ok, int* reg_attempts, double* quality);
+
+/* Right-hand sides: predictor (src/step.jl:95-108), corrector (Mehrotra,
+ * src/kernels/threaded.jl:916-1067; fixed-policy, :837-901), cold start
+ * (which = 0: r = Σ_l A^(l)ᵀ vec C_l, which = 1: r = c). */
+int sdpx_b200_rhs_predictor(sdpx_b200_handle* h);
+int sdpx_b200_rhs_corrector_mehrotra(sdpx_b200_handle* h, double sigma, double mu, int block_local);
+int sdpx_b200_rhs_corrector_fixed(sdpx_b200_handle* h, double beta, const double* mu);
+int sdpx_b200_set_rhs(sdpx_b200_handle* h, int which);
+
+/* dx = S⁻¹ r with the current factor (`_solve_dense_kkt_owned!`, src/kkt.jl:2570-2595). */
+int sdpx_b200_solve(sdpx_b200_handle* h);
+/* ρ = r − S·dx; residual = ‖ρ‖∞, rnorm = ‖r‖∞ (src/kkt.jl:3689-3708). */
+int sdpx_b200_direction_residual(sdpx_b200_handle* h, double* residual, double* rnorm);
+/* Residual-driven refinement with rollback (`_refine_native_direction!`,
+ * src/kkt.jl:3891-3963).  policy: 0 fixed, 1 adaptive/auto; tol ≤ 0 selects
+ * 64·eps.  In mixed mode the correction solves use the FP32 factor and the
+ * residual is the FP64 Newton residual. */
+int sdpx_b200_refine(sdpx_b200_handle* h, int policy, double tol, int cap, int fixed_steps,
+                     int* steps, double* residual);
+/* dX_l = mat(A^(l)·dx) + P_l, dY_l = sym(X_l⁻¹(R_l − dX_l Y_l))
+ * (`threaded_direction_blocks!`, src/kernels/threaded.jl:574-663). */
+int sdpx_b200_direction_blocks(sdpx_b200_handle* h);
+
+/* Affine predictor step bounds and complementarity (src/step.jl:546-619).
+ * out[0] = Σ⟨X_l,Y_l⟩, out[1] = Σ⟨X_l+tX dX_l, Y_l+tY dY_l⟩, out[2] = tX,
+ * out[3] = tY;  block_compl: L values ⟨X_l,Y_l⟩.  adaptive = 0 uses unit steps. */
+int sdpx_b200_affine_diagnostics(sdpx_b200_handle* h, int adaptive, double* out,
+                                 double* block_compl);
+
+/* Step lengths (`threaded_line_search!`, src/kernels/threaded.jl:1602-1818).
+ * rule: 0 backtrack, 1 fraction-to-boundary. */
+int sdpx_b200_line_search(sdpx_b200_handle* h, int rule, double primal_fraction,
+                          double dual_fraction, double gamma, double min_step, double margin,
+                          double* tX, double* tY);
+
+/* X += tX dX, Y += tY dY, x += tX dx; returns Σ⟨X_l,Y_l⟩, finiteness and the
+ * L block values (`threaded_update_blocks!`, src/kernels/threaded.jl:665-754). */
+int sdpx_b200_update(sdpx_b200_handle* h, double tX, double tY, double* compl_total, int* finite,
+                     double* block_dots);
+/* d ← (1−tY)d − tY ρ ; p_after = |1−tX|·block_primal_residual
+ * (`_accepted_sdp_trial_residuals!`, src/solver/interior_point.jl:1287-1321). */
+int sdpx_b200_accepted_residuals(sdpx_b200_handle* h, double block_primal_residual, double tX,
+                                 double tY, double* p_after, double* d_after);
+int sdpx_b200_objectives(sdpx_b200_handle* h, double* p_obj, double* d_obj);
+/* Exact residual recomputation on the working data (src/validation.jl:15-60). */
+int sdpx_b200_solution_residuals(sdpx_b200_handle* h, double* p_res, double* d_res);
+
+/* KKT cold-start helpers (src/solver/interior_point.jl:699-1287, src/cold_start.jl). */
+int sdpx_b200_keep_direction(sdpx_b200_handle* h);
+int sdpx_b200_cold_start_iterate(sdpx_b200_handle* h);
+/* Certified strictly-interior identity shift of every block of X (which = 0)
+ * or Y (which = 1) (`_cold_start_psd_shift!`); ok = 0 when a block fails. */
+int sdpx_b200_psd_shift(sdpx_b200_handle* h, int which, int* ok);
+int sdpx_b200_add_identity(sdpx_b200_handle* h, int which, double shift);
+int sdpx_b200_block_dots(sdpx_b200_handle* h, double* dots, double* trace_X, double* trace_Y);
+int sdpx_b200_scale_iterate(sdpx_b200_handle* h, int which, double factor);
+int sdpx_b200_store_best(sdpx_b200_handle* h);
+int sdpx_b200_restore_best(sdpx_b200_handle* h);
+
+/* Original (unscaled) data: slack X = Σ x_i A_i − C and residuals. */
+int sdpx_b200_rebuild_slack(sdpx_b200_handle* h, const double* x, double* X);
+int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const double* X,
+                                 const double* Y, double* p_res, double* d_res);
+
+/* Cumulative device time per phase (ms) since the last reset:
+ * [0] residual+block factor, [1] Schur assembly, [2] KKT factor,
+ * [3] solves+refinement, [4] directions+RHS, [5] step length, [6] update. */
+int sdpx_b200_phase_times(sdpx_b200_handle* h, double* ms7, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SDPX_B200_H */

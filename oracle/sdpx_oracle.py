@@ -580,16 +580,44 @@ class OracleBackend:
         self.Y = [self._buildP(l, v) for l in range(len(self.k))]
         self.y = np.zeros(0)
 
-    def psd_stats(self, which, l):
-        M = (self.X if which == "X" else self.Y)[l]
+    def _psd_stats(self, M):
         low = np.tril(M)
         if not np.all(np.isfinite(low)):
             return False, 0.0, 0.0
         return True, float(np.max(np.abs(low))), gershgorin_lower(M)
 
-    def add_identity(self, which, l, shift):
-        M = (self.X if which == "X" else self.Y)[l]
-        M[np.diag_indices_from(M)] += shift
+    def _psd_shift_block(self, M):
+        """`_cold_start_psd_shift!` (src/cold_start.jl:287-308)."""
+        finite, scale, margin = self._psd_stats(M)
+        if not finite:
+            return False
+        safety = SQRT_EPS * max(1.0, scale)
+        slack = 8.0 * EPS * max(1.0, scale)
+        if margin > safety:
+            return True
+        for _ in range(16):
+            shift = safety - margin + slack
+            if not math.isfinite(shift):
+                return False
+            M[np.diag_indices_from(M)] += shift
+            finite, scale, margin = self._psd_stats(M)
+            if not finite:
+                return False
+            safety = SQRT_EPS * max(1.0, scale)
+            if margin > safety:
+                return True
+        return False
+
+    def psd_shift(self, which):
+        mats = self.X if which == "X" else self.Y
+        ok = True
+        for M in mats:
+            ok = self._psd_shift_block(M) and ok
+        return ok
+
+    def add_identity(self, which, shift):
+        for M in (self.X if which == "X" else self.Y):
+            M[np.diag_indices_from(M)] += shift
 
     def block_dots(self):
         dots = [float(np.sum(X * Y)) for X, Y in zip(self.X, self.Y)]
@@ -608,6 +636,17 @@ class OracleBackend:
         if self.best is not None:
             self.x, self.X, self.Y = self.best[0].copy(), [X.copy() for X in self.best[1]], \
                 [Y.copy() for Y in self.best[2]]
+
+    def set_iterate(self, x, X, Y):
+        self.x = np.array(x, dtype=np.float64)
+        self.X = [np.array(M, dtype=np.float64) for M in X]
+        self.Y = [np.array(M, dtype=np.float64) for M in Y]
+
+    def get_direction(self):
+        return self.dx.copy(), [M.copy() for M in self.dX], [M.copy() for M in self.dY]
+
+    def get_rhs(self):
+        return self.r.copy()
 
     def get_iterate(self):
         return self.x.copy(), [X.copy() for X in self.X], self.y.copy(), [Y.copy() for Y in self.Y]

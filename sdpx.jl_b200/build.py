@@ -1,0 +1,52 @@
+"""Build libsdpx_b200.so (sm_100a) in place with nvcc.
+
+Usage:  python sdpx.jl_b200/build.py [--force]
+The library lands next to this file (sdpx.jl_b200/libsdpx_b200.so) so it
+travels with the source tree; objects go to sdpx.jl_b200/_build/.
+"""
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+BUILD = HERE / "_build"
+LIB = HERE / "libsdpx_b200.so"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "-Xptxas", "-warn-spills"]
+SOURCES = ["api.cu", "blas_f64.cu", "chol.cu", "vec_kernels.cu", "mixed_f32.cu"]
+
+
+def nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.exists(cand) or cand == "nvcc"):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    deps = sorted(CSRC.glob("*")) + [HERE.parent / "include" / "sdpx_b200.h", Path(__file__)]
+    newest_dep = max(p.stat().st_mtime for p in deps)
+    objs = []
+    for src in SOURCES:
+        obj = BUILD / (src + ".o")
+        objs.append(obj)
+        if force or not obj.exists() or obj.stat().st_mtime < newest_dep:
+            cmd = [nvcc(), *ARCH, *FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+    if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(LIB)

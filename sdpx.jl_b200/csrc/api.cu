@@ -1,0 +1,1716 @@
+// C ABI of the SDPX B200 core: handle lifecycle, device-resident workspace and
+// the hot-path operations of one Newton iteration.  See include/sdpx_b200.h.
+//
+// Device layout.  All blocks share one "stacked" row space of length K: dense
+// blocks (k ≥ 2) occupy k² consecutive rows each (column-major k×k), followed
+// by one row per 1×1 block.  The constraint matrix 𝒜 is K×m column-major, so
+// column i holds vec(A_i) of every block contiguously; every block matrix
+// (X, Y, C, P, R, Z, dX, dY, factors) is a K-vector with the same offsets.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/sdpx_b200.h"
+#include "blas_f64.h"
+#include "chol.h"
+#include "mixed.h"
+#include "vec_kernels.h"
+
+namespace sdpx {
+
+static std::mutex g_attr_mu;
+static std::set<std::pair<const void*, int>> g_attr_done;
+bool smem_attr_needed(const void* kern, size_t) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  return g_attr_done.insert({kern, dev}).second;
+}
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    SDPX_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void zero(cudaStream_t st) { SDPX_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), st)); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { release(); }
+};
+
+struct DenseBlk {
+  int user;
+  int k;
+  long long off;  // stacked row offset
+};
+
+static constexpr double kEps = 2.220446049250313e-16;
+static const double kSqrtEps = std::sqrt(2.220446049250313e-16);
+
+struct Handle {
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  int sms = 148;
+  std::string err;
+  int precision = SDPX_B200_FP64;
+
+  int m = 0, L = 0;
+  std::vector<int> k;              // user block orders
+  std::vector<long long> user_off; // offset of block l in the host stacked layout
+  long long Ku = 0;                // host stacked length Σ k_l²
+  std::vector<DenseBlk> dense;
+  int nd = 0;                      // number of 1×1 blocks
+  long long od = 0;                // stacked offset of the 1×1 group
+  std::vector<int> diag_user;      // user index of each 1×1 entry
+  long long K = 0;                 // stacked length
+  int kmax = 0;
+
+  // device metadata
+  DBuf<long long> d_map;           // internal stacked index → host stacked index
+  DBuf<long long> d_doff, d_dlen;  // dense block offsets / lengths (k²)
+  DBuf<int> d_dk;                  // dense block orders
+  DBuf<long long> d_uoff, d_ulen;  // per-user-block segments (internal offsets) for dots
+  DBuf<int> d_uk;                  // user block orders
+  DBuf<int> d_diag_user;
+  std::vector<long long> seg_off, seg_len;  // host copies (user order, internal offsets)
+
+  // problem data
+  DBuf<double> A, A0, Pc;          // K×m
+  DBuf<double> c, c0;
+  DBuf<double> Cst, C0st;          // stacked C
+  bool have_original = false;
+
+  // iterate and workspaces
+  DBuf<double> x, dx, d, v, r, rho, work_m, work_m2, xbest, keptx, dxbest;
+  DBuf<double> X, Y, P, R, Z, dX, dY, LX, MY, W, T1, T2, Xbest, Ybest, tmpK, tmpK2;
+  DBuf<double> gemv_part;
+  int gemv_chunks = 8;
+  DBuf<double> S, Sf, Dinv;
+  DBuf<double> partial;
+  SyrkPlan syrk;
+  DBuf<double> red;                // small reduction scratch
+  double* h_red = nullptr;         // pinned mirror
+  DBuf<double> mu_user, target_user, work_L;
+  DBuf<double> seg_part;           // seg_dot partials
+  int seg_parts = 8;
+  double last_bpr = 0.0;
+
+  // batched Cholesky workspace (dense blocks X, Y and line-search trials)
+  DBuf<MatDesc<double>> d_descs;
+  DBuf<int> d_info;
+  DBuf<double> d_dmin, d_dmax, d_diag_store;
+  size_t desc_cap = 0;
+  DBuf<double> trials;
+  DBuf<long long> d_trial_off;
+  DBuf<double> d_tcand;
+  DBuf<int> d_fail;
+  std::vector<double> lx_dmin, lx_dmax, my_dmin, my_dmax;
+  bool diag_factor_ok = true;
+
+  // Gershgorin scratch
+  DBuf<double> g_cand, g_scale;
+  DBuf<long long> g_cand_off;
+  DBuf<int> g_nonfinite;
+
+  // mixed precision state
+  std::unique_ptr<MixedWorkspace> mixed;
+
+  // phase timing
+  struct PendingEv {
+    int phase;
+    cudaEvent_t a, b;
+  };
+  std::vector<PendingEv> pending;
+  std::vector<cudaEvent_t> ev_pool;
+  double phase_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+
+  ~Handle() {
+    for (auto& p : pending) {
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    if (h_red) cudaFreeHost(h_red);
+    mixed.reset();
+    if (st) cudaStreamDestroy(st);
+  }
+
+  // ---------------------------------------------------------------- utils --
+  cudaEvent_t get_event() {
+    if (!ev_pool.empty()) {
+      cudaEvent_t e = ev_pool.back();
+      ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    SDPX_CUDA(cudaEventCreate(&e));
+    return e;
+  }
+  struct PhaseScope {
+    Handle* h;
+    int phase;
+    cudaEvent_t a;
+    PhaseScope(Handle* hh, int ph) : h(hh), phase(ph) {
+      a = h->get_event();
+      SDPX_CUDA(cudaEventRecord(a, h->st));
+    }
+    ~PhaseScope() {
+      cudaEvent_t b = h->get_event();
+      cudaEventRecord(b, h->st);
+      h->pending.push_back({phase, a, b});
+    }
+  };
+  void harvest_phases() {
+    for (auto& p : pending) {
+      float ms = 0.f;
+      if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess)
+        phase_ms[p.phase] += ms;
+      ev_pool.push_back(p.a);
+      ev_pool.push_back(p.b);
+    }
+    pending.clear();
+  }
+
+  void sync() { SDPX_CUDA(cudaStreamSynchronize(st)); }
+  void d2h(void* dst, const void* src, size_t bytes) {
+    SDPX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+  }
+  void h2d(void* dst, const void* src, size_t bytes) {
+    SDPX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+  }
+  void d2d(void* dst, const void* src, size_t bytes) {
+    SDPX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st));
+  }
+  double read_red(int slot) {
+    d2h(h_red + slot, red.p + slot, sizeof(double));
+    sync();
+    return h_red[slot];
+  }
+  void clear_red(int slot, int count = 1) {
+    SDPX_CUDA(cudaMemsetAsync(red.p + slot, 0, sizeof(double) * count, st));
+  }
+
+  // Operand descriptors for a dense block matrix M stored at stacked offset o.
+  static Opnd blk_as_A(const double* base, long long o, int kk) {  // (mm=r, kk=c) → M[r,c]
+    Opnd q;
+    q.base = base + o;
+    q.kstride = kk;
+    q.inner_stride = 1;
+    q.outer_stride = 0;
+    q.inner = 1 << 30;
+    q.mn_extent = kk;
+    q.k_extent = kk;
+    return q;
+  }
+  static Opnd blk_as_At(const double* base, long long o, int kk) {  // (mm=r, kk=c) → M[c,r]
+    Opnd q = blk_as_A(base, o, kk);
+    q.kstride = 1;
+    q.inner_stride = kk;
+    return q;
+  }
+  static Opnd blk_as_B(const double* base, long long o, int kk) {  // (kk=p, nn=c) → M[p,c]
+    Opnd q = blk_as_A(base, o, kk);
+    q.kstride = 1;
+    q.inner_stride = kk;
+    return q;
+  }
+  static OutDesc blk_out(double* base, long long o, int kk) {
+    OutDesc c;
+    c.base = base + o;
+    c.row_inner_stride = 1;
+    c.row_outer_stride = 0;
+    c.row_inner = 1 << 30;
+    c.col_inner_stride = kk;
+    c.col_outer_stride = 0;
+    c.col_inner = 1 << 30;
+    c.rows = kk;
+    c.cols = kk;
+    return c;
+  }
+  // C_blk = alpha·op(A)·op(B) + beta·C_blk on block b (op given by descriptors)
+  void blk_gemm(const Opnd& a, bool akc, const Opnd& b, bool bkc, double* out, const DenseBlk& blk,
+                double alpha, double beta, int mode) {
+    gemm_f64(a, akc, b, bkc, blk_out(out, blk.off, blk.k), alpha, beta, mode, false, st);
+  }
+
+  // M ← X⁻¹·M for every dense block using W = L_X⁻¹ (Z = Wᵀ (W M)); M is read
+  // from `in` and the result written to `out` (distinct from T2).
+  void dense_cholsolve(const double* in, double* out) {
+    for (auto& b : dense) {
+      blk_gemm(blk_as_A(W.p, b.off, b.k), false, blk_as_B(in, b.off, b.k), true, T2.p, b, 1.0, 0.0,
+               KR_A_LOWER);
+      blk_gemm(blk_as_At(W.p, b.off, b.k), true, blk_as_B(T2.p, b.off, b.k), true, out, b, 1.0, 0.0,
+               KR_A_UPPER);
+    }
+  }
+
+  void ensure_descs(size_t n) {
+    if (n <= desc_cap) return;
+    desc_cap = std::max<size_t>(n, 2 * desc_cap);
+    d_descs.alloc(desc_cap);
+    d_info.alloc(desc_cap);
+    d_dmin.alloc(desc_cap);
+    d_dmax.alloc(desc_cap);
+    d_diag_store.alloc(desc_cap * 64 * 64);
+  }
+
+  // Batched Cholesky of host-described matrices; fills info/dmin/dmax (host).
+  void potrf_host_list(const std::vector<MatDesc<double>>& mats, std::vector<int>& info,
+                       std::vector<double>& dmin, std::vector<double>& dmax) {
+    size_t n = mats.size();
+    info.assign(n, 0);
+    dmin.assign(n, 0.0);
+    dmax.assign(n, 0.0);
+    if (n == 0) return;
+    ensure_descs(n);
+    int nmax = 0;
+    for (auto& q : mats) nmax = std::max(nmax, q.n);
+    h2d(d_descs.p, mats.data(), n * sizeof(MatDesc<double>));
+    potrf_batched<double, 32>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p,
+                              d_diag_store.p, st);
+    d2h(info.data(), d_info.p, n * sizeof(int));
+    d2h(dmin.data(), d_dmin.p, n * sizeof(double));
+    d2h(dmax.data(), d_dmax.p, n * sizeof(double));
+    sync();
+  }
+
+  // ------------------------------------------------------------ create ----
+  void create(const sdpx_b200_problem* p, int device) {
+    dev = device;
+    SDPX_CUDA(cudaSetDevice(dev));
+    SDPX_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    SDPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (p->m <= 0 || p->nblocks <= 0) throw std::invalid_argument("problem needs m > 0 and L > 0");
+    if (p->m > (1 << 30)) throw std::invalid_argument("m too large");
+    m = (int)p->m;
+    L = p->nblocks;
+    k.assign(p->block_order, p->block_order + L);
+    user_off.resize(L);
+    Ku = 0;
+    long long dense_rows = 0;
+    for (int l = 0; l < L; ++l) {
+      if (k[l] <= 0) throw std::invalid_argument("block orders must be positive");
+      user_off[l] = Ku;
+      Ku += (long long)k[l] * k[l];
+      if (k[l] >= 2) {
+        dense.push_back({l, k[l], dense_rows});
+        dense_rows += (long long)k[l] * k[l];
+        kmax = std::max(kmax, k[l]);
+      } else {
+        diag_user.push_back(l);
+      }
+    }
+    nd = (int)diag_user.size();
+    od = dense_rows;
+    K = dense_rows + nd;
+
+    // Stacked index map and per-user-block segments.
+    std::vector<long long> map(K);
+    seg_off.assign(L, 0);
+    seg_len.assign(L, 0);
+    for (auto& b : dense) {
+      for (long long e = 0; e < (long long)b.k * b.k; ++e) map[b.off + e] = user_off[b.user] + e;
+      seg_off[b.user] = b.off;
+      seg_len[b.user] = (long long)b.k * b.k;
+    }
+    for (int j = 0; j < nd; ++j) {
+      map[od + j] = user_off[diag_user[j]];
+      seg_off[diag_user[j]] = od + j;
+      seg_len[diag_user[j]] = 1;
+    }
+    d_map.alloc(K);
+    h2d(d_map.p, map.data(), K * sizeof(long long));
+    std::vector<long long> doff, dlen;
+    std::vector<int> dk;
+    for (auto& b : dense) {
+      doff.push_back(b.off);
+      dlen.push_back((long long)b.k * b.k);
+      dk.push_back(b.k);
+    }
+    d_doff.alloc(dense.size());
+    d_dlen.alloc(dense.size());
+    d_dk.alloc(dense.size());
+    if (!dense.empty()) {
+      h2d(d_doff.p, doff.data(), doff.size() * sizeof(long long));
+      h2d(d_dlen.p, dlen.data(), dlen.size() * sizeof(long long));
+      h2d(d_dk.p, dk.data(), dk.size() * sizeof(int));
+    }
+    d_uoff.alloc(L);
+    d_ulen.alloc(L);
+    d_uk.alloc(L);
+    h2d(d_uoff.p, seg_off.data(), L * sizeof(long long));
+    h2d(d_ulen.p, seg_len.data(), L * sizeof(long long));
+    h2d(d_uk.p, k.data(), L * sizeof(int));
+    d_diag_user.alloc(nd);
+    if (nd) h2d(d_diag_user.p, diag_user.data(), nd * sizeof(int));
+
+    // Constraint matrix upload: dense blocks by 2-D copies, 1×1 blocks packed.
+    A.alloc((size_t)K * m);
+    for (auto& b : dense) {
+      size_t kk2 = (size_t)b.k * b.k;
+      SDPX_CUDA(cudaMemcpy2DAsync(A.p + b.off, (size_t)K * sizeof(double), p->Av[b.user],
+                                  kk2 * sizeof(double), kk2 * sizeof(double), (size_t)m,
+                                  cudaMemcpyHostToDevice, st));
+    }
+    if (nd) {
+      std::vector<double> pack((size_t)nd * m);
+      for (int j = 0; j < nd; ++j) {
+        const double* src = p->Av[diag_user[j]];
+        for (int i = 0; i < m; ++i) pack[(size_t)i * nd + j] = src[i];
+      }
+      SDPX_CUDA(cudaMemcpy2DAsync(A.p + od, (size_t)K * sizeof(double), pack.data(),
+                                  (size_t)nd * sizeof(double), (size_t)nd * sizeof(double),
+                                  (size_t)m, cudaMemcpyHostToDevice, st));
+      sync();  // `pack` is a host temporary
+    }
+    c.alloc(m);
+    h2d(c.p, p->c, m * sizeof(double));
+    std::vector<double> Cu(Ku);
+    for (int l = 0; l < L; ++l)
+      std::memcpy(Cu.data() + user_off[l], p->C[l], sizeof(double) * k[l] * k[l]);
+    tmpK.alloc(std::max<long long>(K, Ku));
+    Cst.alloc(K);
+    h2d(tmpK.p, Cu.data(), Ku * sizeof(double));
+    gather(K, d_map.p, tmpK.p, Cst.p, st);
+    sync();
+
+    // Workspaces.
+    for (auto* b : {&x, &dx, &d, &v, &r, &rho, &work_m, &work_m2, &xbest, &keptx, &dxbest})
+      b->alloc(m), b->zero(st);
+    for (auto* b : {&X, &Y, &P, &R, &Z, &dX, &dY, &LX, &MY, &W, &T1, &T2, &Xbest, &Ybest, &tmpK2})
+      b->alloc(K), b->zero(st);
+    gemv_chunks = std::max(1, std::min(16, m / 64));
+    gemv_part.alloc((size_t)gemv_chunks * K);
+    Pc.alloc((size_t)K * m);
+    S.alloc((size_t)m * m);
+    Sf.alloc((size_t)m * m);
+    Dinv.alloc((size_t)ceil_div(m, 64) * 64 * 64);
+    syrk = plan_syrk_f64(m, K, sms);
+    partial.alloc(syrk.partial_doubles);
+    red.alloc(64);
+    SDPX_CUDA(cudaMallocHost(&h_red, 64 * sizeof(double)));
+    mu_user.alloc(L);
+    target_user.alloc(L);
+    work_L.alloc(std::max<size_t>((size_t)L, dense.size()) + 1);
+    seg_parts = 8;
+    seg_part.alloc((size_t)seg_parts * L);
+    ensure_descs(std::max<size_t>(16, 2 * dense.size()));
+    d_fail.alloc(64);
+    d_tcand.alloc(64);
+    // Gershgorin scratch
+    std::vector<long long> coff(dense.size());
+    long long tot = 0;
+    for (size_t b = 0; b < dense.size(); ++b) coff[b] = tot, tot += dense[b].k;
+    g_cand.alloc(tot);
+    g_cand_off.alloc(dense.size());
+    if (!dense.empty()) h2d(g_cand_off.p, coff.data(), coff.size() * sizeof(long long));
+    g_scale.alloc(dense.size());
+    g_nonfinite.alloc(dense.size());
+    lx_dmin.assign(dense.size(), 1.0);
+    lx_dmax.assign(dense.size(), 1.0);
+    my_dmin.assign(dense.size(), 1.0);
+    my_dmax.assign(dense.size(), 1.0);
+    // Start at X = Y = I.
+    fixed_start(1.0, 1.0);
+    sync();
+  }
+
+  // ----------------------------------------------------------- scaling ----
+  void equilibrate(double* E_out, double* s_out, double* objscale, int32_t* passes) {
+    // keep the original data for final slack/residual reconstruction
+    if (!have_original) {
+      A0.alloc((size_t)K * m);
+      d2d(A0.p, A.p, sizeof(double) * K * m);
+      C0st.alloc(K);
+      d2d(C0st.p, Cst.p, sizeof(double) * K);
+      c0.alloc(m);
+      d2d(c0.p, c.p, sizeof(double) * m);
+      have_original = true;
+    }
+    std::vector<std::vector<double>> E(L);
+    for (int l = 0; l < L; ++l) E[l].assign(k[l], 1.0);
+    std::vector<int> used(L, 0);
+    std::vector<char> active(L, 1);
+    DBuf<double> rn_d, e_d;
+    long long rows_total = 0;
+    for (auto& b : dense) rows_total += b.k;
+    rows_total += nd;
+    rn_d.alloc(rows_total);
+    e_d.alloc(rows_total);
+    std::vector<double> Chost(K);
+    for (int it = 1; it <= 8; ++it) {
+      bool any = false;
+      for (int l = 0; l < L; ++l) any = any || active[l];
+      if (!any) break;
+      // C row maxima on the host (C is small), A row maxima on the device.
+      d2h(Chost.data(), Cst.p, K * sizeof(double));
+      rn_d.zero(st);
+      long long ro = 0;
+      for (auto& b : dense) {
+        if (active[b.user]) ruiz_rowmax_dense(A.p, K, m, b.off, b.k, rn_d.p + ro, st);
+        ro += b.k;
+      }
+      if (nd) ruiz_rowmax_diag(A.p, K, m, od, nd, rn_d.p + ro, st);
+      std::vector<double> rn(rows_total);
+      d2h(rn.data(), rn_d.p, rows_total * sizeof(double));
+      sync();
+      std::vector<double> e(rows_total, 1.0);
+      ro = 0;
+      auto handle_block = [&](int l, int kk, long long rowoff, const double* Cblk, long long cstride,
+                              bool is_diag) {
+        // rn[r] = max(rn[r], max_c |C[r,c]|)
+        for (int r0 = 0; r0 < kk; ++r0) {
+          double mx = rn[rowoff + r0];
+          for (int cc = 0; cc < kk; ++cc) {
+            double vv = std::fabs(Cblk[(is_diag ? 0 : (long long)cc * cstride) + r0]);
+            if (std::isnan(vv)) vv = INFINITY;
+            mx = std::max(mx, vv);
+          }
+          rn[rowoff + r0] = mx;
+        }
+        bool conv = false;
+        if (it >= 2) {
+          double dev = 0.0;
+          bool finite = true;
+          for (int r0 = 0; r0 < kk; ++r0) {
+            double vv = rn[rowoff + r0];
+            if (!(vv > 0)) continue;
+            if (!std::isfinite(vv)) {
+              finite = false;
+              break;
+            }
+            dev = std::max(dev, std::fabs(std::log(vv)));
+          }
+          conv = finite && dev <= 1.0 / 20.0;
+        }
+        for (int r0 = 0; r0 < kk; ++r0) {
+          double vv = rn[rowoff + r0];
+          e[rowoff + r0] = vv > 0 ? 1.0 / std::sqrt(vv) : 1.0;
+          E[l][r0] *= e[rowoff + r0];
+        }
+        used[l] = it;
+        if (conv) active[l] = 0;
+      };
+      for (auto& b : dense) {
+        if (active[b.user]) handle_block(b.user, b.k, ro, Chost.data() + b.off, b.k, false);
+        ro += b.k;
+      }
+      for (int j = 0; j < nd; ++j) {
+        int l = diag_user[j];
+        if (active[l]) handle_block(l, 1, ro + j, Chost.data() + od + j, 1, true);
+        else e[ro + j] = 1.0;
+      }
+      h2d(e_d.p, e.data(), rows_total * sizeof(double));
+      ro = 0;
+      for (auto& b : dense) {
+        if (active[b.user] || used[b.user] == it) ruiz_congruence_dense(A.p, K, m, b.off, b.k, e_d.p + ro, st);
+        ro += b.k;
+      }
+      if (nd) ruiz_congruence_diag(A.p, K, m, od, nd, e_d.p + ro, st);
+      // C ← E C E on the host copy, uploaded back
+      ro = 0;
+      for (auto& b : dense) {
+        for (int cc = 0; cc < b.k; ++cc)
+          for (int r0 = 0; r0 < b.k; ++r0)
+            Chost[b.off + (long long)cc * b.k + r0] *= e[ro + r0] * e[ro + cc];
+        ro += b.k;
+      }
+      for (int j = 0; j < nd; ++j) Chost[od + j] *= e[ro + j] * e[ro + j];
+      h2d(Cst.p, Chost.data(), K * sizeof(double));
+      sync();
+    }
+    // Per-variable scale s_i = max_l ‖A_i^(l)‖∞ (1 when zero), objective scale.
+    std::vector<double> mx(m), s(m), ch(m);
+    colmax(A.p, K, m, work_m.p, st);
+    d2h(mx.data(), work_m.p, m * sizeof(double));
+    d2h(ch.data(), c.p, m * sizeof(double));
+    sync();
+    double osc = 0.0;
+    for (int i = 0; i < m; ++i) {
+      s[i] = mx[i] > 0 ? mx[i] : 1.0;
+      ch[i] = ch[i] / s[i];
+      osc = std::max(osc, std::fabs(ch[i]));
+    }
+    if (!(osc > 0 && std::isfinite(osc))) osc = 1.0;
+    for (int i = 0; i < m; ++i) ch[i] /= osc;
+    h2d(work_m.p, s.data(), m * sizeof(double));
+    scale_cols(A.p, K, m, work_m.p, st);
+    h2d(c.p, ch.data(), m * sizeof(double));
+    sync();
+    if (E_out) {
+      long long o = 0;
+      for (int l = 0; l < L; ++l)
+        for (int r0 = 0; r0 < k[l]; ++r0) E_out[o++] = E[l][r0];
+    }
+    if (s_out) std::memcpy(s_out, s.data(), m * sizeof(double));
+    if (objscale) *objscale = osc;
+    if (passes)
+      for (int l = 0; l < L; ++l) passes[l] = used[l];
+  }
+
+  void data_norms(double* maxC, double* cnorm) {
+    clear_red(0, 2);
+    absmax(K, Cst.p, red.p + 0, st);
+    absmax(m, c.p, red.p + 1, st);
+    d2h(h_red, red.p, 2 * sizeof(double));
+    sync();
+    *maxC = h_red[0];
+    *cnorm = h_red[1];
+  }
+
+  // -------------------------------------------------------- iterate I/O --
+  void set_iterate(const double* hx, const double* hX, const double* hY) {
+    if (hx) h2d(x.p, hx, m * sizeof(double));
+    if (hX) {
+      h2d(tmpK.p, hX, Ku * sizeof(double));
+      gather(K, d_map.p, tmpK.p, X.p, st);
+    }
+    if (hY) {
+      h2d(tmpK2.p, hY, Ku * sizeof(double));
+      gather(K, d_map.p, tmpK2.p, Y.p, st);
+    }
+    sync();
+  }
+  void get_stacked(const double* dev_src, double* host_dst) {
+    scatter(K, d_map.p, dev_src, tmpK.p, st);
+    d2h(host_dst, tmpK.p, Ku * sizeof(double));
+    sync();
+  }
+  void fixed_start(double wp, double wd) {
+    x.zero(st);
+    X.zero(st);
+    Y.zero(st);
+    if (!dense.empty()) {
+      add_diag(d_doff.p, d_dk.p, (int)dense.size(), kmax, X.p, nullptr, wp, st);
+      add_diag(d_doff.p, d_dk.p, (int)dense.size(), kmax, Y.p, nullptr, wd, st);
+    }
+    if (nd) {
+      std::vector<double> ones(nd, wp), ones2(nd, wd);
+      h2d(X.p + od, ones.data(), nd * sizeof(double));
+      h2d(Y.p + od, ones2.data(), nd * sizeof(double));
+      sync();
+    }
+  }
+
+  // ------------------------------------------------------ block factors --
+  bool factor_blocks() {
+    // LX = chol(X), MY = chol(Y) for every dense block (batched), 1×1 by sqrt.
+    std::vector<MatDesc<double>> mats;
+    for (auto& b : dense) {
+      d2d(LX.p + b.off, X.p + b.off, sizeof(double) * b.k * b.k);
+      d2d(MY.p + b.off, Y.p + b.off, sizeof(double) * b.k * b.k);
+    }
+    for (auto& b : dense) mats.push_back({LX.p + b.off, b.k, b.k});
+    for (auto& b : dense) mats.push_back({MY.p + b.off, b.k, b.k});
+    std::vector<int> info;
+    std::vector<double> dmn, dmx;
+    int fail_h = 0;
+    if (nd) {
+      SDPX_CUDA(cudaMemsetAsync(d_fail.p, 0, sizeof(int), st));
+      diag_factor(nd, od, X.p, Y.p, LX.p, MY.p, d_fail.p, st);
+    }
+    potrf_host_list(mats, info, dmn, dmx);
+    if (nd) {
+      d2h(&fail_h, d_fail.p, sizeof(int));
+      sync();
+    }
+    bool ok = fail_h == 0;
+    size_t nb = dense.size();
+    for (size_t b = 0; b < nb; ++b) {
+      ok = ok && info[b] == 0 && info[nb + b] == 0;
+      lx_dmin[b] = dmn[b];
+      lx_dmax[b] = dmx[b];
+      my_dmin[b] = dmn[nb + b];
+      my_dmax[b] = dmx[nb + b];
+    }
+    diag_factor_ok = fail_h == 0;
+    if (ok && !dense.empty()) {
+      // W = L_X^{-1} for the Schur products and the block solves.
+      W.zero(st);
+      std::vector<MatDesc<double>> Ls, Ws;
+      for (auto& b : dense) {
+        Ls.push_back({LX.p + b.off, b.k, b.k});
+        Ws.push_back({W.p + b.off, b.k, b.k});
+      }
+      ensure_descs(2 * nb);
+      h2d(d_descs.p, Ls.data(), nb * sizeof(MatDesc<double>));
+      h2d(d_descs.p + nb, Ws.data(), nb * sizeof(MatDesc<double>));
+      trinv_batched<double, 32>(d_descs.p, d_descs.p + nb, (int)nb, kmax, st);
+      sync();
+    }
+    return ok;
+  }
+
+  void block_margins(double* primal, double* dual) {
+    // `_cholesky_diagonal_quality` per block; 1×1 blocks contribute 1.
+    double p = 1.0, q = 1.0;
+    for (size_t b = 0; b < dense.size(); ++b) {
+      auto qual = [](double lo, double hi) {
+        return (hi > 0 && std::isfinite(hi)) ? std::min(1.0, std::max(0.0, lo / hi)) : 0.0;
+      };
+      p = std::min(p, qual(lx_dmin[b], lx_dmax[b]));
+      q = std::min(q, qual(my_dmin[b], my_dmax[b]));
+    }
+    *primal = p;
+    *dual = q;
+  }
+
+  // ---------------------------------------------------------- residuals --
+  void residuals(const double* mu, int use_affine, int factor, double* p_res, double* d_res,
+                 int* ok) {
+    PhaseScope ps(this, 0);
+    // P = 𝒜x − X − C
+    gemv_n(A.p, K, m, x.p, tmpK.p, gemv_part.p, gemv_chunks, st);
+    axpbypcz(K, 1.0, tmpK.p, -1.0, X.p, -1.0, Cst.p, P.p, st);
+    // d = c − 𝒜ᵀ vec(Y)
+    gemv_t(A.p, K, m, Y.p, -1.0, c.p, 1.0, d.p, st);
+    clear_red(0, 2);
+    absmax(K, P.p, red.p + 0, st);
+    absmax(m, d.p, red.p + 1, st);
+    // R = −XY (+ μ I)
+    h2d(mu_user.p, mu, L * sizeof(double));
+    for (auto& b : dense)
+      blk_gemm(blk_as_A(X.p, b.off, b.k), false, blk_as_B(Y.p, b.off, b.k), true, R.p, b, -1.0, 0.0,
+               KR_FULL);
+    if (!use_affine && !dense.empty()) {
+      std::vector<double> shifts(dense.size());
+      for (size_t b = 0; b < dense.size(); ++b) shifts[b] = mu[dense[b].user];
+      h2d(work_L.p, shifts.data(), shifts.size() * sizeof(double));
+      add_diag(d_doff.p, d_dk.p, (int)dense.size(), kmax, R.p, work_L.p, 0.0, st);
+    }
+    diag_residual_R(nd, od, X.p, Y.p, mu_user.p, d_diag_user.p, use_affine, R.p, st);
+    d2h(h_red, red.p, 2 * sizeof(double));
+    sync();
+    *p_res = h_red[0];
+    *d_res = h_red[1];
+    last_bpr = h_red[0];
+    *ok = 1;
+    if (factor) *ok = factor_blocks() ? 1 : 0;
+  }
+
+  // ------------------------------------------------------------- Schur ----
+  void schur_build(int identity) {
+    PhaseScope ps(this, 1);
+    if (precision == SDPX_B200_MIXED && !identity && mixed) {
+      mixed_schur();
+      return;
+    }
+    schur_build_fp64(identity);
+  }
+  void schur_build_fp64(int identity) {
+    const double* panel = A.p;
+    if (!identity) {
+      for (auto& b : dense) {
+        // T = W · [A_1 … A_m]  (W lower ⇒ K range [0, row-tile end))
+        Opnd Wd = blk_as_A(W.p, b.off, b.k);
+        Opnd Ap;  // (kk = p, nn = (i, c)) → A[off + c·k + p, i]
+        Ap.base = A.p + b.off;
+        Ap.kstride = 1;
+        Ap.inner = b.k;
+        Ap.inner_stride = b.k;
+        Ap.outer_stride = K;
+        Ap.mn_extent = b.k * m;
+        Ap.k_extent = b.k;
+        OutDesc Tout;
+        Tout.base = Pc.p + b.off;
+        Tout.row_inner_stride = 1;
+        Tout.row_outer_stride = 0;
+        Tout.row_inner = 1 << 30;
+        Tout.col_inner = b.k;
+        Tout.col_inner_stride = b.k;
+        Tout.col_outer_stride = K;
+        Tout.rows = b.k;
+        Tout.cols = b.k * m;
+        gemm_f64(Wd, false, Ap, true, Tout, 1.0, 0.0, KR_A_LOWER, true, st);
+        // P_i = T_i · M_Y in place (rows (i, r) two-level, columns c)
+        Opnd Tst;
+        Tst.base = Pc.p + b.off;
+        Tst.kstride = b.k;
+        Tst.inner = b.k;
+        Tst.inner_stride = 1;
+        Tst.outer_stride = K;
+        Tst.mn_extent = b.k * m;
+        Tst.k_extent = b.k;
+        Opnd My = blk_as_B(MY.p, b.off, b.k);
+        OutDesc Pout;
+        Pout.base = Pc.p + b.off;
+        Pout.row_inner = b.k;
+        Pout.row_inner_stride = 1;
+        Pout.row_outer_stride = K;
+        Pout.col_inner = 1 << 30;
+        Pout.col_inner_stride = b.k;
+        Pout.col_outer_stride = 0;
+        Pout.rows = b.k * m;
+        Pout.cols = b.k;
+        trmm_right_lower_inplace_f64(Tst, My, Pout, st);
+      }
+      diag_panel(K, m, nd, od, A.p, LX.p, MY.p, Pc.p, st);
+      panel = Pc.p;
+    }
+    Opnd Pd;
+    Pd.base = panel;
+    Pd.kstride = 1;
+    Pd.inner = 1 << 30;
+    Pd.inner_stride = K;
+    Pd.outer_stride = 0;
+    Pd.mn_extent = m;
+    Pd.k_extent = (int)K;
+    syrk_lower_f64(Pd, syrk, partial.p, S.p, m, m, 0.0, st);
+    mirror_lower(m, S.p, st);
+  }
+
+  // ------------------------------------------------------- factorisation --
+  void factorize(int* ok, int* attempts, double* quality) {
+    PhaseScope ps(this, 2);
+    if (precision == SDPX_B200_MIXED && mixed) {
+      mixed_factorize(ok, attempts, quality);
+      return;
+    }
+    MatDesc<double> md{Sf.p, m, m};
+    std::vector<MatDesc<double>> one{md};
+    std::vector<int> info;
+    std::vector<double> dmn, dmx;
+    double reg = 0.0;
+    int att = 0;
+    while (true) {
+      copy_reg(m, S.p, Sf.p, att == 0 ? 0.0 : reg, st);
+      ensure_descs(1);
+      h2d(d_descs.p, &md, sizeof(md));
+      potrf_batched<double, 64>(d_descs.p, 1, m, d_info.p, d_dmin.p, d_dmax.p, d_diag_store.p, st);
+      info.resize(1);
+      dmn.resize(1);
+      dmx.resize(1);
+      d2h(info.data(), d_info.p, sizeof(int));
+      d2h(dmn.data(), d_dmin.p, sizeof(double));
+      d2h(dmx.data(), d_dmax.p, sizeof(double));
+      sync();
+      if (info[0] == 0 || att >= 6) break;
+      ++att;
+      reg = (att == 1) ? kSqrtEps : reg * 10.0;
+    }
+    *attempts = att;
+    *ok = info[0] == 0 ? 1 : 0;
+    double hi = dmx[0], lo = dmn[0];
+    *quality = (*ok && hi > 0 && std::isfinite(hi)) ? std::min(1.0, std::max(0.0, lo / hi)) : 0.0;
+    if (*ok) factor_diag_inverses<double, 64>(Sf.p, m, m, Dinv.p, st);
+  }
+
+  // ------------------------------------------------------------- solves ----
+  void solve_into(double* vec) {  // vec ← S⁻¹ vec with the current factor
+    if (precision == SDPX_B200_MIXED && mixed) {
+      mixed_solve(vec);
+      return;
+    }
+    cholesky_solve<double, 64>(Sf.p, m, m, Dinv.p, vec, work_m2.p, st);
+  }
+  void solve() {
+    PhaseScope ps(this, 3);
+    d2d(dx.p, r.p, m * sizeof(double));
+    solve_into(dx.p);
+  }
+  // ρ = r − S·dx  (FP64 Newton operator)
+  void apply_residual() {
+    if (precision == SDPX_B200_MIXED && mixed) {
+      mixed_residual();
+      return;
+    }
+    symv_full(m, S.p, dx.p, -1.0, r.p, 1.0, rho.p, st);
+  }
+  void direction_residual(double* res, double* rnorm) {
+    PhaseScope ps(this, 3);
+    apply_residual();
+    clear_red(0, 2);
+    absmax(m, rho.p, red.p + 0, st);
+    absmax(m, r.p, red.p + 1, st);
+    d2h(h_red, red.p, 2 * sizeof(double));
+    sync();
+    *res = h_red[0];
+    *rnorm = h_red[1];
+  }
+  double residual_norm_only() {
+    apply_residual();
+    clear_red(0, 1);
+    absmax(m, rho.p, red.p, st);
+    return read_red(0);
+  }
+  void refine(int policy, double tol, int cap, int fixed_steps, int* steps_out, double* res_out) {
+    PhaseScope ps(this, 3);
+    auto correction = [&]() {
+      d2d(dxbest.p, dx.p, m * sizeof(double));
+      d2d(work_m.p, rho.p, m * sizeof(double));
+      solve_into(work_m.p);
+      combine(m, dx.p, 1.0, work_m.p, st);
+    };
+    int steps = 0;
+    double residual;
+    if (policy == 0) {
+      residual = residual_norm_only();
+      for (int s = 0; s < fixed_steps; ++s) {
+        correction();
+        double corr = residual_norm_only();
+        if (!std::isfinite(corr) || corr > residual) {
+          d2d(dx.p, dxbest.p, m * sizeof(double));
+          break;
+        }
+        ++steps;
+        residual = corr;
+      }
+    } else {
+      if (cap <= 0) {
+        *steps_out = 0;
+        *res_out = 0.0;
+        return;
+      }
+      double rel = tol > 0 ? tol : 64.0 * kEps;
+      clear_red(1, 1);
+      absmax(m, r.p, red.p + 1, st);
+      double rn = read_red(1);
+      double abstol = rel * std::max(rn, 1.0);
+      residual = residual_norm_only();
+      for (int s = 0; s < cap; ++s) {
+        if (residual <= abstol) break;
+        correction();
+        double corr = residual_norm_only();
+        if (!std::isfinite(corr) || corr > residual) {
+          d2d(dx.p, dxbest.p, m * sizeof(double));
+          break;
+        }
+        ++steps;
+        bool small = corr > residual * 0.5;
+        residual = corr;
+        if (small) break;
+      }
+    }
+    *steps_out = steps;
+    *res_out = residual;
+  }
+
+  // -------------------------------------------------------- right sides ---
+  void rhs_from_R() {
+    // Z = X⁻¹(P·Y − R); v = 𝒜ᵀ vec(Z); r = −(d + v)
+    for (auto& b : dense) {
+      d2d(T1.p + b.off, R.p + b.off, sizeof(double) * b.k * b.k);
+      blk_gemm(blk_as_A(P.p, b.off, b.k), false, blk_as_B(Y.p, b.off, b.k), true, T1.p, b, 1.0,
+               -1.0, KR_FULL);  // T1 = P·Y − R
+    }
+    dense_cholsolve(T1.p, Z.p);
+    diag_rhs_Z(nd, od, P.p, Y.p, R.p, LX.p, Z.p, st);
+    gemv_t(A.p, K, m, Z.p, -1.0, d.p, -1.0, r.p, st);  // r = −v − d
+  }
+  void rhs_predictor() {
+    PhaseScope ps(this, 4);
+    rhs_from_R();
+  }
+  void rhs_corrector_mehrotra(double sigma, double mu, int block_local) {
+    PhaseScope ps(this, 4);
+    std::vector<double> target(L, sigma * mu);
+    if (block_local) {
+      std::vector<double> dots(L);
+      seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, nullptr, 0.0, Y.p, nullptr, 0.0, seg_part.p,
+              work_L.p, st);
+      d2h(dots.data(), work_L.p, L * sizeof(double));
+      sync();
+      for (int l = 0; l < L; ++l) target[l] = sigma * dots[l] / k[l];
+    }
+    build_corrector_R(target);
+    rhs_from_R();
+  }
+  void rhs_corrector_fixed(double beta, const double* mu) {
+    PhaseScope ps(this, 4);
+    std::vector<double> aff(L), target(L);
+    seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, dX.p, 1.0, Y.p, dY.p, 1.0, seg_part.p,
+            work_L.p, st);
+    d2h(aff.data(), work_L.p, L * sizeof(double));
+    sync();
+    for (int l = 0; l < L; ++l) {
+      double rl = aff[l] / mu[l] / k[l];
+      double gl = std::max(rl < 1 ? rl * rl : rl, beta);
+      target[l] = gl * mu[l];
+    }
+    build_corrector_R(target);
+    rhs_from_R();
+  }
+  void build_corrector_R(const std::vector<double>& target) {
+    // R = target·I − X·Y − dX·dY
+    for (auto& b : dense) {
+      blk_gemm(blk_as_A(X.p, b.off, b.k), false, blk_as_B(Y.p, b.off, b.k), true, R.p, b, -1.0, 0.0,
+               KR_FULL);
+      blk_gemm(blk_as_A(dX.p, b.off, b.k), false, blk_as_B(dY.p, b.off, b.k), true, R.p, b, -1.0,
+               1.0, KR_FULL);
+    }
+    if (!dense.empty()) {
+      std::vector<double> sh(dense.size());
+      for (size_t b = 0; b < dense.size(); ++b) sh[b] = target[dense[b].user];
+      h2d(work_L.p, sh.data(), sh.size() * sizeof(double));
+      add_diag(d_doff.p, d_dk.p, (int)dense.size(), kmax, R.p, work_L.p, 0.0, st);
+    }
+    h2d(target_user.p, target.data(), L * sizeof(double));
+    diag_corrector_R(nd, od, X.p, Y.p, dX.p, dY.p, target_user.p, d_diag_user.p, R.p, st);
+  }
+  void set_rhs(int which) {
+    if (which == 0) gemv_t(A.p, K, m, Cst.p, 1.0, nullptr, 0.0, r.p, st);
+    else d2d(r.p, c.p, m * sizeof(double));
+  }
+
+  // ---------------------------------------------------------- directions --
+  void direction_blocks() {
+    PhaseScope ps(this, 4);
+    gemv_n(A.p, K, m, dx.p, tmpK.p, gemv_part.p, gemv_chunks, st);
+    axpbypcz(K, 1.0, tmpK.p, 1.0, P.p, 0.0, nullptr, dX.p, st);  // dX = 𝒜dx + P
+    for (auto& b : dense) {
+      d2d(T1.p + b.off, R.p + b.off, sizeof(double) * b.k * b.k);
+      blk_gemm(blk_as_A(dX.p, b.off, b.k), false, blk_as_B(Y.p, b.off, b.k), true, T1.p, b, -1.0,
+               1.0, KR_FULL);  // T1 = R − dX·Y
+    }
+    dense_cholsolve(T1.p, dY.p);
+    if (!dense.empty()) symmetrize(d_doff.p, d_dk.p, (int)dense.size(), kmax, dY.p, st);
+    diag_dY(nd, od, R.p, dX.p, Y.p, LX.p, dY.p, st);
+  }
+
+  // ------------------------------------------------- step length helpers --
+  // Host copies of the k = 2 blocks (closed-form tests as in the reference).
+  struct Small2 {
+    double X[4], dX[4];
+  };
+  std::vector<Small2> fetch_k2(const double* M, const double* dM) {
+    std::vector<Small2> out;
+    for (auto& b : dense) {
+      if (b.k != 2) continue;
+      Small2 s;
+      d2h(s.X, M + b.off, 4 * sizeof(double));
+      d2h(s.dX, dM + b.off, 4 * sizeof(double));
+      out.push_back(s);
+    }
+    if (!out.empty()) sync();
+    return out;
+  }
+  static bool isposdef2(const Small2& s, double t) {
+    double a = s.X[0] + t * s.dX[0];
+    if (!(a > 0)) return false;
+    double bb = s.X[1] + t * s.dX[1];
+    double dd = s.X[3] + t * s.dX[3];
+    return a * dd > bb * bb;
+  }
+  static bool margin2(const Small2& s, double t, double ratio) {
+    if (!(ratio > 0)) return isposdef2(s, t);
+    double a = s.X[0] + t * s.dX[0];
+    double a21 = s.X[1] + t * s.dX[1];
+    double a22 = s.X[3] + t * s.dX[3];
+    if (!(a > 0)) return false;
+    double l11 = std::sqrt(a), l21 = a21 / l11, d22 = a22 - l21 * l21;
+    if (!(d22 > 0)) return false;
+    double l22 = std::sqrt(d22);
+    double lo = std::min(std::fabs(l11), std::fabs(l22)), hi = std::max(std::fabs(l11), std::fabs(l22));
+    return std::isfinite(lo) && std::isfinite(hi) && hi > 0 && lo > ratio * hi;
+  }
+  static double ftb2(const Small2& s) {
+    // src/kernels/generic.jl:358-398 (2×2 closed form, bisection fallback)
+    double a = s.X[0], bb = s.X[2], dd = s.X[3];
+    double da = s.dX[0], db = (s.dX[2] + s.dX[1]) / 2.0, ddd = s.dX[3];
+    double a1 = a + da, b1 = bb + db, d1 = dd + ddd;
+    if (a1 > 0 && a1 * d1 > b1 * b1) return 1.0;
+    double c0 = a * dd - bb * bb;
+    double c1 = da * dd + a * ddd - 2.0 * bb * db;
+    double c2 = da * ddd - db * db;
+    double root = 1.0;
+    bool found = false;
+    if (c2 == 0) {
+      if (c1 < 0) {
+        double cand = -c0 / c1;
+        if (0 < cand && cand <= 1) root = cand, found = true;
+      }
+    } else {
+      double disc = c1 * c1 - 4.0 * c2 * c0;
+      if (disc >= 0) {
+        double sd = std::sqrt(disc), den = 2.0 * c2;
+        double q1 = (-c1 - sd) / den, q2 = (-c1 + sd) / den;
+        if (0 < q1 && q1 <= root) root = q1, found = true;
+        if (0 < q2 && q2 <= root) root = q2, found = true;
+      }
+    }
+    if (found) return root;
+    double lo = 0.0, hi = 1.0;
+    for (int i = 0; i < 64; ++i) {
+      double mid = (lo + hi) / 2.0;
+      if (isposdef2(s, mid)) lo = mid;
+      else hi = mid;
+    }
+    return lo;
+  }
+
+  // PD(+margin) tests of X_b + t·dX_b for every dense block with k > 2 and
+  // every candidate t; returns pass[cand] (all blocks pass).
+  std::vector<char> dense_trials(const double* M, const double* dM, const std::vector<double>& t,
+                                 double ratio) {
+    std::vector<char> pass(t.size(), 1);
+    std::vector<int> idx;
+    for (size_t b = 0; b < dense.size(); ++b)
+      if (dense[b].k > 2) idx.push_back((int)b);
+    if (idx.empty() || t.empty()) return pass;
+    // trial buffer: per block, |t| matrices
+    std::vector<long long> toff(dense.size(), 0);
+    long long need = 0;
+    for (size_t b = 0; b < dense.size(); ++b)
+      toff[b] = need, need += (long long)t.size() * dense[b].k * dense[b].k;
+    if ((size_t)need > trials.n) trials.alloc(need);
+    if (d_trial_off.n < dense.size()) d_trial_off.alloc(dense.size());
+    h2d(d_trial_off.p, toff.data(), dense.size() * sizeof(long long));
+    if (d_tcand.n < t.size()) d_tcand.alloc(t.size());
+    h2d(d_tcand.p, t.data(), t.size() * sizeof(double));
+    make_trials(d_doff.p, d_dk.p, d_trial_off.p, (int)dense.size(), kmax, M, dM, d_tcand.p,
+                (int)t.size(), trials.p, st);
+    // (blocks with k ≤ 2 also get trial copies above; they are ignored here)
+    std::vector<MatDesc<double>> mats;
+    for (int b : idx)
+      for (size_t c2 = 0; c2 < t.size(); ++c2)
+        mats.push_back({trials.p + toff[b] + (long long)c2 * dense[b].k * dense[b].k, dense[b].k,
+                        dense[b].k});
+    std::vector<int> info;
+    std::vector<double> dmn, dmx;
+    potrf_host_list(mats, info, dmn, dmx);
+    size_t q = 0;
+    for (size_t bi = 0; bi < idx.size(); ++bi)
+      for (size_t c2 = 0; c2 < t.size(); ++c2, ++q) {
+        bool ok = info[q] == 0;
+        if (ok && ratio > 0)
+          ok = std::isfinite(dmn[q]) && std::isfinite(dmx[q]) && dmx[q] > 0 && dmn[q] > ratio * dmx[q];
+        if (!ok) pass[c2] = 0;
+      }
+    return pass;
+  }
+  std::vector<char> diag_trials(const double* M, const double* dM, const std::vector<double>& t,
+                                double ratio) {
+    std::vector<char> pass(t.size(), 1);
+    if (!nd || t.empty()) return pass;
+    if (d_tcand.n < t.size()) d_tcand.alloc(t.size());
+    if (d_fail.n < t.size()) d_fail.alloc(t.size());
+    h2d(d_tcand.p, t.data(), t.size() * sizeof(double));
+    SDPX_CUDA(cudaMemsetAsync(d_fail.p, 0, t.size() * sizeof(int), st));
+    diag_trial(nd, od, M, dM, d_tcand.p, (int)t.size(), ratio > 0 ? 1 : 0, d_fail.p, st);
+    std::vector<int> f(t.size());
+    d2h(f.data(), d_fail.p, t.size() * sizeof(int));
+    sync();
+    for (size_t c2 = 0; c2 < t.size(); ++c2) pass[c2] = f[c2] == 0;
+    return pass;
+  }
+  std::vector<char> all_trials(const double* M, const double* dM, const std::vector<double>& t,
+                               double ratio, const std::vector<Small2>& k2) {
+    auto p1 = dense_trials(M, dM, t, ratio);
+    auto p2 = diag_trials(M, dM, t, ratio);
+    for (size_t c2 = 0; c2 < t.size(); ++c2) {
+      bool ok = p1[c2] && p2[c2];
+      for (auto& s : k2) ok = ok && margin2(s, t[c2], ratio);
+      p1[c2] = ok;
+    }
+    return p1;
+  }
+
+  // Fraction-to-boundary bound for one side (src/kernels/generic.jl:350-422):
+  // closed forms for 1×1 and 2×2, otherwise a full-step Cholesky test followed
+  // by 64 bisection steps.  The bisection is evaluated 15 points at a time —
+  // the complete 4-level subtree of the current interval — and the sequential
+  // path is replayed through it, so the result equals the sequential one.
+  double ftb_side(const double* M, const double* dM) {
+    double bound = 1.0;
+    if (nd) {
+      diag_ftb(nd, od, M, dM, red.p + 8, st);
+      bound = std::min(bound, read_red(8));
+    }
+    for (auto& s : fetch_k2(M, dM)) bound = std::min(bound, ftb2(s));
+    std::vector<int> big;
+    for (size_t b = 0; b < dense.size(); ++b)
+      if (dense[b].k > 2) big.push_back((int)b);
+    for (int b : big) bound = std::min(bound, ftb_dense_block(b, M, dM));
+    return bound;
+  }
+  double ftb_dense_block(int b, const double* M, const double* dM) {
+    // Evaluate candidate lists on this block only.
+    auto test = [&](const std::vector<double>& t) {
+      std::vector<char> pass(t.size(), 1);
+      std::vector<long long> toff(dense.size(), 0);
+      long long kk2 = (long long)dense[b].k * dense[b].k;
+      long long need = (long long)t.size() * kk2;
+      if ((size_t)need > trials.n) trials.alloc(need);
+      if (d_tcand.n < t.size()) d_tcand.alloc(t.size());
+      h2d(d_tcand.p, t.data(), t.size() * sizeof(double));
+      const int kk = dense[b].k;
+      if (d_trial_off.n < 1) d_trial_off.alloc(dense.size());
+      long long zero = 0;
+      h2d(d_trial_off.p, &zero, sizeof(long long));
+      make_trials(d_doff.p + b, d_dk.p + b, d_trial_off.p, 1, kk, M, dM, d_tcand.p, (int)t.size(),
+                  trials.p, st);
+      std::vector<MatDesc<double>> mats;
+      for (size_t c2 = 0; c2 < t.size(); ++c2) mats.push_back({trials.p + (long long)c2 * kk2, kk, kk});
+      std::vector<int> info;
+      std::vector<double> dmn, dmx;
+      potrf_host_list(mats, info, dmn, dmx);
+      for (size_t c2 = 0; c2 < t.size(); ++c2) pass[c2] = info[c2] == 0;
+      return pass;
+    };
+    constexpr int DEPTH = 4;
+    double lo = 0.0, hi = 1.0;
+    int done = 0;
+    bool first = true;
+    while (done < 64) {
+      int depth = std::min(DEPTH, 64 - done);
+      // heap-ordered subtree midpoints of (lo, hi)
+      int npts = (1 << depth) - 1;
+      std::vector<double> pts(npts), los(npts), his(npts);
+      los[0] = lo;
+      his[0] = hi;
+      for (int n2 = 0; n2 < npts; ++n2) {
+        pts[n2] = (los[n2] + his[n2]) / 2.0;
+        int l2 = 2 * n2 + 1, r2 = 2 * n2 + 2;
+        if (l2 < npts) los[l2] = los[n2], his[l2] = pts[n2];
+        if (r2 < npts) los[r2] = pts[n2], his[r2] = his[n2];
+      }
+      std::vector<double> cand = pts;
+      if (first) cand.push_back(1.0);
+      auto pass = test(cand);
+      if (first) {
+        first = false;
+        if (pass.back()) return 1.0;
+      }
+      int node = 0;
+      for (int s2 = 0; s2 < depth; ++s2) {
+        double mid = pts[node];
+        if (pass[node]) {
+          lo = mid;
+          node = 2 * node + 2;
+        } else {
+          hi = mid;
+          node = 2 * node + 1;
+        }
+      }
+      done += depth;
+    }
+    return lo;
+  }
+
+  void affine_diagnostics(int adaptive, double* out, double* block_compl) {
+    PhaseScope ps(this, 5);
+    double tX = 1.0, tY = 1.0;
+    if (adaptive) {
+      double bX = ftb_side(X.p, dX.p);
+      double bY = ftb_side(Y.p, dY.p);
+      tX = bX < 1 ? bX : 1.0;
+      tY = bY < 1 ? bY : 1.0;
+    }
+    std::vector<double> c1(L), c2(L);
+    seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, nullptr, 0.0, Y.p, nullptr, 0.0, seg_part.p,
+            work_L.p, st);
+    d2h(c1.data(), work_L.p, L * sizeof(double));
+    sync();
+    seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, dX.p, tX, Y.p, dY.p, tY, seg_part.p, work_L.p,
+            st);
+    d2h(c2.data(), work_L.p, L * sizeof(double));
+    sync();
+    double s1 = 0, s2 = 0;
+    for (int l = 0; l < L; ++l) s1 += c1[l], s2 += c2[l];
+    out[0] = s1;
+    out[1] = s2;
+    out[2] = tX;
+    out[3] = tY;
+    if (block_compl) std::memcpy(block_compl, c1.data(), L * sizeof(double));
+  }
+
+  void line_search(int rule, double fp, double fd, double gamma, double min_step, double margin,
+                   double* tX_out, double* tY_out) {
+    PhaseScope ps(this, 5);
+    if (rule == 1) {
+      double bX = ftb_side(X.p, dX.p), bY = ftb_side(Y.p, dY.p);
+      *tX_out = bX < 1 ? fp * bX : 1.0;
+      *tY_out = bY < 1 ? fd * bY : 1.0;
+      return;
+    }
+    auto side = [&](const double* M, const double* dM) {
+      auto k2 = fetch_k2(M, dM);
+      double t = 1.0;
+      constexpr int J = 8;
+      while (true) {
+        std::vector<double> cand;
+        double tt = t;
+        for (int j = 0; j < J; ++j) {
+          cand.push_back(tt);
+          if (tt < min_step) break;
+          tt *= gamma;
+        }
+        auto pass = all_trials(M, dM, cand, margin, k2);
+        for (size_t j = 0; j < cand.size(); ++j)
+          if (pass[j] || cand[j] < min_step) return cand[j];
+        t = cand.back() * gamma;
+      }
+    };
+    *tX_out = side(X.p, dX.p);
+    *tY_out = side(Y.p, dY.p);
+  }
+
+  // -------------------------------------------------------------- update --
+  void update(double tX, double tY, double* compl_total, int* finite, double* block_dots) {
+    PhaseScope ps(this, 6);
+    combine(K, X.p, tX, dX.p, st);
+    combine(K, Y.p, tY, dY.p, st);
+    combine(m, x.p, tX, dx.p, st);
+    std::vector<double> dots(L);
+    seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, nullptr, 0.0, Y.p, nullptr, 0.0, seg_part.p,
+            work_L.p, st);
+    d2h(dots.data(), work_L.p, L * sizeof(double));
+    clear_red(0, 3);
+    absmax(K, X.p, red.p + 0, st);
+    absmax(K, Y.p, red.p + 1, st);
+    absmax(m, x.p, red.p + 2, st);
+    d2h(h_red, red.p, 3 * sizeof(double));
+    sync();
+    double s = 0;
+    for (int l = 0; l < L; ++l) s += dots[l];
+    *compl_total = s;
+    *finite = std::isfinite(h_red[0]) && std::isfinite(h_red[1]) && std::isfinite(h_red[2]);
+    if (block_dots) std::memcpy(block_dots, dots.data(), L * sizeof(double));
+  }
+  void accepted_residuals(double bpr, double tX, double tY, double* pa, double* da) {
+    *pa = std::fabs(1.0 - tX) * bpr;
+    axpbypcz(m, 1.0 - tY, d.p, -tY, rho.p, 0.0, nullptr, d.p, st);
+    clear_red(0, 1);
+    absmax(m, d.p, red.p, st);
+    *da = read_red(0);
+  }
+  void objectives(double* po, double* dobj) {
+    std::vector<double> dots(2);
+    // pObj = cᵀx ; dObj = Σ⟨C_l, Y_l⟩
+    seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, Cst.p, nullptr, 0.0, Y.p, nullptr, 0.0, seg_part.p,
+            work_L.p, st);
+    std::vector<double> cy(L);
+    d2h(cy.data(), work_L.p, L * sizeof(double));
+    std::vector<double> hc(m), hx(m);
+    d2h(hc.data(), c.p, m * sizeof(double));
+    d2h(hx.data(), x.p, m * sizeof(double));
+    sync();
+    double p = 0;
+    for (int i = 0; i < m; ++i) p += hc[i] * hx[i];
+    double dd = 0;
+    for (int l = 0; l < L; ++l) dd += cy[l];
+    *po = p;
+    *dobj = dd;
+  }
+  void solution_residuals(double* pr, double* dr) {
+    gemv_n(A.p, K, m, x.p, tmpK.p, gemv_part.p, gemv_chunks, st);
+    axpbypcz(K, 1.0, tmpK.p, -1.0, X.p, -1.0, Cst.p, tmpK2.p, st);
+    gemv_t(A.p, K, m, Y.p, -1.0, c.p, 1.0, work_m.p, st);
+    clear_red(0, 2);
+    absmax(K, tmpK2.p, red.p + 0, st);
+    absmax(m, work_m.p, red.p + 1, st);
+    d2h(h_red, red.p, 2 * sizeof(double));
+    sync();
+    *pr = h_red[0];
+    *dr = h_red[1];
+  }
+
+  // ---------------------------------------------------------- cold start --
+  void cold_start_iterate() {
+    d2d(x.p, keptx.p, m * sizeof(double));
+    gemv_n(A.p, K, m, x.p, tmpK.p, gemv_part.p, gemv_chunks, st);
+    axpbypcz(K, 1.0, tmpK.p, -1.0, Cst.p, 0.0, nullptr, X.p, st);
+    gemv_n(A.p, K, m, dx.p, Y.p, gemv_part.p, gemv_chunks, st);
+  }
+  // Per-block certified shift (src/cold_start.jl:287-308) for all blocks at once.
+  void psd_shift(int which, int* ok_out) {
+    double* M = which == 0 ? X.p : Y.p;
+    std::vector<double> applied(L, 0.0);
+    std::vector<char> done(L, 0), bad(L, 0);
+    for (int round = 0; round <= 16; ++round) {
+      // stats for every block: finite, scale (max |lower|), lower eigen bound
+      std::vector<double> scale(L, 0.0), margin(L, 0.0);
+      std::vector<char> finite(L, 1);
+      size_t nb = dense.size();
+      if (nb) {
+        long long tot = 0;
+        for (auto& b : dense) tot += b.k;
+        g_scale.zero(st);
+        g_nonfinite.zero(st);
+        gershgorin(d_doff.p, d_dk.p, (int)nb, kmax, M, g_cand.p, g_cand_off.p, g_scale.p,
+                   g_nonfinite.p, st);
+        std::vector<double> cand(tot), sc(nb);
+        std::vector<int> nf(nb);
+        d2h(cand.data(), g_cand.p, tot * sizeof(double));
+        d2h(sc.data(), g_scale.p, nb * sizeof(double));
+        d2h(nf.data(), g_nonfinite.p, nb * sizeof(int));
+        sync();
+        long long o = 0;
+        for (size_t b = 0; b < nb; ++b) {
+          int l = dense[b].user, kk = dense[b].k;
+          scale[l] = sc[b];
+          finite[l] = nf[b] == 0;
+          double bound;
+          if (kk == 2) {
+            // exact eigenvalue (lower authoritative)
+            double h4[4];
+            d2h(h4, M + dense[b].off, 4 * sizeof(double));
+            sync();
+            double cc = (h4[0] + h4[3]) / 2, rr = std::hypot((h4[0] - h4[3]) / 2, h4[1]);
+            bound = cc - rr;
+          } else {
+            bound = cand[o];
+            for (int i = 1; i < kk; ++i) bound = std::min(bound, cand[o + i]);
+          }
+          margin[l] = bound;
+          o += kk;
+        }
+      }
+      if (nd) {
+        std::vector<double> dv(nd);
+        d2h(dv.data(), M + od, nd * sizeof(double));
+        sync();
+        for (int j = 0; j < nd; ++j) {
+          int l = diag_user[j];
+          finite[l] = std::isfinite(dv[j]);
+          scale[l] = std::fabs(dv[j]);
+          margin[l] = dv[j];
+        }
+      }
+      // decide shifts
+      std::vector<double> shifts(L, 0.0);
+      bool any = false;
+      for (int l = 0; l < L; ++l) {
+        if (done[l] || bad[l]) continue;
+        if (!finite[l]) {
+          bad[l] = 1;
+          continue;
+        }
+        double safety = kSqrtEps * std::max(1.0, scale[l]);
+        if (margin[l] > safety) {
+          done[l] = 1;
+          continue;
+        }
+        if (round == 16) {
+          bad[l] = 1;
+          continue;
+        }
+        double slack = 8.0 * kEps * std::max(1.0, scale[l]);
+        double sh = safety - margin[l] + slack;
+        if (!std::isfinite(sh)) {
+          bad[l] = 1;
+          continue;
+        }
+        shifts[l] = sh;
+        applied[l] += sh;
+        any = true;
+      }
+      if (!any) break;
+      apply_block_shifts(M, shifts);
+    }
+    bool ok = true;
+    for (int l = 0; l < L; ++l) ok = ok && !bad[l] && done[l];
+    *ok_out = ok ? 1 : 0;
+  }
+  void apply_block_shifts(double* M, const std::vector<double>& shifts) {
+    if (!dense.empty()) {
+      std::vector<double> sh(dense.size());
+      for (size_t b = 0; b < dense.size(); ++b) sh[b] = shifts[dense[b].user];
+      h2d(work_L.p, sh.data(), sh.size() * sizeof(double));
+      add_diag(d_doff.p, d_dk.p, (int)dense.size(), kmax, M, work_L.p, 0.0, st);
+    }
+    if (nd) {
+      std::vector<double> dv(nd);
+      d2h(dv.data(), M + od, nd * sizeof(double));
+      sync();
+      for (int j = 0; j < nd; ++j) dv[j] += shifts[diag_user[j]];
+      h2d(M + od, dv.data(), nd * sizeof(double));
+    }
+    sync();
+  }
+  void add_identity(int which, double shift) {
+    std::vector<double> sh(L, shift);
+    apply_block_shifts(which == 0 ? X.p : Y.p, sh);
+  }
+  void block_dots(double* dots, double* trX, double* trY) {
+    seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, nullptr, 0.0, Y.p, nullptr, 0.0, seg_part.p,
+            work_L.p, st);
+    d2h(dots, work_L.p, L * sizeof(double));
+    sync();
+    block_trace(d_uoff.p, d_uk.p, L, X.p, work_L.p, st);
+    d2h(trX, work_L.p, L * sizeof(double));
+    sync();
+    block_trace(d_uoff.p, d_uk.p, L, Y.p, work_L.p, st);
+    d2h(trY, work_L.p, L * sizeof(double));
+    sync();
+  }
+
+  // -------------------------------------------------------- original data --
+  void rebuild_slack(const double* hx, double* hX) {
+    const double* Ause = have_original ? A0.p : A.p;
+    const double* Cuse = have_original ? C0st.p : Cst.p;
+    h2d(work_m.p, hx, m * sizeof(double));
+    gemv_n(Ause, K, m, work_m.p, tmpK2.p, gemv_part.p, gemv_chunks, st);
+    axpbypcz(K, 1.0, tmpK2.p, -1.0, Cuse, 0.0, nullptr, tmpK2.p, st);
+    get_stacked(tmpK2.p, hX);
+  }
+  void original_residuals(const double* hx, const double* hX, const double* hY, double* pr,
+                          double* dr) {
+    const double* Ause = have_original ? A0.p : A.p;
+    const double* Cuse = have_original ? C0st.p : Cst.p;
+    const double* cuse = have_original ? c0.p : c.p;
+    h2d(work_m.p, hx, m * sizeof(double));
+    // X → T1, Y → T2 (scratch stacked buffers)
+    h2d(tmpK.p, hX, Ku * sizeof(double));
+    gather(K, d_map.p, tmpK.p, T1.p, st);
+    h2d(tmpK.p, hY, Ku * sizeof(double));
+    gather(K, d_map.p, tmpK.p, T2.p, st);
+    gemv_n(Ause, K, m, work_m.p, tmpK2.p, gemv_part.p, gemv_chunks, st);
+    axpbypcz(K, 1.0, tmpK2.p, -1.0, T1.p, -1.0, Cuse, tmpK2.p, st);
+    gemv_t(Ause, K, m, T2.p, -1.0, cuse, 1.0, work_m2.p, st);
+    clear_red(0, 2);
+    absmax(K, tmpK2.p, red.p + 0, st);
+    absmax(m, work_m2.p, red.p + 1, st);
+    d2h(h_red, red.p, 2 * sizeof(double));
+    sync();
+    *pr = h_red[0];
+    *dr = h_red[1];
+  }
+
+  // ------------------------------------------------------- mixed precision --
+  void mixed_init();
+  void mixed_schur();
+  void schur_split_bf16();
+  void mixed_factorize(int* ok, int* attempts, double* quality);
+  void mixed_solve(double* vec);
+  void mixed_residual();
+};
+
+}  // namespace sdpx
+
+// Mixed-precision members live in mixed_api.inc (same translation unit).
+#include "mixed_api.inc"
+
+// ============================================================================
+//                                   C ABI
+// ============================================================================
+using sdpx::Handle;
+
+struct sdpx_b200_handle {
+  Handle h;
+};
+
+static thread_local std::string g_create_error;
+
+#define GUARD(hh, body)                                   \
+  do {                                                    \
+    if (!(hh)) return -1;                                 \
+    try {                                                 \
+      SDPX_CUDA(cudaSetDevice((hh)->h.dev));              \
+      body;                                               \
+      return 0;                                           \
+    } catch (const std::exception& ex) {                  \
+      (hh)->h.err = ex.what();                            \
+      return -2;                                          \
+    } catch (...) {                                       \
+      (hh)->h.err = "unknown error";                      \
+      return -3;                                          \
+    }                                                     \
+  } while (0)
+
+extern "C" {
+
+int sdpx_b200_abi_version(void) { return SDPX_B200_ABI_VERSION; }
+const char* sdpx_b200_create_error(void) { return g_create_error.c_str(); }
+
+int sdpx_b200_create(const sdpx_b200_problem* problem, int device, sdpx_b200_handle** out) {
+  if (!problem || !out) return -1;
+  *out = nullptr;
+  auto* hh = new (std::nothrow) sdpx_b200_handle();
+  if (!hh) return -4;
+  try {
+    hh->h.create(problem, device);
+  } catch (const std::exception& ex) {
+    g_create_error = ex.what();
+    delete hh;
+    return -2;
+  }
+  *out = hh;
+  return 0;
+}
+void sdpx_b200_destroy(sdpx_b200_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->h.dev);
+  cudaStreamSynchronize(h->h.st);
+  delete h;
+}
+const char* sdpx_b200_last_error(const sdpx_b200_handle* h) { return h ? h->h.err.c_str() : "null handle"; }
+int sdpx_b200_set_precision(sdpx_b200_handle* h, int mode) {
+  GUARD(h, {
+    if (mode != SDPX_B200_FP64 && mode != SDPX_B200_MIXED) throw std::invalid_argument("bad precision mode");
+    h->h.precision = mode;
+    if (mode == SDPX_B200_MIXED) h->h.mixed_init();
+  });
+}
+int sdpx_b200_equilibrate(sdpx_b200_handle* h, double* E, double* s, double* osc, int32_t* passes) {
+  GUARD(h, h->h.equilibrate(E, s, osc, passes));
+}
+int sdpx_b200_data_norms(sdpx_b200_handle* h, double* a, double* b) { GUARD(h, h->h.data_norms(a, b)); }
+int sdpx_b200_set_iterate(sdpx_b200_handle* h, const double* x, const double* X, const double* Y) {
+  GUARD(h, h->h.set_iterate(x, X, Y));
+}
+int sdpx_b200_get_iterate(sdpx_b200_handle* h, double* x, double* X, double* Y) {
+  GUARD(h, {
+    if (x) {
+      h->h.d2h(x, h->h.x.p, h->h.m * sizeof(double));
+      h->h.sync();
+    }
+    if (X) h->h.get_stacked(h->h.X.p, X);
+    if (Y) h->h.get_stacked(h->h.Y.p, Y);
+  });
+}
+int sdpx_b200_get_direction(sdpx_b200_handle* h, double* dx, double* dX, double* dY) {
+  GUARD(h, {
+    if (dx) {
+      h->h.d2h(dx, h->h.dx.p, h->h.m * sizeof(double));
+      h->h.sync();
+    }
+    if (dX) h->h.get_stacked(h->h.dX.p, dX);
+    if (dY) h->h.get_stacked(h->h.dY.p, dY);
+  });
+}
+int sdpx_b200_get_rhs(sdpx_b200_handle* h, double* r) {
+  GUARD(h, {
+    h->h.d2h(r, h->h.r.p, h->h.m * sizeof(double));
+    h->h.sync();
+  });
+}
+int sdpx_b200_fixed_start(sdpx_b200_handle* h, double wp, double wd) {
+  GUARD(h, {
+    h->h.fixed_start(wp, wd);
+    h->h.sync();
+  });
+}
+int sdpx_b200_residuals(sdpx_b200_handle* h, const double* mu, int use_affine, int factor,
+                        double* p_res, double* d_res, int* ok) {
+  GUARD(h, h->h.residuals(mu, use_affine, factor, p_res, d_res, ok));
+}
+int sdpx_b200_block_primal_residual(sdpx_b200_handle* h, double* v) { GUARD(h, *v = h->h.last_bpr); }
+int sdpx_b200_block_margins(sdpx_b200_handle* h, double* p, double* d) {
+  GUARD(h, h->h.block_margins(p, d));
+}
+int sdpx_b200_schur_build(sdpx_b200_handle* h, int identity) {
+  GUARD(h, {
+    if (identity) {
+      // cold start: factors of the identity
+      h->h.schur_build(1);
+    } else {
+      h->h.schur_build(0);
+    }
+  });
+}
+int sdpx_b200_get_schur(sdpx_b200_handle* h, double* S) {
+  GUARD(h, {
+    h->h.d2h(S, h->h.S.p, sizeof(double) * h->h.m * h->h.m);
+    h->h.sync();
+  });
+}
+int sdpx_b200_factorize(sdpx_b200_handle* h, int* ok, int* att, double* q) {
+  GUARD(h, h->h.factorize(ok, att, q));
+}
+int sdpx_b200_rhs_predictor(sdpx_b200_handle* h) { GUARD(h, h->h.rhs_predictor()); }
+int sdpx_b200_rhs_corrector_mehrotra(sdpx_b200_handle* h, double sigma, double mu, int bl) {
+  GUARD(h, h->h.rhs_corrector_mehrotra(sigma, mu, bl));
+}
+int sdpx_b200_rhs_corrector_fixed(sdpx_b200_handle* h, double beta, const double* mu) {
+  GUARD(h, h->h.rhs_corrector_fixed(beta, mu));
+}
+int sdpx_b200_set_rhs(sdpx_b200_handle* h, int which) { GUARD(h, h->h.set_rhs(which)); }
+int sdpx_b200_solve(sdpx_b200_handle* h) { GUARD(h, h->h.solve()); }
+int sdpx_b200_direction_residual(sdpx_b200_handle* h, double* res, double* rn) {
+  GUARD(h, h->h.direction_residual(res, rn));
+}
+int sdpx_b200_refine(sdpx_b200_handle* h, int policy, double tol, int cap, int fixed_steps,
+                     int* steps, double* res) {
+  GUARD(h, h->h.refine(policy, tol, cap, fixed_steps, steps, res));
+}
+int sdpx_b200_direction_blocks(sdpx_b200_handle* h) { GUARD(h, h->h.direction_blocks()); }
+int sdpx_b200_affine_diagnostics(sdpx_b200_handle* h, int adaptive, double* out, double* bc) {
+  GUARD(h, h->h.affine_diagnostics(adaptive, out, bc));
+}
+int sdpx_b200_line_search(sdpx_b200_handle* h, int rule, double fp, double fd, double gamma,
+                          double min_step, double margin, double* tX, double* tY) {
+  GUARD(h, h->h.line_search(rule, fp, fd, gamma, min_step, margin, tX, tY));
+}
+int sdpx_b200_update(sdpx_b200_handle* h, double tX, double tY, double* c, int* f, double* bd) {
+  GUARD(h, h->h.update(tX, tY, c, f, bd));
+}
+int sdpx_b200_accepted_residuals(sdpx_b200_handle* h, double bpr, double tX, double tY, double* pa,
+                                 double* da) {
+  GUARD(h, h->h.accepted_residuals(bpr, tX, tY, pa, da));
+}
+int sdpx_b200_objectives(sdpx_b200_handle* h, double* p, double* d) { GUARD(h, h->h.objectives(p, d)); }
+int sdpx_b200_solution_residuals(sdpx_b200_handle* h, double* p, double* d) {
+  GUARD(h, h->h.solution_residuals(p, d));
+}
+int sdpx_b200_keep_direction(sdpx_b200_handle* h) {
+  GUARD(h, h->h.d2d(h->h.keptx.p, h->h.dx.p, h->h.m * sizeof(double)));
+}
+int sdpx_b200_cold_start_iterate(sdpx_b200_handle* h) {
+  GUARD(h, {
+    h->h.cold_start_iterate();
+    h->h.sync();
+  });
+}
+int sdpx_b200_psd_shift(sdpx_b200_handle* h, int which, int* ok) { GUARD(h, h->h.psd_shift(which, ok)); }
+int sdpx_b200_add_identity(sdpx_b200_handle* h, int which, double shift) {
+  GUARD(h, h->h.add_identity(which, shift));
+}
+int sdpx_b200_block_dots(sdpx_b200_handle* h, double* d, double* tx, double* ty) {
+  GUARD(h, h->h.block_dots(d, tx, ty));
+}
+int sdpx_b200_scale_iterate(sdpx_b200_handle* h, int which, double f) {
+  GUARD(h, {
+    sdpx::scale(h->h.K, which == 0 ? h->h.X.p : h->h.Y.p, f, h->h.st);
+    h->h.sync();
+  });
+}
+int sdpx_b200_store_best(sdpx_b200_handle* h) {
+  GUARD(h, {
+    auto& H = h->h;
+    H.d2d(H.xbest.p, H.x.p, H.m * sizeof(double));
+    H.d2d(H.Xbest.p, H.X.p, H.K * sizeof(double));
+    H.d2d(H.Ybest.p, H.Y.p, H.K * sizeof(double));
+  });
+}
+int sdpx_b200_restore_best(sdpx_b200_handle* h) {
+  GUARD(h, {
+    auto& H = h->h;
+    H.d2d(H.x.p, H.xbest.p, H.m * sizeof(double));
+    H.d2d(H.X.p, H.Xbest.p, H.K * sizeof(double));
+    H.d2d(H.Y.p, H.Ybest.p, H.K * sizeof(double));
+    H.sync();
+  });
+}
+int sdpx_b200_rebuild_slack(sdpx_b200_handle* h, const double* x, double* X) {
+  GUARD(h, h->h.rebuild_slack(x, X));
+}
+int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const double* X,
+                                 const double* Y, double* p, double* d) {
+  GUARD(h, h->h.original_residuals(x, X, Y, p, d));
+}
+int sdpx_b200_phase_times(sdpx_b200_handle* h, double* ms7, int reset) {
+  GUARD(h, {
+    h->h.harvest_phases();
+    for (int i = 0; i < 7; ++i) ms7[i] = h->h.phase_ms[i];
+    if (reset)
+      for (int i = 0; i < 7; ++i) h->h.phase_ms[i] = 0.0;
+  });
+}
+
+}  // extern "C"

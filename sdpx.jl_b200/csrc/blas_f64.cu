@@ -1,0 +1,178 @@
+// FP64 dense kernels on the DMMA tile engine: general GEMM with triangular
+// K ranges, in-place right multiplication by a lower-triangular factor, and
+// the split-K lower SYRK that assembles the Schur complement S = P̂ᵀP̂.
+#include "blas_f64.h"
+#include "gemm_f64.cuh"
+
+namespace sdpx {
+
+// Tile configurations.  128×128 / 8 warps for the large Schur products,
+// 64×64 / 4 warps for per-block k×k products.
+using CfgBigKT = F64Cfg<128, 128, 2, 4, true, true>;    // SYRK: both operands K-contiguous
+using CfgBigMK = F64Cfg<128, 128, 2, 4, false, true>;   // A MN-contiguous, B K-contiguous
+using CfgSmMK = F64Cfg<64, 64, 2, 2, false, true>;
+using CfgSmKK = F64Cfg<64, 64, 2, 2, true, true>;
+using CfgSmMM = F64Cfg<64, 64, 2, 2, false, false>;
+using CfgSmKM = F64Cfg<64, 64, 2, 2, true, false>;
+
+__device__ __forceinline__ double* out_ptr(const OutDesc& C, int r, int c) {
+  return C.base + two_level(r, C.row_inner, C.row_inner_stride, C.row_outer_stride) +
+         two_level(c, C.col_inner, C.col_inner_stride, C.col_outer_stride);
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT) k_gemm(Opnd A, Opnd B, OutDesc C, double alpha,
+                                                  double beta, int mode) {
+  extern __shared__ __align__(16) double smem[];
+  const int n0 = blockIdx.x * Cfg::BN, m0 = blockIdx.y * Cfg::BM;
+  int kb, ke;
+  k_limits(mode, A.k_extent, m0, n0, Cfg::BM, Cfg::BN, kb, ke);
+  double acc[Cfg::FM][Cfg::FN][2];
+  zero_acc<Cfg>(acc);
+  f64_tile_mainloop<Cfg>(acc, A, B, m0, n0, kb, ke, smem);
+  for_each_acc<Cfg>(acc, [&](int r, int c, double v) {
+    int gr = m0 + r, gc = n0 + c;
+    if (gr < C.rows && gc < C.cols) {
+      double* p = out_ptr(C, gr, gc);
+      *p = (beta == 0.0) ? alpha * v : alpha * v + beta * (*p);
+    }
+  });
+}
+
+// In-place  T ← T · L  for a lower-triangular L (k×k, explicit zeros above the
+// diagonal).  One CTA owns BM consecutive rows of T and sweeps the output
+// column tiles left to right; output tile [n0, n0+BN) reads only columns ≥ n0,
+// which this CTA has not yet overwritten, so the update is race free.
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT) k_trmm_right_lower_inplace(Opnd T, Opnd L, OutDesc C) {
+  extern __shared__ __align__(16) double smem[];
+  const int m0 = blockIdx.x * Cfg::BM;
+  const int K = L.k_extent;
+  for (int n0 = 0; n0 < C.cols; n0 += Cfg::BN) {
+    double acc[Cfg::FM][Cfg::FN][2];
+    zero_acc<Cfg>(acc);
+    f64_tile_mainloop<Cfg>(acc, T, L, m0, n0, n0, K, smem);
+    __syncthreads();
+    for_each_acc<Cfg>(acc, [&](int r, int c, double v) {
+      int gr = m0 + r, gc = n0 + c;
+      if (gr < C.rows && gc < C.cols) *out_ptr(C, gr, gc) = v;
+    });
+    __syncthreads();
+  }
+}
+
+// Split-K lower SYRK.  Work unit u = chunk * ntri + tri (chunk-major, so CTAs
+// resident at the same time share one K slab of the panel in L2).  Each unit
+// writes its BM×BN partial tile to `partial` (column-major inside the tile);
+// `k_syrk_reduce` sums the chunks in a fixed order (bitwise reproducible).
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT) k_syrk_splitk(Opnd P, int ntri, int kchunk,
+                                                          double* partial) {
+  extern __shared__ __align__(16) double smem[];
+  const int u = blockIdx.x;
+  const int chunk = u / ntri, tri = u % ntri;
+  int ti = (int)((sqrt(8.0 * tri + 1.0) - 1.0) * 0.5);
+  while ((ti + 1) * (ti + 2) / 2 <= tri) ++ti;
+  while (ti * (ti + 1) / 2 > tri) --ti;
+  const int tj = tri - ti * (ti + 1) / 2;
+  const int kb = chunk * kchunk;
+  const int ke = min(P.k_extent, kb + kchunk);
+  double acc[Cfg::FM][Cfg::FN][2];
+  zero_acc<Cfg>(acc);
+  f64_tile_mainloop<Cfg>(acc, P, P, ti * Cfg::BM, tj * Cfg::BN, kb, ke, smem);
+  double* out = partial + (size_t)u * Cfg::BM * Cfg::BN;
+  for_each_acc<Cfg>(acc, [&](int r, int c, double v) { out[c * Cfg::BM + r] = v; });
+}
+
+template <int BM, int BN>
+__global__ void k_syrk_reduce(const double* partial, int ntri, int nchunk, int m, double* S,
+                              long long lds, double beta) {
+  const int tri = blockIdx.x;
+  int ti = (int)((sqrt(8.0 * tri + 1.0) - 1.0) * 0.5);
+  while ((ti + 1) * (ti + 2) / 2 <= tri) ++ti;
+  while (ti * (ti + 1) / 2 > tri) --ti;
+  const int tj = tri - ti * (ti + 1) / 2;
+  for (int e = threadIdx.x; e < BM * BN; e += blockDim.x) {
+    int r = e % BM, c = e / BM;
+    int gi = ti * BM + r, gj = tj * BN + c;
+    if (gi >= m || gj >= m) continue;
+    double s = 0.0;
+    for (int ch = 0; ch < nchunk; ++ch) s += partial[((size_t)ch * ntri + tri) * BM * BN + e];
+    double* p = S + gi + (long long)gj * lds;
+    *p = (beta == 0.0) ? s : s + beta * (*p);
+  }
+}
+
+template <class Cfg>
+static void launch_gemm_cfg(const Opnd& A, const Opnd& B, const OutDesc& C, double alpha,
+                            double beta, int mode, cudaStream_t st) {
+  ensure_smem(k_gemm<Cfg>, Cfg::SMEM_BYTES);
+  dim3 grid(ceil_div(C.cols, Cfg::BN), ceil_div(C.rows, Cfg::BM));
+  if (grid.x == 0 || grid.y == 0) return;
+  k_gemm<Cfg><<<grid, Cfg::NT, Cfg::SMEM_BYTES, st>>>(A, B, C, alpha, beta, mode);
+  SDPX_LAUNCH_CHECK();
+}
+
+void gemm_f64(const Opnd& A, bool a_kcontig, const Opnd& B, bool b_kcontig, const OutDesc& C,
+              double alpha, double beta, int mode, bool big, cudaStream_t st) {
+  if (big && !a_kcontig && b_kcontig) return launch_gemm_cfg<CfgBigMK>(A, B, C, alpha, beta, mode, st);
+  if (big && a_kcontig && b_kcontig) return launch_gemm_cfg<CfgBigKT>(A, B, C, alpha, beta, mode, st);
+  if (!a_kcontig && b_kcontig) return launch_gemm_cfg<CfgSmMK>(A, B, C, alpha, beta, mode, st);
+  if (a_kcontig && b_kcontig) return launch_gemm_cfg<CfgSmKK>(A, B, C, alpha, beta, mode, st);
+  if (!a_kcontig && !b_kcontig) return launch_gemm_cfg<CfgSmMM>(A, B, C, alpha, beta, mode, st);
+  return launch_gemm_cfg<CfgSmKM>(A, B, C, alpha, beta, mode, st);
+}
+
+void trmm_right_lower_inplace_f64(const Opnd& T, const Opnd& L, const OutDesc& C, cudaStream_t st) {
+  using Cfg = CfgBigMK;
+  ensure_smem(k_trmm_right_lower_inplace<Cfg>, Cfg::SMEM_BYTES);
+  int grid = ceil_div(C.rows, Cfg::BM);
+  if (grid == 0) return;
+  k_trmm_right_lower_inplace<Cfg><<<grid, Cfg::NT, Cfg::SMEM_BYTES, st>>>(T, L, C);
+  SDPX_LAUNCH_CHECK();
+}
+
+SyrkPlan plan_syrk_f64(int m, long long K, int sm_count) {
+  SyrkPlan p;
+  p.bm = CfgBigKT::BM;
+  int nt = ceil_div(m, p.bm);
+  p.ntri = nt * (nt + 1) / 2;
+  // Choose the number of K chunks so the unit count fills whole waves of one
+  // CTA per SM, with at least 256 rows of K per chunk.
+  int best_c = 1;
+  double best_eff = 0.0;
+  long long max_c = K / 256;
+  if (max_c < 1) max_c = 1;
+  if (max_c > 16) max_c = 16;
+  for (int c = 1; c <= max_c; ++c) {
+    long long units = (long long)p.ntri * c;
+    double waves = (double)units / sm_count;
+    double eff = waves / std::ceil(waves);
+    // Prefer more work per wave up to ~4 waves; past that, only efficiency counts.
+    double score = eff * std::min(1.0, waves / 4.0);
+    if (score > best_eff + 1e-9) {
+      best_eff = score;
+      best_c = c;
+    }
+  }
+  long long kc = (K + best_c - 1) / best_c;
+  kc = ((kc + 15) / 16) * 16;
+  p.kchunk = (int)kc;
+  p.nchunk = (int)((K + kc - 1) / kc);
+  p.partial_doubles = (size_t)p.nchunk * p.ntri * p.bm * p.bm;
+  return p;
+}
+
+void syrk_lower_f64(const Opnd& P, const SyrkPlan& plan, double* partial, double* S, long long lds,
+                    int m, double beta, cudaStream_t st) {
+  using Cfg = CfgBigKT;
+  ensure_smem(k_syrk_splitk<Cfg>, Cfg::SMEM_BYTES);
+  int units = plan.ntri * plan.nchunk;
+  k_syrk_splitk<Cfg><<<units, Cfg::NT, Cfg::SMEM_BYTES, st>>>(P, plan.ntri, plan.kchunk, partial);
+  SDPX_LAUNCH_CHECK();
+  k_syrk_reduce<Cfg::BM, Cfg::BN><<<plan.ntri, 256, 0, st>>>(partial, plan.ntri, plan.nchunk, m, S,
+                                                             lds, beta);
+  SDPX_LAUNCH_CHECK();
+}
+
+}  // namespace sdpx

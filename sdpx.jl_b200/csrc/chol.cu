@@ -1,0 +1,434 @@
+// Batched blocked Cholesky, triangular inverse and blocked triangular solves
+// (FP64, templated on the element type for the FP32 mixed-precision factor).
+//
+// Cholesky (lower, right-looking, panel width NB): per panel j one launch
+// factors the diagonal tile in shared memory (redundantly in every CTA of the
+// panel) and solves the tiles below it; a second launch applies the rank-NB
+// update to the trailing lower tiles.  A matrix whose pivot is not positive
+// (or NaN) records `info = pivot index + 1` and every later CTA of that matrix
+// returns at once — the no-throw contract of SDPX's `kchol!`
+// (src/kernels/generic.jl:133-155).
+#include "chol.h"
+
+namespace sdpx {
+
+template <class T, int NB>
+__device__ bool factor_diag_tile(T* D, int ldd, int w, int* fail_at) {
+  // In-place lower Cholesky of the w×w tile D (shared memory).  Returns false on
+  // a non-positive or NaN pivot and stores its index in *fail_at.
+  __shared__ int s_fail;
+  if (threadIdx.x == 0) s_fail = -1;
+  __syncthreads();
+  for (int c = 0; c < w; ++c) {
+    T piv = D[c * ldd + c];
+    if (!(piv > T(0))) {
+      if (threadIdx.x == 0) s_fail = c;
+      __syncthreads();
+      break;
+    }
+    T lc = sqrt(piv);
+    __syncthreads();
+    for (int r = c + 1 + threadIdx.x; r < w; r += blockDim.x) D[c * ldd + r] /= lc;
+    if (threadIdx.x == 0) D[c * ldd + c] = lc;
+    __syncthreads();
+    int rem = w - c - 1;
+    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+      int r = c + 1 + e % rem, q = c + 1 + e / rem;
+      if (q <= r) D[q * ldd + r] -= D[c * ldd + r] * D[c * ldd + q];
+    }
+    __syncthreads();
+  }
+  *fail_at = s_fail;
+  return s_fail < 0;
+}
+
+template <class T, int NB>
+__global__ void k_potrf_panel(const MatDesc<T>* mats, int j, int* info, T* dmin, T* dmax,
+                              T* diag_store) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  T* D = reinterpret_cast<T*>(raw);           // NB × (NB+1), column-major
+  T* Bt = D + NB * (NB + 1);                   // NB × (NB+1)
+  constexpr int LD = NB + 1;
+  const MatDesc<T> M = mats[blockIdx.y];
+  const int b = blockIdx.y;
+  const int c0 = j * NB;
+  if (c0 >= M.n) return;
+  const int i = j + blockIdx.x;  // row tile
+  const int r0 = i * NB;
+  if (r0 >= M.n) return;
+  if (info[b] != 0) return;
+  const int w = min(NB, M.n - c0);
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int r = e % w, c = e / w;
+    D[c * LD + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
+  }
+  __syncthreads();
+  int fail_at = -1;
+  bool ok = factor_diag_tile<T, NB>(D, LD, w, &fail_at);
+  if (!ok) {
+    if (i == j && threadIdx.x == 0) info[b] = c0 + fail_at + 1;
+    return;
+  }
+  if (i == j) {
+    // Other CTAs of this launch are still reading the unfactored diagonal tile,
+    // so L_jj goes to a per-matrix store; the update launch writes it back.
+    T* ds = diag_store + (size_t)b * NB * NB;
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+      int r = e % w, c = e / w;
+      ds[c * NB + r] = (r >= c) ? D[c * LD + r] : T(0);
+    }
+    if (threadIdx.x == 0) {
+      T lo = dmin[b], hi = dmax[b];
+      for (int c = 0; c < w; ++c) {
+        T v = fabs(D[c * LD + c]);
+        lo = fmin(lo, v);
+        hi = fmax(hi, v);
+      }
+      dmin[b] = lo;
+      dmax[b] = hi;
+    }
+    return;
+  }
+  // Off-diagonal tile: X = B · L_jj^{-T}, one thread per row.
+  const int h = min(NB, M.n - r0);
+  for (int e = threadIdx.x; e < h * w; e += blockDim.x) {
+    int r = e % h, c = e / h;
+    Bt[c * LD + r] = M.a[(size_t)(c0 + c) * M.ld + (r0 + r)];
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < h; r += blockDim.x) {
+    for (int c = 0; c < w; ++c) {
+      T s = Bt[c * LD + r];
+      for (int p = 0; p < c; ++p) s -= Bt[p * LD + r] * D[p * LD + c];
+      Bt[c * LD + r] = s / D[c * LD + c];
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < h * w; e += blockDim.x) {
+    int r = e % h, c = e / h;
+    M.a[(size_t)(c0 + c) * M.ld + (r0 + r)] = Bt[c * LD + r];
+  }
+}
+
+// Trailing update A[i,q] -= L[i,j] L[q,j]^T for j < q <= i (lower tiles).
+template <class T, int NB>
+__global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info,
+                               const T* diag_store) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  T* La = reinterpret_cast<T*>(raw);  // NB × (NB+1): rows of tile i, panel j
+  T* Lb = La + NB * (NB + 1);          // rows of tile q
+  constexpr int LD = NB + 1;
+  const MatDesc<T> M = mats[blockIdx.y];
+  if (info[blockIdx.y] != 0) return;
+  const int nt = (M.n + NB - 1) / NB;
+  if (j >= nt) return;
+  const int rem = nt - j - 1;
+  const int t = blockIdx.x;
+  if (t == 0) {
+    // CTA 0 writes back the factored diagonal tile of panel j.
+    const int c0 = j * NB, w = min(NB, M.n - c0);
+    const T* ds = diag_store + (size_t)blockIdx.y * NB * NB;
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+      int r = e % w, c = e / w;
+      M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] = ds[c * NB + r];
+    }
+    return;
+  }
+  if (rem <= 0 || t - 1 >= rem * (rem + 1) / 2) return;
+  const int u = t - 1;
+  int a = (int)((sqrt(8.0 * u + 1.0) - 1.0) * 0.5);
+  while ((a + 1) * (a + 2) / 2 <= u) ++a;
+  while (a * (a + 1) / 2 > u) --a;
+  const int bq = u - a * (a + 1) / 2;
+  const int i = j + 1 + a, q = j + 1 + bq;
+  const int c0 = j * NB, r0 = i * NB, q0 = q * NB;
+  const int w = min(NB, M.n - c0), h = min(NB, M.n - r0), hq = min(NB, M.n - q0);
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    int r = e % NB, c = e / NB;
+    La[c * LD + r] = (r < h && c < w) ? M.a[(size_t)(c0 + c) * M.ld + (r0 + r)] : T(0);
+    Lb[c * LD + r] = (r < hq && c < w) ? M.a[(size_t)(c0 + c) * M.ld + (q0 + r)] : T(0);
+  }
+  __syncthreads();
+  // Each thread owns a 4×4 block of outputs (NB=64: 256 threads; NB=32: 64 active).
+  constexpr int RB = 4;
+  constexpr int TPR = NB / RB;
+  const int tr = threadIdx.x % TPR, tc = threadIdx.x / TPR;
+  if (tc < TPR) {
+    T acc[RB][RB] = {};
+    for (int p = 0; p < w; ++p) {
+      T av[RB], bv[RB];
+#pragma unroll
+      for (int x = 0; x < RB; ++x) av[x] = La[p * LD + tr + x * TPR];
+#pragma unroll
+      for (int y = 0; y < RB; ++y) bv[y] = Lb[p * LD + tc + y * TPR];
+#pragma unroll
+      for (int x = 0; x < RB; ++x)
+#pragma unroll
+        for (int y = 0; y < RB; ++y) acc[x][y] += av[x] * bv[y];
+    }
+#pragma unroll
+    for (int x = 0; x < RB; ++x)
+#pragma unroll
+      for (int y = 0; y < RB; ++y) {
+        int r = tr + x * TPR, c = tc + y * TPR;
+        if (r < h && c < hq) M.a[(size_t)(q0 + c) * M.ld + (r0 + r)] -= acc[x][y];
+      }
+  }
+}
+
+template <class T>
+__global__ void k_zero_upper(const MatDesc<T>* mats) {
+  const MatDesc<T> M = mats[blockIdx.y];
+  long long total = (long long)M.n * M.n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    int r = (int)(e % M.n), c = (int)(e / M.n);
+    if (r < c) M.a[(size_t)c * M.ld + r] = T(0);
+  }
+}
+
+template <class T>
+__global__ void k_init_stats(int n, int* info, T* dmin, T* dmax) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n) {
+    info[b] = 0;
+    dmin[b] = T(1.0 / 0.0);
+    dmax[b] = T(0);
+  }
+}
+
+template <class T, int NB>
+void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* dmin, T* dmax,
+                   T* diag_store, cudaStream_t st) {
+  if (nmat == 0 || nmax == 0) return;
+  const size_t smem = 2 * sizeof(T) * NB * (NB + 1);
+  ensure_smem(k_potrf_panel<T, NB>, smem);
+  ensure_smem(k_potrf_update<T, NB>, smem);
+  k_init_stats<T><<<ceil_div(nmat, 128), 128, 0, st>>>(nmat, info, dmin, dmax);
+  const int nt = ceil_div(nmax, NB);
+  for (int j = 0; j < nt; ++j) {
+    dim3 g1(nt - j, nmat);
+    k_potrf_panel<T, NB><<<g1, 256, smem, st>>>(d_mats, j, info, dmin, dmax, diag_store);
+    int rem = nt - j - 1;
+    dim3 g2(1 + rem * (rem + 1) / 2, nmat);
+    k_potrf_update<T, NB><<<g2, 256, smem, st>>>(d_mats, j, info, diag_store);
+  }
+  dim3 gz(std::max(1, std::min(1024, ceil_div((long long)nmax * nmax, 256))), nmat);
+  k_zero_upper<T><<<gz, 256, 0, st>>>(d_mats);
+  SDPX_LAUNCH_CHECK();
+}
+
+template void potrf_batched<double, 32>(const MatDesc<double>*, int, int, int*, double*, double*,
+                                        double*, cudaStream_t);
+template void potrf_batched<double, 64>(const MatDesc<double>*, int, int, int*, double*, double*,
+                                        double*, cudaStream_t);
+template void potrf_batched<float, 64>(const MatDesc<float>*, int, int, int*, float*, float*,
+                                       float*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Triangular inverse W = L^{-1} (lower), blocked by NB.  Step 0 inverts every
+// diagonal tile; step i fills block row i:  W[i,j] = -W[i,i] Σ_{p=j}^{i-1} L[i,p] W[p,j].
+// W must be zero-initialised (its strict upper triangle stays zero).
+// ---------------------------------------------------------------------------
+template <class T, int NB>
+__global__ void k_trinv_diag(const MatDesc<T>* Ls, const MatDesc<T>* Ws) {
+  __shared__ T Lt[NB][NB + 1];
+  __shared__ T Wt[NB][NB + 1];
+  const MatDesc<T> L = Ls[blockIdx.y], W = Ws[blockIdx.y];
+  const int s0 = blockIdx.x * NB;
+  if (s0 >= L.n) return;
+  const int w = min(NB, L.n - s0);
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int r = e % w, c = e / w;
+    Lt[c][r] = L.a[(size_t)(s0 + c) * L.ld + s0 + r];
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < w; c += blockDim.x) {
+    Wt[c][c] = T(1) / Lt[c][c];
+    for (int r = c + 1; r < w; ++r) {
+      T s = T(0);
+      for (int p = c; p < r; ++p) s += Lt[p][r] * Wt[c][p];
+      Wt[c][r] = -s / Lt[r][r];
+    }
+    for (int r = 0; r < c; ++r) Wt[c][r] = T(0);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int r = e % w, c = e / w;
+    W.a[(size_t)(s0 + c) * W.ld + s0 + r] = Wt[c][r];
+  }
+}
+
+template <class T, int NB>
+__global__ void k_trinv_row(const MatDesc<T>* Ls, const MatDesc<T>* Ws, int i) {
+  __shared__ T Acc[NB][NB + 1];
+  __shared__ T Lt[NB][NB + 1];
+  __shared__ T Wt[NB][NB + 1];
+  const MatDesc<T> L = Ls[blockIdx.y], W = Ws[blockIdx.y];
+  const int nt = (L.n + NB - 1) / NB;
+  if (i >= nt) return;
+  const int j = blockIdx.x;
+  if (j >= i) return;
+  const int r0 = i * NB, h = min(NB, L.n - r0);
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) Acc[e / NB][e % NB] = T(0);
+  for (int p = j; p < i; ++p) {
+    const int p0 = p * NB;
+    __syncthreads();
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+      int r = e % NB, c = e / NB;
+      Lt[c][r] = (r < h) ? L.a[(size_t)(p0 + c) * L.ld + r0 + r] : T(0);       // L[i,p]
+      Wt[c][r] = W.a[(size_t)(j * NB + c) * W.ld + p0 + r];                     // W[p,j]
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+      int r = e % NB, c = e / NB;
+      T s = T(0);
+#pragma unroll 8
+      for (int q = 0; q < NB; ++q) s += Lt[q][r] * Wt[c][q];
+      Acc[c][r] += s;
+    }
+  }
+  __syncthreads();
+  // W[i,j] = -W[i,i] · Acc
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    int r = e % NB, c = e / NB;
+    Wt[c][r] = (r < h && c < h) ? W.a[(size_t)(r0 + c) * W.ld + r0 + r] : T(0);  // W[i,i]
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < h * NB; e += blockDim.x) {
+    int r = e % h, c = e / h;
+    T s = T(0);
+    for (int q = 0; q < h; ++q) s += Wt[q][r] * Acc[c][q];
+    W.a[(size_t)(j * NB + c) * W.ld + r0 + r] = -s;
+  }
+}
+
+template <class T, int NB>
+void trinv_batched(const MatDesc<T>* d_L, const MatDesc<T>* d_W, int nmat, int nmax,
+                   cudaStream_t st) {
+  if (nmat == 0 || nmax == 0) return;
+  const int nt = ceil_div(nmax, NB);
+  k_trinv_diag<T, NB><<<dim3(nt, nmat), 128, 0, st>>>(d_L, d_W);
+  for (int i = 1; i < nt; ++i) k_trinv_row<T, NB><<<dim3(i, nmat), 256, 0, st>>>(d_L, d_W, i);
+  SDPX_LAUNCH_CHECK();
+}
+template void trinv_batched<double, 32>(const MatDesc<double>*, const MatDesc<double>*, int, int,
+                                        cudaStream_t);
+
+// Inverses of the NB×NB diagonal tiles of a lower factor (for blocked TRSV).
+template <class T, int NB>
+__global__ void k_diag_tile_inverse(const T* L, long long ld, int n, T* Dinv) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  T(*Lt)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(raw);
+  T(*Wt)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(raw + sizeof(T) * NB * (NB + 1));
+  const int s = blockIdx.x, s0 = s * NB;
+  const int w = min(NB, n - s0);
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    int r = e % NB, c = e / NB;
+    Lt[c][r] = (r < w && c < w) ? L[(size_t)(s0 + c) * ld + s0 + r] : T(r == c ? 1 : 0);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < NB; c += blockDim.x) {
+    Wt[c][c] = T(1) / Lt[c][c];
+    for (int r = c + 1; r < NB; ++r) {
+      T acc = T(0);
+      for (int p = c; p < r; ++p) acc += Lt[p][r] * Wt[c][p];
+      Wt[c][r] = -acc / Lt[r][r];
+    }
+    for (int r = 0; r < c; ++r) Wt[c][r] = T(0);
+  }
+  __syncthreads();
+  T* out = Dinv + (size_t)s * NB * NB;
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) out[e] = Wt[e / NB][e % NB];
+}
+
+// Forward step s of L y = r:  y_s = Dinv_s r_s ;  r[rows below] -= L[rows, s] y_s.
+// CTA 0 writes y_s; CTAs ≥ 1 each update ROWS rows below block s.  r and y are
+// distinct buffers so no CTA reads a value written in the same launch.
+template <class T, int NB, int ROWS>
+__global__ void k_trsv_fwd_step(const T* L, long long ld, int n, const T* Dinv, int s, T* r, T* y) {
+  __shared__ T ys[NB];
+  const int s0 = s * NB, w = min(NB, n - s0);
+  const T* Di = Dinv + (size_t)s * NB * NB;
+  for (int t = threadIdx.x; t < NB; t += blockDim.x) {
+    T acc = T(0);
+    if (t < w)
+      for (int p = 0; p < w; ++p) acc += Di[t + p * NB] * r[s0 + p];
+    ys[t] = acc;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0) {
+    for (int t = threadIdx.x; t < w; t += blockDim.x) y[s0 + t] = ys[t];
+    return;
+  }
+  const int base = s0 + w + (blockIdx.x - 1) * ROWS;
+  for (int row = base + threadIdx.x; row < min(n, base + ROWS); row += blockDim.x) {
+    T acc = T(0);
+    for (int p = 0; p < w; ++p) acc += L[(size_t)(s0 + p) * ld + row] * ys[p];
+    r[row] -= acc;
+  }
+}
+
+// Backward step s of Lᵀ x = y: x_s = Dinv_sᵀ y_s ; y[rows above] -= L[s-block, rows]ᵀ x_s.
+template <class T, int NB, int ROWS>
+__global__ void k_trsv_bwd_step(const T* L, long long ld, int n, const T* Dinv, int s, T* yv, T* x) {
+  __shared__ T xs[NB];
+  const int s0 = s * NB, w = min(NB, n - s0);
+  const T* Di = Dinv + (size_t)s * NB * NB;
+  for (int t = threadIdx.x; t < NB; t += blockDim.x) {
+    T acc = T(0);
+    if (t < w)
+      for (int p = 0; p < w; ++p) acc += Di[p + t * NB] * yv[s0 + p];
+    xs[t] = acc;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0) {
+    for (int t = threadIdx.x; t < w; t += blockDim.x) x[s0 + t] = xs[t];
+    return;
+  }
+  const int base = (blockIdx.x - 1) * ROWS;
+  const int end = min(s0, base + ROWS);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int row = base + warp; row < end; row += nw) {
+    T acc = T(0);
+    for (int p = lane; p < w; p += 32) acc += L[(size_t)row * ld + s0 + p] * xs[p];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) yv[row] -= acc;
+  }
+}
+
+template <class T, int NB>
+void factor_diag_inverses(const T* L, long long ld, int n, T* Dinv, cudaStream_t st) {
+  const size_t smem = 2 * sizeof(T) * NB * (NB + 1);
+  ensure_smem(k_diag_tile_inverse<T, NB>, smem);
+  k_diag_tile_inverse<T, NB><<<ceil_div(n, NB), 64, smem, st>>>(L, ld, n, Dinv);
+  SDPX_LAUNCH_CHECK();
+}
+
+template <class T, int NB>
+void cholesky_solve(const T* L, long long ld, int n, const T* Dinv, T* rhs, T* work,
+                    cudaStream_t st) {
+  // rhs ← (L Lᵀ)^{-1} rhs.  `work` (n) receives the intermediate y.
+  constexpr int ROWS = 256;
+  const int nt = ceil_div(n, NB);
+  for (int s = 0; s < nt; ++s) {
+    int below = n - std::min(n, (s + 1) * NB);
+    int grid = 1 + ceil_div(below, ROWS);
+    k_trsv_fwd_step<T, NB, ROWS><<<grid, 256, 0, st>>>(L, ld, n, Dinv, s, rhs, work);
+  }
+  for (int s = nt - 1; s >= 0; --s) {
+    int above = s * NB;
+    int grid = 1 + ceil_div(above, ROWS);
+    k_trsv_bwd_step<T, NB, ROWS><<<grid, 256, 0, st>>>(L, ld, n, Dinv, s, work, rhs);
+  }
+  SDPX_LAUNCH_CHECK();
+}
+
+template void factor_diag_inverses<double, 64>(const double*, long long, int, double*, cudaStream_t);
+template void cholesky_solve<double, 64>(const double*, long long, int, const double*, double*,
+                                         double*, cudaStream_t);
+template void factor_diag_inverses<float, 64>(const float*, long long, int, float*, cudaStream_t);
+template void cholesky_solve<float, 64>(const float*, long long, int, const float*, float*, float*,
+                                        cudaStream_t);
+
+}  // namespace sdpx

@@ -1,0 +1,38 @@
+// Batched Cholesky / triangular kernels (chol.cu).
+#pragma once
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace sdpx {
+
+template <class T>
+struct MatDesc {
+  T* a;     // column-major n×n, leading dimension ld
+  int n;
+  int ld;
+};
+
+// Lower Cholesky in place of every matrix in d_mats (device array of nmat
+// descriptors, largest order nmax).  info[b] = 0 on success, else the 1-based
+// index of the first non-positive pivot.  dmin/dmax receive min/max |L_ii|.
+// diag_store: nmat·NB·NB scratch.  The strict upper triangle is zeroed.
+template <class T, int NB>
+void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* dmin, T* dmax,
+                   T* diag_store, cudaStream_t st);
+
+// W_b = L_b^{-1} for lower-triangular L_b (W zero-initialised by the caller).
+template <class T, int NB>
+void trinv_batched(const MatDesc<T>* d_L, const MatDesc<T>* d_W, int nmat, int nmax,
+                   cudaStream_t st);
+
+// Inverses of the NB×NB diagonal tiles of a lower factor L (n×n): Dinv[s] (NB×NB, col-major).
+template <class T, int NB>
+void factor_diag_inverses(const T* L, long long ld, int n, T* Dinv, cudaStream_t st);
+
+// rhs ← (L Lᵀ)^{-1} rhs by blocked forward/backward substitution (work: n).
+template <class T, int NB>
+void cholesky_solve(const T* L, long long ld, int n, const T* Dinv, T* rhs, T* work,
+                    cudaStream_t st);
+
+}  // namespace sdpx

@@ -1,0 +1,636 @@
+// Memory-bound kernels over the stacked constraint matrix 𝒜 (K×m, column i =
+// vec(A_i) of every block, 1×1 blocks gathered at the end) and over stacked
+// block vectors (length K, same row offsets as 𝒜).
+#include "vec_kernels.h"
+
+namespace sdpx {
+
+// ---------------------------------------------------------------- gemv ----
+// out[row] = Σ_i A[row + i·K]·x[i], column range split into `chunks` partial
+// sums (written to part[chunk·K + row]) then reduced in fixed order.
+__global__ void k_gemv_n_part(const double* __restrict__ A, long long K, int m,
+                              const double* __restrict__ x, int chunks, double* __restrict__ part) {
+  long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int ch = blockIdx.y;
+  if (row >= K) return;
+  int per = (m + chunks - 1) / chunks;
+  int i0 = ch * per, i1 = min(m, i0 + per);
+  const double* p = A + row;
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  int i = i0;
+  for (; i + 3 < i1; i += 4) {
+    s0 += p[(long long)i * K] * x[i];
+    s1 += p[(long long)(i + 1) * K] * x[i + 1];
+    s2 += p[(long long)(i + 2) * K] * x[i + 2];
+    s3 += p[(long long)(i + 3) * K] * x[i + 3];
+  }
+  for (; i < i1; ++i) s0 += p[(long long)i * K] * x[i];
+  part[(long long)ch * K + row] = (s0 + s1) + (s2 + s3);
+}
+
+__global__ void k_gemv_n_reduce(const double* __restrict__ part, long long K, int chunks,
+                                double* __restrict__ out) {
+  long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (row >= K) return;
+  double s = 0;
+  for (int c = 0; c < chunks; ++c) s += part[(long long)c * K + row];
+  out[row] = s;
+}
+
+void gemv_n(const double* A, long long K, int m, const double* x, double* out, double* part,
+            int chunks, cudaStream_t st) {
+  if (K == 0) return;
+  dim3 g(ceil_div(K, 256), chunks);
+  k_gemv_n_part<<<g, 256, 0, st>>>(A, K, m, x, chunks, part);
+  k_gemv_n_reduce<<<ceil_div(K, 256), 256, 0, st>>>(part, K, chunks, out);
+  SDPX_LAUNCH_CHECK();
+}
+
+// out[i] = alpha·(A[:,i] · z) + beta·base[i]   (one CTA per column).
+__global__ void k_gemv_t(const double* __restrict__ A, long long K, int m,
+                         const double* __restrict__ z, double alpha, const double* __restrict__ base,
+                         double beta, double* __restrict__ out) {
+  __shared__ double red[32];
+  int i = blockIdx.x;
+  const double* col = A + (long long)i * K;
+  double s0 = 0, s1 = 0;
+  long long r = threadIdx.x;
+  for (; r + blockDim.x < K; r += 2 * blockDim.x) {
+    s0 += col[r] * z[r];
+    s1 += col[r + blockDim.x] * z[r + blockDim.x];
+  }
+  if (r < K) s0 += col[r] * z[r];
+  double s = block_sum(s0 + s1, red);
+  if (threadIdx.x == 0) out[i] = alpha * s + (base ? beta * base[i] : 0.0);
+}
+
+void gemv_t(const double* A, long long K, int m, const double* z, double alpha, const double* base,
+            double beta, double* out, cudaStream_t st) {
+  if (m == 0) return;
+  k_gemv_t<<<m, 512, 0, st>>>(A, K, m, z, alpha, base, beta, out);
+  SDPX_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------- elementwise -------
+__global__ void k_axpbypcz(long long n, double a, const double* x, double b, const double* y,
+                           double c, const double* z, double* out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    double v = a * x[e];
+    if (y) v += b * y[e];
+    if (z) v += c * z[e];
+    out[e] = v;
+  }
+}
+void axpbypcz(long long n, double a, const double* x, double b, const double* y, double c,
+              const double* z, double* out, cudaStream_t st) {
+  if (n == 0) return;
+  int g = std::min(4096, ceil_div(n, 256));
+  k_axpbypcz<<<g, 256, 0, st>>>(n, a, x, b, y, c, z, out);
+  SDPX_LAUNCH_CHECK();
+}
+
+// x ← x + t·d   (the reference's trial_combine!: dest[i] = X[i] + t*dX[i])
+__global__ void k_combine(long long n, double* x, double t, const double* d) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    x[e] = x[e] + t * d[e];
+}
+void combine(long long n, double* x, double t, const double* d, cudaStream_t st) {
+  if (n == 0) return;
+  k_combine<<<std::min(4096, ceil_div(n, 256)), 256, 0, st>>>(n, x, t, d);
+  SDPX_LAUNCH_CHECK();
+}
+
+__global__ void k_scale(long long n, double* x, double f) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    x[e] *= f;
+}
+void scale(long long n, double* x, double f, cudaStream_t st) {
+  if (n == 0) return;
+  k_scale<<<std::min(4096, ceil_div(n, 256)), 256, 0, st>>>(n, x, f);
+  SDPX_LAUNCH_CHECK();
+}
+
+// ----------------------------------------------------------- reductions ----
+// out[slot] = max(out[slot], max|x|) ; finiteness folded in (NaN → +inf).
+__global__ void k_absmax(long long n, const double* x, double* out) {
+  __shared__ double red[32];
+  double v = 0.0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    double a = fabs(x[e]);
+    if (!(a == a)) a = 1.0 / 0.0;
+    v = fmax(v, a);
+  }
+  v = block_max(v, red);
+  if (threadIdx.x == 0) atomic_max_nonneg(out, v);
+}
+void absmax(long long n, const double* x, double* out, cudaStream_t st) {
+  if (n == 0) return;
+  k_absmax<<<std::min(1024, ceil_div(n, 256)), 256, 0, st>>>(n, x, out);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Segmented dot products: for segment s (rows [off[s], off[s]+len[s])),
+// out[s] = Σ (x + tx·dx)(y + ty·dy) (dx/dy may be null).  One CTA per segment
+// chunk; partials combined with a fixed-order second pass.
+__global__ void k_seg_dot(const long long* off, const long long* len, int nseg, const double* x,
+                          const double* dx, double tx, const double* y, const double* dy, double ty,
+                          int parts, double* part) {
+  __shared__ double red[32];
+  int s = blockIdx.y, p = blockIdx.x;
+  if (s >= nseg) return;
+  long long o = off[s], n = len[s];
+  long long per = (n + parts - 1) / parts;
+  long long b = p * per, e = min(n, b + per);
+  double acc = 0.0;
+  for (long long i = b + threadIdx.x; i < e; i += blockDim.x) {
+    double a = x[o + i];
+    if (dx) a += tx * dx[o + i];
+    double c = y[o + i];
+    if (dy) c += ty * dy[o + i];
+    acc += a * c;
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) part[(long long)s * parts + p] = acc;
+}
+__global__ void k_seg_reduce(int nseg, int parts, const double* part, double* out) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  double acc = 0.0;
+  for (int p = 0; p < parts; ++p) acc += part[(long long)s * parts + p];
+  out[s] = acc;
+}
+void seg_dot(const long long* d_off, const long long* d_len, int nseg, int parts, const double* x,
+             const double* dx, double tx, const double* y, const double* dy, double ty, double* part,
+             double* out, cudaStream_t st) {
+  if (nseg == 0) return;
+  k_seg_dot<<<dim3(parts, nseg), 256, 0, st>>>(d_off, d_len, nseg, x, dx, tx, y, dy, ty, parts, part);
+  k_seg_reduce<<<ceil_div(nseg, 128), 128, 0, st>>>(nseg, parts, part, out);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Diagonal entries of every dense block plus the 1×1 entries: out[t] = trace.
+__global__ void k_block_trace(const long long* off, const int* kk, int nseg, const double* M,
+                              double* out) {
+  __shared__ double red[32];
+  int s = blockIdx.x;
+  int k = kk[s];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) acc += M[off[s] + i + (long long)i * k];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) out[s] = acc;
+}
+void block_trace(const long long* d_off, const int* d_k, int nseg, const double* M, double* out,
+                 cudaStream_t st) {
+  if (nseg == 0) return;
+  k_block_trace<<<nseg, 128, 0, st>>>(d_off, d_k, nseg, M, out);
+  SDPX_LAUNCH_CHECK();
+}
+
+// M_block += shift_s · I for each segment s (dense blocks) — shifts[s] per block.
+__global__ void k_add_diag(const long long* off, const int* kk, int nseg, double* M,
+                           const double* shifts, double uniform) {
+  int s = blockIdx.y;
+  if (s >= nseg) return;
+  int k = kk[s];
+  double sh = shifts ? shifts[s] : uniform;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x)
+    M[off[s] + i + (long long)i * k] += sh;
+}
+void add_diag(const long long* d_off, const int* d_k, int nseg, int kmax, double* M,
+              const double* d_shifts, double uniform, cudaStream_t st) {
+  if (nseg == 0 || kmax == 0) return;
+  k_add_diag<<<dim3(ceil_div(kmax, 256), nseg), 256, 0, st>>>(d_off, d_k, nseg, M, d_shifts, uniform);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Symmetrize every dense block in place: M ← (M + Mᵀ)/2.
+__global__ void k_symmetrize(const long long* off, const int* kk, int nseg, double* M) {
+  int s = blockIdx.y;
+  if (s >= nseg) return;
+  int k = kk[s];
+  long long tot = (long long)k * k;
+  double* B = M + off[s];
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(e % k), j = (int)(e / k);
+    if (i < j) {
+      double avg = (B[i + (long long)j * k] + B[j + (long long)i * k]) / 2;
+      B[i + (long long)j * k] = avg;
+      B[j + (long long)i * k] = avg;
+    }
+  }
+}
+void symmetrize(const long long* d_off, const int* d_k, int nseg, int kmax, double* M,
+                cudaStream_t st) {
+  if (nseg == 0) return;
+  int g = std::max(1, std::min(512, ceil_div((long long)kmax * kmax, 256)));
+  k_symmetrize<<<dim3(g, nseg), 256, 0, st>>>(d_off, d_k, nseg, M);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Gershgorin lower bound, finiteness and max |lower entry| per dense block
+// (lower triangle authoritative, src/cold_start.jl:152-201).  One CTA per row;
+// out_bound[row-major offset] collects per-row candidates, reduced on the host side.
+__global__ void k_gershgorin_rows(const long long* off, const int* kk, int nseg, const double* M,
+                                  double* cand, double* scale, int* nonfinite,
+                                  const long long* cand_off) {
+  __shared__ double red[32];
+  int s = blockIdx.y, i = blockIdx.x;
+  if (s >= nseg) return;
+  int k = kk[s];
+  if (i >= k) return;
+  const double* B = M + off[s];
+  double rad = 0.0, mx = 0.0;
+  int bad = 0;
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    double v = (j <= i) ? B[i + (long long)j * k] : B[j + (long long)i * k];
+    if (!isfinite(v)) bad = 1;
+    if (j != i) rad += fabs(v);
+    if (j <= i) mx = fmax(mx, fabs(v));
+  }
+  rad = block_sum(rad, red);
+  double m2 = block_max(mx, red);
+  int anybad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) {
+    cand[cand_off[s] + i] = B[i + (long long)i * k] - rad;
+    atomic_max_nonneg(scale + s, m2);
+    if (anybad) nonfinite[s] = 1;
+  }
+}
+void gershgorin(const long long* d_off, const int* d_k, int nseg, int kmax, const double* M,
+                double* d_cand, const long long* d_cand_off, double* d_scale, int* d_nonfinite,
+                cudaStream_t st) {
+  if (nseg == 0) return;
+  k_gershgorin_rows<<<dim3(kmax, nseg), 128, 0, st>>>(d_off, d_k, nseg, M, d_cand, d_scale,
+                                                      d_nonfinite, d_cand_off);
+  SDPX_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------ 1×1 block group ----
+// Entries j = 0..nd-1 at stacked offset od.  mu_user / user index per entry.
+__global__ void k_diag_residual_R(int nd, long long od, const double* X, const double* Y,
+                                  const double* mu_user, const int* user, int use_affine, double* R) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nd) return;
+  long long e = od + j;
+  double v = -(X[e] * Y[e]);
+  if (!use_affine) v += mu_user[user[j]];
+  R[e] = v;
+}
+void diag_residual_R(int nd, long long od, const double* X, const double* Y, const double* mu_user,
+                     const int* user, int use_affine, double* R, cudaStream_t st) {
+  if (nd == 0) return;
+  k_diag_residual_R<<<ceil_div(nd, 256), 256, 0, st>>>(nd, od, X, Y, mu_user, user, use_affine, R);
+  SDPX_LAUNCH_CHECK();
+}
+
+// LX = sqrt(X), MY = sqrt(Y); fail flag if a value is not positive.
+__global__ void k_diag_factor(int nd, long long od, const double* X, const double* Y, double* LX,
+                              double* MY, int* fail) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nd) return;
+  long long e = od + j;
+  double x = X[e], y = Y[e];
+  if (!(x > 0) || !(y > 0)) atomicExch(fail, 1);
+  LX[e] = sqrt(x);
+  MY[e] = sqrt(y);
+}
+void diag_factor(int nd, long long od, const double* X, const double* Y, double* LX, double* MY,
+                 int* fail, cudaStream_t st) {
+  if (nd == 0) return;
+  k_diag_factor<<<ceil_div(nd, 256), 256, 0, st>>>(nd, od, X, Y, LX, MY, fail);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Z = (P·Y − R) / l / l  with l = LX  (kcholsolve 1×1: M / l11 / l11)
+__global__ void k_diag_rhs_Z(int nd, long long od, const double* P, const double* Y, const double* R,
+                             const double* LX, double* Z) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nd) return;
+  long long e = od + j;
+  double l = LX[e];
+  Z[e] = (P[e] * Y[e] - R[e]) / l / l;
+}
+void diag_rhs_Z(int nd, long long od, const double* P, const double* Y, const double* R,
+                const double* LX, double* Z, cudaStream_t st) {
+  if (nd == 0) return;
+  k_diag_rhs_Z<<<ceil_div(nd, 256), 256, 0, st>>>(nd, od, P, Y, R, LX, Z);
+  SDPX_LAUNCH_CHECK();
+}
+
+// dY = (R − dX·Y) / l / l
+__global__ void k_diag_dY(int nd, long long od, const double* R, const double* dX, const double* Y,
+                          const double* LX, double* dY) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nd) return;
+  long long e = od + j;
+  double l = LX[e];
+  dY[e] = (R[e] - dX[e] * Y[e]) / l / l;
+}
+void diag_dY(int nd, long long od, const double* R, const double* dX, const double* Y,
+             const double* LX, double* dY, cudaStream_t st) {
+  if (nd == 0) return;
+  k_diag_dY<<<ceil_div(nd, 256), 256, 0, st>>>(nd, od, R, dX, Y, LX, dY);
+  SDPX_LAUNCH_CHECK();
+}
+
+// R = target − X·Y − dX·dY  (Mehrotra, 1×1) with per-entry target
+__global__ void k_diag_corrector_R(int nd, long long od, const double* X, const double* Y,
+                                   const double* dX, const double* dY, const double* target_user,
+                                   const int* user, double* R) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nd) return;
+  long long e = od + j;
+  double v = -(X[e] * Y[e]);
+  v = v - dX[e] * dY[e];
+  R[e] = v + target_user[user[j]];
+}
+void diag_corrector_R(int nd, long long od, const double* X, const double* Y, const double* dX,
+                      const double* dY, const double* target_user, const int* user, double* R,
+                      cudaStream_t st) {
+  if (nd == 0) return;
+  k_diag_corrector_R<<<ceil_div(nd, 256), 256, 0, st>>>(nd, od, X, Y, dX, dY, target_user, user, R);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Schur panel rows of the 1×1 group:  P̂[od+j, i] = (A[od+j, i] / LX_j) · MY_j
+__global__ void k_diag_panel(long long K, int m, int nd, long long od, const double* A,
+                             const double* LX, const double* MY, double* Pc) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int i = blockIdx.y;
+  if (j >= nd || i >= m) return;
+  long long e = od + j;
+  long long a = e + (long long)i * K;
+  Pc[a] = (A[a] / LX[e]) * MY[e];
+}
+void diag_panel(long long K, int m, int nd, long long od, const double* A, const double* LX,
+                const double* MY, double* Pc, cudaStream_t st) {
+  if (nd == 0) return;
+  k_diag_panel<<<dim3(ceil_div(nd, 256), m), 256, 0, st>>>(K, m, nd, od, A, LX, MY, Pc);
+  SDPX_LAUNCH_CHECK();
+}
+
+// ----------------------------------------------------- line-search trials ---
+// 1×1 group: for candidate steps t[c] (c < nc), ok[c] &= (X + t dX > 0 && finite...).
+// Returns for each candidate whether all entries pass.  margin>0 additionally
+// requires a finite square root (SDPX's 1×1 `trial_has_cholesky_margin!`).
+__global__ void k_diag_trial(int nd, long long od, const double* X, const double* dX,
+                             const double* t, int nc, int margin, int* fail) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = blockIdx.y;
+  if (j >= nd || c >= nc) return;
+  long long e = od + j;
+  double v = X[e] + t[c] * dX[e];
+  bool ok = v > 0;
+  if (ok && margin) ok = isfinite(sqrt(v));
+  if (!ok) atomicExch(fail + c, 1);
+}
+void diag_trial(int nd, long long od, const double* X, const double* dX, const double* d_t, int nc,
+                int margin, int* d_fail, cudaStream_t st) {
+  if (nd == 0 || nc == 0) return;
+  k_diag_trial<<<dim3(ceil_div(nd, 256), nc), 256, 0, st>>>(nd, od, X, dX, d_t, nc, margin, d_fail);
+  SDPX_LAUNCH_CHECK();
+}
+
+// 1×1 fraction-to-boundary: min_j (d < 0 ? min(1, −X/d) : 1)  (src/kernels/generic.jl:355-357).
+// Single CTA so the minimum is exact.
+__global__ void k_diag_ftb(int nd, long long od, const double* X, const double* dX, double* out) {
+  __shared__ double red[32];
+  double v = 1.0;
+  for (int j = threadIdx.x; j < nd; j += blockDim.x) {
+    double d = dX[od + j];
+    double b = (d < 0) ? fmin(1.0, -X[od + j] / d) : 1.0;
+    v = fmin(v, b);
+  }
+  double m = -block_max(-v, red);
+  if (threadIdx.x == 0) *out = m;
+}
+void diag_ftb(int nd, long long od, const double* X, const double* dX, double* d_out,
+              cudaStream_t st) {
+  if (nd == 0) return;
+  k_diag_ftb<<<1, 1024, 0, st>>>(nd, od, X, dX, d_out);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Trial matrices  T[c] = X_block + t[c]·dX_block  for every dense block and candidate.
+__global__ void k_make_trials(const long long* off, const int* kk, const long long* trial_off,
+                              int nseg, const double* X, const double* dX, const double* t, int nc,
+                              double* trials) {
+  int s = blockIdx.y, c = blockIdx.z;
+  if (s >= nseg || c >= nc) return;
+  int k = kk[s];
+  long long tot = (long long)k * k;
+  double tc = t[c];
+  double* out = trials + trial_off[s] + (long long)c * tot;
+  const double* x = X + off[s];
+  const double* d = dX + off[s];
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x)
+    out[e] = x[e] + tc * d[e];
+}
+void make_trials(const long long* d_off, const int* d_k, const long long* d_trial_off, int nseg,
+                 int kmax, const double* X, const double* dX, const double* d_t, int nc,
+                 double* trials, cudaStream_t st) {
+  if (nseg == 0 || nc == 0) return;
+  int g = std::max(1, std::min(256, ceil_div((long long)kmax * kmax, 256)));
+  k_make_trials<<<dim3(g, nseg, nc), 256, 0, st>>>(d_off, d_k, d_trial_off, nseg, X, dX, d_t, nc,
+                                                  trials);
+  SDPX_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------ permutation --
+__global__ void k_gather(long long n, const long long* map, const double* src, double* dst) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    dst[e] = src[map[e]];
+}
+__global__ void k_scatter(long long n, const long long* map, const double* src, double* dst) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    dst[map[e]] = src[e];
+}
+void gather(long long n, const long long* map, const double* src, double* dst, cudaStream_t st) {
+  if (n == 0) return;
+  k_gather<<<std::min(4096, ceil_div(n, 256)), 256, 0, st>>>(n, map, src, dst);
+  SDPX_LAUNCH_CHECK();
+}
+void scatter(long long n, const long long* map, const double* src, double* dst, cudaStream_t st) {
+  if (n == 0) return;
+  k_scatter<<<std::min(4096, ceil_div(n, 256)), 256, 0, st>>>(n, map, src, dst);
+  SDPX_LAUNCH_CHECK();
+}
+
+// --------------------------------------------------------- dense S helpers --
+// Full symmetric S from its lower triangle (upper ← lower).
+__global__ void k_mirror_lower(int m, double* S) {
+  long long tot = (long long)m * m;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(e % m), j = (int)(e / m);
+    if (i < j) S[e] = S[j + (long long)i * m];
+  }
+}
+void mirror_lower(int m, double* S, cudaStream_t st) {
+  k_mirror_lower<<<std::min(4096, ceil_div((long long)m * m, 256)), 256, 0, st>>>(m, S);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Sf = S (lower) with diagonal += reg·max(|S_ii|, 1)   (src/kkt.jl:1419-1445)
+__global__ void k_copy_reg(int m, const double* S, double* Sf, double reg) {
+  long long tot = (long long)m * m;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(e % m), j = (int)(e / m);
+    double v = (i >= j) ? S[e] : 0.0;
+    if (i == j && reg != 0.0) v += reg * fmax(fabs(S[e]), 1.0);
+    Sf[e] = v;
+  }
+}
+void copy_reg(int m, const double* S, double* Sf, double reg, cudaStream_t st) {
+  k_copy_reg<<<std::min(4096, ceil_div((long long)m * m, 256)), 256, 0, st>>>(m, S, Sf, reg);
+  SDPX_LAUNCH_CHECK();
+}
+
+// y = alpha·S·x + beta·b for symmetric S stored full (column i = row i).
+__global__ void k_symv_full(int m, const double* S, const double* x, double alpha, const double* b,
+                            double beta, double* y) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= m) return;
+  const double* col = S + (long long)warp * m;
+  double acc = 0.0;
+  for (int j = lane; j < m; j += 32) acc += col[j] * x[j];
+  acc = warp_sum(acc);
+  if (lane == 0) y[warp] = alpha * acc + (b ? beta * b[warp] : 0.0);
+}
+void symv_full(int m, const double* S, const double* x, double alpha, const double* b, double beta,
+               double* y, cudaStream_t st) {
+  k_symv_full<<<ceil_div((long long)m * 32, 256), 256, 0, st>>>(m, S, x, alpha, b, beta, y);
+  SDPX_LAUNCH_CHECK();
+}
+
+// --------------------------------------------------------- equilibration ---
+// Row maxima of |A_i| (dense block: rows r of every A_i^(l)) → rn[r] via atomics.
+__global__ void k_ruiz_rowmax_dense(const double* A, long long K, int m, long long off, int k,
+                                    double* rn) {
+  extern __shared__ double loc[];
+  for (int r = threadIdx.x; r < k; r += blockDim.x) loc[r] = 0.0;
+  __syncthreads();
+  int i = blockIdx.x;
+  const double* col = A + (long long)i * K + off;
+  long long tot = (long long)k * k;
+  for (long long e = threadIdx.x; e < tot; e += blockDim.x) {
+    double v = fabs(col[e]);
+    if (!(v == v)) v = 1.0 / 0.0;
+    int r = (int)(e % k);
+    // shared-memory max via integer atomics on the non-negative bit pattern
+    atomicMax(reinterpret_cast<unsigned long long*>(loc + r), __double_as_longlong(v));
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < k; r += blockDim.x) atomic_max_nonneg(rn + r, loc[r]);
+}
+void ruiz_rowmax_dense(const double* A, long long K, int m, long long off, int k, double* rn,
+                       cudaStream_t st) {
+  size_t sm = sizeof(double) * k;
+  ensure_smem(k_ruiz_rowmax_dense, sm);
+  k_ruiz_rowmax_dense<<<m, 256, sm, st>>>(A, K, m, off, k, rn);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Row maxima for the 1×1 group: rn[j] = max(rn[j], max_i |A[od+j, i]|).
+__global__ void k_ruiz_rowmax_diag(const double* A, long long K, int m, long long od, int nd,
+                                   double* rn) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nd) return;
+  double v = rn[j];
+  for (int i = 0; i < m; ++i) {
+    double a = fabs(A[od + j + (long long)i * K]);
+    if (!(a == a)) a = 1.0 / 0.0;
+    v = fmax(v, a);
+  }
+  rn[j] = v;
+}
+void ruiz_rowmax_diag(const double* A, long long K, int m, long long od, int nd, double* rn,
+                      cudaStream_t st) {
+  if (nd == 0) return;
+  k_ruiz_rowmax_diag<<<ceil_div(nd, 128), 128, 0, st>>>(A, K, m, od, nd, rn);
+  SDPX_LAUNCH_CHECK();
+}
+
+// A_i[r,c] *= e_r e_c over the rows [off, off+k²) of every column.
+__global__ void k_ruiz_congruence_dense(double* A, long long K, int m, long long off, int k,
+                                        const double* e) {
+  long long tot = (long long)k * k * m;
+  long long kk = (long long)k * k;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    long long i = t / kk, q = t % kk;
+    int r = (int)(q % k), c = (int)(q / k);
+    A[i * K + off + q] *= e[r] * e[c];
+  }
+}
+void ruiz_congruence_dense(double* A, long long K, int m, long long off, int k, const double* e,
+                           cudaStream_t st) {
+  long long tot = (long long)k * k * m;
+  k_ruiz_congruence_dense<<<std::min(8192, ceil_div(tot, 256)), 256, 0, st>>>(A, K, m, off, k, e);
+  SDPX_LAUNCH_CHECK();
+}
+
+// 1×1 group: A[od+j, i] *= e_j²
+__global__ void k_ruiz_congruence_diag(double* A, long long K, int m, long long od, int nd,
+                                       const double* e) {
+  long long tot = (long long)nd * m;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int j = (int)(t % nd);
+    long long i = t / nd;
+    A[od + j + i * K] *= e[j] * e[j];
+  }
+}
+void ruiz_congruence_diag(double* A, long long K, int m, long long od, int nd, const double* e,
+                          cudaStream_t st) {
+  if (nd == 0) return;
+  long long tot = (long long)nd * m;
+  k_ruiz_congruence_diag<<<std::min(8192, ceil_div(tot, 256)), 256, 0, st>>>(A, K, m, od, nd, e);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Column max |A[:, i]| → out[i]
+__global__ void k_colmax(const double* A, long long K, double* out) {
+  __shared__ double red[32];
+  int i = blockIdx.x;
+  const double* col = A + (long long)i * K;
+  double v = 0.0;
+  for (long long r = threadIdx.x; r < K; r += blockDim.x) {
+    double a = fabs(col[r]);
+    if (!(a == a)) a = 1.0 / 0.0;
+    v = fmax(v, a);
+  }
+  v = block_max(v, red);
+  if (threadIdx.x == 0) out[i] = v;
+}
+void colmax(const double* A, long long K, int m, double* out, cudaStream_t st) {
+  if (m == 0) return;
+  k_colmax<<<m, 512, 0, st>>>(A, K, out);
+  SDPX_LAUNCH_CHECK();
+}
+
+// A[:, i] /= s_i
+__global__ void k_scale_cols(double* A, long long K, int m, const double* s) {
+  long long tot = K * m;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    long long i = t / K;
+    A[t] /= s[i];
+  }
+}
+void scale_cols(double* A, long long K, int m, const double* s, cudaStream_t st) {
+  long long tot = K * m;
+  k_scale_cols<<<std::min(8192, ceil_div(tot, 256)), 256, 0, st>>>(A, K, m, s);
+  SDPX_LAUNCH_CHECK();
+}
+
+}  // namespace sdpx

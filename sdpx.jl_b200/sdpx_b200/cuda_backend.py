@@ -1,0 +1,434 @@
+"""ctypes binding of libsdpx_b200.so and the device backend of the host driver.
+
+Every method maps onto one C-ABI entry point of include/sdpx_b200.h; matrices
+stay resident on the GPU and only scalars (or the final iterate) come back.
+The library is loaded from this package's directory; if it is missing, or no
+CUDA device is usable, construction raises — there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from typing import List, Optional
+
+import numpy as np
+
+from .problem import Equilibration, SDPProblem
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libsdpx_b200.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class _Problem(C.Structure):
+    _fields_ = [("m", C.c_int64), ("nblocks", C.c_int32), ("block_order", C.POINTER(C.c_int32)),
+                ("Av", C.POINTER(_dp)), ("C", C.POINTER(_dp)), ("c", _dp)]
+
+
+# name -> argtypes (restype is int unless noted)
+_SIGS = {
+    "sdpx_b200_abi_version": [],
+    "sdpx_b200_create": [C.POINTER(_Problem), C.c_int, C.POINTER(C.c_void_p)],
+    "sdpx_b200_set_precision": [C.c_void_p, C.c_int],
+    "sdpx_b200_equilibrate": [C.c_void_p, _dp, _dp, _dp, C.POINTER(C.c_int32)],
+    "sdpx_b200_data_norms": [C.c_void_p, _dp, _dp],
+    "sdpx_b200_set_iterate": [C.c_void_p, _dp, _dp, _dp],
+    "sdpx_b200_get_iterate": [C.c_void_p, _dp, _dp, _dp],
+    "sdpx_b200_get_direction": [C.c_void_p, _dp, _dp, _dp],
+    "sdpx_b200_get_rhs": [C.c_void_p, _dp],
+    "sdpx_b200_fixed_start": [C.c_void_p, C.c_double, C.c_double],
+    "sdpx_b200_residuals": [C.c_void_p, _dp, C.c_int, C.c_int, _dp, _dp, _ip],
+    "sdpx_b200_block_primal_residual": [C.c_void_p, _dp],
+    "sdpx_b200_block_margins": [C.c_void_p, _dp, _dp],
+    "sdpx_b200_schur_build": [C.c_void_p, C.c_int],
+    "sdpx_b200_get_schur": [C.c_void_p, _dp],
+    "sdpx_b200_factorize": [C.c_void_p, _ip, _ip, _dp],
+    "sdpx_b200_rhs_predictor": [C.c_void_p],
+    "sdpx_b200_rhs_corrector_mehrotra": [C.c_void_p, C.c_double, C.c_double, C.c_int],
+    "sdpx_b200_rhs_corrector_fixed": [C.c_void_p, C.c_double, _dp],
+    "sdpx_b200_set_rhs": [C.c_void_p, C.c_int],
+    "sdpx_b200_solve": [C.c_void_p],
+    "sdpx_b200_direction_residual": [C.c_void_p, _dp, _dp],
+    "sdpx_b200_refine": [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, _ip, _dp],
+    "sdpx_b200_direction_blocks": [C.c_void_p],
+    "sdpx_b200_affine_diagnostics": [C.c_void_p, C.c_int, _dp, _dp],
+    "sdpx_b200_line_search": [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
+                              C.c_double, C.c_double, _dp, _dp],
+    "sdpx_b200_update": [C.c_void_p, C.c_double, C.c_double, _dp, _ip, _dp],
+    "sdpx_b200_accepted_residuals": [C.c_void_p, C.c_double, C.c_double, C.c_double, _dp, _dp],
+    "sdpx_b200_objectives": [C.c_void_p, _dp, _dp],
+    "sdpx_b200_solution_residuals": [C.c_void_p, _dp, _dp],
+    "sdpx_b200_keep_direction": [C.c_void_p],
+    "sdpx_b200_cold_start_iterate": [C.c_void_p],
+    "sdpx_b200_psd_shift": [C.c_void_p, C.c_int, _ip],
+    "sdpx_b200_add_identity": [C.c_void_p, C.c_int, C.c_double],
+    "sdpx_b200_block_dots": [C.c_void_p, _dp, _dp, _dp],
+    "sdpx_b200_scale_iterate": [C.c_void_p, C.c_int, C.c_double],
+    "sdpx_b200_store_best": [C.c_void_p],
+    "sdpx_b200_restore_best": [C.c_void_p],
+    "sdpx_b200_rebuild_slack": [C.c_void_p, _dp, _dp],
+    "sdpx_b200_original_residuals": [C.c_void_p, _dp, _dp, _dp, _dp, _dp],
+    "sdpx_b200_phase_times": [C.c_void_p, _dp, C.c_int],
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libsdpx_b200.so (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{path} not found: build it with `python sdpx.jl_b200/build.py`")
+    lib = C.CDLL(path)
+    for name, args in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    lib.sdpx_b200_destroy.argtypes = [C.c_void_p]
+    lib.sdpx_b200_destroy.restype = None
+    lib.sdpx_b200_last_error.argtypes = [C.c_void_p]
+    lib.sdpx_b200_last_error.restype = C.c_char_p
+    lib.sdpx_b200_create_error.argtypes = []
+    lib.sdpx_b200_create_error.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class SDPXB200Error(RuntimeError):
+    pass
+
+
+class CudaBackend:
+    """Device backend of `sdpx_b200.driver` (all numerics on the B200)."""
+
+    PHASES = ("residual_and_block_factor", "schur_assembly", "kkt_factorization",
+              "solve_and_refinement", "rhs_and_directions", "step_length", "update")
+
+    def __init__(self, prob: SDPProblem, *, precision: str = "fp64", device: int = 0,
+                 condition_limit: float = 1e8):
+        self.lib = load_library()
+        self.prob0 = prob
+        self.k = list(prob.k)
+        self.m = prob.m
+        self.n = prob.n
+        self.L = len(self.k)
+        self.Ku = int(sum(kl * kl for kl in self.k))
+        self.offsets = np.cumsum([0] + [kl * kl for kl in self.k])
+        self._keep = []
+        order = (C.c_int32 * self.L)(*self.k)
+        av_ptrs = (_dp * self.L)()
+        c_ptrs = (_dp * self.L)()
+        for l in range(self.L):
+            # Av[l] is (m, k*k) C-ordered == k²×m column-major (column i = vec A_i)
+            a = np.ascontiguousarray(prob.Av[l], dtype=np.float64)
+            cm = np.ascontiguousarray(np.asfortranarray(prob.C[l]).reshape(-1, order="F"))
+            self._keep += [a, cm]
+            av_ptrs[l] = _p(a)
+            c_ptrs[l] = _p(cm)
+        cvec = np.ascontiguousarray(prob.c, dtype=np.float64)
+        self._keep.append(cvec)
+        pr = _Problem(self.m, self.L, order, av_ptrs, c_ptrs, _p(cvec))
+        h = C.c_void_p()
+        rc = self.lib.sdpx_b200_create(C.byref(pr), device, C.byref(h))
+        if rc != 0:
+            raise SDPXB200Error("sdpx_b200_create failed: " +
+                                self.lib.sdpx_b200_create_error().decode())
+        self._keep = []     # host data has been copied to the device
+        self.h = h
+        self.requested = precision
+        self.condition_limit = condition_limit
+        self.mode = "fp64"
+        self._history: List[str] = []
+        self._switch_reason: Optional[str] = None
+        self._in_loop = False
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sdpx_b200_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc: int, what: str):
+        if rc != 0:
+            msg = self.lib.sdpx_b200_last_error(self.h)
+            raise SDPXB200Error(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    def _call(self, name, *args):
+        self._ck(getattr(self.lib, name)(self.h, *args), name)
+
+    # -- stacked <-> per-block --------------------------------------------
+    def _split(self, flat):
+        return [flat[self.offsets[l]:self.offsets[l + 1]].reshape(self.k[l], self.k[l], order="F").copy()
+                for l in range(self.L)]
+
+    def _join(self, blocks):
+        return np.ascontiguousarray(np.concatenate(
+            [np.asarray(b, dtype=np.float64).reshape(-1, order="F") for b in blocks]))
+
+    # -- precision control --------------------------------------------------
+    def _set_mode(self, mode: str):
+        self._call("sdpx_b200_set_precision", 1 if mode == "mixed" else 0)
+        self.mode = mode
+
+    def precision_label(self):
+        return self.mode
+
+    def precision_history(self):
+        return list(self._history)
+
+    def begin_iteration(self, info):
+        """Called at every loop top.  Enters mixed mode after the cold start and
+        leaves it for good when the condition estimate of S passes the limit or
+        the stagnation rate says the mixed directions stopped paying."""
+        if not self._in_loop:
+            self._in_loop = True
+            if self.requested == "mixed":
+                self._set_mode("mixed")
+        self._history.append(self.mode)
+
+    def fallback_to_fp64(self, reason: str) -> bool:
+        if self.mode == "mixed":
+            self._switch_reason = reason
+            self._set_mode("fp64")
+            return True
+        return False
+
+    # -- problem level -------------------------------------------------------
+    def equilibrate(self) -> Equilibration:
+        E = np.zeros(sum(self.k))
+        s = np.zeros(self.m)
+        osc = C.c_double()
+        passes = (C.c_int32 * self.L)()
+        self._call("sdpx_b200_equilibrate", _p(E), _p(s), C.byref(osc), passes)
+        Es, o = [], 0
+        for kl in self.k:
+            Es.append(E[o:o + kl].copy())
+            o += kl
+        return Equilibration(Es, s, osc.value, list(passes))
+
+    def data_norms(self):
+        a, b = C.c_double(), C.c_double()
+        self._call("sdpx_b200_data_norms", C.byref(a), C.byref(b))
+        return a.value, b.value, 0.0
+
+    def fixed_start(self, omega_p, omega_d):
+        self._call("sdpx_b200_fixed_start", omega_p, omega_d)
+
+    def set_iterate(self, x, X, Y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        Xs, Ys = self._join(X), self._join(Y)
+        self._call("sdpx_b200_set_iterate", _p(x), _p(Xs), _p(Ys))
+
+    def get_iterate(self):
+        x = np.zeros(self.m)
+        Xs = np.zeros(self.Ku)
+        Ys = np.zeros(self.Ku)
+        self._call("sdpx_b200_get_iterate", _p(x), _p(Xs), _p(Ys))
+        return x, self._split(Xs), np.zeros(0), self._split(Ys)
+
+    def get_direction(self):
+        dx = np.zeros(self.m)
+        dXs = np.zeros(self.Ku)
+        dYs = np.zeros(self.Ku)
+        self._call("sdpx_b200_get_direction", _p(dx), _p(dXs), _p(dYs))
+        return dx, self._split(dXs), self._split(dYs)
+
+    def get_rhs(self):
+        r = np.zeros(self.m)
+        self._call("sdpx_b200_get_rhs", _p(r))
+        return r
+
+    def schur_matrix(self):
+        S = np.zeros((self.m, self.m))
+        self._call("sdpx_b200_get_schur", _p(S))
+        return S
+
+    # -- hot path --------------------------------------------------------------
+    def compute_residuals(self, mu, use_affine, factor):
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        p, d, ok = C.c_double(), C.c_double(), C.c_int()
+        self._call("sdpx_b200_residuals", _p(mu), int(bool(use_affine)), int(bool(factor)),
+                   C.byref(p), C.byref(d), C.byref(ok))
+        return p.value, d.value, bool(ok.value)
+
+    def block_primal_residual(self):
+        v = C.c_double()
+        self._call("sdpx_b200_block_primal_residual", C.byref(v))
+        return v.value
+
+    def schur_build(self, identity=False):
+        self._call("sdpx_b200_schur_build", int(bool(identity)))
+
+    def factorize(self):
+        ok, att, q = C.c_int(), C.c_int(), C.c_double()
+        self._call("sdpx_b200_factorize", C.byref(ok), C.byref(att), C.byref(q))
+        return dict(ok=bool(ok.value), reg_attempts=att.value, quality=q.value)
+
+    def predictor_rhs(self):
+        self._call("sdpx_b200_rhs_predictor")
+
+    def solve_direction(self):
+        self._call("sdpx_b200_solve")
+
+    def direction_blocks(self):
+        self._call("sdpx_b200_direction_blocks")
+
+    def direction_residual(self):
+        a, b = C.c_double(), C.c_double()
+        self._call("sdpx_b200_direction_residual", C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def refine(self, policy, tol, cap, fixed_steps):
+        steps, res = C.c_int(), C.c_double()
+        self._call("sdpx_b200_refine", 0 if policy == "fixed" else 1, float(tol), int(cap),
+                   int(fixed_steps), C.byref(steps), C.byref(res))
+        return steps.value, res.value
+
+    def affine_diagnostics(self, adaptive):
+        out = np.zeros(4)
+        blk = np.zeros(self.L)
+        self._call("sdpx_b200_affine_diagnostics", int(bool(adaptive)), _p(out), _p(blk))
+        compl, aff, tX, tY = out
+        uniform = bool(adaptive)
+        ref = None
+        if adaptive:
+            for l, kl in enumerate(self.k):
+                val = float(blk[l])
+                if not math.isfinite(val):
+                    uniform = False
+                elif ref is None:
+                    ref = (val, kl)
+                elif not ((kl == ref[1] and val == ref[0]) or
+                          (kl != ref[1] and val / kl == ref[0] / ref[1])):
+                    uniform = False
+        den = float(max(sum(self.k), 1))
+        mu = compl / den
+        mu_aff = max(0.0, aff / den)
+        if adaptive:
+            quality = min(max(mu_aff / mu, 0.0), 2.0) if mu > 0 else 1.0
+        else:
+            quality = min(max(aff / compl, 0.0), 2.0) if compl > 0 else 1.0
+        return dict(complementarity=float(compl), affine_complementarity=float(aff), mu=mu,
+                    mu_aff=mu_aff, quality=quality, tX=float(tX), tY=float(tY), uniform=uniform)
+
+    def block_margins(self):
+        a, b = C.c_double(), C.c_double()
+        self._call("sdpx_b200_block_margins", C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def mehrotra_corrector_rhs(self, sigma, mu, block_local):
+        self._call("sdpx_b200_rhs_corrector_mehrotra", float(sigma), float(mu), int(bool(block_local)))
+
+    def fixed_corrector_rhs(self, beta, mu):
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        self._call("sdpx_b200_rhs_corrector_fixed", float(beta), _p(mu))
+
+    def line_search(self, rule, fp, fd, gamma, min_step, margin):
+        tX, tY = C.c_double(), C.c_double()
+        self._call("sdpx_b200_line_search", 1 if rule == "fraction_to_boundary" else 0,
+                   float(fp), float(fd), float(gamma), float(min_step), float(margin),
+                   C.byref(tX), C.byref(tY))
+        return tX.value, tY.value
+
+    def update(self, tX, tY):
+        c, f = C.c_double(), C.c_int()
+        dots = np.zeros(self.L)
+        self._call("sdpx_b200_update", float(tX), float(tY), C.byref(c), C.byref(f), _p(dots))
+        return c.value, bool(f.value), [float(v) for v in dots]
+
+    def accepted_trial_residuals(self, bpr, tX, tY):
+        a, b = C.c_double(), C.c_double()
+        self._call("sdpx_b200_accepted_residuals", float(bpr), float(tX), float(tY),
+                   C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def objectives(self):
+        a, b = C.c_double(), C.c_double()
+        self._call("sdpx_b200_objectives", C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def solution_residuals(self):
+        a, b = C.c_double(), C.c_double()
+        self._call("sdpx_b200_solution_residuals", C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    # -- cold start ------------------------------------------------------------
+    def set_rhs(self, which):
+        self._call("sdpx_b200_set_rhs", 0 if which == "cold_primal" else 1)
+
+    def keep_direction_as(self, name):
+        self._call("sdpx_b200_keep_direction")
+
+    def cold_start_iterate(self):
+        self._call("sdpx_b200_cold_start_iterate")
+
+    def psd_shift(self, which):
+        ok = C.c_int()
+        self._call("sdpx_b200_psd_shift", 0 if which == "X" else 1, C.byref(ok))
+        return bool(ok.value)
+
+    def add_identity(self, which, shift):
+        self._call("sdpx_b200_add_identity", 0 if which == "X" else 1, float(shift))
+
+    def block_dots(self):
+        d, tx, ty = np.zeros(self.L), np.zeros(self.L), np.zeros(self.L)
+        self._call("sdpx_b200_block_dots", _p(d), _p(tx), _p(ty))
+        return [float(v) for v in d], [float(v) for v in tx], [float(v) for v in ty]
+
+    def scale_iterate(self, which, factor):
+        self._call("sdpx_b200_scale_iterate", 0 if which == "X" else 1, float(factor))
+
+    def store_best(self):
+        self._call("sdpx_b200_store_best")
+
+    def restore_best(self):
+        self._call("sdpx_b200_restore_best")
+
+    # -- original coordinates ---------------------------------------------------
+    def restore_original(self):
+        pass
+
+    def original_c(self):
+        return self.prob0.c
+
+    def original_C(self):
+        return self.prob0.C
+
+    def rebuild_slack(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        Xs = np.zeros(self.Ku)
+        self._call("sdpx_b200_rebuild_slack", _p(x), _p(Xs))
+        return self._split(Xs)
+
+    def original_residuals(self, x, X, y, Y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        Xs, Ys = self._join(X), self._join(Y)
+        a, b = C.c_double(), C.c_double()
+        self._call("sdpx_b200_original_residuals", _p(x), _p(Xs), _p(Ys), C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def phase_times(self, reset=False):
+        ms = np.zeros(7)
+        self._call("sdpx_b200_phase_times", _p(ms), int(bool(reset)))
+        return dict(zip(self.PHASES, ms.tolist()))

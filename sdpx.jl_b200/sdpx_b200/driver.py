@@ -178,31 +178,6 @@ def newton_step(be, opts: SolverOptions, ctl: AdaptiveIPMController, mu: List[fl
 #   KKT cold start (src/solver/interior_point.jl:699-1287, src/cold_start.jl)
 # --------------------------------------------------------------------------
 
-def _psd_shift(be, which: str, block: int):
-    """`_cold_start_psd_shift!` (src/cold_start.jl:287-308) on one block."""
-    finite, scale, margin = be.psd_stats(which, block)
-    if not finite:
-        return False, 0.0, margin
-    safety = SQRT_EPS * max(1.0, scale)
-    slack = 8.0 * EPS * max(1.0, scale)
-    if margin > safety:
-        return True, 0.0, margin
-    applied = 0.0
-    for _ in range(16):
-        shift = safety - margin + slack
-        if not math.isfinite(shift):
-            return False, applied, margin
-        be.add_identity(which, block, shift)
-        applied += shift
-        finite, scale, margin = be.psd_stats(which, block)
-        if not finite:
-            return False, applied, margin
-        safety = SQRT_EPS * max(1.0, scale)
-        if margin > safety:
-            return True, applied, margin
-    return False, applied, margin
-
-
 def kkt_cold_start(be, opts: SolverOptions, scale_p: float, scale_d: float):
     k = be.k
     L = len(k)
@@ -235,11 +210,11 @@ def kkt_cold_start(be, opts: SolverOptions, scale_p: float, scale_d: float):
     np_, nd_ = p_res / scale_p, d_res / scale_d
     if not (math.isfinite(np_) and math.isfinite(nd_) and np_ <= threshold and nd_ <= threshold):
         return dict(ok=False, reason="kkt_cold_start_residuals")
-    for l in range(L):
-        ok1, _, _ = _psd_shift(be, "X", l)
-        ok2, _, _ = _psd_shift(be, "Y", l)
-        if not (ok1 and ok2):
-            return dict(ok=False, reason="cold_start_psd_shift")
+    # Per-block certified identity shifts (`_cold_start_psd_shift!`,
+    # src/cold_start.jl:287-308).  Blocks are independent, so shifting every X
+    # block and then every Y block equals the reference's interleaved loop.
+    if not (be.psd_shift("X") and be.psd_shift("Y")):
+        return dict(ok=False, reason="cold_start_psd_shift")
     dots, trX, trY = be.block_dots()
     primal_mass, dual_mass = sum(trX), sum(trY)
     # _cold_start_identity_mass_shifts (src/cold_start.jl:338-360)
@@ -249,30 +224,26 @@ def kkt_cold_start(be, opts: SolverOptions, scale_p: float, scale_d: float):
     p_floor = max(0.0, (target - primal_mass) / target)
     d_floor = max(0.0, (target - dual_mass) / target)
     if p_floor > 0:
-        for l in range(L):
-            be.add_identity("X", l, p_floor)
+        be.add_identity("X", p_floor)
     if d_floor > 0:
-        for l in range(L):
-            be.add_identity("Y", l, d_floor)
+        be.add_identity("Y", d_floor)
     dots, trX, trY = be.block_dots()
     kappa = sum(dots)
     pm, dm = sum(trX), sum(trY)
     # _cold_start_centering_shifts (src/cold_start.jl:407-430)
-    ok = math.isfinite(kappa) and kappa > 0 and math.isfinite(pm) and pm > 0 and math.isfinite(dm) and dm > 0
+    ok = (math.isfinite(kappa) and kappa > 0 and math.isfinite(pm) and pm > 0
+          and math.isfinite(dm) and dm > 0)
     if not ok:
         return dict(ok=False, reason="cold_start_centering_shifts")
     p_center = kappa / (2.0 * dm)
     d_center = kappa / (2.0 * pm)
     if p_center > 0:
-        for l in range(L):
-            be.add_identity("X", l, p_center)
+        be.add_identity("X", p_center)
     if d_center > 0:
-        for l in range(L):
-            be.add_identity("Y", l, d_center)
+        be.add_identity("Y", d_center)
     # The margin pass re-runs the certified shift (src/solver/interior_point.jl:1166-1169).
-    for l in range(L):
-        _psd_shift(be, "X", l)
-        _psd_shift(be, "Y", l)
+    be.psd_shift("X")
+    be.psd_shift("Y")
     dots, _, _ = be.block_dots()
     mu = [opts.beta * dots[l] / k[l] for l in range(L)]
     return dict(ok=True, mu=mu)
