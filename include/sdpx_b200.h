@@ -158,6 +158,14 @@ int sdpx_b200_rebuild_slack(sdpx_b200_handle* h, const double* x, double* X);
 int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const double* X,
                                  const double* Y, double* p_res, double* d_res);
 
+/* Restore the data as uploaded (undo sdpx_b200_equilibrate) and reset the
+ * iterate to x = 0, X = Y = I, so one handle can run repeated solves. */
+int sdpx_b200_reset(sdpx_b200_handle* h);
+/* The handle's CUDA stream (cudaStream_t), for callers that time or order work on it. */
+int sdpx_b200_get_stream(sdpx_b200_handle* h, void** stream);
+/* Number of kernels this library has launched in this process. */
+int sdpx_b200_launch_count(uint64_t* count);
+
 /* Cumulative device time per phase (ms) since the last reset:
  * [0] residual+block factor, [1] Schur assembly, [2] KKT factor,
  * [3] solves+refinement, [4] directions+RHS, [5] step length, [6] update. */

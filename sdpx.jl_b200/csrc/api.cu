@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -24,6 +25,10 @@
 #include "vec_kernels.h"
 
 namespace sdpx {
+
+static std::atomic<unsigned long long> g_launches{0};
+void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(); }
 
 static std::mutex g_attr_mu;
 static std::set<std::pair<const void*, int>> g_attr_done;
@@ -561,6 +566,19 @@ struct Handle {
     if (objscale) *objscale = osc;
     if (passes)
       for (int l = 0; l < L; ++l) passes[l] = used[l];
+  }
+
+  void reset() {
+    if (have_original) {
+      d2d(A.p, A0.p, sizeof(double) * K * m);
+      d2d(Cst.p, C0st.p, sizeof(double) * K);
+      d2d(c.p, c0.p, sizeof(double) * m);
+    }
+    precision = SDPX_B200_FP64;
+    fixed_start(1.0, 1.0);
+    sync();
+    harvest_phases();
+    for (double& v : phase_ms) v = 0.0;
   }
 
   void data_norms(double* maxC, double* cnorm) {
@@ -1703,6 +1721,13 @@ int sdpx_b200_rebuild_slack(sdpx_b200_handle* h, const double* x, double* X) {
 int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const double* X,
                                  const double* Y, double* p, double* d) {
   GUARD(h, h->h.original_residuals(x, X, Y, p, d));
+}
+int sdpx_b200_reset(sdpx_b200_handle* h) { GUARD(h, h->h.reset()); }
+int sdpx_b200_get_stream(sdpx_b200_handle* h, void** stream) { GUARD(h, *stream = (void*)h->h.st); }
+int sdpx_b200_launch_count(uint64_t* count) {
+  if (!count) return -1;
+  *count = sdpx::launch_count();
+  return 0;
 }
 int sdpx_b200_phase_times(sdpx_b200_handle* h, double* ms7, int reset) {
   GUARD(h, {

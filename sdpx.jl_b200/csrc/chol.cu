@@ -215,7 +215,7 @@ void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* d
   }
   dim3 gz(std::max(1, std::min(1024, ceil_div((long long)nmax * nmax, 256))), nmat);
   k_zero_upper<T><<<gz, 256, 0, st>>>(d_mats);
-  SDPX_LAUNCH_CHECK();
+  SDPX_LAUNCH_CHECK_N(2 + 2 * nt);
 }
 
 template void potrf_batched<double, 32>(const MatDesc<double>*, int, int, int*, double*, double*,
@@ -310,7 +310,7 @@ void trinv_batched(const MatDesc<T>* d_L, const MatDesc<T>* d_W, int nmat, int n
   const int nt = ceil_div(nmax, NB);
   k_trinv_diag<T, NB><<<dim3(nt, nmat), 128, 0, st>>>(d_L, d_W);
   for (int i = 1; i < nt; ++i) k_trinv_row<T, NB><<<dim3(i, nmat), 256, 0, st>>>(d_L, d_W, i);
-  SDPX_LAUNCH_CHECK();
+  SDPX_LAUNCH_CHECK_N(nt);
 }
 template void trinv_batched<double, 32>(const MatDesc<double>*, const MatDesc<double>*, int, int,
                                         cudaStream_t);
@@ -421,7 +421,7 @@ void cholesky_solve(const T* L, long long ld, int n, const T* Dinv, T* rhs, T* w
     int grid = 1 + ceil_div(above, ROWS);
     k_trsv_bwd_step<T, NB, ROWS><<<grid, 256, 0, st>>>(L, ld, n, Dinv, s, work, rhs);
   }
-  SDPX_LAUNCH_CHECK();
+  SDPX_LAUNCH_CHECK_N(2 * nt);
 }
 
 template void factor_diag_inverses<double, 64>(const double*, long long, int, double*, cudaStream_t);

@@ -22,7 +22,15 @@ struct CudaError : std::runtime_error {
                               " (" + __FILE__ + ":" + std::to_string(__LINE__) + ")"); \
   } while (0)
 
-#define SDPX_LAUNCH_CHECK() SDPX_CUDA(cudaGetLastError())
+// Every launch site ends with SDPX_LAUNCH_CHECK(n): check the launch and add n
+// to the process-wide kernel-launch counter (sdpx_b200_launch_count).
+void note_launches(unsigned long long n);
+#define SDPX_LAUNCH_CHECK_N(n)        \
+  do {                                \
+    SDPX_CUDA(cudaGetLastError());    \
+    ::sdpx::note_launches(n);         \
+  } while (0)
+#define SDPX_LAUNCH_CHECK() SDPX_LAUNCH_CHECK_N(1)
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 

@@ -43,7 +43,7 @@ void gemv_n(const double* A, long long K, int m, const double* x, double* out, d
   dim3 g(ceil_div(K, 256), chunks);
   k_gemv_n_part<<<g, 256, 0, st>>>(A, K, m, x, chunks, part);
   k_gemv_n_reduce<<<ceil_div(K, 256), 256, 0, st>>>(part, K, chunks, out);
-  SDPX_LAUNCH_CHECK();
+  SDPX_LAUNCH_CHECK_N(2);
 }
 
 // out[i] = alpha·(A[:,i] · z) + beta·base[i]   (one CTA per column).
@@ -169,7 +169,7 @@ void seg_dot(const long long* d_off, const long long* d_len, int nseg, int parts
   if (nseg == 0) return;
   k_seg_dot<<<dim3(parts, nseg), 256, 0, st>>>(d_off, d_len, nseg, x, dx, tx, y, dy, ty, parts, part);
   k_seg_reduce<<<ceil_div(nseg, 128), 128, 0, st>>>(nseg, parts, part, out);
-  SDPX_LAUNCH_CHECK();
+  SDPX_LAUNCH_CHECK_N(2);
 }
 
 // Diagonal entries of every dense block plus the 1×1 entries: out[t] = trace.

@@ -72,6 +72,9 @@ _SIGS = {
     "sdpx_b200_rebuild_slack": [C.c_void_p, _dp, _dp],
     "sdpx_b200_original_residuals": [C.c_void_p, _dp, _dp, _dp, _dp, _dp],
     "sdpx_b200_phase_times": [C.c_void_p, _dp, C.c_int],
+    "sdpx_b200_reset": [C.c_void_p],
+    "sdpx_b200_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
+    "sdpx_b200_launch_count": [C.POINTER(C.c_uint64)],
 }
 
 _lib = None
@@ -427,6 +430,27 @@ class CudaBackend:
         a, b = C.c_double(), C.c_double()
         self._call("sdpx_b200_original_residuals", _p(x), _p(Xs), _p(Ys), C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def reset(self):
+        """Restore the uploaded data and the start iterate for another solve."""
+        self._call("sdpx_b200_reset")
+        self.mode = "fp64"
+        self._in_loop = False
+        self._history = []
+        self._switch_reason = None
+
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        self._call("sdpx_b200_get_stream", C.byref(p))
+        return int(p.value or 0)
+
+    @staticmethod
+    def launch_count() -> int:
+        lib = load_library()
+        v = C.c_uint64()
+        if lib.sdpx_b200_launch_count(C.byref(v)) != 0:
+            raise SDPXB200Error("launch_count failed")
+        return int(v.value)
 
     def phase_times(self, reset=False):
         ms = np.zeros(7)

@@ -74,3 +74,23 @@ def test_sdpa_generator_is_strictly_feasible():
     r = oracle_solve(prob)
     assert r.status.value == "Optimal"
     assert r.relative_gap <= 1e-8
+
+
+def test_dense_gate_iteration_count_is_summation_order_sensitive():
+    """The sdp_dense gate's iteration count moves with the summation order of
+    ⟨A_i, Y⟩ alone (the objective does not): the evidence behind the GPU gate
+    test's ±2 slack on this one problem."""
+    import numpy as np
+    from sdpx_b200.driver import solve_with_backend
+    from oracle.sdpx_oracle import OracleBackend
+
+    class Pairwise(OracleBackend):
+        def _accumulate(self, l, M):
+            return np.einsum("ij,j->i", self.Av[l], M.reshape(-1))
+
+    opts = SolverOptions().with_tolerance(1e-8)
+    a = solve_with_backend(OracleBackend(G.gate_dense()), opts)
+    b = solve_with_backend(Pairwise(G.gate_dense()), opts)
+    assert a.status.value == b.status.value == "Optimal"
+    assert abs(a.pObj - b.pObj) / abs(a.pObj) < 1e-10
+    assert abs(a.iterations - b.iterations) <= 2
