@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark: time to a 1e-8 relative duality gap on the m = 2000 dense SDP.
+
+Workload (one "step" = one complete solve to 1e-8 relative gap): the seeded
+SDPA-form instance with PSD blocks of order 400 and 200 plus 500 nonnegatives
+and m = 2000 constraints (generator `sdpx_b200.generators.sdpa_dense`), solved
+with SDPX's dense interior-point algorithm on the B200 in the mixed-precision
+mode; the plain FP64 device path is timed on the same instance for the
+mixed-vs-FP64 ratio.  Inputs (3.2 GB of constraint data) are larger than L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 (torchrun, one rank per GPU) every rank solves its own independent
+instance (replicas; no collective on the data path); `value` is the maximum
+time over ranks.  `--impl reference` times the CPU restatement of the
+reference algorithm (SDPX.jl itself is Julia and cannot run here) on rank 0.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "sdpx.jl_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+WORKLOADS = {
+    "sdp_m2000": dict(m=2000, blocks=[400, 200], lp=500,
+                      label="dense SDP (SDPA form), PSD blocks 400+200 + 500 LP, m=2000"),
+    "sdp_m100": dict(m=100, blocks=[50], lp=0,
+                     label="dense SDP (SDPA form), one PSD block n=50, m=100"),
+}
+TOL = 1e-8
+# Iterations of the CPU restatement on sdp_m2000 (seed 0) to 1e-8, used to
+# scale the reference arm's one-iteration samples to a time-to-gap.
+CPU_ITERATIONS_M2000 = None
+
+
+def schur_flops(m, blocks, lp):
+    """Algorithmic Schur flops per build: Σ_l [2 k³ m + m(m+1) k²] (TRSM + TRMM + lower SYRK)."""
+    f = sum(2.0 * k ** 3 * m + m * (m + 1.0) * k ** 2 for k in blocks)
+    f += lp * (2.0 * m + m * (m + 1.0))
+    return f
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, physical_index):
+        self.idx = physical_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8 and parts[0] == str(self.idx):
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = self.rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        reasons = []
+        for col, name in ((4, "hw_slowdown"), (5, "hw_thermal_slowdown"),
+                          (6, "sw_thermal_slowdown"), (7, "sw_power_cap")):
+            if any(r[col].lower() == "active" for r in rows):
+                reasons.append(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": num(rows[0][2]), "reasons": reasons, "samples": len(rows)}
+
+
+def physical_gpu_index(local):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local < len(ids) and ids[local].isdigit():
+            return int(ids[local])
+    return local
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def cpu_sample(prob, blocks, lp, gpu_iterations):
+    """Time one Newton iteration of the CPU restatement on the same instance."""
+    import numpy as np
+    from oracle.sdpx_oracle import OracleBackend
+    from sdpx_b200.controller import AdaptiveIPMController, SolverOptions
+    from sdpx_b200.driver import kkt_cold_start, newton_step
+
+    opts = SolverOptions().with_tolerance(TOL)
+    be = OracleBackend(prob)
+    max_C, c_norm, _ = be.data_norms()
+    cs = kkt_cold_start(be, opts, 1.0 + max_C, 1.0 + c_norm)
+    ctl = AdaptiveIPMController(opts)
+    t0 = time.perf_counter()
+    res = newton_step(be, opts, ctl, cs["mu"], iteration=1, relative_gap=1.0,
+                      primal_scale=1.0 + max_C, dual_scale=1.0 + c_norm)
+    p = res["params"]
+    be.line_search("backtrack", p.primal_fraction_to_boundary, p.dual_fraction_to_boundary,
+                   p.backtracking_factor, p.minimum_step, math.sqrt(2.220446049250313e-16))
+    t_iter = time.perf_counter() - t0
+    return t_iter
+
+
+def cpu_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        n = [i.get("num_threads") for i in threadpool_info() if i.get("user_api") == "blas"]
+        if n and n[0]:
+            return int(n[0])
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def run_reference(args, world, rank):
+    """CPU restatement of the reference algorithm (the oracle port)."""
+    if rank != 0:
+        return
+    from sdpx_b200 import generators as G
+    wl = WORKLOADS[args.workload]
+    prob = G.sdpa_dense(m=wl["m"], blocks=wl["blocks"], lp=wl["lp"], seed=0)
+    iters = CPU_ITERATIONS_M2000 if args.workload == "sdp_m2000" else None
+    samples = []
+    for s in range(args.warmup + args.steps):
+        t_it = cpu_sample(prob, wl["blocks"], wl["lp"], None)
+        if s >= args.warmup:
+            samples.append(t_it)
+    t_it = statistics.median(samples)
+    n_it = iters or 20
+    value = t_it * n_it
+    line = {
+        "impl": "reference", "metric": "time-to-1e-8 relative duality gap, m=2000 dense SDP",
+        "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_it * 1000.0, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["label"], "m": wl["m"], "blocks": wl["blocks"], "lp": wl["lp"],
+                   "tolerance": TOL},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": cpu_threads(), "kind": "port",
+                         "sample": (f"one Newton iteration (residuals, Schur, Cholesky, predictor/"
+                                    f"corrector, refinement, line search) of the same instance per "
+                                    f"step, median of {args.steps}, × {n_it} iterations")},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    from sdpx_b200 import SolverOptions, generators as G
+    from sdpx_b200.cuda_backend import CudaBackend
+    from sdpx_b200.driver import solve_with_backend
+    from sdpx_b200.problem import SDPProblem
+
+    wl = WORKLOADS[args.workload]
+    prob = G.sdpa_dense(m=wl["m"], blocks=wl["blocks"], lp=wl["lp"], seed=rank)
+    F = schur_flops(wl["m"], wl["blocks"], wl["lp"])
+    opts_mixed = SolverOptions(precision="mixed").with_tolerance(TOL)
+    opts_fp64 = SolverOptions(precision="fp64").with_tolerance(TOL)
+
+    be = CudaBackend(prob, precision="mixed", device=local)
+    stream = torch.cuda.ExternalStream(be.stream_handle())
+
+    def one_solve(mode):
+        be.reset()
+        be.requested = mode
+        return solve_with_backend(be, opts_mixed if mode == "mixed" else opts_fp64)
+
+    for _ in range(args.warmup):
+        one_solve("mixed")
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(physical_gpu_index(local))
+    clocks.start()
+    launches0 = CudaBackend.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    results = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        results.append(one_solve("mixed"))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clock_info = clocks.stop()
+    launches = CudaBackend.launch_count() - launches0
+    ms_total = ev0.elapsed_time(ev1)
+    ms_per_step = max_over_ranks(ms_total / args.steps, world)
+    last = results[-1]
+    phases_mixed = be.phase_times(reset=True)
+
+    # Dominant kernel: the Schur assembly, timed live at the final iterate.
+    def time_schur(reps=5):
+        es = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        be.compute_residuals([0.0] * prob.L, True, True)
+        be.schur_build()
+        es[0].record(stream)
+        for _ in range(reps):
+            be.schur_build()
+        es[1].record(stream)
+        torch.cuda.synchronize()
+        return es[0].elapsed_time(es[1]) / reps
+
+    be._set_mode("mixed")
+    schur_ms_mixed = time_schur()
+    be._set_mode("fp64")
+    schur_ms_fp64 = time_schur()
+
+    # Plain FP64 device path on the same instance.
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r64 = one_solve("fp64")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fp64_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
+
+    # FP64 reference throughput of this GPU (cuBLAS DGEMM), context for the FP64 roofline.
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record()
+    for _ in range(3):
+        torch.matmul(a, b)
+    g1.record()
+    torch.cuda.synchronize()
+    dgemm_tflops = 3 * 2 * 8192 ** 3 / (g0.elapsed_time(g1) / 1000.0) / 1e12
+    del a, b
+
+    # End-to-end through the public API from pinned host buffers.
+    pinned = []
+    Avp = []
+    for A in prob.Av:
+        t = torch.empty(A.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = A
+        pinned.append(t)
+        Avp.append(t.numpy())
+    prob_p = SDPProblem(prob.c, prob.k, Avp, prob.C, prob.B, prob.b)
+    h2d = sum(A.nbytes for A in prob.Av) + sum(C.nbytes for C in prob.C) + prob.c.nbytes
+    d2h = prob.c.nbytes + 2 * sum(C.nbytes for C in prob.C)
+    be.close()
+    torch.cuda.synchronize()
+    e2e_times = []
+    for _ in range(max(1, min(args.steps, 2))):
+        t0 = time.perf_counter()
+        with CudaBackend(prob_p, precision="mixed", device=local) as be2:
+            r_e2e = solve_with_backend(be2, opts_mixed)
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(statistics.median(e2e_times), world)
+
+    peaks, peak_kind = measured_peaks()
+    achieved = F / (schur_ms_mixed / 1000.0) / 1e12
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            t_it = cpu_sample(prob, wl["blocks"], wl["lp"], last.iterations)
+            cpu = {"value": t_it * last.iterations, "unit": "s", "cores": cpu_threads(),
+                   "kind": "port",
+                   "sample": (f"one Newton iteration of the same instance on the CPU "
+                              f"restatement (NumPy/OpenBLAS), {t_it:.2f} s, × the "
+                              f"{last.iterations} iterations of the GPU solve")}
+        line = {
+            "metric": "time-to-1e-8 relative duality gap (mixed-precision B200 path), m=2000 dense SDP",
+            "value": ms_per_step / 1000.0, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 in/out; Schur assembly mode per precision_trace, FP32 factor, FP64 refinement",
+            "data": "synthetic",
+            "config": {"workload": wl["label"], "m": wl["m"], "blocks": wl["blocks"],
+                       "lp": wl["lp"], "tolerance": TOL, "seed": "rank",
+                       "l2": "inputs (constraint data 3.2 GB) larger than L2; not flushed",
+                       "parallelism": "replicas (independent instance per GPU)"},
+            "status": last.status.value, "iterations": last.iterations,
+            "objective": last.pObj, "relative_gap": last.relative_gap,
+            "precision_trace": "".join("m" if p == "mixed" else "d" for p in last.precision_trace),
+            "fp64_gpu": {"value": fp64_s, "unit": "s", "iterations": r64.iterations,
+                         "status": r64.status.value, "objective": r64.pObj},
+            "speedup_mixed_vs_fp64": fp64_s / (ms_per_step / 1000.0),
+            "schur": {"flops_per_build": F, "ms_mixed": schur_ms_mixed, "ms_fp64": schur_ms_fp64,
+                      "tflops_mixed": achieved, "tflops_fp64": F / (schur_ms_fp64 / 1000) / 1e12,
+                      "dgemm_tflops_measured": dgemm_tflops},
+            "phase_ms_per_solve": {k: v / args.steps for k, v in phases_mixed.items()},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "Schur assembly (left/right block products + lower SYRK)",
+                         "peak_kind": f"bf16_tflops of {peak_kind} MEASURED_PEAKS.json; "
+                                      f"achieved counts FP64-equivalent algorithmic flops"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "status": r_e2e.status.value},
+            "gpu_launches": launches,
+            "clocks": clock_info,
+        }
+        print(json.dumps(line), flush=True)
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="sdp_m2000")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
