@@ -16,7 +16,7 @@ LIB = HERE / "libsdpx_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
-SOURCES = ["api.cu", "blas_f64.cu", "chol.cu", "vec_kernels.cu", "mixed_f32.cu"]
+SOURCES = ["api.cu", "blas_f64.cu", "chol.cu", "vec_kernels.cu", "mixed_f32.cu", "schur_bf16.cu"]
 
 
 def nvcc():

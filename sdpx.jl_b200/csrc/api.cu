@@ -22,6 +22,7 @@
 #include "blas_f64.h"
 #include "chol.h"
 #include "mixed.h"
+#include "schur_bf16.h"
 #include "vec_kernels.h"
 
 namespace sdpx {
@@ -437,6 +438,7 @@ struct Handle {
 
   // ----------------------------------------------------------- scaling ----
   void equilibrate(double* E_out, double* s_out, double* objscale, int32_t* passes) {
+    if (mixed) mixed->a_planes_valid = false;
     // keep the original data for final slack/residual reconstruction
     if (!have_original) {
       A0.alloc((size_t)K * m);
@@ -569,6 +571,7 @@ struct Handle {
   }
 
   void reset() {
+    if (mixed) mixed->a_planes_valid = false;
     if (have_original) {
       d2d(A.p, A0.p, sizeof(double) * K * m);
       d2d(Cst.p, C0st.p, sizeof(double) * K);
@@ -1502,6 +1505,7 @@ struct Handle {
 
   // ------------------------------------------------------- mixed precision --
   void mixed_init();
+  void mixed_check_err();
   void mixed_schur();
   void schur_split_bf16();
   void mixed_factorize(int* ok, int* attempts, double* quality);

@@ -1,11 +1,28 @@
 // Mixed-precision workspace of the B200 core: FP32 factor of the Schur
 // complement and buffers of the split-BF16 Schur assembly.
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 namespace sdpx {
 
 struct MixedWorkspace {
+  // split-BF16 Schur assembly buffers (allocated on first use)
+  bool planes_ready = false;   // buffers allocated
+  bool a_planes_valid = false; // planes of the current (scaled) constraint data
+  long long Kp = 0;            // padded stacked K of the plane layout
+  std::vector<int> kp;         // padded order per dense block
+  std::vector<long long> po;   // plane offset per dense block
+  long long pog = 0;           // plane offset of the 1×1 group
+  long long Ts = 0;            // per-variable stride of the T planes
+  void* Apl[3] = {nullptr, nullptr, nullptr};
+  void* Ppl[3] = {nullptr, nullptr, nullptr};
+  void* Tpl[3] = {nullptr, nullptr, nullptr};
+  void* Wpl[3] = {nullptr, nullptr, nullptr};
+  void* Lpl[3] = {nullptr, nullptr, nullptr};
+  float* partial = nullptr;
+  int* err = nullptr;
   float* Sf = nullptr;      // m×m FP32 factor
   float* Dinv = nullptr;    // FP32 inverses of the 64×64 diagonal tiles
   float* v32 = nullptr;     // m
@@ -18,8 +35,11 @@ struct MixedWorkspace {
   double cond_estimate = 1.0;
   ~MixedWorkspace() {
     for (void* p : {(void*)Sf, (void*)Dinv, (void*)v32, (void*)w32, (void*)info, (void*)dmin,
-                    (void*)dmax, (void*)diag_store, desc})
+                    (void*)dmax, (void*)diag_store, desc, (void*)partial, (void*)err})
       if (p) cudaFree(p);
+    for (int i = 0; i < 3; ++i)
+      for (void* p : {Apl[i], Ppl[i], Tpl[i], Wpl[i], Lpl[i]})
+        if (p) cudaFree(p);
   }
 };
 

@@ -1,0 +1,61 @@
+// Split-BF16 tcgen05 GEMM engine (schur_bf16.cu).
+#pragma once
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+
+namespace sdpx {
+
+// Row r of an operand/output starts at base + (r / inner)·os + (r % inner)·is elements.
+struct RowMap {
+  long long base;
+  int inner;
+  long long is, os;
+  int extent;
+};
+
+// Three BF16 planes of a K-major operand: element (row, k) of plane p is
+// plane[p][row_off(row) + k], valid for k < kvalid (zero-filled beyond).
+struct PlaneOpnd {
+  const __nv_bfloat16* plane[3];
+  RowMap rows;
+  int kvalid;
+};
+
+// Output planes: element (row, col) at plane[p][row_off(row) + (col / col_inner)·col_os + col % col_inner].
+// col_inner, row offsets and col_extent are multiples of 8 (16-byte stores of 8 columns).
+struct OutMap {
+  __nv_bfloat16* plane[3];
+  RowMap rows;
+  int col_inner;
+  long long col_os;
+  int col_extent;
+};
+
+struct SplitSyrkPlan {
+  int ntri = 0, nchunk = 0, kchunk = 0;
+  size_t partial_floats = 0;
+};
+
+size_t split_gemm_smem_bytes();
+// out = A·Bᵀ (A rows × B rows, contraction over k < Ktot), split into planes.
+// kmode: 0 full K, 1 A lower-triangular (k ≤ row), 2 B lower-triangular (k ≥ col).
+void split_gemm_planes(const PlaneOpnd& A, const PlaneOpnd& B, const OutMap& out, int kmode,
+                       int Ktot, int* err, cudaStream_t st);
+SplitSyrkPlan plan_split_syrk(int m, long long Kp, int sm_count);
+// Lower tiles of S (m×m FP64, column-major) = P̂ᵀP̂ over K = Kp, FP32 chunk tiles summed in FP64.
+void split_syrk(const PlaneOpnd& P, int m, int Kp, const SplitSyrkPlan& plan, float* partial,
+                double* S, int* err, cudaStream_t st);
+
+void split_A_dense(const double* A, long long K, int m, long long off, int k, int kp,
+                   __nv_bfloat16* const* planes, long long Kp, long long o, cudaStream_t st);
+void split_diag_rows(const double* A, long long K, int m, long long od, int nd, const double* LX,
+                     const double* MY, __nv_bfloat16* const* planes, long long Kp, long long o,
+                     cudaStream_t st);
+void split_small(const double* M, int k, int kp, bool row_major, __nv_bfloat16* const* planes,
+                 cudaStream_t st);
+
+}  // namespace sdpx
