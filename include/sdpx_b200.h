@@ -166,6 +166,28 @@ int sdpx_b200_get_stream(sdpx_b200_handle* h, void** stream);
 /* Number of kernels this library has launched in this process. */
 int sdpx_b200_launch_count(uint64_t* count);
 
+/* Allocation-free Gram (Schur) product — no counterpart in the reference.
+ *
+ * S = Pᵀ P for a K×m column-major FP64 matrix P already in device memory
+ * (column i is one variable's stacked vector, as in the Schur assembly with
+ * the identity metric), written as the full symmetric m×m column-major S.
+ * It performs no allocation: the split-K partial tiles use a fixed 32 MiB
+ * device array compiled into the library, so it suits callers that cannot
+ * call cudaMalloc — runtimes that own all device memory through their own
+ * pool (e.g. a Julia or Python caching allocator) or serving loops where an
+ * implicit cudaMalloc/cudaFree would synchronise the device.
+ *   - m ≤ 2048 (the array holds one K chunk of every lower 128×128 tile);
+ *     larger m returns an error and leaves S untouched.
+ *   - The first call on each device looks up the array's device address with
+ *     that device current; make that first call before any stream capture.
+ *   - Every call on a device shares the one array: calls that overlap on the
+ *     GPU (different streams, or different host threads) race.  Serialise them.
+ *   - stream: a cudaStream_t (NULL = legacy default stream); the call is
+ *     asynchronous with respect to the host.
+ * Every GPU that loads the library keeps the array until the process exits. */
+int sdpx_b200_gram_noalloc(const double* P, int64_t K, int32_t m, double* S, void* stream);
+const char* sdpx_b200_gram_noalloc_error(void);
+
 /* Cumulative device time per phase (ms) since the last reset:
  * [0] residual+block factor, [1] Schur assembly, [2] KKT factor,
  * [3] solves+refinement, [4] directions+RHS, [5] step length, [6] update. */

@@ -1733,6 +1733,23 @@ int sdpx_b200_launch_count(uint64_t* count) {
   *count = sdpx::launch_count();
   return 0;
 }
+static thread_local std::string g_noalloc_error;
+const char* sdpx_b200_gram_noalloc_error(void) { return g_noalloc_error.c_str(); }
+int sdpx_b200_gram_noalloc(const double* P, int64_t K, int32_t m, double* S, void* stream) {
+  if (!P || !S) return -1;
+  try {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    sdpx::syrk_lower_f64_noalloc(P, K, m, S, st);
+    sdpx::mirror_lower(m, S, st);
+    return 0;
+  } catch (const std::invalid_argument& ex) {
+    g_noalloc_error = ex.what();
+    return -1;
+  } catch (const std::exception& ex) {
+    g_noalloc_error = ex.what();
+    return -2;
+  }
+}
 int sdpx_b200_phase_times(sdpx_b200_handle* h, double* ms7, int reset) {
   GUARD(h, {
     h->h.harvest_phases();

@@ -4,6 +4,9 @@
 #include "blas_f64.h"
 #include "gemm_f64.cuh"
 
+#include <mutex>
+#include <stdexcept>
+
 namespace sdpx {
 
 // Tile configurations.  128×128 / 8 warps for the large Schur products,
@@ -173,6 +176,73 @@ void syrk_lower_f64(const Opnd& P, const SyrkPlan& plan, double* partial, double
   k_syrk_reduce<Cfg::BM, Cfg::BN><<<plan.ntri, 256, 0, st>>>(partial, plan.ntri, plan.nchunk, m, S,
                                                              lds, beta);
   SDPX_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the split-K lower Gram product S = PᵀP.
+//
+// The split-K partial tiles live in a fixed file-scope device array instead of
+// caller- or library-allocated memory.  Its capacity bounds the problem size:
+// one K chunk per lower 128×128 tile must fit, i.e. ntri·128·128 doubles with
+// ntri = t(t+1)/2, t = ceil(m/128), so m ≤ 2048.  Every GPU that loads the
+// library holds the array until the process exits, and all calls share it.
+// ---------------------------------------------------------------------------
+static constexpr size_t kNoAllocScratchDoubles = (size_t)4 << 20;  // 32 MiB
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[64] = {};
+
+// Device address of the scratch array on the current device.  The array's
+// host-side name is only a stand-in, so the address is looked up once per
+// device with that device current and cached; a failed lookup is reported.
+static double* noalloc_scratch_address() {
+  int dev = 0;
+  SDPX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      throw CudaError(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+size_t gram_noalloc_capacity_doubles() { return kNoAllocScratchDoubles; }
+
+void syrk_lower_f64_noalloc(const double* P, long long K, int m, double* S, cudaStream_t st) {
+  using Cfg = CfgBigKT;
+  const int nt = ceil_div(m, Cfg::BM);
+  const long long ntri = (long long)nt * (nt + 1) / 2;
+  const long long tile = (long long)Cfg::BM * Cfg::BN;
+  if (m <= 0 || K <= 0) throw std::invalid_argument("gram: m and K must be positive");
+  if (ntri * tile > (long long)kNoAllocScratchDoubles)
+    throw std::invalid_argument("gram (allocation-free): m = " + std::to_string(m) +
+                                " exceeds the fixed scratch (m ≤ 2048)");
+  double* scratch = noalloc_scratch_address();
+  int dev = 0, sms = 148;
+  SDPX_CUDA(cudaGetDevice(&dev));
+  SDPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  // As many K chunks as the scratch holds, capped by the normal plan.
+  SyrkPlan plan = plan_syrk_f64(m, K, sms);
+  long long max_chunks = (long long)kNoAllocScratchDoubles / (ntri * tile);
+  int nchunk = (int)std::max<long long>(1, std::min<long long>(plan.nchunk, max_chunks));
+  long long kc = (K + nchunk - 1) / nchunk;
+  kc = ((kc + 15) / 16) * 16;
+  plan.kchunk = (int)kc;
+  plan.nchunk = (int)((K + kc - 1) / kc);
+  Opnd Pd;
+  Pd.base = P;
+  Pd.kstride = 1;
+  Pd.inner = 1 << 30;
+  Pd.inner_stride = K;
+  Pd.outer_stride = 0;
+  Pd.mn_extent = m;
+  Pd.k_extent = (int)K;
+  syrk_lower_f64(Pd, plan, scratch, S, m, m, 0.0, st);
 }
 
 }  // namespace sdpx

@@ -25,4 +25,9 @@ SyrkPlan plan_syrk_f64(int m, long long K, int sm_count);
 void syrk_lower_f64(const Opnd& P, const SyrkPlan& plan, double* partial, double* S, long long lds,
                     int m, double beta, cudaStream_t st);
 
+// Allocation-free S = PᵀP (lower tiles then mirrored by the caller), split-K
+// scratch in a fixed device array; throws std::invalid_argument when m > 2048.
+void syrk_lower_f64_noalloc(const double* P, long long K, int m, double* S, cudaStream_t st);
+size_t gram_noalloc_capacity_doubles();
+
 }  // namespace sdpx
