@@ -56,6 +56,9 @@ int sdpx_b200_create(const sdpx_b200_problem* problem, int device, sdpx_b200_han
 void sdpx_b200_destroy(sdpx_b200_handle* h);
 const char* sdpx_b200_last_error(const sdpx_b200_handle* h);
 int sdpx_b200_set_precision(sdpx_b200_handle* h, int mode);
+/* Current precision mode (mixed mode switches itself to FP64 when the guard
+ * fails), number of such switches, and the last FP32-factor condition estimate. */
+int sdpx_b200_get_precision(sdpx_b200_handle* h, int* mode, int* fallbacks, double* cond_estimate);
 
 /* Ruiz + per-variable + objective scaling of the resident data in place
  * (`equilibrate`, src/ingest.jl:1431-1519).  Outputs: E (Σ k_l, per block

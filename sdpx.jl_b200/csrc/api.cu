@@ -115,6 +115,9 @@ struct Handle {
   DBuf<double> seg_part;           // seg_dot partials
   int seg_parts = 8;
   double last_bpr = 0.0;
+  int mixed_predicted_steps = 32;  // from the last FP32 factor's condition estimate
+  long long mixed_guard_steps = 0;
+  int mixed_fallbacks = 0;
 
   // batched Cholesky workspace (dense blocks X, Y and line-search trials)
   DBuf<MatDesc<double>> d_descs;
@@ -124,6 +127,7 @@ struct Handle {
   DBuf<double> trials;
   DBuf<long long> d_trial_off;
   DBuf<double> d_tcand;
+  DBuf<TrialDesc> d_trial_desc;
   DBuf<int> d_fail;
   std::vector<double> lx_dmin, lx_dmax, my_dmin, my_dmax;
   bool diag_factor_ok = true;
@@ -287,8 +291,12 @@ struct Handle {
     int nmax = 0;
     for (auto& q : mats) nmax = std::max(nmax, q.n);
     h2d(d_descs.p, mats.data(), n * sizeof(MatDesc<double>));
-    potrf_batched<double, 32>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p,
-                              d_diag_store.p, st);
+    if (nmax >= 192)
+      potrf_batched<double, 64>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p,
+                                d_diag_store.p, st);
+    else
+      potrf_batched<double, 32>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p,
+                                d_diag_store.p, st);
     d2h(info.data(), d_info.p, n * sizeof(int));
     d2h(dmin.data(), d_dmin.p, n * sizeof(double));
     d2h(dmax.data(), d_dmax.p, n * sizeof(double));
@@ -572,6 +580,9 @@ struct Handle {
 
   void reset() {
     if (mixed) mixed->a_planes_valid = false;
+    mixed_fallbacks = 0;
+    mixed_guard_steps = 0;
+    mixed_predicted_steps = 32;
     if (have_original) {
       d2d(A.p, A0.p, sizeof(double) * K * m);
       d2d(Cst.p, C0st.p, sizeof(double) * K);
@@ -800,7 +811,12 @@ struct Handle {
     PhaseScope ps(this, 2);
     if (precision == SDPX_B200_MIXED && mixed) {
       mixed_factorize(ok, attempts, quality);
-      return;
+      if (*ok && mixed_predicted_steps <= 32) return;
+      // Static rejection: the FP32 factor of the split-assembled S is not
+      // predicted to converge in ≤ 32 refinements (or failed) — FP64 from here.
+      precision = SDPX_B200_FP64;
+      ++mixed_fallbacks;
+      schur_build_fp64(0);
     }
     MatDesc<double> md{Sf.p, m, m};
     std::vector<MatDesc<double>> one{md};
@@ -843,6 +859,54 @@ struct Handle {
     PhaseScope ps(this, 3);
     d2d(dx.p, r.p, m * sizeof(double));
     solve_into(dx.p);
+    if (precision == SDPX_B200_MIXED && mixed) mixed_guard();
+  }
+  // Mixed-precision solve guard (the reference's `_solve_mixed_kkt_guarded!`,
+  // src/kernels/mixed_precision_kkt.jl:1431-1586): refine the low-precision
+  // solution against the FP64 Newton operator until ‖r − S dx‖∞ ≤ 1e-8·max(‖r‖∞,1),
+  // at most min(predicted, 32) corrections, stopping when a correction does
+  // not reduce the residual.  On failure the iteration continues on the FP64
+  // path: S is reassembled and factored in FP64 and dx re-solved.
+  void mixed_guard() {
+    double res, rn;
+    direction_residual(&res, &rn);
+    const double target = 1e-8 * std::max(rn, 1.0);
+    if (std::isfinite(res) && res <= target) return;
+    int cap = std::min(mixed_predicted_steps, 32);
+    bool ok = false;
+    if (std::isfinite(res)) {
+      for (int s = 0; s < cap; ++s) {
+        d2d(dxbest.p, dx.p, m * sizeof(double));
+        d2d(work_m.p, rho.p, m * sizeof(double));
+        solve_into(work_m.p);
+        combine(m, dx.p, 1.0, work_m.p, st);
+        double corr = residual_norm_only();
+        ++mixed_guard_steps;
+        if (!std::isfinite(corr) || corr >= res) {
+          d2d(dx.p, dxbest.p, m * sizeof(double));
+          break;
+        }
+        res = corr;
+        if (res <= target) {
+          ok = true;
+          break;
+        }
+      }
+    }
+    if (!ok) switch_to_fp64_now();
+  }
+  // Leave mixed mode for good within the current iteration: FP64 Schur,
+  // FP64 factor, and re-solve of the current right-hand side.
+  void switch_to_fp64_now() {
+    precision = SDPX_B200_FP64;
+    ++mixed_fallbacks;
+    schur_build_fp64(0);
+    int ok = 0, att = 0;
+    double q = 0.0;
+    factorize(&ok, &att, &q);
+    if (!ok) throw CudaError("FP64 fallback factorisation failed");
+    d2d(dx.p, r.p, m * sizeof(double));
+    solve_into(dx.p);
   }
   // ρ = r − S·dx  (FP64 Newton operator)
   void apply_residual() {
@@ -879,6 +943,28 @@ struct Handle {
     };
     int steps = 0;
     double residual;
+    if (precision == SDPX_B200_MIXED && mixed) {
+      // `_refine_mixed_direction!` (src/kernels/mixed_precision_kkt.jl:1634-1680)
+      double rel = tol > 0 ? tol : 64.0 * kEps;
+      clear_red(1, 1);
+      absmax(m, r.p, red.p + 1, st);
+      double abstol = rel * std::max(read_red(1), 1.0);
+      residual = residual_norm_only();
+      for (int s = 0; s < 32; ++s) {
+        if (residual <= abstol) break;
+        correction();
+        double corr = residual_norm_only();
+        if (!std::isfinite(corr) || corr >= residual) {
+          d2d(dx.p, dxbest.p, m * sizeof(double));
+          break;
+        }
+        ++steps;
+        residual = corr;
+      }
+      *steps_out = steps;
+      *res_out = residual;
+      return;
+    }
     if (policy == 0) {
       residual = residual_norm_only();
       for (int s = 0; s < fixed_steps; ++s) {
@@ -1141,94 +1227,154 @@ struct Handle {
     return p1;
   }
 
-  // Fraction-to-boundary bound for one side (src/kernels/generic.jl:350-422):
-  // closed forms for 1×1 and 2×2, otherwise a full-step Cholesky test followed
-  // by 64 bisection steps.  The bisection is evaluated 15 points at a time —
-  // the complete 4-level subtree of the current interval — and the sequential
-  // path is replayed through it, so the result equals the sequential one.
-  double ftb_side(const double* M, const double* dM) {
-    double bound = 1.0;
-    if (nd) {
-      diag_ftb(nd, od, M, dM, red.p + 8, st);
-      bound = std::min(bound, read_red(8));
+  // One trial matrix  out = M_b + t·dM_b  of dense block b (side-specific M, dM).
+  struct TrialReq {
+    const double* M;
+    const double* dM;
+    int b;
+    double t;
+  };
+  // Build all requested trial matrices, factor them in one batch and return
+  // (info == 0, min |L_ii|, max |L_ii|) per request.
+  void run_trials(const std::vector<TrialReq>& reqs, std::vector<int>& info,
+                  std::vector<double>& dmn, std::vector<double>& dmx) {
+    size_t n = reqs.size();
+    info.clear();
+    dmn.clear();
+    dmx.clear();
+    if (n == 0) return;
+    std::vector<long long> off(n);
+    long long need = 0;
+    int nmax = 0;
+    for (size_t q = 0; q < n; ++q) {
+      int kk = dense[reqs[q].b].k;
+      off[q] = need;
+      need += (long long)kk * kk;
+      nmax = std::max(nmax, kk);
     }
-    for (auto& s : fetch_k2(M, dM)) bound = std::min(bound, ftb2(s));
-    std::vector<int> big;
-    for (size_t b = 0; b < dense.size(); ++b)
-      if (dense[b].k > 2) big.push_back((int)b);
-    for (int b : big) bound = std::min(bound, ftb_dense_block(b, M, dM));
-    return bound;
+    if ((size_t)need > trials.n) trials.alloc(std::max<size_t>(need, trials.n * 2));
+    std::vector<TrialDesc> td(n);
+    for (size_t q = 0; q < n; ++q) {
+      const DenseBlk& B = dense[reqs[q].b];
+      td[q] = {reqs[q].M + B.off, reqs[q].dM + B.off, trials.p + off[q], reqs[q].t, B.k};
+    }
+    if (d_trial_desc.n < n) d_trial_desc.alloc(std::max<size_t>(n, 2 * d_trial_desc.n));
+    h2d(d_trial_desc.p, td.data(), n * sizeof(TrialDesc));
+    make_trials_list(d_trial_desc.p, (int)n, nmax, st);
+    std::vector<MatDesc<double>> mats(n);
+    for (size_t q = 0; q < n; ++q) mats[q] = {trials.p + off[q], dense[reqs[q].b].k, dense[reqs[q].b].k};
+    potrf_host_list(mats, info, dmn, dmx);
   }
-  double ftb_dense_block(int b, const double* M, const double* dM) {
-    // Evaluate candidate lists on this block only.
-    auto test = [&](const std::vector<double>& t) {
-      std::vector<char> pass(t.size(), 1);
-      std::vector<long long> toff(dense.size(), 0);
-      long long kk2 = (long long)dense[b].k * dense[b].k;
-      long long need = (long long)t.size() * kk2;
-      if ((size_t)need > trials.n) trials.alloc(need);
-      if (d_tcand.n < t.size()) d_tcand.alloc(t.size());
-      h2d(d_tcand.p, t.data(), t.size() * sizeof(double));
-      const int kk = dense[b].k;
-      if (d_trial_off.n < 1) d_trial_off.alloc(dense.size());
-      long long zero = 0;
-      h2d(d_trial_off.p, &zero, sizeof(long long));
-      make_trials(d_doff.p + b, d_dk.p + b, d_trial_off.p, 1, kk, M, dM, d_tcand.p, (int)t.size(),
-                  trials.p, st);
-      std::vector<MatDesc<double>> mats;
-      for (size_t c2 = 0; c2 < t.size(); ++c2) mats.push_back({trials.p + (long long)c2 * kk2, kk, kk});
+
+  // Fraction-to-boundary bounds of both sides (src/kernels/generic.jl:350-422):
+  // closed forms for 1×1 and 2×2 blocks, otherwise a full-step Cholesky test
+  // followed by 64 bisection steps.  Every (side, block) bisection advances in
+  // the same rounds: each round factors, in one batch, the complete 4-level
+  // subtree of midpoints of every unfinished interval, and the sequential
+  // bisection path is replayed through it — the result equals the sequential one.
+  void ftb_bounds(double* boundX, double* boundY) {
+    double b2[2] = {1.0, 1.0};
+    const double* Ms[2] = {X.p, Y.p};
+    const double* dMs[2] = {dX.p, dY.p};
+    for (int side = 0; side < 2; ++side) {
+      if (nd) {
+        diag_ftb(nd, od, Ms[side], dMs[side], red.p + 8 + side, st);
+      }
+      for (auto& s2 : fetch_k2(Ms[side], dMs[side])) b2[side] = std::min(b2[side], ftb2(s2));
+    }
+    if (nd) {
+      d2h(h_red + 8, red.p + 8, 2 * sizeof(double));
+      sync();
+      b2[0] = std::min(b2[0], h_red[8]);
+      b2[1] = std::min(b2[1], h_red[9]);
+    }
+    struct Bis {
+      int side, b;
+      double lo = 0.0, hi = 1.0;
+      int done = 0;
+      bool first = true, finished = false;
+      double result = 1.0;
+    };
+    std::vector<Bis> probs;
+    for (int side = 0; side < 2; ++side)
+      for (size_t b = 0; b < dense.size(); ++b)
+        if (dense[b].k > 2) {
+          Bis q;
+          q.side = side;
+          q.b = (int)b;
+          probs.push_back(q);
+        }
+    constexpr int DEPTH = 4;
+    while (true) {
+      std::vector<TrialReq> reqs;
+      std::vector<std::vector<double>> pts(probs.size());
+      std::vector<size_t> first_req(probs.size());
+      for (size_t q = 0; q < probs.size(); ++q) {
+        Bis& P = probs[q];
+        if (P.finished) continue;
+        int depth = std::min(DEPTH, 64 - P.done);
+        int npts = (1 << depth) - 1;
+        std::vector<double> los(npts), his(npts);
+        pts[q].assign(npts, 0.0);
+        los[0] = P.lo;
+        his[0] = P.hi;
+        for (int n2 = 0; n2 < npts; ++n2) {
+          pts[q][n2] = (los[n2] + his[n2]) / 2.0;
+          int l2 = 2 * n2 + 1, r2 = 2 * n2 + 2;
+          if (l2 < npts) los[l2] = los[n2], his[l2] = pts[q][n2];
+          if (r2 < npts) los[r2] = pts[q][n2], his[r2] = his[n2];
+        }
+        first_req[q] = reqs.size();
+        for (double t : pts[q]) reqs.push_back({Ms[P.side], dMs[P.side], P.b, t});
+        if (P.first) reqs.push_back({Ms[P.side], dMs[P.side], P.b, 1.0});
+      }
+      if (reqs.empty()) break;
       std::vector<int> info;
       std::vector<double> dmn, dmx;
-      potrf_host_list(mats, info, dmn, dmx);
-      for (size_t c2 = 0; c2 < t.size(); ++c2) pass[c2] = info[c2] == 0;
-      return pass;
-    };
-    constexpr int DEPTH = 4;
-    double lo = 0.0, hi = 1.0;
-    int done = 0;
-    bool first = true;
-    while (done < 64) {
-      int depth = std::min(DEPTH, 64 - done);
-      // heap-ordered subtree midpoints of (lo, hi)
-      int npts = (1 << depth) - 1;
-      std::vector<double> pts(npts), los(npts), his(npts);
-      los[0] = lo;
-      his[0] = hi;
-      for (int n2 = 0; n2 < npts; ++n2) {
-        pts[n2] = (los[n2] + his[n2]) / 2.0;
-        int l2 = 2 * n2 + 1, r2 = 2 * n2 + 2;
-        if (l2 < npts) los[l2] = los[n2], his[l2] = pts[n2];
-        if (r2 < npts) los[r2] = pts[n2], his[r2] = his[n2];
-      }
-      std::vector<double> cand = pts;
-      if (first) cand.push_back(1.0);
-      auto pass = test(cand);
-      if (first) {
-        first = false;
-        if (pass.back()) return 1.0;
-      }
-      int node = 0;
-      for (int s2 = 0; s2 < depth; ++s2) {
-        double mid = pts[node];
-        if (pass[node]) {
-          lo = mid;
-          node = 2 * node + 2;
-        } else {
-          hi = mid;
-          node = 2 * node + 1;
+      run_trials(reqs, info, dmn, dmx);
+      for (size_t q = 0; q < probs.size(); ++q) {
+        Bis& P = probs[q];
+        if (P.finished) continue;
+        const size_t f = first_req[q];
+        const int npts = (int)pts[q].size();
+        if (P.first) {
+          P.first = false;
+          if (info[f + npts] == 0) {  // full step stays positive definite
+            P.finished = true;
+            P.result = 1.0;
+            continue;
+          }
+        }
+        int node = 0, depth = 0;
+        while (node < npts) {
+          double mid = pts[q][node];
+          if (info[f + node] == 0) {
+            P.lo = mid;
+            node = 2 * node + 2;
+          } else {
+            P.hi = mid;
+            node = 2 * node + 1;
+          }
+          ++depth;
+        }
+        P.done += depth;
+        if (P.done >= 64) {
+          P.finished = true;
+          P.result = P.lo;
         }
       }
-      done += depth;
     }
-    return lo;
+    for (auto& P : probs) b2[P.side] = std::min(b2[P.side], P.result);
+    *boundX = b2[0];
+    *boundY = b2[1];
   }
 
   void affine_diagnostics(int adaptive, double* out, double* block_compl) {
     PhaseScope ps(this, 5);
     double tX = 1.0, tY = 1.0;
     if (adaptive) {
-      double bX = ftb_side(X.p, dX.p);
-      double bY = ftb_side(Y.p, dY.p);
+      double bX, bY;
+      ftb_bounds(&bX, &bY);
       tX = bX < 1 ? bX : 1.0;
       tY = bY < 1 ? bY : 1.0;
     }
@@ -1254,31 +1400,72 @@ struct Handle {
                    double* tX_out, double* tY_out) {
     PhaseScope ps(this, 5);
     if (rule == 1) {
-      double bX = ftb_side(X.p, dX.p), bY = ftb_side(Y.p, dY.p);
+      double bX, bY;
+      ftb_bounds(&bX, &bY);
       *tX_out = bX < 1 ? fp * bX : 1.0;
       *tY_out = bY < 1 ? fd * bY : 1.0;
       return;
     }
-    auto side = [&](const double* M, const double* dM) {
-      auto k2 = fetch_k2(M, dM);
-      double t = 1.0;
-      constexpr int J = 8;
-      while (true) {
-        std::vector<double> cand;
-        double tt = t;
+    // Backtracking (src/kernels/threaded.jl:1751-1818): the first t in 1, γ, γ², …
+    // whose trial passes every block (Cholesky + diagonal-ratio margin), or the
+    // first t below min_step.  Candidates of both sides are factored together,
+    // eight per side per round.
+    const double* Ms[2] = {X.p, Y.p};
+    const double* dMs[2] = {dX.p, dY.p};
+    std::vector<Small2> k2[2] = {fetch_k2(X.p, dX.p), fetch_k2(Y.p, dY.p)};
+    double t_next[2] = {1.0, 1.0};
+    double result[2] = {1.0, 1.0};
+    bool done[2] = {false, false};
+    constexpr int J = 8;
+    while (!(done[0] && done[1])) {
+      std::vector<double> cand[2];
+      for (int side = 0; side < 2; ++side) {
+        if (done[side]) continue;
+        double tt = t_next[side];
         for (int j = 0; j < J; ++j) {
-          cand.push_back(tt);
+          cand[side].push_back(tt);
           if (tt < min_step) break;
           tt *= gamma;
         }
-        auto pass = all_trials(M, dM, cand, margin, k2);
-        for (size_t j = 0; j < cand.size(); ++j)
-          if (pass[j] || cand[j] < min_step) return cand[j];
-        t = cand.back() * gamma;
       }
-    };
-    *tX_out = side(X.p, dX.p);
-    *tY_out = side(Y.p, dY.p);
+      // dense blocks with k > 2: one batch for both sides
+      std::vector<TrialReq> reqs;
+      std::vector<int> big;
+      for (size_t b = 0; b < dense.size(); ++b)
+        if (dense[b].k > 2) big.push_back((int)b);
+      for (int side = 0; side < 2; ++side)
+        for (int b : big)
+          for (double t : cand[side]) reqs.push_back({Ms[side], dMs[side], b, t});
+      std::vector<int> info;
+      std::vector<double> dmn, dmx;
+      run_trials(reqs, info, dmn, dmx);
+      size_t q = 0;
+      for (int side = 0; side < 2; ++side) {
+        if (done[side]) continue;
+        std::vector<char> pass(cand[side].size(), 1);
+        for (size_t bi = 0; bi < big.size(); ++bi)
+          for (size_t c2 = 0; c2 < cand[side].size(); ++c2, ++q) {
+            bool ok = info[q] == 0;
+            if (ok && margin > 0)
+              ok = std::isfinite(dmn[q]) && std::isfinite(dmx[q]) && dmx[q] > 0 &&
+                   dmn[q] > margin * dmx[q];
+            if (!ok) pass[c2] = 0;
+          }
+        auto pd = diag_trials(Ms[side], dMs[side], cand[side], margin);
+        for (size_t c2 = 0; c2 < cand[side].size(); ++c2) {
+          bool ok = pass[c2] && pd[c2];
+          for (auto& s2 : k2[side]) ok = ok && margin2(s2, cand[side][c2], margin);
+          if (ok || cand[side][c2] < min_step) {
+            result[side] = cand[side][c2];
+            done[side] = true;
+            break;
+          }
+        }
+        if (!done[side]) t_next[side] = cand[side].back() * gamma;
+      }
+    }
+    *tX_out = result[0];
+    *tY_out = result[1];
   }
 
   // -------------------------------------------------------------- update --
@@ -1727,6 +1914,13 @@ int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const dou
   GUARD(h, h->h.original_residuals(x, X, Y, p, d));
 }
 int sdpx_b200_reset(sdpx_b200_handle* h) { GUARD(h, h->h.reset()); }
+int sdpx_b200_get_precision(sdpx_b200_handle* h, int* mode, int* fallbacks, double* cond_estimate) {
+  GUARD(h, {
+    *mode = h->h.precision;
+    if (fallbacks) *fallbacks = h->h.mixed_fallbacks;
+    if (cond_estimate) *cond_estimate = h->h.mixed ? h->h.mixed->cond_estimate : 0.0;
+  });
+}
 int sdpx_b200_get_stream(sdpx_b200_handle* h, void** stream) { GUARD(h, *stream = (void*)h->h.st); }
 int sdpx_b200_launch_count(uint64_t* count) {
   if (!count) return -1;

@@ -442,6 +442,23 @@ void make_trials(const long long* d_off, const int* d_k, const long long* d_tria
   SDPX_LAUNCH_CHECK();
 }
 
+// Trial matrices from a descriptor list: out_q = X_q + t_q·dX_q (k_q × k_q).
+__global__ void k_make_trials_list(const TrialDesc* d, int n) {
+  const int q = blockIdx.y;
+  if (q >= n) return;
+  const TrialDesc T = d[q];
+  const long long tot = (long long)T.k * T.k;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x)
+    T.out[e] = T.X[e] + T.t * T.dX[e];
+}
+void make_trials_list(const TrialDesc* d_list, int n, int kmax, cudaStream_t st) {
+  if (n == 0) return;
+  int g = std::max(1, std::min(64, ceil_div((long long)kmax * kmax, 256)));
+  k_make_trials_list<<<dim3(g, n), 256, 0, st>>>(d_list, n);
+  SDPX_LAUNCH_CHECK();
+}
+
 // ------------------------------------------------------------ permutation --
 __global__ void k_gather(long long n, const long long* map, const double* src, double* dst) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;

@@ -6,6 +6,15 @@
 
 namespace sdpx {
 
+struct TrialDesc {
+  const double* X;
+  const double* dX;
+  double* out;
+  double t;
+  int k;
+};
+void make_trials_list(const TrialDesc* d_list, int n, int kmax, cudaStream_t st);
+
 void gemv_n(const double* A, long long K, int m, const double* x, double* out, double* part,
             int chunks, cudaStream_t st);
 void gemv_t(const double* A, long long K, int m, const double* z, double alpha, const double* base,

@@ -73,6 +73,7 @@ _SIGS = {
     "sdpx_b200_original_residuals": [C.c_void_p, _dp, _dp, _dp, _dp, _dp],
     "sdpx_b200_phase_times": [C.c_void_p, _dp, C.c_int],
     "sdpx_b200_reset": [C.c_void_p],
+    "sdpx_b200_get_precision": [C.c_void_p, _ip, _ip, _dp],
     "sdpx_b200_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
     "sdpx_b200_launch_count": [C.POINTER(C.c_uint64)],
 }
@@ -194,8 +195,16 @@ class CudaBackend:
         self._call("sdpx_b200_set_precision", 1 if mode == "mixed" else 0)
         self.mode = mode
 
-    def precision_label(self):
+    def _sync_mode(self):
+        mode, fb, cond = C.c_int(), C.c_int(), C.c_double()
+        self._call("sdpx_b200_get_precision", C.byref(mode), C.byref(fb), C.byref(cond))
+        self.mode = "mixed" if mode.value == 1 else "fp64"
+        self.fallbacks = fb.value
+        self.cond_estimate = cond.value
         return self.mode
+
+    def precision_label(self):
+        return self._sync_mode() if getattr(self, "h", None) else self.mode
 
     def precision_history(self):
         return list(self._history)
@@ -208,7 +217,7 @@ class CudaBackend:
             self._in_loop = True
             if self.requested == "mixed":
                 self._set_mode("mixed")
-        self._history.append(self.mode)
+        self._history.append(self._sync_mode())
 
     def fallback_to_fp64(self, reason: str) -> bool:
         if self.mode == "mixed":
