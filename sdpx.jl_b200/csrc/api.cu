@@ -14,6 +14,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <map>
 #include <set>
 #include <string>
 #include <vector>
@@ -32,12 +33,17 @@ void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_o
 unsigned long long launch_count() { return g_launches.load(); }
 
 static std::mutex g_attr_mu;
-static std::set<std::pair<const void*, int>> g_attr_done;
-bool smem_attr_needed(const void* kern, size_t) {
+static std::map<std::pair<const void*, int>, size_t> g_attr_done;
+// True when `kern` on the current device has not yet been opted in to at
+// least `bytes` of dynamic shared memory (records the new size).
+bool smem_attr_needed(const void* kern, size_t bytes) {
   int dev = 0;
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lk(g_attr_mu);
-  return g_attr_done.insert({kern, dev}).second;
+  size_t& have = g_attr_done[{kern, dev}];
+  if (have >= bytes) return false;
+  have = bytes;
+  return true;
 }
 
 template <class T>
@@ -409,7 +415,7 @@ struct Handle {
     for (auto* b : {&X, &Y, &P, &R, &Z, &dX, &dY, &LX, &MY, &W, &T1, &T2, &Xbest, &Ybest, &tmpK2})
       b->alloc(K), b->zero(st);
     gemv_chunks = std::max(1, std::min(16, m / 64));
-    gemv_part.alloc((size_t)gemv_chunks * K);
+    gemv_part.alloc((size_t)gemv_chunks * std::max<long long>(K, m));
     Pc.alloc((size_t)K * m);
     S.alloc((size_t)m * m);
     Sf.alloc((size_t)m * m);

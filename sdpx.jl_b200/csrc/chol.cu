@@ -9,6 +9,7 @@
 // returns at once — the no-throw contract of SDPX's `kchol!`
 // (src/kernels/generic.jl:133-155).
 #include "chol.h"
+#include "blas_f64.h"
 
 namespace sdpx {
 
@@ -89,24 +90,91 @@ __global__ void k_potrf_panel(const MatDesc<T>* mats, int j, int* info, T* dmin,
     }
     return;
   }
-  // Off-diagonal tile: X = B · L_jj^{-T}, one thread per row.
+  // Off-diagonal tile: X = B · L_jj^{-T}, right-looking over the columns of the
+  // tile so every step is parallel over its rows and remaining columns.
   const int h = min(NB, M.n - r0);
   for (int e = threadIdx.x; e < h * w; e += blockDim.x) {
     int r = e % h, c = e / h;
     Bt[c * LD + r] = M.a[(size_t)(c0 + c) * M.ld + (r0 + r)];
   }
   __syncthreads();
-  for (int r = threadIdx.x; r < h; r += blockDim.x) {
-    for (int c = 0; c < w; ++c) {
-      T s = Bt[c * LD + r];
-      for (int p = 0; p < c; ++p) s -= Bt[p * LD + r] * D[p * LD + c];
-      Bt[c * LD + r] = s / D[c * LD + c];
+  for (int c = 0; c < w; ++c) {
+    const T dcc = D[c * LD + c];
+    for (int r = threadIdx.x; r < h; r += blockDim.x) Bt[c * LD + r] /= dcc;
+    __syncthreads();
+    const int rem = w - c - 1;
+    for (int e = threadIdx.x; e < h * rem; e += blockDim.x) {
+      int r = e % h, q = c + 1 + e / h;
+      Bt[q * LD + r] -= Bt[c * LD + r] * D[c * LD + q];
     }
+    __syncthreads();
   }
-  __syncthreads();
   for (int e = threadIdx.x; e < h * w; e += blockDim.x) {
     int r = e % h, c = e / h;
     M.a[(size_t)(c0 + c) * M.ld + (r0 + r)] = Bt[c * LD + r];
+  }
+}
+
+// Whole panel in shared memory (orders n ≤ PANEL_MAX_ROWS): one CTA per matrix
+// loads rows [c0, n) of panel j, factors it right-looking (pivot, scale, rank-1
+// update of the panel's remaining columns) and writes it back; the trailing
+// tiles are then updated by k_potrf_update.  Replaces the per-tile panel
+// launch for the k ≤ 416 blocks of the line-search trials and block factors.
+template <class T, int NB>
+__global__ void k_potrf_panel_smem(const MatDesc<T>* mats, int j, int* info, T* dmin, T* dmax) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  T* Pn = reinterpret_cast<T*>(raw);  // rows × NB, column-major with ld = rows_pad
+  __shared__ int s_fail;
+  const MatDesc<T> M = mats[blockIdx.x];
+  const int b = blockIdx.x;
+  const int c0 = j * NB;
+  if (c0 >= M.n || info[b] != 0) return;
+  const int w = min(NB, M.n - c0);
+  const int rows = M.n - c0;
+  const int ld = rows | 1;  // odd stride: conflict-free column walks
+  for (int e = threadIdx.x; e < rows * w; e += blockDim.x) {
+    int r = e % rows, c = e / rows;
+    Pn[c * ld + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
+  }
+  if (threadIdx.x == 0) s_fail = -1;
+  __syncthreads();
+  for (int c = 0; c < w; ++c) {
+    const T piv = Pn[c * ld + c];
+    if (!(piv > T(0))) {
+      if (threadIdx.x == 0) s_fail = c;
+      break;  // uniform: every thread read the same pivot
+    }
+    const T lc = sqrt(piv);
+    __syncthreads();
+    for (int r = c + 1 + threadIdx.x; r < rows; r += blockDim.x) Pn[c * ld + r] /= lc;
+    if (threadIdx.x == 0) Pn[c * ld + c] = lc;
+    __syncthreads();
+    const int rem = w - c - 1;
+    const int height = rows - c - 1;
+    for (int e = threadIdx.x; e < height * rem; e += blockDim.x) {
+      int r = c + 1 + e % height, q = c + 1 + e / height;
+      if (r >= q) Pn[q * ld + r] -= Pn[c * ld + r] * Pn[c * ld + q];
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (s_fail >= 0) {
+    if (threadIdx.x == 0) info[b] = c0 + s_fail + 1;
+    return;
+  }
+  for (int e = threadIdx.x; e < rows * w; e += blockDim.x) {
+    int r = e % rows, c = e / rows;
+    M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] = (r >= c) ? Pn[c * ld + r] : T(0);
+  }
+  if (threadIdx.x == 0) {
+    T lo = dmin[b], hi = dmax[b];
+    for (int c = 0; c < w; ++c) {
+      T v = fabs(Pn[c * ld + c]);
+      lo = fmin(lo, v);
+      hi = fmax(hi, v);
+    }
+    dmin[b] = lo;
+    dmax[b] = hi;
   }
 }
 
@@ -125,7 +193,8 @@ __global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info,
   const int rem = nt - j - 1;
   const int t = blockIdx.x;
   if (t == 0) {
-    // CTA 0 writes back the factored diagonal tile of panel j.
+    // CTA 0 writes back the factored diagonal tile of panel j (tiled panel path).
+    if (!diag_store) return;
     const int c0 = j * NB, w = min(NB, M.n - c0);
     const T* ds = diag_store + (size_t)blockIdx.y * NB * NB;
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
@@ -206,12 +275,24 @@ void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* d
   ensure_smem(k_potrf_update<T, NB>, smem);
   k_init_stats<T><<<ceil_div(nmat, 128), 128, 0, st>>>(nmat, info, dmin, dmax);
   const int nt = ceil_div(nmax, NB);
+  const int rows_pad = nmax | 1;
+  const size_t panel_smem = sizeof(T) * (size_t)rows_pad * NB;
+  const bool whole_panel = panel_smem <= 224 * 1024;
+  if (whole_panel) ensure_smem(k_potrf_panel_smem<T, NB>, panel_smem);
   for (int j = 0; j < nt; ++j) {
-    dim3 g1(nt - j, nmat);
-    k_potrf_panel<T, NB><<<g1, 256, smem, st>>>(d_mats, j, info, dmin, dmax, diag_store);
     int rem = nt - j - 1;
-    dim3 g2(1 + rem * (rem + 1) / 2, nmat);
-    k_potrf_update<T, NB><<<g2, 256, smem, st>>>(d_mats, j, info, diag_store);
+    if (whole_panel) {
+      k_potrf_panel_smem<T, NB><<<nmat, 512, panel_smem, st>>>(d_mats, j, info, dmin, dmax);
+      if (rem > 0) {
+        dim3 g2(1 + rem * (rem + 1) / 2, nmat);
+        k_potrf_update<T, NB><<<g2, 256, smem, st>>>(d_mats, j, info, nullptr);
+      }
+    } else {
+      dim3 g1(nt - j, nmat);
+      k_potrf_panel<T, NB><<<g1, 256, smem, st>>>(d_mats, j, info, dmin, dmax, diag_store);
+      dim3 g2(1 + rem * (rem + 1) / 2, nmat);
+      k_potrf_update<T, NB><<<g2, 256, smem, st>>>(d_mats, j, info, diag_store);
+    }
   }
   dim3 gz(std::max(1, std::min(1024, ceil_div((long long)nmax * nmax, 256))), nmat);
   k_zero_upper<T><<<gz, 256, 0, st>>>(d_mats);
@@ -425,6 +506,76 @@ void cholesky_solve(const T* L, long long ld, int n, const T* Dinv, T* rhs, T* w
 }
 
 template void factor_diag_inverses<double, 64>(const double*, long long, int, double*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Explicit inverse of a lower-triangular factor by recursive doubling:
+//   inv([A 0; B C]) = [A⁻¹ 0; −C⁻¹ B A⁻¹  C⁻¹],
+// leaves are the 64×64 diagonal tiles (inverted in shared memory); every
+// combination is two DMMA GEMMs with triangular K ranges.
+// ---------------------------------------------------------------------------
+__global__ void k_diag_tiles_to_matrix(const double* Dinv, int n, double* Linv) {
+  const int s = blockIdx.x, s0 = s * 64;
+  const int w = min(64, n - s0);
+  const double* D = Dinv + (size_t)s * 64 * 64;
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int r = e % w, c = e / w;
+    Linv[(size_t)(s0 + c) * n + s0 + r] = D[r + c * 64];
+  }
+}
+
+void trinv_recursive_f64(const double* L, int n, double* Linv, double* Dinv, double* tmp,
+                         cudaStream_t st) {
+  SDPX_CUDA(cudaMemsetAsync(Linv, 0, sizeof(double) * (size_t)n * n, st));
+  factor_diag_inverses<double, 64>(L, n, n, Dinv, st);
+  const int nt = ceil_div(n, 64);
+  k_diag_tiles_to_matrix<<<nt, 256, 0, st>>>(Dinv, n, Linv);
+  SDPX_LAUNCH_CHECK();
+  auto sub = [&](const double* base, int r0, int c0, int rows, int cols, bool kcontig) {
+    Opnd o;
+    o.base = base + r0 + (size_t)c0 * n;
+    o.inner = 1 << 30;
+    o.outer_stride = 0;
+    if (kcontig) {  // operand as B: (kk = row, nn = col)
+      o.kstride = 1;
+      o.inner_stride = n;
+      o.mn_extent = cols;
+      o.k_extent = rows;
+    } else {  // operand as A: (mm = row, kk = col)
+      o.kstride = n;
+      o.inner_stride = 1;
+      o.mn_extent = rows;
+      o.k_extent = cols;
+    }
+    return o;
+  };
+  auto out = [&](double* base, int r0, int c0, int rows, int cols) {
+    OutDesc d;
+    d.base = base + r0 + (size_t)c0 * n;
+    d.row_inner_stride = 1;
+    d.row_outer_stride = 0;
+    d.row_inner = 1 << 30;
+    d.col_inner_stride = n;
+    d.col_outer_stride = 0;
+    d.col_inner = 1 << 30;
+    d.rows = rows;
+    d.cols = cols;
+    return d;
+  };
+  for (int g = 1; g < nt; g *= 2) {
+    for (int i0 = 0; i0 < nt; i0 += 2 * g) {
+      const int a0 = i0 * 64, a1 = std::min(n, (i0 + g) * 64);
+      const int c0 = a1, c1 = std::min(n, (i0 + 2 * g) * 64);
+      if (c0 >= n) continue;
+      const int ra = a1 - a0, rc = c1 - c0;
+      // T = B · A⁻¹   (B = L[c0:c1, a0:a1], A⁻¹ lower: k ≥ col)
+      gemm_f64(sub(L, c0, a0, rc, ra, false), false, sub(Linv, a0, a0, ra, ra, true), true,
+               out(tmp, c0, a0, rc, ra), 1.0, 0.0, KR_B_LOWER, false, st);
+      // Linv[c0:c1, a0:a1] = −C⁻¹ · T   (C⁻¹ lower: k ≤ row)
+      gemm_f64(sub(Linv, c0, c0, rc, rc, false), false, sub(tmp, c0, a0, rc, ra, true), true,
+               out(Linv, c0, a0, rc, ra), -1.0, 0.0, KR_A_LOWER, false, st);
+    }
+  }
+}
 template void cholesky_solve<double, 64>(const double*, long long, int, const double*, double*,
                                          double*, cudaStream_t);
 template void factor_diag_inverses<float, 64>(const float*, long long, int, float*, cudaStream_t);

@@ -35,4 +35,9 @@ template <class T, int NB>
 void cholesky_solve(const T* L, long long ld, int n, const T* Dinv, T* rhs, T* work,
                     cudaStream_t st);
 
+// Linv = L⁻¹ (n×n, column-major, ld n) by recursive doubling over 64×64 tiles.
+// Dinv: ceil(n/64)·64·64 scratch, tmp: n·n scratch.
+void trinv_recursive_f64(const double* L, int n, double* Linv, double* Dinv, double* tmp,
+                         cudaStream_t st);
+
 }  // namespace sdpx

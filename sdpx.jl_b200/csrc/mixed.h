@@ -23,6 +23,10 @@ struct MixedWorkspace {
   void* Lpl[3] = {nullptr, nullptr, nullptr};
   float* partial = nullptr;
   int* err = nullptr;
+  double* L64 = nullptr;    // FP32 factor promoted to FP64
+  double* Linv = nullptr;   // explicit inverse of the factor (preconditioner apply)
+  double* Dinv64 = nullptr;
+  double* tmp64 = nullptr;
   float* Sf = nullptr;      // m×m FP32 factor
   float* Dinv = nullptr;    // FP32 inverses of the 64×64 diagonal tiles
   float* v32 = nullptr;     // m
@@ -35,7 +39,8 @@ struct MixedWorkspace {
   double cond_estimate = 1.0;
   ~MixedWorkspace() {
     for (void* p : {(void*)Sf, (void*)Dinv, (void*)v32, (void*)w32, (void*)info, (void*)dmin,
-                    (void*)dmax, (void*)diag_store, desc, (void*)partial, (void*)err})
+                    (void*)dmax, (void*)diag_store, desc, (void*)partial, (void*)err, (void*)L64,
+                    (void*)Linv, (void*)Dinv64, (void*)tmp64})
       if (p) cudaFree(p);
     for (int i = 0; i < 3; ++i)
       for (void* p : {Apl[i], Ppl[i], Tpl[i], Wpl[i], Lpl[i]})
