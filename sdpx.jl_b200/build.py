@@ -16,7 +16,11 @@ LIB = HERE / "libsdpx_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
-SOURCES = ["api.cu", "blas_f64.cu", "chol.cu", "vec_kernels.cu", "mixed_f32.cu", "schur_bf16.cu"]
+SOURCES = ["api.cu", "blas_f64.cu", "chol.cu", "vec_kernels.cu", "mixed_f32.cu", "schur_bf16.cu",
+           "normal.cu"]
+# Per-file flags.  normal.cu evaluates the reference's scalar cone recurrences
+# and must round every product and sum separately (no FMA contraction).
+FILE_FLAGS = {"normal.cu": ["--fmad=false"]}
 
 
 def nvcc():
@@ -28,14 +32,14 @@ def nvcc():
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
-    deps = sorted(CSRC.glob("*")) + [HERE.parent / "include" / "sdpx_b200.h", Path(__file__)]
+    deps = sorted(CSRC.glob("*")) + sorted((HERE.parent / "include").glob("*.h")) + [Path(__file__)]
     newest_dep = max(p.stat().st_mtime for p in deps)
     objs = []
     for src in SOURCES:
         obj = BUILD / (src + ".o")
         objs.append(obj)
         if force or not obj.exists() or obj.stat().st_mtime < newest_dep:
-            cmd = [nvcc(), *ARCH, *FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
+            cmd = [nvcc(), *ARCH, *FLAGS, *FILE_FLAGS.get(src, []), "-c", str(CSRC / src), "-o", str(obj)]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)

@@ -22,6 +22,7 @@
 #include "../../include/sdpx_b200.h"
 #include "blas_f64.h"
 #include "chol.h"
+#include "dbuf.h"
 #include "mixed.h"
 #include "schur_bf16.h"
 #include "vec_kernels.h"
@@ -46,24 +47,6 @@ bool smem_attr_needed(const void* kern, size_t bytes) {
   return true;
 }
 
-template <class T>
-struct DBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  void alloc(size_t count) {
-    release();
-    if (count == 0) count = 1;
-    SDPX_CUDA(cudaMalloc(&p, count * sizeof(T)));
-    n = count;
-  }
-  void zero(cudaStream_t st) { SDPX_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), st)); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  ~DBuf() { release(); }
-};
 
 struct DenseBlk {
   int user;

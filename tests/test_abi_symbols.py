@@ -1,19 +1,22 @@
-"""The C-ABI library exports every entry point include/sdpx_b200.h declares
+"""The C-ABI library exports every entry point that include/*.h declares
 (CPU-only: loads the shared object, makes no device call)."""
 import ctypes
+import glob
 import os
 import re
 
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "sdpx_b200.h")
+HEADERS = sorted(glob.glob(os.path.join(ROOT, "include", "*.h")))
 LIB = os.path.join(ROOT, "sdpx.jl_b200", "libsdpx_b200.so")
 
 
 def declared_symbols():
-    text = open(HEADER).read()
-    return sorted(set(re.findall(r"\b(sdpx_b200_[a-z0-9_]+)\s*\(", text)))
+    names = set()
+    for h in HEADERS:
+        names |= set(re.findall(r"\b(sdpx_b200_[a-z0-9_]+)\s*\(", open(h).read()))
+    return sorted(names)
 
 
 @pytest.fixture(scope="module")
@@ -27,7 +30,9 @@ def lib():
 def test_header_declares_core_entry_points():
     names = declared_symbols()
     for must in ("sdpx_b200_create", "sdpx_b200_schur_build", "sdpx_b200_factorize",
-                 "sdpx_b200_solve", "sdpx_b200_refine", "sdpx_b200_line_search"):
+                 "sdpx_b200_solve", "sdpx_b200_refine", "sdpx_b200_line_search",
+                 "sdpx_b200_normal_nt_scaling", "sdpx_b200_normal_factorize",
+                 "sdpx_b200_normal_solve"):
         assert must in names
 
 
