@@ -37,6 +37,10 @@ WORKLOADS = {
                      label="dense SDP (SDPA form), one PSD block n=50, m=100"),
 }
 TOL = 1e-8
+# LP standard form + Lorentz cones: the reduced normal matrix Q = Bᵀ D⁻¹ B + δI.
+NORMAL_WORKLOAD = dict(m=3000, n_lp=20000, cones=[64] * 100, density=0.1,
+                       label="LP+SOC reduced normal matrix: 3000 equalities x (20000 LP + "
+                             "100 Lorentz cones x 64) variables, 10%-dense N(0,1)")
 # Iterations of the CPU restatement on sdp_m2000 (seed 0) to 1e-8, used to
 # scale the reference arm's one-iteration samples to a time-to-gap.
 CPU_ITERATIONS_M2000 = 15  # CPU restatement, seed 0, tolerance 1e-8 (measured: Optimal in 15)
@@ -217,6 +221,90 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def bench_normal(args, world, rank, local, dgemm_tflops):
+    """Assembly + factor of the LP+SOC reduced normal matrix (FP64 SYRK of the
+    NT/LP-scaled operand, Cholesky), device-timed on the handle's stream, plus
+    an end-to-end run through the public API from pinned host memory."""
+    import numpy as np
+    import torch
+    from sdpx_b200 import generators as G
+    from sdpx_b200.normal import NormalSystem
+
+    wl = NORMAL_WORKLOAD
+    m = wl["m"]
+    B, w, s, z = G.lp_soc_standard(m, wl["n_lp"], wl["cones"], wl["density"], seed=rank)
+    n = B.shape[0]
+    flops = m * (m + 1.0) * n
+    reg = 1e-9
+    rhs = np.random.default_rng(rank + 1).standard_normal(n + m)
+    with NormalSystem(B, wl["n_lp"], wl["cones"], device=local) as ns:
+        stream = torch.cuda.ExternalStream(ns.stream_handle())
+        assert ns.soc_nt_scaling(s, z)[0]
+        for _ in range(args.warmup):
+            ns.factor_reduced(w, reg)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            ok, att, _ = ns.factor_reduced(w, reg)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        step_ms = ev[0].elapsed_time(ev[1]) / args.steps
+        asm_ms, fac_ms = ns.times()
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            ns.solve_factor(rhs)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        solve_ms = ev[0].elapsed_time(ev[1]) / args.steps
+    # End to end: upload from pinned memory, NT scaling, assembly + factor, solve, read back.
+    Bp = torch.empty((m, n), dtype=torch.float64, pin_memory=True)
+    Bp.numpy()[...] = B.T
+    Bh = Bp.numpy().T
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with NormalSystem(Bh, wl["n_lp"], wl["cones"], device=local) as ns:
+        ns.soc_nt_scaling(s, z)
+        ok_e2e = ns.factor_reduced(w, reg)[0]
+        ns.solve_factor(rhs)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    out = {
+        "workload": wl["label"], "flops_per_assembly": flops,
+        "ms_per_step": max_over_ranks(step_ms, world),
+        "assemble_ms": asm_ms, "factor_ms": fac_ms, "solve_ms": solve_ms,
+        "tflops_assembly": flops / (asm_ms / 1000.0) / 1e12,
+        "frac_of_dgemm_measured": flops / (asm_ms / 1000.0) / 1e12 / dgemm_tflops,
+        "factor_ok": bool(ok), "attempts": att,
+        "e2e": {"value": e2e_s, "unit": "s", "ok": bool(ok_e2e),
+                "h2d_bytes_per_step": int(B.nbytes + w.nbytes + s.nbytes + z.nbytes + rhs.nbytes),
+                "d2h_bytes_per_step": int(rhs.nbytes + 8 * 4 * len(wl["cones"]) + 16 * s.size)},
+        "step": "NT scaling held; one step = pack + scale + FP64 SYRK + Cholesky (factor_reduced)",
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = normal_cpu_baseline(B, w, s, z, wl, reg)
+    return out
+
+
+def normal_cpu_baseline(B, w, s, z, wl, reg):
+    """The oracle's normal matrix (LP: A·D⁻¹·Aᵀ; cones: A_k·Hs_k⁻¹·A_kᵀ with the
+    dense per-cone metric, as the reference's BLAS path forms it) on the host."""
+    import numpy as np
+    from oracle import cone_oracle as O
+    n_lp = wl["n_lp"]
+    _, Dinv, _ = O.lp_pack(w, np.arange(n_lp), np.ones(n_lp), reg)
+    scal, o = [], 0
+    for q in wl["cones"]:
+        ok, wv, lam, eta, eta2 = O.nt_scaling(list(s[o:o + q]), list(z[o:o + q]))
+        scal.append((wv, eta, eta2))
+        o += q
+    A = np.ascontiguousarray(B.T)
+    t0 = time.perf_counter()
+    O.normal_matrix(A, n_lp, wl["cones"], Dinv, scal, reg)
+    dt = time.perf_counter() - t0
+    return {"value": dt * 1000.0, "unit": "ms", "cores": cpu_threads(), "kind": "port",
+            "sample": "one full assembly of the same normal matrix (NumPy/OpenBLAS GEMMs)"}
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -322,6 +410,8 @@ def run_ours(args, world, rank, local):
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(statistics.median(e2e_times), world)
 
+    normal = bench_normal(args, world, rank, local, dgemm_tflops)
+
     peaks, peak_kind = measured_peaks()
     achieved = F / (schur_ms_mixed / 1000.0) / 1e12
     peak = float(peaks.get("bf16_tflops", 1590.0))
@@ -366,6 +456,7 @@ def run_ours(args, world, rank, local):
                     "d2h_bytes_per_step": d2h, "status": r_e2e.status.value},
             "gpu_launches": launches,
             "clocks": clock_info,
+            "normal_lp_soc": normal,
         }
         print(json.dumps(line), flush=True)
     return line

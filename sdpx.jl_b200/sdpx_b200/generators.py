@@ -152,3 +152,29 @@ def _assemble(c, A_sdpx, C_sdpx, blocks, lp) -> SDPProblem:
             Av.append(np.ascontiguousarray(a[:, j:j + 1]))
             Cs.append(np.array([[cvec[j]]]))
     return SDPProblem(np.ascontiguousarray(c), ks, Av, Cs, np.zeros((m, 0)), np.zeros(0))
+
+
+def lp_soc_standard(m: int, n_lp: int, cones: Sequence[int], density: float = 0.1,
+                    seed: int = 0):
+    """Interior point of a standard-form LP + Lorentz-cone system.
+
+    Draw order (numpy default_rng(seed)): A (m × n, n = n_lp + Σq) as N(0,1)
+    entries under a Bernoulli(density) mask (normals first, then the mask);
+    LP slacks x, duals s ~ U(0.5, 1.5); per cone a slack point (t, u) and then
+    a dual point, u ~ N(0,1)^{q−1}, t = 1.5‖u‖ + 1 (strictly inside the cone).
+
+    Returns (B, weights, s, z): B = Aᵀ (n × m, the reduced system's
+    variable-major layout), LP weights s/x, and the cone slack and dual points
+    (Σq each)."""
+    rng = np.random.default_rng(seed)
+    n = n_lp + int(sum(cones))
+    A = rng.standard_normal((m, n)) * (rng.random((m, n)) < density)
+    x = rng.uniform(0.5, 1.5, n_lp)
+    s_lp = rng.uniform(0.5, 1.5, n_lp)
+    sc, zc = [], []
+    for q in cones:
+        for dst in (sc, zc):
+            u = rng.standard_normal(q - 1)
+            dst.append(np.concatenate([[1.5 * np.linalg.norm(u) + 1.0], u]))
+    cat = (lambda v: np.concatenate(v)) if cones else (lambda v: np.zeros(0))
+    return np.asfortranarray(A.T), s_lp / x, cat(sc), cat(zc)

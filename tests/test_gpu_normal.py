@@ -193,9 +193,9 @@ def test_regularization_retries(N):
     B = rng.standard_normal((n_lp, m))
     w = rng.uniform(0.5, 2.0, n_lp)
     with N.NormalSystem(B, n_lp) as ns:
-        ok, att, used = ns.factor_reduced(w, 1e-18, max_attempts=8)
+        ok, att, used = ns.factor_reduced(w, 1e-16, max_attempts=8)
         assert ok and 2 <= att <= 8
-        r = 1e-18
+        r = 1e-16
         for _ in range(att - 1):
             r *= 10.0
         assert used == r
