@@ -191,6 +191,45 @@ int sdpx_b200_launch_count(uint64_t* count);
 int sdpx_b200_gram_noalloc(const double* P, int64_t K, int32_t m, double* S, void* stream);
 const char* sdpx_b200_gram_noalloc_error(void);
 
+/* Cold-path result certificate in original coordinates — SDPX's
+ * `result_certificate` (src/validation.jl:948-1115), optimality kind, n = 0.
+ * Residuals and componentwise backward errors are one device pass each over
+ * the original constraint data; block PSD checks factor symmetrised, shifted
+ * copies with the batched Cholesky (closed forms for 1×1 and 2×2 blocks,
+ * shift bisection for blocks of order ≤ 4, as the reference).  A NaN
+ * residual is reported as +inf (the certificate is invalid either way). */
+typedef struct {
+  int32_t valid;                     /* 1 when failures == 0                       */
+  int32_t failures;                  /* bitmask of SDPX_B200_CERT_*                */
+  int32_t primal_psd_failing_blocks; /* number of X blocks failing the PSD check   */
+  int32_t dual_psd_failing_blocks;   /* number of Y blocks failing the PSD check   */
+  double primal_objective, dual_objective, gap, gap_relative;
+  double primal_residual, dual_residual;               /* max(affine, cone violation) */
+  double primal_affine_residual, dual_affine_residual;
+  double primal_cone_violation, dual_cone_violation;
+  double primal_residual_scaled, dual_residual_scaled;
+  double equality_backward_error, equality_strict_backward_error; /* 0 (no equality rows) */
+  double primal_block_backward_error, primal_block_strict_backward_error;
+  double dual_backward_error, dual_strict_backward_error;
+  double complementarity, complementarity_relative;
+} sdpx_b200_certificate_result;
+
+#define SDPX_B200_CERT_NONFINITE 1
+#define SDPX_B200_CERT_PRIMAL_RESIDUAL 2
+#define SDPX_B200_CERT_EQUALITY_BACKWARD_ERROR 4
+#define SDPX_B200_CERT_PRIMAL_BLOCK_BACKWARD_ERROR 8
+#define SDPX_B200_CERT_DUAL_RESIDUAL 16
+#define SDPX_B200_CERT_DUAL_BACKWARD_ERROR 32
+#define SDPX_B200_CERT_DUALITY_GAP 64
+#define SDPX_B200_CERT_PRIMAL_PSD 128
+#define SDPX_B200_CERT_DUAL_PSD 256
+
+/* x (m), X and Y (stacked, original coordinates).  legacy_gap = 1 selects the
+ * `termination = :legacy` gap test 0 ≤ gap ≤ eps_gap, else gap_rel ≤ eps_gap. */
+int sdpx_b200_certificate(sdpx_b200_handle* h, const double* x, const double* X, const double* Y,
+                          double eps_primal, double eps_dual, double eps_gap, int32_t legacy_gap,
+                          sdpx_b200_certificate_result* out);
+
 /* Cumulative device time per phase (ms) since the last reset:
  * [0] residual+block factor, [1] Schur assembly, [2] KKT factor,
  * [3] solves+refinement, [4] directions+RHS, [5] step length, [6] update. */

@@ -21,6 +21,7 @@
 
 #include "../../include/sdpx_b200.h"
 #include "blas_f64.h"
+#include "certificate.h"
 #include "chol.h"
 #include "dbuf.h"
 #include "mixed.h"
@@ -123,6 +124,7 @@ struct Handle {
 
   // Gershgorin scratch
   DBuf<double> g_cand, g_scale;
+  DBuf<double> cert_part, cert_rows, cert_cols, cert_sym, cert_stats, cert_shift;
   DBuf<long long> g_cand_off;
   DBuf<int> g_nonfinite;
 
@@ -1679,6 +1681,258 @@ struct Handle {
     *dr = h_red[1];
   }
 
+  // ---------------------------------------------------------- certificate --
+  // Per-block PSD check of `_block_psd_certificate` (src/validation.jl:765-904).
+  struct PsdDetail {
+    bool ok = true, finite = true, resolved = true;
+    double symmetry = 0.0, allowed = 0.0, required = 0.0;
+  };
+  // Lower Cholesky pass/fail of (M + Mᵀ)/2 + shift·I for a small block (host,
+  // the unblocked column algorithm; a pivot that is not > 0 fails).
+  static bool small_shifted_chol(const double* M, int k, double shift) {
+    double S[16];
+    for (int c = 0; c < k; ++c)
+      for (int r = 0; r < k; ++r) S[r + c * k] = (M[r + c * k] + M[c + r * k]) / 2.0;
+    for (int i = 0; i < k; ++i) S[i + i * k] += shift;
+    for (int j = 0; j < k; ++j) {
+      double d = S[j + j * k];
+      for (int p = 0; p < j; ++p) d -= S[j + p * k] * S[j + p * k];
+      if (!(d > 0.0)) return false;
+      d = std::sqrt(d);
+      S[j + j * k] = d;
+      for (int i = j + 1; i < k; ++i) {
+        double v = S[i + j * k];
+        for (int p = 0; p < j; ++p) v -= S[i + p * k] * S[j + p * k];
+        S[i + j * k] = v / d;
+      }
+    }
+    return true;
+  }
+  // PSD details of every user block of the stacked device matrix M.
+  std::vector<PsdDetail> psd_certificate(const double* M, double tol) {
+    const double base = std::max(tol, 128.0 * kEps);
+    std::vector<PsdDetail> det(L);
+    size_t nb = dense.size();
+    std::vector<double> stats(3 * nb);
+    if (nb) {
+      cert_block_stats(d_doff.p, d_dk.p, (int)nb, M, cert_stats.p, st);
+      d2h(stats.data(), cert_stats.p, 3 * nb * sizeof(double));
+    }
+    std::vector<double> dv(nd);
+    if (nd) d2h(dv.data(), M + od, nd * sizeof(double));
+    sync();
+    for (int j = 0; j < nd; ++j) {
+      PsdDetail& d = det[diag_user[j]];
+      d.finite = std::isfinite(dv[j]);
+      d.allowed = base * std::max(std::fabs(dv[j]), 1.0);
+      if (!d.finite) {
+        d.ok = false;
+        d.resolved = false;
+        d.required = d.allowed;
+        continue;
+      }
+      d.required = std::max(0.0, -dv[j]);
+      d.ok = d.required <= d.allowed;
+    }
+    std::vector<size_t> chol0;
+    for (size_t b = 0; b < nb; ++b) {
+      PsdDetail& d = det[dense[b].user];
+      const int kk = dense[b].k;
+      d.finite = stats[3 * b] == 0.0;
+      d.allowed = base * std::max(stats[3 * b + 1], 1.0);
+      d.symmetry = stats[3 * b + 2];
+      if (!d.finite) {
+        d.ok = false;
+        d.resolved = false;
+        d.required = d.allowed;
+        continue;
+      }
+      if (kk == 2) {
+        double h4[4];
+        d2h(h4, M + dense[b].off, 4 * sizeof(double));
+        sync();
+        double off = (h4[2] + h4[1]) / 2.0, center = (h4[0] + h4[3]) / 2.0;
+        double radius = std::hypot((h4[0] - h4[3]) / 2.0, off);
+        d.required = std::max(0.0, -(center - radius));
+        d.ok = d.required <= d.allowed && d.symmetry <= d.allowed;
+        continue;
+      }
+      chol0.push_back(b);
+    }
+    // Cholesky of the symmetrised blocks at shift 0, then at the allowed shift.
+    auto factor_with = [&](const std::vector<size_t>& sel, const std::vector<double>& shift_of,
+                           std::vector<int>& info) {
+      std::vector<double> sh(nb, 0.0);
+      for (size_t q = 0; q < sel.size(); ++q) sh[sel[q]] = shift_of[q];
+      h2d(cert_shift.p, sh.data(), nb * sizeof(double));
+      cert_sym_shift(d_doff.p, d_dk.p, (int)nb, kmax, M, cert_shift.p, cert_sym.p, st);
+      std::vector<MatDesc<double>> mats;
+      for (size_t b : sel) mats.push_back({cert_sym.p + dense[b].off, dense[b].k, dense[b].k});
+      std::vector<double> dmn, dmx;
+      potrf_host_list(mats, info, dmn, dmx);
+    };
+    std::vector<int> info;
+    factor_with(chol0, std::vector<double>(chol0.size(), 0.0), info);
+    std::vector<size_t> large_fail;
+    std::vector<double> large_shift;
+    for (size_t q = 0; q < chol0.size(); ++q) {
+      size_t b = chol0[q];
+      PsdDetail& d = det[dense[b].user];
+      if (info[q] == 0) {
+        d.required = 0.0;
+        d.ok = d.symmetry <= d.allowed;
+        continue;
+      }
+      const int kk = dense[b].k;
+      if (kk > 4) {
+        large_fail.push_back(b);
+        large_shift.push_back(d.allowed);
+        continue;
+      }
+      // order 3 or 4: allowed-shift test, doubling and 48-step bisection on the host
+      double h16[16];
+      d2h(h16, M + dense[b].off, kk * kk * sizeof(double));
+      sync();
+      bool allowed_ok = small_shifted_chol(h16, kk, d.allowed);
+      double lower = 0.0, upper = d.allowed;
+      bool resolved = allowed_ok;
+      if (!resolved) {
+        lower = upper;
+        for (int it = 0; it < 64; ++it) {
+          double cand = upper + upper;
+          if (!std::isfinite(cand)) break;
+          upper = cand;
+          if (small_shifted_chol(h16, kk, upper)) {
+            resolved = true;
+            break;
+          }
+          lower = upper;
+        }
+      }
+      if (resolved)
+        for (int it = 0; it < 48; ++it) {
+          double mid = (lower + upper) / 2.0;
+          if (small_shifted_chol(h16, kk, mid))
+            upper = mid;
+          else
+            lower = mid;
+        }
+      d.ok = allowed_ok && d.symmetry <= d.allowed;
+      d.required = upper;
+      d.resolved = resolved;
+    }
+    if (!large_fail.empty()) {
+      factor_with(large_fail, large_shift, info);
+      for (size_t q = 0; q < large_fail.size(); ++q) {
+        PsdDetail& d = det[dense[large_fail[q]].user];
+        d.ok = info[q] == 0 && d.symmetry <= d.allowed;
+        d.required = d.allowed;
+        d.resolved = false;
+      }
+    }
+    return det;
+  }
+  static double psd_violation(const std::vector<PsdDetail>& det, int* failing) {
+    double v = 0.0;
+    *failing = 0;
+    for (const auto& d : det) {
+      if (d.ok) continue;
+      ++*failing;
+      if (!d.finite) v = INFINITY;
+      if (std::isinf(v)) continue;
+      double excess = std::max(0.0, d.symmetry - d.allowed);
+      double shift = d.resolved ? d.required : d.allowed;
+      v = std::max(v, std::max(excess, shift));
+    }
+    return v;
+  }
+
+  void certificate(const double* hx, const double* hX, const double* hY, double ep, double ed,
+                   double eg, int legacy, sdpx_b200_certificate_result* out) {
+    const double* Ause = have_original ? A0.p : A.p;
+    const double* Cuse = have_original ? C0st.p : Cst.p;
+    const double* cuse = have_original ? c0.p : c.p;
+    if (cert_rows.n < (size_t)(3 * K)) {
+      cert_part.alloc((size_t)3 * gemv_chunks * K);
+      cert_rows.alloc((size_t)3 * K);
+      cert_cols.alloc((size_t)3 * m);
+      cert_sym.alloc(K);
+      cert_stats.alloc(3 * std::max<size_t>(dense.size(), 1));
+      cert_shift.alloc(std::max<size_t>(dense.size(), 1));
+    }
+    h2d(work_m.p, hx, m * sizeof(double));
+    h2d(tmpK.p, hX, Ku * sizeof(double));
+    gather(K, d_map.p, tmpK.p, T1.p, st);
+    h2d(tmpK.p, hY, Ku * sizeof(double));
+    gather(K, d_map.p, tmpK.p, T2.p, st);
+    double* rows = cert_rows.p;
+    double* cols = cert_cols.p;
+    cert_primal_rows(Ause, K, m, work_m.p, T1.p, Cuse, cert_part.p, gemv_chunks, rows, rows + K,
+                     rows + 2 * K, st);
+    cert_dual_cols(Ause, K, m, T2.p, cuse, cols, cols + m, cols + 2 * m, st);
+    clear_red(0, 14);
+    absmax(K, rows, red.p + 0, st);
+    absmax(K, rows + K, red.p + 1, st);
+    absmax(K, rows + 2 * K, red.p + 2, st);
+    absmax(m, cols, red.p + 3, st);
+    absmax(m, cols + m, red.p + 4, st);
+    absmax(m, cols + 2 * m, red.p + 5, st);
+    absmax(K, Cuse, red.p + 6, st);
+    absmax(m, cuse, red.p + 7, st);
+    cert_dot(m, work_m.p, cuse, red.p + 8, st);  // c·x, non-finite x
+    cert_dot(K, T2.p, Cuse, red.p + 10, st);     // Σ⟨C_l, Y_l⟩, non-finite Y
+    cert_dot(K, T1.p, T2.p, red.p + 12, st);     // Σ⟨X_l, Y_l⟩, non-finite X
+    double r[14];
+    d2h(r, red.p, sizeof(r));
+    sync();
+    int pfail = 0, dfail = 0;
+    double pviol = psd_violation(psd_certificate(T1.p, std::max(ep, eg)), &pfail);
+    double dviol = psd_violation(psd_certificate(T2.p, std::max(ed, eg)), &dfail);
+
+    sdpx_b200_certificate_result cr{};
+    cr.primal_objective = r[8];
+    cr.dual_objective = r[10];
+    cr.gap = cr.primal_objective - cr.dual_objective;
+    double oscale =
+        std::max(1.0, (std::fabs(cr.primal_objective) + std::fabs(cr.dual_objective)) / 2.0);
+    cr.gap_relative = std::fabs(cr.gap) / oscale;
+    cr.complementarity = r[12];
+    cr.complementarity_relative = std::fabs(cr.complementarity) / oscale;
+    cr.primal_affine_residual = r[0];
+    cr.dual_affine_residual = r[3];
+    cr.primal_cone_violation = pviol;
+    cr.dual_cone_violation = dviol;
+    cr.primal_residual = std::max(r[0], pviol);
+    cr.dual_residual = std::max(r[3], dviol);
+    cr.primal_residual_scaled = cr.primal_residual / (1.0 + r[6]);
+    cr.dual_residual_scaled = cr.dual_residual / (1.0 + r[7]);
+    cr.primal_block_backward_error = r[1];
+    cr.primal_block_strict_backward_error = r[2];
+    cr.dual_backward_error = r[4];
+    cr.dual_strict_backward_error = r[5];
+    cr.primal_psd_failing_blocks = pfail;
+    cr.dual_psd_failing_blocks = dfail;
+    bool primal_finite = std::isfinite(cr.primal_objective) && std::isfinite(cr.primal_residual) &&
+                         r[9] == 0.0 && r[13] == 0.0;
+    bool dual_finite = std::isfinite(cr.dual_objective) && std::isfinite(cr.dual_residual) &&
+                       r[11] == 0.0;
+    bool finite = primal_finite && dual_finite && std::isfinite(cr.gap_relative) &&
+                  std::isfinite(cr.complementarity);
+    bool gap_ok = legacy ? (0.0 <= cr.gap && cr.gap <= eg) : (cr.gap_relative <= eg);
+    int f = 0;
+    if (!finite) f |= SDPX_B200_CERT_NONFINITE;
+    if (!(cr.primal_residual_scaled <= ep)) f |= SDPX_B200_CERT_PRIMAL_RESIDUAL;
+    if (!(cr.primal_block_backward_error <= ep)) f |= SDPX_B200_CERT_PRIMAL_BLOCK_BACKWARD_ERROR;
+    if (!(cr.dual_residual_scaled <= ed)) f |= SDPX_B200_CERT_DUAL_RESIDUAL;
+    if (!(cr.dual_backward_error <= ed)) f |= SDPX_B200_CERT_DUAL_BACKWARD_ERROR;
+    if (!gap_ok) f |= SDPX_B200_CERT_DUALITY_GAP;
+    if (pfail) f |= SDPX_B200_CERT_PRIMAL_PSD;
+    if (dfail) f |= SDPX_B200_CERT_DUAL_PSD;
+    cr.failures = f;
+    cr.valid = f == 0;
+    *out = cr;
+  }
+
   // ------------------------------------------------------- mixed precision --
   void mixed_init();
   void mixed_check_err();
@@ -1897,6 +2151,14 @@ int sdpx_b200_restore_best(sdpx_b200_handle* h) {
 }
 int sdpx_b200_rebuild_slack(sdpx_b200_handle* h, const double* x, double* X) {
   GUARD(h, h->h.rebuild_slack(x, X));
+}
+int sdpx_b200_certificate(sdpx_b200_handle* h, const double* x, const double* X, const double* Y,
+                          double eps_primal, double eps_dual, double eps_gap, int32_t legacy_gap,
+                          sdpx_b200_certificate_result* out) {
+  GUARD(h, {
+    if (!x || !X || !Y || !out) throw std::invalid_argument("certificate: NULL argument");
+    h->h.certificate(x, X, Y, eps_primal, eps_dual, eps_gap, legacy_gap, out);
+  });
 }
 int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const double* X,
                                  const double* Y, double* p, double* d) {

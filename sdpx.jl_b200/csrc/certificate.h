@@ -1,0 +1,35 @@
+// Device passes of the cold-path result certificate (certificate.cu).
+#pragma once
+#include "common.cuh"
+
+namespace sdpx {
+
+// Primal block backward errors over the stacked rows of A (K×m):
+//   R_r = Σ_i A[r,i]·x_i − X_r − C_r,
+//   nominal_r = |C_r| + Σ_i |A[r,i]|,  realized_r = |X_r| + |C_r| + Σ_i |A[r,i]|·|x_i|;
+// writes |R_r|, |R_r|/(nominal+realized) and |R_r|/realized (0/0 → 0, r/0 → ∞).
+// part: 3·chunks·K scratch.
+void cert_primal_rows(const double* A, long long K, int m, const double* x, const double* X,
+                      const double* C, double* part, int chunks, double* absR, double* mixed,
+                      double* strict, cudaStream_t st);
+
+// Dual backward errors per variable i:
+//   v_i = c_i − Σ_r A[r,i]·Y_r, nominal_i = |c_i| + Σ_r |A[r,i]|,
+//   realized_i = |c_i| + Σ_r |A[r,i]|·|Y_r|.
+void cert_dual_cols(const double* A, long long K, int m, const double* Y, const double* c,
+                    double* absv, double* mixed, double* strict, cudaStream_t st);
+
+// out[0] += Σ a·b (single CTA, fixed order within the launch); out[1] += count of
+// non-finite entries of a (as a double).
+void cert_dot(long long n, const double* a, const double* b, double* out, cudaStream_t st);
+
+// Per dense block b (stacked offset off[b], order k[b]) of M: out[3b] = number of
+// non-finite entries, out[3b+1] = max |M|, out[3b+2] = max |M_rc − M_cr|.
+void cert_block_stats(const long long* off, const int* k, int nb, const double* M, double* out,
+                      cudaStream_t st);
+
+// S_b = (M_b + M_bᵀ)/2 + shift[b]·I into the same offsets of S.
+void cert_sym_shift(const long long* off, const int* k, int nb, int kmax, const double* M,
+                    const double* shift, double* S, cudaStream_t st);
+
+}  // namespace sdpx

@@ -4,6 +4,9 @@ Public surface mirrors SDPX's qualified entry points:
 
 * `ingest(c, A, C, B, b)`  ↔ `SDPX.ingest` (src/ingest.jl:620,797)
 * `solve(prob; tolerance)` ↔ `SDPX.solve(prob; tolerance)` (src/solver/interior_point.jl:3654)
+* `certificate(prob, result)` ↔ `result_certificate(prob, result)` (src/validation.jl:948)
+* `normal.NormalSystem`     ↔ the LP standard-form reduced system and Lorentz NT
+  scaling (src/lp_solver.jl, src/soc_lorentz_kernels.jl, src/soc_native.jl)
 
 `solve` runs on the CUDA backend (`libsdpx_b200.so`, sm_100a) and raises if
 the library or a GPU is unavailable; there is no CPU fallback.
@@ -13,22 +16,39 @@ from .driver import SDPResult, Status, solve_with_backend
 from .problem import Equilibration, SDPProblem, ingest, unequilibrate
 
 __all__ = ["SolverOptions", "SDPResult", "Status", "SDPProblem", "Equilibration", "ingest",
-           "unequilibrate", "solve", "solve_with_backend"]
+           "unequilibrate", "solve", "solve_with_backend", "certificate"]
 
 
 def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
           maximum_iterations: int = 200, scaling: str = "auto", device: int = 0,
-          trace=None, **kwargs) -> SDPResult:
+          trace=None, certificate: bool = False, **kwargs) -> SDPResult:
     """Solve `prob` on the B200 (mirrors `SDPX.solve(prob; tolerance)`).
 
     `precision="fp64"` is the plain FP64 device path; `precision="mixed"`
     assembles the Schur complement with split-BF16 tensor-core products, factors
     it in FP32 and refines the Newton system in FP64, switching to the FP64 path
     when the condition estimate or the stagnation detector calls for it.
+    `certificate=True` attaches the device-computed cold-path certificate
+    (`result.certificate`) before the device data is released.
     """
     from .cuda_backend import CudaBackend
     opts = SolverOptions(iter_max=maximum_iterations, scaling=scaling, precision=precision,
                          **kwargs).with_tolerance(tolerance)
     with CudaBackend(prob, precision=precision, device=device,
                      condition_limit=opts.mixed_condition_limit) as be:
-        return solve_with_backend(be, opts, trace=trace)
+        result = solve_with_backend(be, opts, trace=trace)
+        if certificate:
+            result.certificate = be.certificate(result.x, result.X, result.Y, opts.eps_primal,
+                                                opts.eps_dual, opts.eps_gap)
+        return result
+
+
+def certificate(prob: SDPProblem, result: SDPResult, *, eps_primal: float = 1e-10,
+                eps_dual: float = 1e-10, eps_gap: float = 1e-10, legacy_gap: bool = False,
+                device: int = 0) -> dict:
+    """`result_certificate(prob, result, opts)` (src/validation.jl:948-1115) for the
+    optimality kind, recomputed on the B200 from the original data."""
+    from .cuda_backend import CudaBackend
+    with CudaBackend(prob, device=device) as be:
+        return be.certificate(result.x, result.X, result.Y, eps_primal, eps_dual, eps_gap,
+                              legacy_gap)

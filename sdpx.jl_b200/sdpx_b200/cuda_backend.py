@@ -28,6 +28,26 @@ class _Problem(C.Structure):
                 ("Av", C.POINTER(_dp)), ("C", C.POINTER(_dp)), ("c", _dp)]
 
 
+class CertificateResult(C.Structure):
+    """Mirror of sdpx_b200_certificate_result (include/sdpx_b200.h)."""
+    _fields_ = [("valid", C.c_int32), ("failures", C.c_int32),
+                ("primal_psd_failing_blocks", C.c_int32), ("dual_psd_failing_blocks", C.c_int32)] + [
+        (name, C.c_double) for name in (
+            "primal_objective", "dual_objective", "gap", "gap_relative", "primal_residual",
+            "dual_residual", "primal_affine_residual", "dual_affine_residual",
+            "primal_cone_violation", "dual_cone_violation", "primal_residual_scaled",
+            "dual_residual_scaled", "equality_backward_error", "equality_strict_backward_error",
+            "primal_block_backward_error", "primal_block_strict_backward_error",
+            "dual_backward_error", "dual_strict_backward_error", "complementarity",
+            "complementarity_relative")]
+
+
+# Failure bits of the certificate, named as SDPX's failure symbols (src/validation.jl:1069-1096).
+CERTIFICATE_FAILURES = (
+    (1, "nonfinite"), (2, "primal_residual"), (4, "equality_backward_error"),
+    (8, "primal_block_backward_error"), (16, "dual_residual"), (32, "dual_backward_error"),
+    (64, "duality_gap"), (128, "primal_psd"), (256, "dual_psd"))
+
 # name -> argtypes (restype is int unless noted)
 _SIGS = {
     "sdpx_b200_abi_version": [],
@@ -71,6 +91,8 @@ _SIGS = {
     "sdpx_b200_restore_best": [C.c_void_p],
     "sdpx_b200_rebuild_slack": [C.c_void_p, _dp, _dp],
     "sdpx_b200_original_residuals": [C.c_void_p, _dp, _dp, _dp, _dp, _dp],
+    "sdpx_b200_certificate": [C.c_void_p, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double,
+                              C.c_int32, C.POINTER(CertificateResult)],
     "sdpx_b200_phase_times": [C.c_void_p, _dp, C.c_int],
     "sdpx_b200_reset": [C.c_void_p],
     "sdpx_b200_get_precision": [C.c_void_p, _ip, _ip, _dp],
@@ -439,6 +461,22 @@ class CudaBackend:
         a, b = C.c_double(), C.c_double()
         self._call("sdpx_b200_original_residuals", _p(x), _p(Xs), _p(Ys), C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def certificate(self, x, X, Y, eps_primal=1e-10, eps_dual=1e-10, eps_gap=1e-10,
+                    legacy_gap=False) -> dict:
+        """Cold-path certificate of (x, X, Y) against the original data
+        (`result_certificate`, src/validation.jl:948-1115)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        Xs, Ys = self._join(X), self._join(Y)
+        out = CertificateResult()
+        self._call("sdpx_b200_certificate", _p(x), _p(Xs), _p(Ys), float(eps_primal),
+                   float(eps_dual), float(eps_gap), 1 if legacy_gap else 0, C.byref(out))
+        d = {name: getattr(out, name) for name, _ in CertificateResult._fields_}
+        d["valid"] = bool(out.valid)
+        d["failures"] = [name for bit, name in CERTIFICATE_FAILURES if out.failures & bit]
+        d["available"] = True
+        d["kind"] = "optimality"
+        return d
 
     def reset(self):
         """Restore the uploaded data and the start iterate for another solve."""

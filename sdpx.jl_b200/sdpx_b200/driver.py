@@ -59,6 +59,7 @@ class SDPResult:
     history: List[Dict[str, Any]] = field(default_factory=list)
     precision_trace: List[str] = field(default_factory=list)
     seconds: float = 0.0
+    certificate: Optional[Dict[str, Any]] = None
 
     @property
     def relative_gap(self) -> float:

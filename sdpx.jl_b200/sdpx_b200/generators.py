@@ -56,6 +56,17 @@ def toy_t1() -> SDPProblem:
     return ingest([2.0, 3.0], [A], [C])
 
 
+def readme_moment() -> SDPProblem:
+    """The quick-start moment SDP of the reference's README (README.md:44-75):
+    maximize W2 s.t. W0 = 1, W0 − W2 − W4 = 0, [[W0, W2], [W2, W4]] ⪰ 0.
+    The two equality rows eliminate W0 = 1 and W4 = 1 − W2, leaving the core
+    form min −W2 s.t. W2·[[0,1],[1,−1]] − [[−1,0],[0,−1]] ⪰ 0; the optimum is
+    W2 = (√5 − 1)/2 (objective −0.618034…)."""
+    A = np.array([[0.0, 1.0], [1.0, -1.0]])
+    C = np.array([[-1.0, 0.0], [0.0, -1.0]])
+    return _assemble(np.array([-1.0]), [A.reshape(1, 2, 2)], [C], [2], 0)
+
+
 def gate_dense(variables: int = 180, side: int = 8, blocks: int = 3, seed: int = 5) -> SDPProblem:
     """`dense_sdp` (benchmark/gates.jl:151-199).  Julia comprehensions fill
     column-major, so the side×side draw is filled column by column."""
