@@ -112,7 +112,7 @@ struct Handle {
   // batched Cholesky workspace (dense blocks X, Y and line-search trials)
   DBuf<MatDesc<double>> d_descs;
   DBuf<int> d_info;
-  DBuf<double> d_dmin, d_dmax, d_diag_store;
+  DBuf<double> d_dmin, d_dmax;
   size_t desc_cap = 0;
   DBuf<double> trials;
   DBuf<long long> d_trial_off;
@@ -267,7 +267,6 @@ struct Handle {
     d_info.alloc(desc_cap);
     d_dmin.alloc(desc_cap);
     d_dmax.alloc(desc_cap);
-    d_diag_store.alloc(desc_cap * 64 * 64);
   }
 
   // Batched Cholesky of host-described matrices; fills info/dmin/dmax (host).
@@ -283,11 +282,9 @@ struct Handle {
     for (auto& q : mats) nmax = std::max(nmax, q.n);
     h2d(d_descs.p, mats.data(), n * sizeof(MatDesc<double>));
     if (nmax >= 192)
-      potrf_batched<double, 64>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p,
-                                d_diag_store.p, st);
+      potrf_batched<double, 64>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p, st);
     else
-      potrf_batched<double, 32>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p,
-                                d_diag_store.p, st);
+      potrf_batched<double, 32>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p, st);
     d2h(info.data(), d_info.p, n * sizeof(int));
     d2h(dmin.data(), d_dmin.p, n * sizeof(double));
     d2h(dmax.data(), d_dmax.p, n * sizeof(double));
@@ -819,7 +816,7 @@ struct Handle {
       copy_reg(m, S.p, Sf.p, att == 0 ? 0.0 : reg, st);
       ensure_descs(1);
       h2d(d_descs.p, &md, sizeof(md));
-      potrf_batched<double, 64>(d_descs.p, 1, m, d_info.p, d_dmin.p, d_dmax.p, d_diag_store.p, st);
+      potrf_batched<double, 64>(d_descs.p, 1, m, d_info.p, d_dmin.p, d_dmax.p, st);
       info.resize(1);
       dmn.resize(1);
       dmx.resize(1);

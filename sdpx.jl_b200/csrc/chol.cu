@@ -1,130 +1,135 @@
-// Batched blocked Cholesky, triangular inverse and blocked triangular solves
-// (FP64, templated on the element type for the FP32 mixed-precision factor).
+// Cholesky (lower, right-looking, panel width NB).  Orders whose NB-wide
+// panel fits in shared memory (the line-search trials and block factors) take
+// one launch per panel that factors the whole panel in place; larger orders
+// factor the diagonal tile once (one CTA per matrix), solve the rows below it
+// with one thread per row, and update the trailing lower tiles.  A matrix whose
+// pivot is not positive (or NaN) records `info = pivot index + 1` and every
+// later CTA of that matrix returns at once — the no-throw contract of SDPX's
+// `kchol!` (src/kernels/generic.jl:133-155).
 //
-// Cholesky (lower, right-looking, panel width NB): per panel j one launch
-// factors the diagonal tile in shared memory (redundantly in every CTA of the
-// panel) and solves the tiles below it; a second launch applies the rank-NB
-// update to the trailing lower tiles.  A matrix whose pivot is not positive
-// (or NaN) records `info = pivot index + 1` and every later CTA of that matrix
-// returns at once — the no-throw contract of SDPX's `kchol!`
-// (src/kernels/generic.jl:133-155).
+// Column loops inside a tile are laid out warp-per-column, lane-per-row (no
+// per-element index division); every right-looking step rounds exactly as the
+// scalar column algorithm: l_cc = sqrt(a_cc), l_rc = a_rc / l_cc,
+// a_rq -= l_rc · l_qc.
 #include "chol.h"
 #include "blas_f64.h"
 
 namespace sdpx {
 
-template <class T, int NB>
-__device__ bool factor_diag_tile(T* D, int ldd, int w, int* fail_at) {
-  // In-place lower Cholesky of the w×w tile D (shared memory).  Returns false on
-  // a non-positive or NaN pivot and stores its index in *fail_at.
+// Right-looking factor of the leading w columns of the rows×w panel P (shared,
+// column-major, leading dimension ld; rows ≥ w).  Returns the failing column
+// or -1.  All threads of the CTA take part.
+template <class T>
+__device__ int factor_panel_smem(T* P, int ld, int rows, int w) {
   __shared__ int s_fail;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   if (threadIdx.x == 0) s_fail = -1;
   __syncthreads();
   for (int c = 0; c < w; ++c) {
-    T piv = D[c * ldd + c];
+    const T piv = P[c * ld + c];
     if (!(piv > T(0))) {
       if (threadIdx.x == 0) s_fail = c;
-      __syncthreads();
-      break;
+      break;  // uniform: every thread read the same pivot
     }
-    T lc = sqrt(piv);
+    const T lc = sqrt(piv);
     __syncthreads();
-    for (int r = c + 1 + threadIdx.x; r < w; r += blockDim.x) D[c * ldd + r] /= lc;
-    if (threadIdx.x == 0) D[c * ldd + c] = lc;
+    for (int r = c + 1 + threadIdx.x; r < rows; r += blockDim.x) P[c * ld + r] /= lc;
+    if (threadIdx.x == 0) P[c * ld + c] = lc;
     __syncthreads();
-    int rem = w - c - 1;
-    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
-      int r = c + 1 + e % rem, q = c + 1 + e / rem;
-      if (q <= r) D[q * ldd + r] -= D[c * ldd + r] * D[c * ldd + q];
+    for (int q = c + 1 + warp; q < w; q += nwarps) {
+      const T lq = P[c * ld + q];
+      for (int r = q + lane; r < rows; r += 32) P[q * ld + r] -= P[c * ld + r] * lq;
     }
     __syncthreads();
   }
-  *fail_at = s_fail;
-  return s_fail < 0;
+  __syncthreads();
+  return s_fail;
 }
 
+template <class T>
+__device__ void note_pivots(const T* P, int ld, int w, T* dmin, T* dmax, int b) {
+  if (threadIdx.x != 0) return;
+  T lo = dmin[b], hi = dmax[b];
+  for (int c = 0; c < w; ++c) {
+    T v = fabs(P[c * ld + c]);
+    lo = fmin(lo, v);
+    hi = fmax(hi, v);
+  }
+  dmin[b] = lo;
+  dmax[b] = hi;
+}
+
+// Tiled path, step 1: factor the diagonal tile of panel j (one CTA per matrix).
 template <class T, int NB>
-__global__ void k_potrf_panel(const MatDesc<T>* mats, int j, int* info, T* dmin, T* dmax,
-                              T* diag_store) {
-  extern __shared__ __align__(16) unsigned char raw[];
-  T* D = reinterpret_cast<T*>(raw);           // NB × (NB+1), column-major
-  T* Bt = D + NB * (NB + 1);                   // NB × (NB+1)
+__global__ void k_potrf_diag(const MatDesc<T>* mats, int j, int* info, T* dmin, T* dmax) {
+  __shared__ T D[NB * (NB + 1)];
   constexpr int LD = NB + 1;
-  const MatDesc<T> M = mats[blockIdx.y];
-  const int b = blockIdx.y;
+  const int b = blockIdx.x;
+  const MatDesc<T> M = mats[b];
   const int c0 = j * NB;
-  if (c0 >= M.n) return;
-  const int i = j + blockIdx.x;  // row tile
-  const int r0 = i * NB;
-  if (r0 >= M.n) return;
-  if (info[b] != 0) return;
+  if (c0 >= M.n || info[b] != 0) return;
   const int w = min(NB, M.n - c0);
   for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
     int r = e % w, c = e / w;
     D[c * LD + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
   }
-  __syncthreads();
-  int fail_at = -1;
-  bool ok = factor_diag_tile<T, NB>(D, LD, w, &fail_at);
-  if (!ok) {
-    if (i == j && threadIdx.x == 0) info[b] = c0 + fail_at + 1;
+  const int fail = factor_panel_smem<T>(D, LD, w, w);
+  if (fail >= 0) {
+    if (threadIdx.x == 0) info[b] = c0 + fail + 1;
     return;
   }
-  if (i == j) {
-    // Other CTAs of this launch are still reading the unfactored diagonal tile,
-    // so L_jj goes to a per-matrix store; the update launch writes it back.
-    T* ds = diag_store + (size_t)b * NB * NB;
-    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-      int r = e % w, c = e / w;
-      ds[c * NB + r] = (r >= c) ? D[c * LD + r] : T(0);
-    }
-    if (threadIdx.x == 0) {
-      T lo = dmin[b], hi = dmax[b];
-      for (int c = 0; c < w; ++c) {
-        T v = fabs(D[c * LD + c]);
-        lo = fmin(lo, v);
-        hi = fmax(hi, v);
-      }
-      dmin[b] = lo;
-      dmax[b] = hi;
-    }
-    return;
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int r = e % w, c = e / w;
+    if (r >= c) M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] = D[c * LD + r];
   }
-  // Off-diagonal tile: X = B · L_jj^{-T}, right-looking over the columns of the
-  // tile so every step is parallel over its rows and remaining columns.
-  const int h = min(NB, M.n - r0);
-  for (int e = threadIdx.x; e < h * w; e += blockDim.x) {
-    int r = e % h, c = e / h;
-    Bt[c * LD + r] = M.a[(size_t)(c0 + c) * M.ld + (r0 + r)];
-  }
-  __syncthreads();
-  for (int c = 0; c < w; ++c) {
-    const T dcc = D[c * LD + c];
-    for (int r = threadIdx.x; r < h; r += blockDim.x) Bt[c * LD + r] /= dcc;
-    __syncthreads();
-    const int rem = w - c - 1;
-    for (int e = threadIdx.x; e < h * rem; e += blockDim.x) {
-      int r = e % h, q = c + 1 + e / h;
-      Bt[q * LD + r] -= Bt[c * LD + r] * D[c * LD + q];
-    }
-    __syncthreads();
-  }
-  for (int e = threadIdx.x; e < h * w; e += blockDim.x) {
-    int r = e % h, c = e / h;
-    M.a[(size_t)(c0 + c) * M.ld + (r0 + r)] = Bt[c * LD + r];
-  }
+  note_pivots(D, LD, w, dmin, dmax, b);
 }
 
-// Whole panel in shared memory (orders n ≤ PANEL_MAX_ROWS): one CTA per matrix
-// loads rows [c0, n) of panel j, factors it right-looking (pivot, scale, rank-1
-// update of the panel's remaining columns) and writes it back; the trailing
-// tiles are then updated by k_potrf_update.  Replaces the per-tile panel
-// launch for the k ≤ 416 blocks of the line-search trials and block factors.
+// Tiled path, step 2: rows below the diagonal tile, X = B · L_jj^{-T}, one
+// thread per row with the row held in registers (forward substitution in the
+// column order of the right-looking panel factor).
+template <class T, int NB>
+__global__ void __launch_bounds__(128) k_potrf_trsm_rows(const MatDesc<T>* mats, int j,
+                                                         const int* info) {
+  __shared__ T D[NB * (NB + 1)];
+  constexpr int LD = NB + 1;
+  const int b = blockIdx.y;
+  const MatDesc<T> M = mats[b];
+  const int c0 = j * NB;
+  if (c0 >= M.n || info[b] != 0) return;
+  const int w = min(NB, M.n - c0);
+  const int first = c0 + w + blockIdx.x * blockDim.x;
+  if (first >= M.n) return;
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int r = e % w, c = e / w;
+    D[c * LD + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
+  }
+  __syncthreads();
+  const int r = first + threadIdx.x;
+  if (r >= M.n) return;
+  T x[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) x[c] = (c < w) ? M.a[(size_t)(c0 + c) * M.ld + r] : T(0);
+#pragma unroll
+  for (int c = 0; c < NB; ++c) {
+    if (c < w) {
+      x[c] /= D[c * LD + c];
+#pragma unroll
+      for (int q = c + 1; q < NB; ++q) x[q] -= x[c] * D[c * LD + q];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NB; ++c)
+    if (c < w) M.a[(size_t)(c0 + c) * M.ld + r] = x[c];
+}
+
+// Whole panel in shared memory (orders n with n·NB elements ≤ 224 KB): one CTA
+// per matrix loads rows [c0, n) of panel j, factors it in place and writes it
+// back; the trailing tiles are then updated by k_potrf_update.
 template <class T, int NB>
 __global__ void k_potrf_panel_smem(const MatDesc<T>* mats, int j, int* info, T* dmin, T* dmax) {
   extern __shared__ __align__(16) unsigned char raw[];
-  T* Pn = reinterpret_cast<T*>(raw);  // rows × NB, column-major with ld = rows_pad
-  __shared__ int s_fail;
+  T* Pn = reinterpret_cast<T*>(raw);  // rows × NB, column-major with ld = rows | 1
   const MatDesc<T> M = mats[blockIdx.x];
   const int b = blockIdx.x;
   const int c0 = j * NB;
@@ -136,52 +141,21 @@ __global__ void k_potrf_panel_smem(const MatDesc<T>* mats, int j, int* info, T* 
     int r = e % rows, c = e / rows;
     Pn[c * ld + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
   }
-  if (threadIdx.x == 0) s_fail = -1;
-  __syncthreads();
-  for (int c = 0; c < w; ++c) {
-    const T piv = Pn[c * ld + c];
-    if (!(piv > T(0))) {
-      if (threadIdx.x == 0) s_fail = c;
-      break;  // uniform: every thread read the same pivot
-    }
-    const T lc = sqrt(piv);
-    __syncthreads();
-    for (int r = c + 1 + threadIdx.x; r < rows; r += blockDim.x) Pn[c * ld + r] /= lc;
-    if (threadIdx.x == 0) Pn[c * ld + c] = lc;
-    __syncthreads();
-    const int rem = w - c - 1;
-    const int height = rows - c - 1;
-    for (int e = threadIdx.x; e < height * rem; e += blockDim.x) {
-      int r = c + 1 + e % height, q = c + 1 + e / height;
-      if (r >= q) Pn[q * ld + r] -= Pn[c * ld + r] * Pn[c * ld + q];
-    }
-    __syncthreads();
-  }
-  __syncthreads();
-  if (s_fail >= 0) {
-    if (threadIdx.x == 0) info[b] = c0 + s_fail + 1;
+  const int fail = factor_panel_smem<T>(Pn, ld, rows, w);
+  if (fail >= 0) {
+    if (threadIdx.x == 0) info[b] = c0 + fail + 1;
     return;
   }
   for (int e = threadIdx.x; e < rows * w; e += blockDim.x) {
     int r = e % rows, c = e / rows;
     M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] = (r >= c) ? Pn[c * ld + r] : T(0);
   }
-  if (threadIdx.x == 0) {
-    T lo = dmin[b], hi = dmax[b];
-    for (int c = 0; c < w; ++c) {
-      T v = fabs(Pn[c * ld + c]);
-      lo = fmin(lo, v);
-      hi = fmax(hi, v);
-    }
-    dmin[b] = lo;
-    dmax[b] = hi;
-  }
+  note_pivots(Pn, ld, w, dmin, dmax, b);
 }
 
 // Trailing update A[i,q] -= L[i,j] L[q,j]^T for j < q <= i (lower tiles).
 template <class T, int NB>
-__global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info,
-                               const T* diag_store) {
+__global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info) {
   extern __shared__ __align__(16) unsigned char raw[];
   T* La = reinterpret_cast<T*>(raw);  // NB × (NB+1): rows of tile i, panel j
   T* Lb = La + NB * (NB + 1);          // rows of tile q
@@ -191,20 +165,8 @@ __global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info,
   const int nt = (M.n + NB - 1) / NB;
   if (j >= nt) return;
   const int rem = nt - j - 1;
-  const int t = blockIdx.x;
-  if (t == 0) {
-    // CTA 0 writes back the factored diagonal tile of panel j (tiled panel path).
-    if (!diag_store) return;
-    const int c0 = j * NB, w = min(NB, M.n - c0);
-    const T* ds = diag_store + (size_t)blockIdx.y * NB * NB;
-    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-      int r = e % w, c = e / w;
-      M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] = ds[c * NB + r];
-    }
-    return;
-  }
-  if (rem <= 0 || t - 1 >= rem * (rem + 1) / 2) return;
-  const int u = t - 1;
+  const int u = blockIdx.x;
+  if (rem <= 0 || u >= rem * (rem + 1) / 2) return;
   int a = (int)((sqrt(8.0 * u + 1.0) - 1.0) * 0.5);
   while ((a + 1) * (a + 2) / 2 <= u) ++a;
   while (a * (a + 1) / 2 > u) --a;
@@ -268,10 +230,9 @@ __global__ void k_init_stats(int n, int* info, T* dmin, T* dmax) {
 
 template <class T, int NB>
 void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* dmin, T* dmax,
-                   T* diag_store, cudaStream_t st) {
+                   cudaStream_t st) {
   if (nmat == 0 || nmax == 0) return;
   const size_t smem = 2 * sizeof(T) * NB * (NB + 1);
-  ensure_smem(k_potrf_panel<T, NB>, smem);
   ensure_smem(k_potrf_update<T, NB>, smem);
   k_init_stats<T><<<ceil_div(nmat, 128), 128, 0, st>>>(nmat, info, dmin, dmax);
   const int nt = ceil_div(nmax, NB);
@@ -279,32 +240,39 @@ void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* d
   const size_t panel_smem = sizeof(T) * (size_t)rows_pad * NB;
   const bool whole_panel = panel_smem <= 224 * 1024;
   if (whole_panel) ensure_smem(k_potrf_panel_smem<T, NB>, panel_smem);
+  int launches = 2;
   for (int j = 0; j < nt; ++j) {
     int rem = nt - j - 1;
     if (whole_panel) {
       k_potrf_panel_smem<T, NB><<<nmat, 512, panel_smem, st>>>(d_mats, j, info, dmin, dmax);
-      if (rem > 0) {
-        dim3 g2(1 + rem * (rem + 1) / 2, nmat);
-        k_potrf_update<T, NB><<<g2, 256, smem, st>>>(d_mats, j, info, nullptr);
-      }
+      ++launches;
     } else {
-      dim3 g1(nt - j, nmat);
-      k_potrf_panel<T, NB><<<g1, 256, smem, st>>>(d_mats, j, info, dmin, dmax, diag_store);
-      dim3 g2(1 + rem * (rem + 1) / 2, nmat);
-      k_potrf_update<T, NB><<<g2, 256, smem, st>>>(d_mats, j, info, diag_store);
+      k_potrf_diag<T, NB><<<nmat, 256, 0, st>>>(d_mats, j, info, dmin, dmax);
+      ++launches;
+      const int below = nmax - (j + 1) * NB;
+      if (below > 0) {
+        dim3 gt(ceil_div(below, 128), nmat);
+        k_potrf_trsm_rows<T, NB><<<gt, 128, 0, st>>>(d_mats, j, info);
+        ++launches;
+      }
+    }
+    if (rem > 0) {
+      dim3 g2(rem * (rem + 1) / 2, nmat);
+      k_potrf_update<T, NB><<<g2, 256, smem, st>>>(d_mats, j, info);
+      ++launches;
     }
   }
   dim3 gz(std::max(1, std::min(1024, ceil_div((long long)nmax * nmax, 256))), nmat);
   k_zero_upper<T><<<gz, 256, 0, st>>>(d_mats);
-  SDPX_LAUNCH_CHECK_N(2 + 2 * nt);
+  SDPX_LAUNCH_CHECK_N(launches);
 }
 
 template void potrf_batched<double, 32>(const MatDesc<double>*, int, int, int*, double*, double*,
-                                        double*, cudaStream_t);
+                                        cudaStream_t);
 template void potrf_batched<double, 64>(const MatDesc<double>*, int, int, int*, double*, double*,
-                                        double*, cudaStream_t);
+                                        cudaStream_t);
 template void potrf_batched<float, 64>(const MatDesc<float>*, int, int, int*, float*, float*,
-                                       float*, cudaStream_t);
+                                       cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Triangular inverse W = L^{-1} (lower), blocked by NB.  Step 0 inverts every

@@ -34,12 +34,11 @@ struct MixedWorkspace {
   int* info = nullptr;
   float* dmin = nullptr;
   float* dmax = nullptr;
-  float* diag_store = nullptr;
   void* desc = nullptr;
   double cond_estimate = 1.0;
   ~MixedWorkspace() {
     for (void* p : {(void*)Sf, (void*)Dinv, (void*)v32, (void*)w32, (void*)info, (void*)dmin,
-                    (void*)dmax, (void*)diag_store, desc, (void*)partial, (void*)err, (void*)L64,
+                    (void*)dmax, desc, (void*)partial, (void*)err, (void*)L64,
                     (void*)Linv, (void*)Dinv64, (void*)tmp64})
       if (p) cudaFree(p);
     for (int i = 0; i < 3; ++i)

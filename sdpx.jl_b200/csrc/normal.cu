@@ -282,7 +282,7 @@ struct NormalHandle {
   DBuf<int> d_dim, d_row, d_ok, d_info;
   DBuf<double> B, Bh, coef, weights, D, Dinv, Dis, w, lam, eta, eta2, s, z, v, out;
   DBuf<double> Q, F, Finv_diag, partial, rhs, t, red, work, u, gemv_part;
-  DBuf<double> dmin, dmax, diag_store;
+  DBuf<double> dmin, dmax;
   DBuf<MatDesc<double>> descs;
   SyrkPlan plan;
   int gemv_chunks = 8;
@@ -354,7 +354,6 @@ struct NormalHandle {
     d_info.alloc(1);
     dmin.alloc(1);
     dmax.alloc(1);
-    diag_store.alloc(64 * 64);
     descs.alloc(1);
     sync();
   }
@@ -503,7 +502,7 @@ struct NormalHandle {
       }
       MatDesc<double> md{F.p, m, m};
       h2d(descs.p, &md, sizeof(md));
-      potrf_batched<double, 64>(descs.p, 1, m, d_info.p, dmin.p, dmax.p, diag_store.p, st);
+      potrf_batched<double, 64>(descs.p, 1, m, d_info.p, dmin.p, dmax.p, st);
       SDPX_CUDA(cudaEventRecord(ev[2], st));
       d2h(&info, d_info.p, sizeof(int));
       sync();
