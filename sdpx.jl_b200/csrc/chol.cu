@@ -19,31 +19,89 @@ namespace sdpx {
 // Right-looking factor of the leading w columns of the rows×w panel P (shared,
 // column-major, leading dimension ld; rows ≥ w).  Returns the failing column
 // or -1.  All threads of the CTA take part.
+//
+// Blocked by 8 columns: every thread factors the 8×8 diagonal block in its own
+// registers (identical arithmetic in every thread, so the pivot test is
+// uniform), thread 0 stores it, each row below the block is solved in
+// registers (x = a · L_bb^{-T}), and the trailing columns of the panel receive
+// the rank-8 update with the block's rows read as warp broadcasts.  Every
+// element sees its updates in increasing column order, as in the unblocked
+// right-looking loop (l_cc = sqrt(a_cc), l_rc = a_rc / l_cc, a_rq -= l_rc·l_qc).
 template <class T>
 __device__ int factor_panel_smem(T* P, int ld, int rows, int w) {
-  __shared__ int s_fail;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  if (threadIdx.x == 0) s_fail = -1;
   __syncthreads();
-  for (int c = 0; c < w; ++c) {
-    const T piv = P[c * ld + c];
-    if (!(piv > T(0))) {
-      if (threadIdx.x == 0) s_fail = c;
-      break;  // uniform: every thread read the same pivot
+  for (int kb = 0; kb < w; kb += 8) {
+    const int kw = min(8, w - kb);
+    // 8×8 diagonal block in registers (lower part used)
+    T D[8][8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        D[c][r] = (c < kw && r < kw && r >= c) ? P[(kb + c) * ld + kb + r] : T(0);
+    int fail = -1;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if (c < kw && fail < 0) {
+        const T piv = D[c][c];
+        if (!(piv > T(0))) {
+          fail = c;
+        } else {
+          const T lc = sqrt(piv);
+          D[c][c] = lc;
+#pragma unroll
+          for (int r = c + 1; r < 8; ++r) D[c][r] /= lc;
+#pragma unroll
+          for (int q = c + 1; q < 8; ++q)
+#pragma unroll
+            for (int r = q; r < 8; ++r) D[q][r] -= D[c][r] * D[c][q];
+        }
+      }
     }
-    const T lc = sqrt(piv);
+    if (fail >= 0) return kb + fail;  // uniform: every thread computed the same block
+    __syncthreads();                   // every thread has read the block
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+          if (c < kw && r < kw && r >= c) P[(kb + c) * ld + kb + r] = D[c][r];
+    }
+    // rows below the block: x = a · L_bb^{-T}
+    for (int r = kb + kw + threadIdx.x; r < rows; r += blockDim.x) {
+      T x[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) x[c] = (c < kw) ? P[(kb + c) * ld + r] : T(0);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < kw) {
+          x[c] /= D[c][c];
+#pragma unroll
+          for (int q = c + 1; q < 8; ++q) x[q] -= x[c] * D[c][q];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c < kw) P[(kb + c) * ld + r] = x[c];
+    }
     __syncthreads();
-    for (int r = c + 1 + threadIdx.x; r < rows; r += blockDim.x) P[c * ld + r] /= lc;
-    if (threadIdx.x == 0) P[c * ld + c] = lc;
-    __syncthreads();
-    for (int q = c + 1 + warp; q < w; q += nwarps) {
-      const T lq = P[c * ld + q];
-      for (int r = q + lane; r < rows; r += 32) P[q * ld + r] -= P[c * ld + r] * lq;
+    // trailing panel columns q ∈ [kb+kw, w), rows r ≥ q
+    for (int r = kb + kw + threadIdx.x; r < rows; r += blockDim.x) {
+      T x[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) x[c] = (c < kw) ? P[(kb + c) * ld + r] : T(0);
+      const int qe = min(w, r + 1);
+      for (int q = kb + kw; q < qe; ++q) {
+        T a = P[q * ld + r];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < kw) a -= x[c] * P[(kb + c) * ld + q];
+        P[q * ld + r] = a;
+      }
     }
     __syncthreads();
   }
-  __syncthreads();
-  return s_fail;
+  return -1;
 }
 
 template <class T>
@@ -127,7 +185,7 @@ __global__ void __launch_bounds__(128) k_potrf_trsm_rows(const MatDesc<T>* mats,
 // per matrix loads rows [c0, n) of panel j, factors it in place and writes it
 // back; the trailing tiles are then updated by k_potrf_update.
 template <class T, int NB>
-__global__ void k_potrf_panel_smem(const MatDesc<T>* mats, int j, int* info, T* dmin, T* dmax) {
+__global__ void __launch_bounds__(512) k_potrf_panel_smem(const MatDesc<T>* mats, int j, int* info, T* dmin, T* dmax) {
   extern __shared__ __align__(16) unsigned char raw[];
   T* Pn = reinterpret_cast<T*>(raw);  // rows × NB, column-major with ld = rows | 1
   const MatDesc<T> M = mats[blockIdx.x];
