@@ -188,6 +188,25 @@ struct Handle {
   }
 
   void sync() { SDPX_CUDA(cudaStreamSynchronize(st)); }
+
+  // Residual reuse across consecutive C-ABI calls.  Every entry point bumps
+  // call_seq; a call that leaves ρ = r − S·dx consistent with dx records
+  // rho_seq = call_seq and the norm.  Only the very next call, and only the
+  // refinement and the acceptance-gate residual, may take that norm instead of
+  // applying the operator again (the operator is deterministic, so the value is
+  // identical).
+  unsigned long long call_seq = 0, rho_seq = ~0ull;
+  double rho_norm = 0.0;
+  void mark_rho_fresh(double norm) {
+    rho_seq = call_seq;
+    rho_norm = norm;
+  }
+  bool take_rho_cache(double* norm) {
+    bool hit = rho_seq + 1 == call_seq;
+    rho_seq = ~0ull;
+    if (hit) *norm = rho_norm;
+    return hit;
+  }
   void d2h(void* dst, const void* src, size_t bytes) {
     SDPX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
   }
@@ -857,9 +876,13 @@ struct Handle {
   // path: S is reassembled and factored in FP64 and dx re-solved.
   void mixed_guard() {
     double res, rn;
-    direction_residual(&res, &rn);
+    direction_residual(&res, &rn, false);
+    rho_seq = ~0ull;  // re-marked below only if dx ends consistent with ρ
     const double target = 1e-8 * std::max(rn, 1.0);
-    if (std::isfinite(res) && res <= target) return;
+    if (std::isfinite(res) && res <= target) {
+      mark_rho_fresh(res);
+      return;
+    }
     int cap = std::min(mixed_predicted_steps, 32);
     bool ok = false;
     if (std::isfinite(res)) {
@@ -881,7 +904,10 @@ struct Handle {
         }
       }
     }
-    if (!ok) switch_to_fp64_now();
+    if (!ok)
+      switch_to_fp64_now();
+    else
+      mark_rho_fresh(res);
   }
   // Leave mixed mode for good within the current iteration: FP64 Schur,
   // FP64 factor, and re-solve of the current right-hand side.
@@ -904,18 +930,23 @@ struct Handle {
     }
     symv_full(m, S.p, dx.p, -1.0, r.p, 1.0, rho.p, st);
   }
-  void direction_residual(double* res, double* rnorm) {
+  void direction_residual(double* res, double* rnorm, bool allow_cache = true) {
     PhaseScope ps(this, 3);
-    apply_residual();
+    double cached = 0.0;
+    const bool hit = allow_cache && take_rho_cache(&cached);
+    if (!hit) apply_residual();
     clear_red(0, 2);
-    absmax(m, rho.p, red.p + 0, st);
+    if (!hit) absmax(m, rho.p, red.p + 0, st);
     absmax(m, r.p, red.p + 1, st);
     d2h(h_red, red.p, 2 * sizeof(double));
     sync();
-    *res = h_red[0];
+    *res = hit ? cached : h_red[0];
     *rnorm = h_red[1];
+    mark_rho_fresh(*res);
   }
-  double residual_norm_only() {
+  double residual_norm_only(bool allow_cache = false) {
+    double cached = 0.0;
+    if (allow_cache && take_rho_cache(&cached)) return cached;
     apply_residual();
     clear_red(0, 1);
     absmax(m, rho.p, red.p, st);
@@ -937,29 +968,34 @@ struct Handle {
       clear_red(1, 1);
       absmax(m, r.p, red.p + 1, st);
       double abstol = rel * std::max(read_red(1), 1.0);
-      residual = residual_norm_only();
+      residual = residual_norm_only(true);
+      bool consistent = true;
       for (int s = 0; s < 32; ++s) {
         if (residual <= abstol) break;
         correction();
         double corr = residual_norm_only();
         if (!std::isfinite(corr) || corr >= residual) {
           d2d(dx.p, dxbest.p, m * sizeof(double));
+          consistent = false;
           break;
         }
         ++steps;
         residual = corr;
       }
+      if (consistent) mark_rho_fresh(residual);
       *steps_out = steps;
       *res_out = residual;
       return;
     }
+    bool consistent = true;
     if (policy == 0) {
-      residual = residual_norm_only();
+      residual = residual_norm_only(true);
       for (int s = 0; s < fixed_steps; ++s) {
         correction();
         double corr = residual_norm_only();
         if (!std::isfinite(corr) || corr > residual) {
           d2d(dx.p, dxbest.p, m * sizeof(double));
+          consistent = false;
           break;
         }
         ++steps;
@@ -976,13 +1012,14 @@ struct Handle {
       absmax(m, r.p, red.p + 1, st);
       double rn = read_red(1);
       double abstol = rel * std::max(rn, 1.0);
-      residual = residual_norm_only();
+      residual = residual_norm_only(true);
       for (int s = 0; s < cap; ++s) {
         if (residual <= abstol) break;
         correction();
         double corr = residual_norm_only();
         if (!std::isfinite(corr) || corr > residual) {
           d2d(dx.p, dxbest.p, m * sizeof(double));
+          consistent = false;
           break;
         }
         ++steps;
@@ -991,6 +1028,7 @@ struct Handle {
         if (small) break;
       }
     }
+    if (consistent) mark_rho_fresh(residual);
     *steps_out = steps;
     *res_out = residual;
   }
@@ -1960,6 +1998,7 @@ static thread_local std::string g_create_error;
   do {                                                    \
     if (!(hh)) return -1;                                 \
     try {                                                 \
+      ++(hh)->h.call_seq;                                 \
       SDPX_CUDA(cudaSetDevice((hh)->h.dev));              \
       body;                                               \
       return 0;                                           \

@@ -14,6 +14,11 @@
 //   S   = P̂ᵀ P̂ (lower)     (A, B: variables' stacked P̂ columns, split K)
 // CTA tile 128×128, K tile 64, two smem stages of 6 operand tiles (96 KB each),
 // MMA M=128 N=128 K=16 issued by one thread, completion tracked by mbarriers.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "schur_bf16.h"
 #include "umma.cuh"
 
@@ -241,6 +246,131 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (warp == 0) umma::tmem_dealloc(tmem, 128);
 }
 
+// ---------------------------------------------------------------------------
+// Lower SYRK S = P̂ᵀP̂ fed by TMA.  One CTA per (K chunk, lower 128×128 tile),
+// 128 threads: thread 0 produces (24 TMA boxes of 128 rows × 32 BF16 per stage:
+// three planes of the A rows and of the B rows, 64-byte swizzle), thread 32
+// issues the 12 MMAs of a stage (2 K steps × the 6 plane products) and commits
+// them to the stage's "empty" barrier, all four warps then drain the FP32 TMEM
+// tile.  Four 48 KB stages.  Rows beyond m and K beyond Kp arrive as zeros
+// (TMA out-of-bounds fill).  Every wait is bounded and records a device error
+// instead of spinning; the producer waits for all of its own copies before the
+// CTA leaves.
+// ---------------------------------------------------------------------------
+constexpr int SK = 32;                          // K per stage
+constexpr int SNST = 4;                         // stages
+constexpr int SPLANE_BYTES = TM * SK * 2;       // 8 KB: 128 rows × 64 B
+constexpr int SSTAGE_BYTES = 6 * SPLANE_BYTES;  // 48 KB
+constexpr size_t SSMEM_BYTES = SNST * SSTAGE_BYTES + 1024 + 256;
+
+struct SyrkMaps {
+  CUtensorMap plane[3];
+};
+
+struct SyrkShared {
+  uint64_t full[SNST], empty[SNST], done;
+  uint32_t tmem;
+};
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_split_syrk_tma(const __grid_constant__ SyrkMaps maps, int ntri, int kchunk, int Ktot,
+                     float* partial, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  SyrkShared* sh = reinterpret_cast<SyrkShared*>(smem + SNST * SSTAGE_BYTES);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < SNST; ++s) {
+      umma::mbar_init(&sh->full[s], 1);
+      umma::mbar_init(&sh->empty[s], 1);
+    }
+    umma::mbar_init(&sh->done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  if (warp == 0) umma::tmem_alloc(&sh->tmem, 128);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = sh->tmem;
+
+  const int u = blockIdx.x;
+  const int chunk = u / ntri, tri = u % ntri;
+  int ti, tj;
+  tri_index(tri, ti, tj);
+  const int r0 = ti * TM, c0 = tj * TN;
+  const int kb = chunk * kchunk;
+  const int ke = min(Ktot, kb + kchunk);
+  const int ntiles = ke > kb ? (ke - kb + SK - 1) / SK : 0;
+
+  if (threadIdx.x == 0) {
+    // producer
+    int issued = 0;
+    for (int t = 0; t < ntiles; ++t) {
+      const int s = t % SNST;
+      if (t >= SNST && !umma::mbar_wait_bounded(&sh->empty[s], ((t / SNST) - 1) & 1, err)) break;
+      umma::mbar_expect_tx(&sh->full[s], SSTAGE_BYTES);
+      const uint32_t base = umma::smem_u32(smem + s * SSTAGE_BYTES);
+      const int k = kb + t * SK;
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        umma::tma_load_2d(base + p * SPLANE_BYTES, &maps.plane[p], k, r0, &sh->full[s]);
+        umma::tma_load_2d(base + (3 + p) * SPLANE_BYTES, &maps.plane[p], k, c0, &sh->full[s]);
+      }
+      ++issued;
+    }
+    // drain: every issued stage has landed before the CTA may leave
+    for (int t = max(0, issued - SNST); t < issued; ++t)
+      umma::mbar_wait_bounded(&sh->full[t % SNST], (t / SNST) & 1, err);
+  } else if (threadIdx.x == 32) {
+    // MMA issuer
+    constexpr uint32_t IDESC = umma::idesc_bf16_f32(TM, TN);
+    const int pa[6] = {0, 0, 1, 0, 1, 2};
+    const int pb[6] = {0, 1, 0, 2, 1, 0};
+    for (int t = 0; t < ntiles; ++t) {
+      const int s = t % SNST;
+      if (!umma::mbar_wait_bounded(&sh->full[s], (t / SNST) & 1, err)) break;
+      umma::fence_after_sync();
+      const uint32_t base = umma::smem_u32(smem + s * SSTAGE_BYTES);
+#pragma unroll
+      for (int ks = 0; ks < SK / 16; ++ks) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const uint64_t ad = umma::smem_desc_sw64(base + pa[q] * SPLANE_BYTES + ks * 32);
+          const uint64_t bd = umma::smem_desc_sw64(base + (3 + pb[q]) * SPLANE_BYTES + ks * 32);
+          umma::mma_bf16(tmem, ad, bd, IDESC, (t > 0 || ks > 0 || q > 0) ? 1u : 0u);
+        }
+      }
+      umma::commit(&sh->empty[s]);
+    }
+    umma::commit(&sh->done);  // arrives once every MMA issued above has completed
+  }
+  __syncwarp();
+  const bool ok = umma::mbar_wait_bounded(&sh->done, 0, err);
+  umma::fence_after_sync();
+  const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+
+  // Epilogue: warp w owns accumulator rows [32w, 32w+32) (TMEM lanes).
+  if (all_ok && ntiles > 0) {
+    const int row = warp * 32 + lane;
+    for (int cb = 0; cb < TN; cb += 32) {
+      float v[32];
+      umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
+      float* dst = partial + (size_t)blockIdx.x * TM * TN + (size_t)row * TN + cb;
+#pragma unroll
+      for (int q = 0; q < 32; q += 4)
+        *reinterpret_cast<float4*>(dst + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+    }
+  } else if (ntiles == 0) {
+    const int row = warp * 32 + lane;
+    float* dst = partial + (size_t)blockIdx.x * TM * TN + (size_t)row * TN;
+    for (int q = 0; q < TN; q += 4) *reinterpret_cast<float4*>(dst + q) = make_float4(0, 0, 0, 0);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, 128);
+}
+
 __global__ void k_reduce_partials(const float* partial, int ntri, int nchunk, int m, double* S) {
   const int tri = blockIdx.x;
   int ti, tj;
@@ -344,13 +474,49 @@ SplitSyrkPlan plan_split_syrk(int m, long long Kp, int sm_count) {
   return p;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  if (!fn) throw CudaError("cuTensorMapEncodeTiled is not available");
+  return fn;
+}
+
+// Tensor map of one plane: rows × Kp BF16, row-major; box 32 × 128, 64-byte swizzle.
+static void encode_plane_map(CUtensorMap* map, const __nv_bfloat16* plane, int rows, long long Kp) {
+  if ((reinterpret_cast<uintptr_t>(plane) & 15) != 0 || (Kp * 2) % 16 != 0)
+    throw std::invalid_argument("split SYRK: plane base or row pitch not 16-byte aligned");
+  cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
+  cuuint32_t box[2] = {(cuuint32_t)SK, (cuuint32_t)TM};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = tensor_map_encoder()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                                    const_cast<__nv_bfloat16*>(plane), dims, strides, box, estr,
+                                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+}
+
 void split_syrk(const PlaneOpnd& P, int m, int Kp, const SplitSyrkPlan& plan, float* partial,
                 double* S, int* err, cudaStream_t st) {
-  ensure_smem(k_split_gemm<0>, SMEM_BYTES);
-  OutMap none{};
+  if (P.rows.is != Kp || P.rows.base != 0 || Kp % SK != 0 || plan.kchunk % SK != 0)
+    throw std::invalid_argument("split SYRK: planes must be m × Kp row-major, Kp and chunks ≡ 0 mod 32");
+  SyrkMaps maps;
+  for (int p = 0; p < 3; ++p) encode_plane_map(&maps.plane[p], P.plane[p], m, Kp);
+  ensure_smem(k_split_syrk_tma, SSMEM_BYTES);
   const int units = plan.ntri * plan.nchunk;
-  k_split_gemm<0><<<units, NTHREADS, SMEM_BYTES, st>>>(P, P, none, 0, Kp, plan.ntri, plan.kchunk,
-                                                       partial, err);
+  k_split_syrk_tma<<<units, NTHREADS, SSMEM_BYTES, st>>>(maps, plan.ntri, plan.kchunk, Kp, partial,
+                                                        err);
   k_reduce_partials<<<plan.ntri, 256, 0, st>>>(partial, plan.ntri, plan.nchunk, m, S);
   SDPX_LAUNCH_CHECK_N(2);
 }

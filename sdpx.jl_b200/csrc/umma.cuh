@@ -28,6 +28,21 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
   return d;
 }
 
+// Same, for the K-major 64-byte-swizzle layout a TMA load with
+// CU_TENSOR_MAP_SWIZZLE_64B writes: rows of 64 bytes, 8-row atoms of 512 bytes
+// (SBO = 512), leading-byte-offset field 1 (unused for swizzled K-major),
+// layout type 4 (bits 61-63).  Advancing along K by 16 BF16 elements adds 32
+// bytes to the start address; the tile base must be 512-byte aligned.
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(512 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)4 << 61;
+  return d;
+}
+
 // Instruction descriptor, kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
 // (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 = 0), N>>3 at bits 17-22,
 // M>>4 at bits 24-28.
@@ -116,6 +131,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parit
     __nanosleep(32);
   }
   return true;
+}
+
+// Arm `mbar` for `bytes` of incoming TMA data (one arrival of this thread).
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mbar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// 2D tiled TMA load (no multicast) of the box at (x = inner, y = outer) into
+// shared memory, completing `bytes` on `mbar`.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int x, int y,
+                                            uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          dst),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(mbar))
+      : "memory");
 }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
