@@ -14,6 +14,7 @@ struct MixedWorkspace {
   long long Kp = 0;            // padded stacked K of the plane layout
   std::vector<int> kp;         // padded order per dense block
   std::vector<long long> po;   // plane offset per dense block
+  std::vector<long long> ao;   // constraint-plane region of each dense block
   long long pog = 0;           // plane offset of the 1×1 group
   long long Ts = 0;            // per-variable stride of the T planes
   void* Apl[3] = {nullptr, nullptr, nullptr};

@@ -8,12 +8,19 @@
 // into K chunks whose FP32 tiles are summed in FP64, so the accumulation error
 // does not grow with K.
 //
-// One engine serves the three products of the Schur assembly
+// One TMA-fed engine serves the three products of the Schur assembly
 //   T_i = L_X⁻¹ A_i         (A operand: rows of W = L_X⁻¹; B operand: columns of A_i)
 //   P_i = T_i · L_Y         (A operand: rows of T_i;       B operand: columns of L_Y)
 //   S   = P̂ᵀ P̂ (lower)     (A, B: variables' stacked P̂ columns, split K)
-// CTA tile 128×128, K tile 64, two smem stages of 6 operand tiles (96 KB each),
-// MMA M=128 N=128 K=16 issued by one thread, completion tracked by mbarriers.
+// Every operand plane is a row-major 2D BF16 tensor (rows × K, row pitch a
+// multiple of 8 elements) described by a TMA tensor map.  CTA tile 128×128,
+// 128 threads: thread 0 produces (6 TMA boxes of 128 rows × 32 BF16 per stage,
+// 64-byte swizzle, four 48 KB stages), thread 32 issues the 12 MMAs of a stage
+// (M=128 N=128 K=16, 2 K steps × 6 plane products) and commits them to the
+// stage's "empty" barrier; all four warps then drain the FP32 TMEM tile.  Rows
+// and K beyond a tensor's extent arrive as zeros (TMA out-of-bounds fill).
+// Every wait is bounded and records a device error instead of spinning; the
+// producer waits for all of its own copies before the CTA leaves.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -26,57 +33,17 @@ namespace sdpx {
 
 namespace {
 
-constexpr int TM = 128, TN = 128, TK = 64;
+constexpr int TM = 128, TN = 128;
 constexpr int NTHREADS = 128;
-constexpr int TILE_BYTES = TM * TK * 2;        // 16 KB per operand plane tile
-constexpr int STAGE_BYTES = 6 * TILE_BYTES;    // A0 A1 A2 B0 B1 B2
-constexpr int NSTAGE = 2;
-constexpr uint32_t LBO = 128;                  // core matrices adjacent along K
-constexpr uint32_t SBO = (TK / 8) * 128;       // 8-row groups
-constexpr size_t SMEM_BYTES = NSTAGE * STAGE_BYTES + 256;
-
-__device__ __forceinline__ uint32_t tile_off(int row, int k) {
-  return (uint32_t)((row >> 3) * SBO + (k >> 3) * LBO + (row & 7) * 16 + (k & 7) * 2);
-}
+constexpr int SK = 32;                          // K per stage
+constexpr int SNST = 4;                         // stages
+constexpr int SPLANE_BYTES = TM * SK * 2;       // 8 KB: 128 rows × 64 B
+constexpr int SSTAGE_BYTES = 6 * SPLANE_BYTES;  // 48 KB
+constexpr size_t SSMEM_BYTES = SNST * SSTAGE_BYTES + 1024 + 256;
 
 __device__ __forceinline__ long long row_off(const RowMap& r, int row) {
   return r.base + (long long)(row / r.inner) * r.os + (long long)(row % r.inner) * r.is;
 }
-
-// Stage loader: rows [r0, r0+128) of A, [c0, c0+128) of B, K slice [k0, k0+64).
-struct Loader {
-  long long a_off[8], b_off[8];  // per owned row (-1 = out of range)
-  __device__ void init(const PlaneOpnd& A, const PlaneOpnd& B, int r0, int c0) {
-    const int tid = threadIdx.x;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      int row = tid / 8 + 16 * j;
-      int ga = r0 + row, gb = c0 + row;
-      a_off[j] = ga < A.rows.extent ? row_off(A.rows, ga) : -1;
-      b_off[j] = gb < B.rows.extent ? row_off(B.rows, gb) : -1;
-    }
-  }
-  __device__ void issue(unsigned char* stage, const PlaneOpnd& A, const PlaneOpnd& B, int k0) const {
-    const int tid = threadIdx.x;
-    const int kc = (tid & 7) * 8;  // element offset of this thread's 16-byte chunk
-    const int k = k0 + kc;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      int row = tid / 8 + 16 * j;
-      uint32_t so = tile_off(row, kc);
-      bool va = a_off[j] >= 0 && k < A.kvalid;
-      bool vb = b_off[j] >= 0 && k < B.kvalid;
-#pragma unroll
-      for (int p = 0; p < 3; ++p) {
-        const __nv_bfloat16* ga = va ? A.plane[p] + a_off[j] + k : A.plane[p];
-        const __nv_bfloat16* gb = vb ? B.plane[p] + b_off[j] + k : B.plane[p];
-        umma::cp_async16(stage + p * TILE_BYTES + so, ga, va);
-        umma::cp_async16(stage + (3 + p) * TILE_BYTES + so, gb, vb);
-      }
-    }
-    asm volatile("cp.async.commit_group;\n" ::);
-  }
-};
 
 __device__ __forceinline__ void split3(float v, __nv_bfloat16& h0, __nv_bfloat16& h1,
                                        __nv_bfloat16& h2) {
@@ -84,76 +51,6 @@ __device__ __forceinline__ void split3(float v, __nv_bfloat16& h0, __nv_bfloat16
   float r = v - __bfloat162float(h0);
   h1 = __float2bfloat16_rn(r);
   h2 = __float2bfloat16_rn(r - __bfloat162float(h1));
-}
-
-// Accumulate the six plane products over K range [kb, ke) into TMEM.
-// Returns false when a bounded wait gave up.
-__device__ bool mainloop(const PlaneOpnd& A, const PlaneOpnd& B, int r0, int c0, int kb, int ke,
-                         unsigned char* smem, uint64_t* mbar, uint32_t* phase, uint32_t tmem,
-                         int* err) {
-  const int ntiles = (ke > kb) ? (ke - kb + TK - 1) / TK : 0;
-  Loader ld;
-  ld.init(A, B, r0, c0);
-  constexpr uint32_t IDESC = umma::idesc_bf16_f32(TM, TN);
-  bool ok = true;
-  if (ntiles == 0) return true;
-  ld.issue(smem, A, B, kb);
-  for (int t = 0; t < ntiles; ++t) {
-    const int s = t & 1;
-    if (t + 1 < ntiles) {
-      const int s2 = (t + 1) & 1;
-      if (t + 1 >= NSTAGE) {
-        // stage s2 was read by the MMAs of tile t-1: wait for their commit
-        if (!umma::mbar_wait_bounded(&mbar[s2], phase[s2], err)) ok = false;
-        phase[s2] ^= 1u;
-      }
-      ld.issue(smem + s2 * STAGE_BYTES, A, B, kb + (t + 1) * TK);
-      asm volatile("cp.async.wait_group 1;\n" ::);
-    } else {
-      asm volatile("cp.async.wait_group 0;\n" ::);
-    }
-    umma::fence_proxy_async_smem();
-    // uniform decision: every thread leaves the loop together
-    if (!__syncthreads_and(ok ? 1 : 0)) {
-      ok = false;
-      break;
-    }
-    if (threadIdx.x == 0) {
-      umma::fence_after_sync();
-      const uint32_t base = umma::smem_u32(smem + s * STAGE_BYTES);
-#pragma unroll
-      for (int ks = 0; ks < TK / 16; ++ks) {
-        const uint32_t koff = ks * 2 * LBO;
-        // (a, b) plane pairs with a + b ≤ 2
-        const int pa[6] = {0, 0, 1, 0, 1, 2};
-        const int pb[6] = {0, 1, 0, 2, 1, 0};
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          uint64_t ad = umma::smem_desc(base + pa[q] * TILE_BYTES + koff, LBO, SBO);
-          uint64_t bd = umma::smem_desc(base + (3 + pb[q]) * TILE_BYTES + koff, LBO, SBO);
-          umma::mma_bf16(tmem, ad, bd, IDESC, (t > 0 || ks > 0 || q > 0) ? 1u : 0u);
-        }
-      }
-      umma::commit(&mbar[s]);
-    }
-    __syncthreads();
-  }
-  // wait for the last committed stage (covers all earlier MMAs of this thread)
-  if (ok && ntiles > 0) {
-    const int s = (ntiles - 1) & 1;
-    if (!umma::mbar_wait_bounded(&mbar[s], phase[s], err)) ok = false;
-    phase[s] ^= 1u;
-    if (ntiles >= 2) {
-      // the other stage's last commit completed earlier (MMAs complete in order);
-      // consume its pending phase so both barriers agree with `phase`.
-      const int o = s ^ 1;
-      if (!umma::mbar_wait_bounded(&mbar[o], phase[o], err)) ok = false;
-      phase[o] ^= 1u;
-    }
-  }
-  ok = __syncthreads_and(ok ? 1 : 0) != 0;
-  umma::fence_after_sync();
-  return ok;
 }
 
 __device__ inline void tri_index(int tri, int& ti, int& tj) {
@@ -164,122 +61,22 @@ __device__ inline void tri_index(int tri, int& ti, int& tj) {
   tj = tri - a * (a + 1) / 2;
 }
 
-struct KernelShared {
-  uint64_t mbar[2];
-  uint32_t tmem;
+struct TmaMaps {
+  CUtensorMap a[3], b[3];
 };
 
-template <int MODE>
-__global__ void __launch_bounds__(NTHREADS, 1)
-    k_split_gemm(PlaneOpnd A, PlaneOpnd B, OutMap out, int kmode, int Ktot, int ntri, int kchunk,
-                 float* partial, int* err) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* smem = smem_raw;
-  KernelShared* ks = reinterpret_cast<KernelShared*>(smem_raw + NSTAGE * STAGE_BYTES);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
-    umma::mbar_init(&ks->mbar[0], 1);
-    umma::mbar_init(&ks->mbar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
-  }
-  if (warp == 0) umma::tmem_alloc(&ks->tmem, 128);
-  umma::fence_before_sync();
-  __syncthreads();
-  umma::fence_after_sync();
-  const uint32_t tmem = ks->tmem;
-  uint32_t phase[2] = {0u, 0u};
-
-  int r0, c0, kb, ke;
-  if (MODE == 0) {  // SYRK: unit = chunk-major (chunk, lower tile)
-    const int u = blockIdx.x;
-    const int chunk = u / ntri, tri = u % ntri;
-    int ti, tj;
-    tri_index(tri, ti, tj);
-    r0 = ti * TM;
-    c0 = tj * TN;
-    kb = chunk * kchunk;
-    ke = min(Ktot, kb + kchunk);
-  } else {
-    r0 = blockIdx.y * TM;
-    c0 = blockIdx.x * TN;
-    kb = 0;
-    ke = Ktot;
-    if (kmode == 1) ke = min(Ktot, ((r0 + TM + TK - 1) / TK) * TK);  // A lower triangular
-    if (kmode == 2) kb = (c0 / TK) * TK;                                // B lower triangular
-  }
-  bool ok = mainloop(A, B, r0, c0, kb, ke, smem, ks->mbar, phase, tmem, err);
-
-  // Epilogue: warp w owns accumulator rows [32w, 32w+32) (TMEM lanes).
-  const int row = warp * 32 + lane;
-  if (ok) {
-    for (int cb = 0; cb < TN; cb += 32) {
-      float v[32];
-      umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
-      if (MODE == 0) {
-        float* dst = partial + (size_t)blockIdx.x * TM * TN + (size_t)row * TN + cb;
-#pragma unroll
-        for (int q = 0; q < 32; q += 4)
-          *reinterpret_cast<float4*>(dst + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
-      } else {
-        const int grow = r0 + row;
-        if (grow < out.rows.extent) {
-          const long long ro = row_off(out.rows, grow);
-#pragma unroll
-          for (int q = 0; q < 32; q += 8) {
-            const int gcol = c0 + cb + q;
-            if (gcol >= out.col_extent) continue;
-            const long long co = (long long)(gcol / out.col_inner) * out.col_os +
-                                 (long long)(gcol % out.col_inner);
-            __align__(16) __nv_bfloat16 h[3][8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) split3(v[q + e], h[0][e], h[1][e], h[2][e]);
-#pragma unroll
-            for (int p = 0; p < 3; ++p)
-              *reinterpret_cast<uint4*>(out.plane[p] + ro + co) = *reinterpret_cast<uint4*>(h[p]);
-          }
-        }
-      }
-    }
-  }
-  umma::fence_before_sync();
-  __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tmem, 128);
-}
-
-// ---------------------------------------------------------------------------
-// Lower SYRK S = P̂ᵀP̂ fed by TMA.  One CTA per (K chunk, lower 128×128 tile),
-// 128 threads: thread 0 produces (24 TMA boxes of 128 rows × 32 BF16 per stage:
-// three planes of the A rows and of the B rows, 64-byte swizzle), thread 32
-// issues the 12 MMAs of a stage (2 K steps × the 6 plane products) and commits
-// them to the stage's "empty" barrier, all four warps then drain the FP32 TMEM
-// tile.  Four 48 KB stages.  Rows beyond m and K beyond Kp arrive as zeros
-// (TMA out-of-bounds fill).  Every wait is bounded and records a device error
-// instead of spinning; the producer waits for all of its own copies before the
-// CTA leaves.
-// ---------------------------------------------------------------------------
-constexpr int SK = 32;                          // K per stage
-constexpr int SNST = 4;                         // stages
-constexpr int SPLANE_BYTES = TM * SK * 2;       // 8 KB: 128 rows × 64 B
-constexpr int SSTAGE_BYTES = 6 * SPLANE_BYTES;  // 48 KB
-constexpr size_t SSMEM_BYTES = SNST * SSTAGE_BYTES + 1024 + 256;
-
-struct SyrkMaps {
-  CUtensorMap plane[3];
-};
-
-struct SyrkShared {
+struct PipeShared {
   uint64_t full[SNST], empty[SNST], done;
   uint32_t tmem;
 };
 
-__global__ void __launch_bounds__(NTHREADS, 1)
-    k_split_syrk_tma(const __grid_constant__ SyrkMaps maps, int ntri, int kchunk, int Ktot,
-                     float* partial, int* err) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* smem = reinterpret_cast<unsigned char*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  SyrkShared* sh = reinterpret_cast<SyrkShared*>(smem + SNST * SSTAGE_BYTES);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+__device__ __forceinline__ unsigned char* aligned_smem(unsigned char* raw) {
+  return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(raw) + 1023) &
+                                          ~uintptr_t(1023));
+}
+
+// Barrier set-up and the 128-column TMEM accumulator (all threads).
+__device__ __forceinline__ uint32_t pipe_init(PipeShared* sh) {
   if (threadIdx.x == 0) {
     for (int s = 0; s < SNST; ++s) {
       umma::mbar_init(&sh->full[s], 1);
@@ -288,21 +85,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     umma::mbar_init(&sh->done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
-  if (warp == 0) umma::tmem_alloc(&sh->tmem, 128);
+  if ((threadIdx.x >> 5) == 0) umma::tmem_alloc(&sh->tmem, 128);
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
-  const uint32_t tmem = sh->tmem;
+  return sh->tmem;
+}
 
-  const int u = blockIdx.x;
-  const int chunk = u / ntri, tri = u % ntri;
-  int ti, tj;
-  tri_index(tri, ti, tj);
-  const int r0 = ti * TM, c0 = tj * TN;
-  const int kb = chunk * kchunk;
-  const int ke = min(Ktot, kb + kchunk);
-  const int ntiles = ke > kb ? (ke - kb + SK - 1) / SK : 0;
-
+// Accumulate A[ra:ra+128, k]·B[rb:rb+128, k]ᵀ over `ntiles` K tiles starting
+// at kb into TMEM.  Returns true on every thread when all waits succeeded.
+__device__ bool pipe_mainloop(const TmaMaps& maps, int ra, int rb, int kb, int ntiles,
+                              unsigned char* smem, PipeShared* sh, uint32_t tmem, int* err) {
   if (threadIdx.x == 0) {
     // producer
     int issued = 0;
@@ -314,8 +107,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const int k = kb + t * SK;
 #pragma unroll
       for (int p = 0; p < 3; ++p) {
-        umma::tma_load_2d(base + p * SPLANE_BYTES, &maps.plane[p], k, r0, &sh->full[s]);
-        umma::tma_load_2d(base + (3 + p) * SPLANE_BYTES, &maps.plane[p], k, c0, &sh->full[s]);
+        umma::tma_load_2d(base + p * SPLANE_BYTES, &maps.a[p], k, ra, &sh->full[s]);
+        umma::tma_load_2d(base + (3 + p) * SPLANE_BYTES, &maps.b[p], k, rb, &sh->full[s]);
       }
       ++issued;
     }
@@ -348,27 +141,96 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   __syncwarp();
   const bool ok = umma::mbar_wait_bounded(&sh->done, 0, err);
   umma::fence_after_sync();
-  const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+  return __syncthreads_and(ok ? 1 : 0) != 0;
+}
 
-  // Epilogue: warp w owns accumulator rows [32w, 32w+32) (TMEM lanes).
-  if (all_ok && ntiles > 0) {
-    const int row = warp * 32 + lane;
+__device__ __forceinline__ void pipe_release(uint32_t tmem) {
+  umma::fence_before_sync();
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) umma::tmem_dealloc(tmem, 128);
+}
+
+// Lower SYRK S = P̂ᵀP̂: one CTA per (K chunk, lower 128×128 tile); the FP32
+// tile goes to `partial` (summed over chunks in FP64 by k_reduce_partials).
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_split_syrk_tma(const __grid_constant__ TmaMaps maps, int ntri, int kchunk, int Ktot,
+                     float* partial, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = aligned_smem(smem_raw);
+  PipeShared* sh = reinterpret_cast<PipeShared*>(smem + SNST * SSTAGE_BYTES);
+  const uint32_t tmem = pipe_init(sh);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x;
+  const int chunk = u / ntri, tri = u % ntri;
+  int ti, tj;
+  tri_index(tri, ti, tj);
+  const int kb = chunk * kchunk;
+  const int ke = min(Ktot, kb + kchunk);
+  const int ntiles = ke > kb ? (ke - kb + SK - 1) / SK : 0;
+  const bool ok = pipe_mainloop(maps, ti * TM, tj * TN, kb, ntiles, smem, sh, tmem, err);
+  const int row = warp * 32 + lane;
+  float* dst0 = partial + (size_t)blockIdx.x * TM * TN + (size_t)row * TN;
+  if (ok && ntiles > 0) {
     for (int cb = 0; cb < TN; cb += 32) {
       float v[32];
       umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
-      float* dst = partial + (size_t)blockIdx.x * TM * TN + (size_t)row * TN + cb;
 #pragma unroll
       for (int q = 0; q < 32; q += 4)
-        *reinterpret_cast<float4*>(dst + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+        *reinterpret_cast<float4*>(dst0 + cb + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
     }
   } else if (ntiles == 0) {
-    const int row = warp * 32 + lane;
-    float* dst = partial + (size_t)blockIdx.x * TM * TN + (size_t)row * TN;
-    for (int q = 0; q < TN; q += 4) *reinterpret_cast<float4*>(dst + q) = make_float4(0, 0, 0, 0);
+    for (int q = 0; q < TN; q += 4) *reinterpret_cast<float4*>(dst0 + q) = make_float4(0, 0, 0, 0);
   }
-  umma::fence_before_sync();
-  __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tmem, 128);
+  pipe_release(tmem);
+}
+
+// out = A·Bᵀ split into three BF16 output planes.  Grid: x over B rows (output
+// columns), y over A rows.  kmode 0 full K, 1 A lower-triangular (k ≤ row),
+// 2 B lower-triangular (k ≥ col).
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_split_gemm_tma(const __grid_constant__ TmaMaps maps, OutMap out, int kmode, int Ktot,
+                     int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = aligned_smem(smem_raw);
+  PipeShared* sh = reinterpret_cast<PipeShared*>(smem + SNST * SSTAGE_BYTES);
+  const uint32_t tmem = pipe_init(sh);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r0 = blockIdx.y * TM, c0 = blockIdx.x * TN;
+  int kb = 0, ke = Ktot;
+  if (kmode == 1) ke = min(Ktot, r0 + TM);
+  if (kmode == 2) kb = (c0 / SK) * SK;
+  const int ntiles = ke > kb ? (ke - kb + SK - 1) / SK : 0;
+  const bool ok = pipe_mainloop(maps, r0, c0, kb, ntiles, smem, sh, tmem, err);
+  const int row = warp * 32 + lane;
+  const int grow = r0 + row;
+  if (ok) {  // CTA-uniform: tcgen05.ld is warp-collective, only the stores are per row
+    const bool live = grow < out.rows.extent;
+    const long long ro = live ? row_off(out.rows, grow) : 0;
+    for (int cb = 0; cb < TN; cb += 32) {
+      float v[32];
+      if (ntiles > 0) {
+        umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 32; ++q) v[q] = 0.f;
+      }
+      if (!live) continue;
+#pragma unroll
+      for (int q = 0; q < 32; q += 8) {
+        const int gcol = c0 + cb + q;
+        if (gcol >= out.col_extent) continue;
+        const long long co = (long long)(gcol / out.col_inner) * out.col_os +
+                             (long long)(gcol % out.col_inner);
+        __align__(16) __nv_bfloat16 h[3][8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) split3(v[q + e], h[0][e], h[1][e], h[2][e]);
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+          *reinterpret_cast<uint4*>(out.plane[p] + ro + co) = *reinterpret_cast<uint4*>(h[p]);
+      }
+    }
+  }
+  pipe_release(tmem);
 }
 
 __global__ void k_reduce_partials(const float* partial, int ntri, int nchunk, int m, double* S) {
@@ -439,17 +301,6 @@ __global__ void k_split_small(const double* M, int k, int kp, int row_major, __n
 
 }  // namespace
 
-size_t split_gemm_smem_bytes() { return SMEM_BYTES; }
-
-void split_gemm_planes(const PlaneOpnd& A, const PlaneOpnd& B, const OutMap& out, int kmode,
-                       int Ktot, int* err, cudaStream_t st) {
-  ensure_smem(k_split_gemm<1>, SMEM_BYTES);
-  dim3 grid(ceil_div(out.col_extent, TN), ceil_div(out.rows.extent, TM));
-  if (grid.x == 0 || grid.y == 0) return;
-  k_split_gemm<1><<<grid, NTHREADS, SMEM_BYTES, st>>>(A, B, out, kmode, Ktot, 0, 0, nullptr, err);
-  SDPX_LAUNCH_CHECK();
-}
-
 SplitSyrkPlan plan_split_syrk(int m, long long Kp, int sm_count) {
   SplitSyrkPlan p;
   const int nt = ceil_div(m, TM);
@@ -467,7 +318,7 @@ SplitSyrkPlan plan_split_syrk(int m, long long Kp, int sm_count) {
     if (eff > best + 1e-9) best = eff, best_c = c;
   }
   long long kc = (Kp + best_c - 1) / best_c;
-  kc = ((kc + TK - 1) / TK) * TK;
+  kc = ((kc + 63) / 64) * 64;
   p.kchunk = (int)kc;
   p.nchunk = (int)((Kp + kc - 1) / kc);
   p.partial_floats = (size_t)p.nchunk * p.ntri * TM * TN;
@@ -491,12 +342,15 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// Tensor map of one plane: rows × Kp BF16, row-major; box 32 × 128, 64-byte swizzle.
-static void encode_plane_map(CUtensorMap* map, const __nv_bfloat16* plane, int rows, long long Kp) {
-  if ((reinterpret_cast<uintptr_t>(plane) & 15) != 0 || (Kp * 2) % 16 != 0)
-    throw std::invalid_argument("split SYRK: plane base or row pitch not 16-byte aligned");
-  cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
+// Tensor map of one plane: rows × kext BF16, row-major with a pitch of `pitch`
+// elements; box 32 (K) × 128 (rows), 64-byte swizzle, zeros out of bounds.
+static void encode_plane_map(CUtensorMap* map, const __nv_bfloat16* plane, long long rows,
+                             long long kext, long long pitch) {
+  if ((reinterpret_cast<uintptr_t>(plane) & 15) != 0 || (pitch * 2) % 16 != 0 || kext > pitch ||
+      rows <= 0 || kext <= 0)
+    throw std::invalid_argument("split GEMM: plane base or pitch not 16-byte aligned");
+  cuuint64_t dims[2] = {(cuuint64_t)kext, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)pitch * 2};
   cuuint32_t box[2] = {(cuuint32_t)SK, (cuuint32_t)TM};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = tensor_map_encoder()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
@@ -507,12 +361,29 @@ static void encode_plane_map(CUtensorMap* map, const __nv_bfloat16* plane, int r
   if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
 
-void split_syrk(const PlaneOpnd& P, int m, int Kp, const SplitSyrkPlan& plan, float* partial,
+void split_gemm_planes(const Plane2D& A, const Plane2D& B, int Ktot, const OutMap& out, int kmode,
+                       int* err, cudaStream_t st) {
+  if (out.rows.extent <= 0 || out.col_extent <= 0 || Ktot <= 0) return;
+  TmaMaps maps;
+  for (int p = 0; p < 3; ++p) {
+    encode_plane_map(&maps.a[p], A.plane[p], A.rows, Ktot, A.pitch);
+    encode_plane_map(&maps.b[p], B.plane[p], B.rows, Ktot, B.pitch);
+  }
+  ensure_smem(k_split_gemm_tma, SSMEM_BYTES);
+  dim3 grid(ceil_div(out.col_extent, TN), ceil_div(out.rows.extent, TM));
+  k_split_gemm_tma<<<grid, NTHREADS, SSMEM_BYTES, st>>>(maps, out, kmode, Ktot, err);
+  SDPX_LAUNCH_CHECK();
+}
+
+void split_syrk(const Plane2D& P, int m, int Kp, const SplitSyrkPlan& plan, float* partial,
                 double* S, int* err, cudaStream_t st) {
-  if (P.rows.is != Kp || P.rows.base != 0 || Kp % SK != 0 || plan.kchunk % SK != 0)
+  if (P.pitch != Kp || Kp % SK != 0 || plan.kchunk % SK != 0)
     throw std::invalid_argument("split SYRK: planes must be m × Kp row-major, Kp and chunks ≡ 0 mod 32");
-  SyrkMaps maps;
-  for (int p = 0; p < 3; ++p) encode_plane_map(&maps.plane[p], P.plane[p], m, Kp);
+  TmaMaps maps;
+  for (int p = 0; p < 3; ++p) {
+    encode_plane_map(&maps.a[p], P.plane[p], m, Kp, Kp);
+    maps.b[p] = maps.a[p];
+  }
   ensure_smem(k_split_syrk_tma, SSMEM_BYTES);
   const int units = plan.ntri * plan.nchunk;
   k_split_syrk_tma<<<units, NTHREADS, SSMEM_BYTES, st>>>(maps, plan.ntri, plan.kchunk, Kp, partial,

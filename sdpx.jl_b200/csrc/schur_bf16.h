@@ -17,12 +17,14 @@ struct RowMap {
   int extent;
 };
 
-// Three BF16 planes of a K-major operand: element (row, k) of plane p is
-// plane[p][row_off(row) + k], valid for k < kvalid (zero-filled beyond).
-struct PlaneOpnd {
+// Three BF16 planes of a K-major operand stored as a row-major 2D tensor:
+// element (row, k) of plane p is plane[p][row·pitch + k] for row < rows
+// (pitch a multiple of 8 elements, bases 16-byte aligned).  Rows and K beyond
+// the tensor read as zeros.
+struct Plane2D {
   const __nv_bfloat16* plane[3];
-  RowMap rows;
-  int kvalid;
+  long long rows;
+  long long pitch;
 };
 
 // Output planes: element (row, col) at plane[p][row_off(row) + (col / col_inner)·col_os + col % col_inner].
@@ -40,14 +42,13 @@ struct SplitSyrkPlan {
   size_t partial_floats = 0;
 };
 
-size_t split_gemm_smem_bytes();
 // out = A·Bᵀ (A rows × B rows, contraction over k < Ktot), split into planes.
 // kmode: 0 full K, 1 A lower-triangular (k ≤ row), 2 B lower-triangular (k ≥ col).
-void split_gemm_planes(const PlaneOpnd& A, const PlaneOpnd& B, const OutMap& out, int kmode,
-                       int Ktot, int* err, cudaStream_t st);
+void split_gemm_planes(const Plane2D& A, const Plane2D& B, int Ktot, const OutMap& out, int kmode,
+                       int* err, cudaStream_t st);
 SplitSyrkPlan plan_split_syrk(int m, long long Kp, int sm_count);
 // Lower tiles of S (m×m FP64, column-major) = P̂ᵀP̂ over K = Kp, FP32 chunk tiles summed in FP64.
-void split_syrk(const PlaneOpnd& P, int m, int Kp, const SplitSyrkPlan& plan, float* partial,
+void split_syrk(const Plane2D& P, int m, int Kp, const SplitSyrkPlan& plan, float* partial,
                 double* S, int* err, cudaStream_t st);
 
 void split_A_dense(const double* A, long long K, int m, long long off, int k, int kp,
