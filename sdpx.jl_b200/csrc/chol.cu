@@ -7,10 +7,9 @@
 // later CTA of that matrix returns at once — the no-throw contract of SDPX's
 // `kchol!` (src/kernels/generic.jl:133-155).
 //
-// Column loops inside a tile are laid out warp-per-column, lane-per-row (no
-// per-element index division); every right-looking step rounds exactly as the
-// scalar column algorithm: l_cc = sqrt(a_cc), l_rc = a_rc / l_cc,
-// a_rq -= l_rc · l_qc.
+// Inside a panel the columns are processed in blocks of 8: l_cc = sqrt(a_cc),
+// l_rc = a_rc · (1/l_cc) (the reciprocal scaling of LAPACK's dpotf2),
+// a_rq -= l_rc · l_qc, every element updated in increasing column order.
 #include "chol.h"
 #include "blas_f64.h"
 
@@ -20,52 +19,65 @@ namespace sdpx {
 // column-major, leading dimension ld; rows ≥ w).  Returns the failing column
 // or -1.  All threads of the CTA take part.
 //
-// Blocked by 8 columns: every thread factors the 8×8 diagonal block in its own
-// registers (identical arithmetic in every thread, so the pivot test is
-// uniform), thread 0 stores it, each row below the block is solved in
-// registers (x = a · L_bb^{-T}), and the trailing columns of the panel receive
-// the rank-8 update with the block's rows read as warp broadcasts.  Every
-// element sees its updates in increasing column order, as in the unblocked
-// right-looking loop (l_cc = sqrt(a_cc), l_rc = a_rc / l_cc, a_rq -= l_rc·l_qc).
+// Blocked by 8 columns: thread 0 factors the 8×8 diagonal block (l_cc =
+// sqrt(a_cc), column below scaled by 1/l_cc, as LAPACK's unblocked dpotf2
+// does) and publishes it with the reciprocal pivots; each row below the block
+// is solved in registers (x = a · L_bb^{-T}); the trailing columns of the panel
+// receive the rank-8 update with the block's rows read as warp broadcasts.
+// Every element sees its updates in increasing column order.
 template <class T>
 __device__ int factor_panel_smem(T* P, int ld, int rows, int w) {
+  __shared__ T sD[8][8];
+  __shared__ T sInv[8];
+  __shared__ int s_fail;
   __syncthreads();
   for (int kb = 0; kb < w; kb += 8) {
     const int kw = min(8, w - kb);
-    // 8×8 diagonal block in registers (lower part used)
-    T D[8][8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c)
-#pragma unroll
-      for (int r = 0; r < 8; ++r)
-        D[c][r] = (c < kw && r < kw && r >= c) ? P[(kb + c) * ld + kb + r] : T(0);
-    int fail = -1;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      if (c < kw && fail < 0) {
-        const T piv = D[c][c];
-        if (!(piv > T(0))) {
-          fail = c;
-        } else {
-          const T lc = sqrt(piv);
-          D[c][c] = lc;
-#pragma unroll
-          for (int r = c + 1; r < 8; ++r) D[c][r] /= lc;
-#pragma unroll
-          for (int q = c + 1; q < 8; ++q)
-#pragma unroll
-            for (int r = q; r < 8; ++r) D[q][r] -= D[c][r] * D[c][q];
-        }
-      }
-    }
-    if (fail >= 0) return kb + fail;  // uniform: every thread computed the same block
-    __syncthreads();                   // every thread has read the block
     if (threadIdx.x == 0) {
+      T D[8][8];
 #pragma unroll
       for (int c = 0; c < 8; ++c)
 #pragma unroll
         for (int r = 0; r < 8; ++r)
+          D[c][r] = (c < kw && r < kw && r >= c) ? P[(kb + c) * ld + kb + r] : T(0);
+      int fail = -1;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < kw && fail < 0) {
+          const T piv = D[c][c];
+          if (!(piv > T(0))) {
+            fail = c;
+          } else {
+            const T lc = sqrt(piv);
+            const T inv = T(1) / lc;
+            D[c][c] = lc;
+            sInv[c] = inv;
+#pragma unroll
+            for (int r = c + 1; r < 8; ++r) D[c][r] *= inv;
+#pragma unroll
+            for (int q = c + 1; q < 8; ++q)
+#pragma unroll
+              for (int r = q; r < 8; ++r) D[q][r] -= D[c][r] * D[c][q];
+          }
+        }
+      }
+      s_fail = fail;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          sD[c][r] = D[c][r];
           if (c < kw && r < kw && r >= c) P[(kb + c) * ld + kb + r] = D[c][r];
+        }
+    }
+    __syncthreads();
+    if (s_fail >= 0) return kb + s_fail;  // uniform after the barrier
+    T D[8][8], inv[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      inv[c] = sInv[c];
+#pragma unroll
+      for (int r = c + 1; r < 8; ++r) D[c][r] = sD[c][r];
     }
     // rows below the block: x = a · L_bb^{-T}
     for (int r = kb + kw + threadIdx.x; r < rows; r += blockDim.x) {
@@ -75,7 +87,7 @@ __device__ int factor_panel_smem(T* P, int ld, int rows, int w) {
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         if (c < kw) {
-          x[c] /= D[c][c];
+          x[c] *= inv[c];
 #pragma unroll
           for (int q = c + 1; q < 8; ++q) x[q] -= x[c] * D[c][q];
         }
@@ -145,7 +157,8 @@ __global__ void k_potrf_diag(const MatDesc<T>* mats, int j, int* info, T* dmin, 
 
 // Tiled path, step 2: rows below the diagonal tile, X = B · L_jj^{-T}, one
 // thread per row with the row held in registers (forward substitution in the
-// column order of the right-looking panel factor).
+// column order of the right-looking panel factor, scaling by the reciprocal
+// pivots).
 template <class T, int NB>
 __global__ void __launch_bounds__(128) k_potrf_trsm_rows(const MatDesc<T>* mats, int j,
                                                          const int* info) {
@@ -162,6 +175,8 @@ __global__ void __launch_bounds__(128) k_potrf_trsm_rows(const MatDesc<T>* mats,
     int r = e % w, c = e / w;
     D[c * LD + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
   }
+  __shared__ T inv[NB];
+  for (int c = threadIdx.x; c < w; c += blockDim.x) inv[c] = T(1) / D[c * LD + c];
   __syncthreads();
   const int r = first + threadIdx.x;
   if (r >= M.n) return;
@@ -171,7 +186,7 @@ __global__ void __launch_bounds__(128) k_potrf_trsm_rows(const MatDesc<T>* mats,
 #pragma unroll
   for (int c = 0; c < NB; ++c) {
     if (c < w) {
-      x[c] /= D[c * LD + c];
+      x[c] *= inv[c];
 #pragma unroll
       for (int q = c + 1; q < NB; ++q) x[q] -= x[c] * D[c * LD + q];
     }
