@@ -176,6 +176,7 @@ __global__ void __launch_bounds__(128) k_potrf_trsm_rows(const MatDesc<T>* mats,
     D[c * LD + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
   }
   __shared__ T inv[NB];
+  __syncthreads();  // the diagonal tile is loaded
   for (int c = threadIdx.x; c < w; c += blockDim.x) inv[c] = T(1) / D[c * LD + c];
   __syncthreads();
   const int r = first + threadIdx.x;
