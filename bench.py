@@ -37,6 +37,10 @@ WORKLOADS = {
                      label="dense SDP (SDPA form), one PSD block n=50, m=100"),
 }
 TOL = 1e-8
+# DRAM bytes (read + write) of one k_split_syrk_tma launch on the sdp_m2000
+# workload, from one ncu capture of dram__bytes_read.sum + dram__bytes_write.sum
+# (a single-pass metric set) on that workload.
+SPLIT_SYRK_DRAM_BYTES = None
 # LP standard form + Lorentz cones: the reduced normal matrix Q = Bᵀ D⁻¹ B + δI.
 NORMAL_WORKLOAD = dict(m=3000, n_lp=20000, cones=[64] * 100, density=0.1,
                        label="LP+SOC reduced normal matrix: 3000 equalities x (20000 LP + "
@@ -363,8 +367,10 @@ def run_ours(args, world, rank, local):
 
     be._set_mode("mixed")
     schur_ms_mixed = time_schur()
+    kt_mixed = be.kernel_times()
     be._set_mode("fp64")
     schur_ms_fp64 = time_schur()
+    kt_fp64 = be.kernel_times()
 
     # Plain FP64 device path on the same instance.
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -415,8 +421,19 @@ def run_ours(args, world, rank, local):
     normal = bench_normal(args, world, rank, local, dgemm_tflops)
 
     peaks, peak_kind = measured_peaks()
-    achieved = F / (schur_ms_mixed / 1000.0) / 1e12
     peak = float(peaks.get("bf16_tflops", 1590.0))
+    # Dominant tensor-core kernel of the mixed path: the split-BF16 lower SYRK.
+    # Algorithmic work m(m+1)·K (K = Σ k_l² + #1×1 blocks, FP64-equivalent);
+    # the hardware issues 6 BF16 products per FP64-equivalent product over the
+    # lower 128×128 tiles and the padded stacked length Kp.
+    K_alg = sum(k * k for k in wl["blocks"]) + wl["lp"]
+    Kp = ((sum(k * ((k + 7) // 8 * 8) for k in wl["blocks"]) + (wl["lp"] + 7) // 8 * 8 + 63)
+          // 64 * 64)
+    ntile = (wl["m"] + 127) // 128
+    hw_flops = ntile * (ntile + 1) // 2 * 128 * 128 * 2.0 * Kp * 6
+    syrk_flops = wl["m"] * (wl["m"] + 1.0) * K_alg
+    syrk_ms = kt_mixed["split_syrk"]
+    achieved = syrk_flops / (syrk_ms / 1000.0) / 1e12
     line = None
     if rank == 0:
         cpu = None
@@ -445,14 +462,28 @@ def run_ours(args, world, rank, local):
                          "status": r64.status.value, "objective": r64.pObj},
             "speedup_mixed_vs_fp64": fp64_s / (ms_per_step / 1000.0),
             "schur": {"flops_per_build": F, "ms_mixed": schur_ms_mixed, "ms_fp64": schur_ms_fp64,
-                      "tflops_mixed": achieved, "tflops_fp64": F / (schur_ms_fp64 / 1000) / 1e12,
+                      "tflops_mixed": F / (schur_ms_mixed / 1000) / 1e12,
+                      "tflops_fp64": F / (schur_ms_fp64 / 1000) / 1e12,
+                      "kernel_ms_mixed": {k: kt_mixed[k] for k in ("split_syrk",
+                                                                   "split_block_products")},
+                      "kernel_ms_fp64": {k: kt_fp64[k] for k in ("fp64_syrk",
+                                                                 "fp64_block_products")},
+                      "fp64_syrk_tflops": syrk_flops / (kt_fp64["fp64_syrk"] / 1000) / 1e12
+                      if kt_fp64["fp64_syrk"] > 0 else None,
                       "dgemm_tflops_measured": dgemm_tflops},
             "phase_ms_last_solve": phases_mixed,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "kernel": "Schur assembly (left/right block products + lower SYRK)",
+                         "frac": achieved / peak, "traffic": SPLIT_SYRK_DRAM_BYTES,
+                         "kernel": "k_split_syrk_tma (split-BF16 lower SYRK of the Schur "
+                                   "assembly, one launch per build)",
+                         "algorithmic_flops_per_launch": syrk_flops,
+                         "launch_ms": syrk_ms,
+                         "algorithmic_bytes_per_launch": 6.0 * wl["m"] * Kp,
+                         "hardware_flops_per_launch": hw_flops,
+                         "hardware_frac": hw_flops / (syrk_ms / 1000.0) / 1e12 / peak,
                          "peak_kind": f"bf16_tflops of {peak_kind} MEASURED_PEAKS.json; "
-                                      f"achieved counts FP64-equivalent algorithmic flops"},
+                                      f"achieved counts FP64-equivalent algorithmic flops "
+                                      f"(6 BF16 products each, so frac <= 1/6)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "status": r_e2e.status.value,

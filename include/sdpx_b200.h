@@ -230,6 +230,13 @@ int sdpx_b200_certificate(sdpx_b200_handle* h, const double* x, const double* X,
                           double eps_primal, double eps_dual, double eps_gap, int32_t legacy_gap,
                           sdpx_b200_certificate_result* out);
 
+/* Instrumentation (no counterpart in the reference): device time (ms) of the
+ * most recent launch of the Schur kernels, measured with events on the
+ * handle's stream: [0] split-BF16 SYRK kernel, [1] split-BF16 block products
+ * of all blocks, [2] FP64 SYRK (split-K kernel and reduction), [3] FP64 block
+ * products of all blocks; 0 where none ran yet. */
+int sdpx_b200_kernel_times(sdpx_b200_handle* h, double* ms4);
+
 /* Cumulative device time per phase (ms) since the last reset:
  * [0] residual+block factor, [1] Schur assembly, [2] KKT factor,
  * [3] solves+refinement, [4] directions+RHS, [5] step length, [6] update. */

@@ -140,7 +140,39 @@ struct Handle {
   std::vector<cudaEvent_t> ev_pool;
   double phase_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 
+  // Last device duration (ms) of the Schur kernels: [0] split-BF16 SYRK kernel,
+  // [1] split-BF16 block products (all blocks), [2] FP64 SYRK (split-K kernel and
+  // reduction), [3] FP64 block products (all blocks).
+  cudaEvent_t kt_ev[4][2] = {};
+  bool kt_armed[4] = {};
+  double kt_ms[4] = {0, 0, 0, 0};
+  void kt_create(int k) {
+    for (int j = 0; j < 2; ++j)
+      if (!kt_ev[k][j]) SDPX_CUDA(cudaEventCreate(&kt_ev[k][j]));
+  }
+  void kt_begin(int k) {
+    kt_create(k);
+    SDPX_CUDA(cudaEventRecord(kt_ev[k][0], st));
+  }
+  void kt_end(int k) {
+    SDPX_CUDA(cudaEventRecord(kt_ev[k][1], st));
+    kt_armed[k] = true;
+  }
+  void kt_harvest() {
+    for (int k = 0; k < 4; ++k) {
+      if (!kt_armed[k]) continue;
+      float ms = 0.f;
+      SDPX_CUDA(cudaEventSynchronize(kt_ev[k][1]));
+      SDPX_CUDA(cudaEventElapsedTime(&ms, kt_ev[k][0], kt_ev[k][1]));
+      kt_ms[k] = ms;
+      kt_armed[k] = false;
+    }
+  }
+
   ~Handle() {
+    for (auto& row : kt_ev)
+      for (auto e : row)
+        if (e) cudaEventDestroy(e);
     for (auto& p : pending) {
       cudaEventDestroy(p.a);
       cudaEventDestroy(p.b);
@@ -754,6 +786,7 @@ struct Handle {
   void schur_build_fp64(int identity) {
     const double* panel = A.p;
     if (!identity) {
+      kt_begin(3);
       for (auto& b : dense) {
         // T = W · [A_1 … A_m]  (W lower ⇒ K range [0, row-tile end))
         Opnd Wd = blk_as_A(W.p, b.off, b.k);
@@ -798,6 +831,7 @@ struct Handle {
         Pout.cols = b.k;
         trmm_right_lower_inplace_f64(Tst, My, Pout, st);
       }
+      kt_end(3);
       diag_panel(K, m, nd, od, A.p, LX.p, MY.p, Pc.p, st);
       panel = Pc.p;
     }
@@ -809,7 +843,9 @@ struct Handle {
     Pd.outer_stride = 0;
     Pd.mn_extent = m;
     Pd.k_extent = (int)K;
+    kt_begin(2);
     syrk_lower_f64(Pd, syrk, partial.p, S.p, m, m, 0.0, st);
+    kt_end(2);
     mirror_lower(m, S.p, st);
   }
 
@@ -2230,6 +2266,13 @@ int sdpx_b200_gram_noalloc(const double* P, int64_t K, int32_t m, double* S, voi
     g_noalloc_error = ex.what();
     return -2;
   }
+}
+int sdpx_b200_kernel_times(sdpx_b200_handle* h, double* ms4) {
+  GUARD(h, {
+    if (!ms4) throw std::invalid_argument("kernel_times: NULL output");
+    h->h.kt_harvest();
+    for (int i = 0; i < 4; ++i) ms4[i] = h->h.kt_ms[i];
+  });
 }
 int sdpx_b200_phase_times(sdpx_b200_handle* h, double* ms7, int reset) {
   GUARD(h, {

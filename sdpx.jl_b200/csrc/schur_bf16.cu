@@ -376,7 +376,7 @@ void split_gemm_planes(const Plane2D& A, const Plane2D& B, int Ktot, const OutMa
 }
 
 void split_syrk(const Plane2D& P, int m, int Kp, const SplitSyrkPlan& plan, float* partial,
-                double* S, int* err, cudaStream_t st) {
+                double* S, int* err, cudaStream_t st, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
   if (P.pitch != Kp || Kp % SK != 0 || plan.kchunk % SK != 0)
     throw std::invalid_argument("split SYRK: planes must be m × Kp row-major, Kp and chunks ≡ 0 mod 32");
   TmaMaps maps;
@@ -386,8 +386,10 @@ void split_syrk(const Plane2D& P, int m, int Kp, const SplitSyrkPlan& plan, floa
   }
   ensure_smem(k_split_syrk_tma, SSMEM_BYTES);
   const int units = plan.ntri * plan.nchunk;
+  if (ev_begin) SDPX_CUDA(cudaEventRecord(ev_begin, st));
   k_split_syrk_tma<<<units, NTHREADS, SSMEM_BYTES, st>>>(maps, plan.ntri, plan.kchunk, Kp, partial,
                                                         err);
+  if (ev_end) SDPX_CUDA(cudaEventRecord(ev_end, st));
   k_reduce_partials<<<plan.ntri, 256, 0, st>>>(partial, plan.ntri, plan.nchunk, m, S);
   SDPX_LAUNCH_CHECK_N(2);
 }

@@ -48,8 +48,10 @@ void split_gemm_planes(const Plane2D& A, const Plane2D& B, int Ktot, const OutMa
                        int* err, cudaStream_t st);
 SplitSyrkPlan plan_split_syrk(int m, long long Kp, int sm_count);
 // Lower tiles of S (m×m FP64, column-major) = P̂ᵀP̂ over K = Kp, FP32 chunk tiles summed in FP64.
+// ev_begin/ev_end (optional) are recorded around the SYRK kernel alone.
 void split_syrk(const Plane2D& P, int m, int Kp, const SplitSyrkPlan& plan, float* partial,
-                double* S, int* err, cudaStream_t st);
+                double* S, int* err, cudaStream_t st, cudaEvent_t ev_begin = nullptr,
+                cudaEvent_t ev_end = nullptr);
 
 void split_A_dense(const double* A, long long K, int m, long long off, int k, int kp,
                    __nv_bfloat16* const* planes, long long Kp, long long o, cudaStream_t st);

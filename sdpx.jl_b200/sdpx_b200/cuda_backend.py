@@ -94,6 +94,7 @@ _SIGS = {
     "sdpx_b200_certificate": [C.c_void_p, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double,
                               C.c_int32, C.POINTER(CertificateResult)],
     "sdpx_b200_phase_times": [C.c_void_p, _dp, C.c_int],
+    "sdpx_b200_kernel_times": [C.c_void_p, _dp],
     "sdpx_b200_reset": [C.c_void_p],
     "sdpx_b200_get_precision": [C.c_void_p, _ip, _ip, _dp],
     "sdpx_b200_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
@@ -485,6 +486,13 @@ class CudaBackend:
         self._in_loop = False
         self._history = []
         self._switch_reason = None
+
+    def kernel_times(self) -> dict:
+        """Device ms of the latest Schur kernel launches (see sdpx_b200_kernel_times)."""
+        out = np.zeros(4)
+        self._call("sdpx_b200_kernel_times", _p(out))
+        return dict(split_syrk=float(out[0]), split_block_products=float(out[1]),
+                    fp64_syrk=float(out[2]), fp64_block_products=float(out[3]))
 
     def stream_handle(self) -> int:
         p = C.c_void_p()
