@@ -40,7 +40,7 @@ TOL = 1e-8
 # DRAM bytes (read + write) of one k_split_syrk_tma launch on the sdp_m2000
 # workload, from one ncu capture of dram__bytes_read.sum + dram__bytes_write.sum
 # (a single-pass metric set) on that workload.
-SPLIT_SYRK_DRAM_BYTES = None
+SPLIT_SYRK_DRAM_BYTES = 2.44e9 + 0.6335e9
 # LP standard form + Lorentz cones: the reduced normal matrix Q = Bᵀ D⁻¹ B + δI.
 NORMAL_WORKLOAD = dict(m=3000, n_lp=20000, cones=[64] * 100, density=0.1,
                        label="LP+SOC reduced normal matrix: 3000 equalities x (20000 LP + "
@@ -55,6 +55,22 @@ def schur_flops(m, blocks, lp):
     f = sum(2.0 * k ** 3 * m + m * (m + 1.0) * k ** 2 for k in blocks)
     f += lp * (2.0 * m + m * (m + 1.0))
     return f
+
+
+def syrk_units(m, Kp, sm_count=148):
+    """CTAs (lower 128×128 tiles × K chunks) of the split SYRK, as the library plans them."""
+    nt = (m + 127) // 128
+    ntri = nt * (nt + 1) // 2
+    base_c = max(1, (Kp + 4095) // 4096)
+    best_c, best = base_c, -1.0
+    for c in range(base_c, 2 * base_c + 9):
+        waves = ntri * c / sm_count
+        eff = waves / math.ceil(waves)
+        if eff > best + 1e-9:
+            best, best_c = eff, c
+    kc = (Kp + best_c - 1) // best_c
+    kc = (kc + 63) // 64 * 64
+    return ntri * ((Kp + kc - 1) // kc)
 
 
 def dist_setup():
@@ -478,7 +494,8 @@ def run_ours(args, world, rank, local):
                                    "assembly, one launch per build)",
                          "algorithmic_flops_per_launch": syrk_flops,
                          "launch_ms": syrk_ms,
-                         "algorithmic_bytes_per_launch": 6.0 * wl["m"] * Kp,
+                         "algorithmic_bytes_per_launch":
+                             6.0 * wl["m"] * Kp + 4.0 * 128 * 128 * syrk_units(wl["m"], Kp),
                          "hardware_flops_per_launch": hw_flops,
                          "hardware_frac": hw_flops / (syrk_ms / 1000.0) / 1e12 / peak,
                          "peak_kind": f"bf16_tflops of {peak_kind} MEASURED_PEAKS.json; "

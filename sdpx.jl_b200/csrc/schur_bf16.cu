@@ -184,18 +184,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   pipe_release(tmem);
 }
 
-// out = A·Bᵀ split into three BF16 output planes.  Grid: x over B rows (output
-// columns), y over A rows.  kmode 0 full K, 1 A lower-triangular (k ≤ row),
-// 2 B lower-triangular (k ≥ col).
+// out = A·Bᵀ split into three BF16 output planes.  The grid's fast index runs
+// over the operand with fewer tiles (a_fast: x over A rows, y over B rows;
+// otherwise the reverse), so the CTAs that share a tile of the large operand
+// run together and read it from L2.  kmode 0 full K, 1 A lower-triangular
+// (k ≤ row), 2 B lower-triangular (k ≥ col).
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_split_gemm_tma(const __grid_constant__ TmaMaps maps, OutMap out, int kmode, int Ktot,
-                     int* err) {
+                     int a_fast, int* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = aligned_smem(smem_raw);
   PipeShared* sh = reinterpret_cast<PipeShared*>(smem + SNST * SSTAGE_BYTES);
   const uint32_t tmem = pipe_init(sh);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int r0 = blockIdx.y * TM, c0 = blockIdx.x * TN;
+  const int r0 = (a_fast ? blockIdx.x : blockIdx.y) * TM;
+  const int c0 = (a_fast ? blockIdx.y : blockIdx.x) * TN;
   int kb = 0, ke = Ktot;
   if (kmode == 1) ke = min(Ktot, r0 + TM);
   if (kmode == 2) kb = (c0 / SK) * SK;
@@ -370,8 +373,11 @@ void split_gemm_planes(const Plane2D& A, const Plane2D& B, int Ktot, const OutMa
     encode_plane_map(&maps.b[p], B.plane[p], B.rows, Ktot, B.pitch);
   }
   ensure_smem(k_split_gemm_tma, SSMEM_BYTES);
-  dim3 grid(ceil_div(out.col_extent, TN), ceil_div(out.rows.extent, TM));
-  k_split_gemm_tma<<<grid, NTHREADS, SSMEM_BYTES, st>>>(maps, out, kmode, Ktot, err);
+  const int ta = ceil_div(out.rows.extent, TM), tb = ceil_div(out.col_extent, TN);
+  const int a_fast = (ta < tb && tb <= 65535) ? 1 : 0;  // grid.y is limited to 65535
+  if (!a_fast && ta > 65535) throw std::invalid_argument("split GEMM: too many tiles");
+  dim3 grid(a_fast ? ta : tb, a_fast ? tb : ta);
+  k_split_gemm_tma<<<grid, NTHREADS, SSMEM_BYTES, st>>>(maps, out, kmode, Ktot, a_fast, err);
   SDPX_LAUNCH_CHECK();
 }
 
