@@ -18,28 +18,20 @@ using CfgSmKK = F64Cfg<64, 64, 2, 2, true, true>;
 using CfgSmMM = F64Cfg<64, 64, 2, 2, false, false>;
 using CfgSmKM = F64Cfg<64, 64, 2, 2, true, false>;
 
-__device__ __forceinline__ double* out_ptr(const OutDesc& C, int r, int c) {
-  return C.base + two_level(r, C.row_inner, C.row_inner_stride, C.row_outer_stride) +
-         two_level(c, C.col_inner, C.col_inner_stride, C.col_outer_stride);
-}
-
+// Grid: the fast index runs over the dimension with fewer tiles (rows_fast: x
+// over row tiles), so CTAs sharing a tile of the larger operand run together.
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::NT) k_gemm(Opnd A, Opnd B, OutDesc C, double alpha,
-                                                  double beta, int mode) {
+                                                  double beta, int mode, int rows_fast) {
   extern __shared__ __align__(16) double smem[];
-  const int n0 = blockIdx.x * Cfg::BN, m0 = blockIdx.y * Cfg::BM;
+  const int n0 = (rows_fast ? blockIdx.y : blockIdx.x) * Cfg::BN;
+  const int m0 = (rows_fast ? blockIdx.x : blockIdx.y) * Cfg::BM;
   int kb, ke;
   k_limits(mode, A.k_extent, m0, n0, Cfg::BM, Cfg::BN, kb, ke);
   double acc[Cfg::FM][Cfg::FN][2];
   zero_acc<Cfg>(acc);
   f64_tile_mainloop<Cfg>(acc, A, B, m0, n0, kb, ke, smem);
-  for_each_acc<Cfg>(acc, [&](int r, int c, double v) {
-    int gr = m0 + r, gc = n0 + c;
-    if (gr < C.rows && gc < C.cols) {
-      double* p = out_ptr(C, gr, gc);
-      *p = (beta == 0.0) ? alpha * v : alpha * v + beta * (*p);
-    }
-  });
+  store_acc<Cfg>(acc, C, m0, n0, alpha, beta);
 }
 
 // In-place  T ← T · L  for a lower-triangular L (k×k, explicit zeros above the
@@ -56,10 +48,7 @@ __global__ void __launch_bounds__(Cfg::NT) k_trmm_right_lower_inplace(Opnd T, Op
     zero_acc<Cfg>(acc);
     f64_tile_mainloop<Cfg>(acc, T, L, m0, n0, n0, K, smem);
     __syncthreads();
-    for_each_acc<Cfg>(acc, [&](int r, int c, double v) {
-      int gr = m0 + r, gc = n0 + c;
-      if (gr < C.rows && gc < C.cols) *out_ptr(C, gr, gc) = v;
-    });
+    store_acc<Cfg>(acc, C, m0, n0, 1.0, 0.0);
     __syncthreads();
   }
 }
@@ -110,9 +99,12 @@ template <class Cfg>
 static void launch_gemm_cfg(const Opnd& A, const Opnd& B, const OutDesc& C, double alpha,
                             double beta, int mode, cudaStream_t st) {
   ensure_smem(k_gemm<Cfg>, Cfg::SMEM_BYTES);
-  dim3 grid(ceil_div(C.cols, Cfg::BN), ceil_div(C.rows, Cfg::BM));
-  if (grid.x == 0 || grid.y == 0) return;
-  k_gemm<Cfg><<<grid, Cfg::NT, Cfg::SMEM_BYTES, st>>>(A, B, C, alpha, beta, mode);
+  const int tr = ceil_div(C.rows, Cfg::BM), tc = ceil_div(C.cols, Cfg::BN);
+  if (tr == 0 || tc == 0) return;
+  const int rows_fast = (tr < tc && tc <= 65535) ? 1 : 0;  // grid.y is limited to 65535
+  if (!rows_fast && tr > 65535) throw std::invalid_argument("gemm_f64: too many row tiles");
+  dim3 grid(rows_fast ? tr : tc, rows_fast ? tc : tr);
+  k_gemm<Cfg><<<grid, Cfg::NT, Cfg::SMEM_BYTES, st>>>(A, B, C, alpha, beta, mode, rows_fast);
   SDPX_LAUNCH_CHECK();
 }
 

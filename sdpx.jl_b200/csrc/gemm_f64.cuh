@@ -160,6 +160,41 @@ __device__ __forceinline__ void for_each_acc(double (&acc)[Cfg::FM][Cfg::FN][2],
       }
 }
 
+// Write alpha·acc (+ beta·C when beta ≠ 0) through C's two-level addressing:
+// the column offsets of this thread's fragments are formed once, the row
+// offset once per fragment row (instead of two index divisions per element).
+template <class Cfg>
+__device__ __forceinline__ void store_acc(double (&acc)[Cfg::FM][Cfg::FN][2], const OutDesc& C,
+                                          int m0, int n0, double alpha, double beta) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = warp / Cfg::WARPS_N, wn = warp % Cfg::WARPS_N;
+  long long co[Cfg::FN][2];
+#pragma unroll
+  for (int fn = 0; fn < Cfg::FN; ++fn)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int col = n0 + wn * Cfg::WTN + fn * 8 + 2 * t + c;
+      co[fn][c] = col < C.cols
+                      ? two_level(col, C.col_inner, C.col_inner_stride, C.col_outer_stride)
+                      : -1;
+    }
+#pragma unroll
+  for (int fm = 0; fm < Cfg::FM; ++fm) {
+    const int row = m0 + wm * Cfg::WTM + fm * 8 + g;
+    if (row >= C.rows) continue;
+    double* rp = C.base + two_level(row, C.row_inner, C.row_inner_stride, C.row_outer_stride);
+#pragma unroll
+    for (int fn = 0; fn < Cfg::FN; ++fn)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        if (co[fn][c] < 0) continue;
+        double* q = rp + co[fn][c];
+        *q = (beta == 0.0) ? alpha * acc[fm][fn][c] : alpha * acc[fm][fn][c] + beta * (*q);
+      }
+  }
+}
+
 __device__ __forceinline__ void k_limits(int mode, int K, int m0, int n0, int BM, int BN, int& kb,
                                          int& ke) {
   kb = 0;
