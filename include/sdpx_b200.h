@@ -237,6 +237,12 @@ int sdpx_b200_certificate(sdpx_b200_handle* h, const double* x, const double* X,
  * products of all blocks; 0 where none ran yet. */
 int sdpx_b200_kernel_times(sdpx_b200_handle* h, double* ms4);
 
+/* Instrumentation (no counterpart in the reference), counts since the last
+ * reset: [0] applications of the matrix-free FP64 Newton operator (mixed-mode
+ * residuals), [1] mixed-guard correction steps, [2] switches from mixed to
+ * FP64, [3] Schur builds. */
+int sdpx_b200_counters(sdpx_b200_handle* h, int64_t* out4);
+
 /* Cumulative device time per phase (ms) since the last reset:
  * [0] residual+block factor, [1] Schur assembly, [2] KKT factor,
  * [3] solves+refinement, [4] directions+RHS, [5] step length, [6] update. */

@@ -107,6 +107,8 @@ struct Handle {
   double last_bpr = 0.0;
   int mixed_predicted_steps = 32;  // from the last FP32 factor's condition estimate
   long long mixed_guard_steps = 0;
+  long long operator_applications = 0;  // matrix-free FP64 Newton operator (mixed mode)
+  long long schur_builds = 0;
   int mixed_fallbacks = 0;
 
   // batched Cholesky workspace (dense blocks X, Y and line-search trials)
@@ -621,6 +623,8 @@ struct Handle {
     if (mixed) mixed->a_planes_valid = false;
     mixed_fallbacks = 0;
     mixed_guard_steps = 0;
+    operator_applications = 0;
+    schur_builds = 0;
     mixed_predicted_steps = 32;
     if (have_original) {
       d2d(A.p, A0.p, sizeof(double) * K * m);
@@ -776,6 +780,7 @@ struct Handle {
 
   // ------------------------------------------------------------- Schur ----
   void schur_build(int identity) {
+    ++schur_builds;
     PhaseScope ps(this, 1);
     if (precision == SDPX_B200_MIXED && !identity && mixed) {
       mixed_schur();
@@ -2242,6 +2247,15 @@ int sdpx_b200_get_precision(sdpx_b200_handle* h, int* mode, int* fallbacks, doub
     *mode = h->h.precision;
     if (fallbacks) *fallbacks = h->h.mixed_fallbacks;
     if (cond_estimate) *cond_estimate = h->h.mixed ? h->h.mixed->cond_estimate : 0.0;
+  });
+}
+int sdpx_b200_counters(sdpx_b200_handle* h, int64_t* out4) {
+  GUARD(h, {
+    if (!out4) throw std::invalid_argument("counters: NULL output");
+    out4[0] = h->h.operator_applications;
+    out4[1] = h->h.mixed_guard_steps;
+    out4[2] = h->h.mixed_fallbacks;
+    out4[3] = h->h.schur_builds;
   });
 }
 int sdpx_b200_get_stream(sdpx_b200_handle* h, void** stream) { GUARD(h, *stream = (void*)h->h.st); }

@@ -95,6 +95,7 @@ _SIGS = {
                               C.c_int32, C.POINTER(CertificateResult)],
     "sdpx_b200_phase_times": [C.c_void_p, _dp, C.c_int],
     "sdpx_b200_kernel_times": [C.c_void_p, _dp],
+    "sdpx_b200_counters": [C.c_void_p, C.POINTER(C.c_int64)],
     "sdpx_b200_reset": [C.c_void_p],
     "sdpx_b200_get_precision": [C.c_void_p, _ip, _ip, _dp],
     "sdpx_b200_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
@@ -493,6 +494,13 @@ class CudaBackend:
         self._call("sdpx_b200_kernel_times", _p(out))
         return dict(split_syrk=float(out[0]), split_block_products=float(out[1]),
                     fp64_syrk=float(out[2]), fp64_block_products=float(out[3]))
+
+    def counters(self) -> dict:
+        """Operator applications, guard steps, FP64 switches, Schur builds since reset."""
+        out = (C.c_int64 * 4)()
+        self._call("sdpx_b200_counters", out)
+        return dict(operator_applications=out[0], guard_steps=out[1], fp64_switches=out[2],
+                    schur_builds=out[3])
 
     def stream_handle(self) -> int:
         p = C.c_void_p()
