@@ -3,10 +3,12 @@
 // Every FP64 (or FP32) operand value v is carried as three BF16 "planes"
 // v ≈ v0 + v1 + v2 (v0 = bf16(v), v1 = bf16(v − v0), v2 = bf16(v − v0 − v1),
 // 24 significant bits).  A product Σ_k a_k b_k is formed as the six plane
-// products with i + j ≤ 2, all accumulated in one FP32 TMEM accumulator
-// (the dropped terms are below 2^-24 relative).  Long contractions are cut
-// into K chunks whose FP32 tiles are summed in FP64, so the accumulation error
-// does not grow with K.
+// products with i + j ≤ 2 (the dropped terms are below 2^-24 relative) in two
+// FP32 TMEM accumulators: the leading product a0·b0 in one, the five
+// lower-order products (≈ 2^-8 of it) in the other, so each MMA instruction
+// rounds at the magnitude of what it adds; the two are added once in the
+// epilogue.  Long contractions are cut into K chunks whose FP32 tiles are
+// summed in FP64, so the accumulation error does not grow with K.
 //
 // One TMA-fed engine serves the three products of the Schur assembly
 //   T_i = L_X⁻¹ A_i         (A operand: rows of W = L_X⁻¹; B operand: columns of A_i)
@@ -75,7 +77,8 @@ __device__ __forceinline__ unsigned char* aligned_smem(unsigned char* raw) {
                                           ~uintptr_t(1023));
 }
 
-// Barrier set-up and the 128-column TMEM accumulator (all threads).
+// Barrier set-up and the TMEM accumulators (all threads): columns [0, 128)
+// hold the leading product a0·b0, columns [128, 256) the lower-order products.
 __device__ __forceinline__ uint32_t pipe_init(PipeShared* sh) {
   if (threadIdx.x == 0) {
     for (int s = 0; s < SNST; ++s) {
@@ -85,7 +88,7 @@ __device__ __forceinline__ uint32_t pipe_init(PipeShared* sh) {
     umma::mbar_init(&sh->done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
-  if ((threadIdx.x >> 5) == 0) umma::tmem_alloc(&sh->tmem, 128);
+  if ((threadIdx.x >> 5) == 0) umma::tmem_alloc(&sh->tmem, 256);
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
@@ -131,7 +134,9 @@ __device__ bool pipe_mainloop(const TmaMaps& maps, int ra, int rb, int kb, int n
         for (int q = 0; q < 6; ++q) {
           const uint64_t ad = umma::smem_desc_sw64(base + pa[q] * SPLANE_BYTES + ks * 32);
           const uint64_t bd = umma::smem_desc_sw64(base + (3 + pb[q]) * SPLANE_BYTES + ks * 32);
-          umma::mma_bf16(tmem, ad, bd, IDESC, (t > 0 || ks > 0 || q > 0) ? 1u : 0u);
+          // q = 0 → leading accumulator; q ≥ 1 → lower-order accumulator (first write at q = 1)
+          const uint32_t acc = (t > 0 || ks > 0 || q > 1) ? 1u : 0u;
+          umma::mma_bf16(q == 0 ? tmem : tmem + 128, ad, bd, IDESC, acc);
         }
       }
       umma::commit(&sh->empty[s]);
@@ -144,10 +149,21 @@ __device__ bool pipe_mainloop(const TmaMaps& maps, int ra, int rb, int kb, int n
   return __syncthreads_and(ok ? 1 : 0) != 0;
 }
 
+// 32 columns [cb, cb+32) of this warp's 32 accumulator rows: leading plus
+// lower-order accumulator (one FP32 addition).
+__device__ __forceinline__ void tile_ld32(uint32_t tmem, int warp, int cb, float (&v)[32]) {
+  float lo[32];
+  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  umma::tmem_ld32(tmem + lane_base + (uint32_t)cb, v);
+  umma::tmem_ld32(tmem + lane_base + 128u + (uint32_t)cb, lo);
+#pragma unroll
+  for (int q = 0; q < 32; ++q) v[q] += lo[q];
+}
+
 __device__ __forceinline__ void pipe_release(uint32_t tmem) {
   umma::fence_before_sync();
   __syncthreads();
-  if ((threadIdx.x >> 5) == 0) umma::tmem_dealloc(tmem, 128);
+  if ((threadIdx.x >> 5) == 0) umma::tmem_dealloc(tmem, 256);
 }
 
 // Lower SYRK S = P̂ᵀP̂: one CTA per (K chunk, lower 128×128 tile); the FP32
@@ -173,7 +189,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (ok && ntiles > 0) {
     for (int cb = 0; cb < TN; cb += 32) {
       float v[32];
-      umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
+      tile_ld32(tmem, warp, cb, v);
 #pragma unroll
       for (int q = 0; q < 32; q += 4)
         *reinterpret_cast<float4*>(dst0 + cb + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
@@ -212,7 +228,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     for (int cb = 0; cb < TN; cb += 32) {
       float v[32];
       if (ntiles > 0) {
-        umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
+        tile_ld32(tmem, warp, cb, v);
       } else {
 #pragma unroll
         for (int q = 0; q < 32; ++q) v[q] = 0.f;
