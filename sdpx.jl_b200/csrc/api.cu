@@ -1371,8 +1371,15 @@ struct Handle {
           q.b = (int)b;
           probs.push_back(q);
         }
-    constexpr int DEPTH = 4;
+    // Each round evaluates a complete tree of the next `depth` bisection steps
+    // of every unfinished problem in one batched Cholesky; the deepest tree
+    // that keeps the batch within about one trial matrix per SM is used (a
+    // round costs about the same for any batch up to one wave).
     while (true) {
+      int active = 0;
+      for (auto& P : probs) active += P.finished ? 0 : 1;
+      int DEPTH = 4;
+      while (DEPTH < 7 && active * ((1 << (DEPTH + 1)) - 1) <= sms - 16) ++DEPTH;
       std::vector<TrialReq> reqs;
       std::vector<std::vector<double>> pts(probs.size());
       std::vector<size_t> first_req(probs.size());
@@ -1425,7 +1432,11 @@ struct Handle {
           ++depth;
         }
         P.done += depth;
-        if (P.done >= 64) {
+        // Once [lo, hi] holds no double strictly inside, every remaining
+        // midpoint equals hi (a failing point: the full step or a failed trial)
+        // or lo > 0 (a passing trial), so the remaining steps leave lo as it is.
+        const double mid = (P.lo + P.hi) / 2.0;
+        if (P.done >= 64 || mid == P.hi || (mid == P.lo && P.lo > 0.0)) {
           P.finished = true;
           P.result = P.lo;
         }
