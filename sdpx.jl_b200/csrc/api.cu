@@ -109,6 +109,10 @@ struct Handle {
   long long mixed_guard_steps = 0;
   long long operator_applications = 0;  // matrix-free FP64 Newton operator (mixed mode)
   long long schur_builds = 0;
+  // The current S is the identity-metric S = 𝒜ᵀ𝒜 of the KKT cold start (so
+  // the matrix-free operator of the mixed guard is 𝒜ᵀ𝒜, and an FP64 rebuild
+  // must rebuild that same matrix).
+  bool identity_metric = false;
   int mixed_fallbacks = 0;
 
   // batched Cholesky workspace (dense blocks X, Y and line-search trials)
@@ -623,6 +627,7 @@ struct Handle {
     if (mixed) mixed->a_planes_valid = false;
     mixed_fallbacks = 0;
     mixed_guard_steps = 0;
+    identity_metric = false;
     operator_applications = 0;
     schur_builds = 0;
     mixed_predicted_steps = 32;
@@ -782,8 +787,9 @@ struct Handle {
   void schur_build(int identity) {
     ++schur_builds;
     PhaseScope ps(this, 1);
-    if (precision == SDPX_B200_MIXED && !identity && mixed) {
-      mixed_schur();
+    identity_metric = identity != 0;
+    if (precision == SDPX_B200_MIXED && mixed) {
+      schur_split_bf16(identity != 0);
       return;
     }
     schur_build_fp64(identity);
@@ -864,7 +870,7 @@ struct Handle {
       // predicted to converge in ≤ 32 refinements (or failed) — FP64 from here.
       precision = SDPX_B200_FP64;
       ++mixed_fallbacks;
-      schur_build_fp64(0);
+      schur_build_fp64(identity_metric ? 1 : 0);
     }
     MatDesc<double> md{Sf.p, m, m};
     std::vector<MatDesc<double>> one{md};
@@ -955,7 +961,7 @@ struct Handle {
   void switch_to_fp64_now() {
     precision = SDPX_B200_FP64;
     ++mixed_fallbacks;
-    schur_build_fp64(0);
+    schur_build_fp64(identity_metric ? 1 : 0);
     int ok = 0, att = 0;
     double q = 0.0;
     factorize(&ok, &att, &q);
@@ -2023,8 +2029,7 @@ struct Handle {
   // ------------------------------------------------------- mixed precision --
   void mixed_init();
   void mixed_check_err();
-  void mixed_schur();
-  void schur_split_bf16();
+  void schur_split_bf16(bool identity);
   void mixed_factorize(int* ok, int* attempts, double* quality);
   void mixed_solve(double* vec);
   void mixed_residual();
