@@ -314,12 +314,6 @@ class CudaBackend:
         return v.value
 
     def schur_build(self, identity=False):
-        # A mixed-precision solve runs its KKT cold start in mixed mode too: the
-        # identity-metric S = 𝒜ᵀ𝒜 is assembled by the split engine, factored in
-        # FP32 and the cold-start solves are refined against the FP64 operator
-        # 𝒜ᵀ𝒜, so they reach the FP64 solution.
-        if identity and self.requested == "mixed" and not self._in_loop and self.mode != "mixed":
-            self._set_mode("mixed")
         self._call("sdpx_b200_schur_build", int(bool(identity)))
 
     def factorize(self):
