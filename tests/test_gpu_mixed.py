@@ -68,3 +68,31 @@ def test_mixed_solve_matches_fp64_solve(cuda):
     assert rmx.dObj == pytest.approx(r64.dObj, rel=1e-7)
     assert rmx.relative_gap <= 1e-8
     assert "mixed" in rmx.precision_trace
+
+
+def test_mixed_identity_schur_and_guarded_solve(cuda):
+    """The identity-metric S = 𝒜ᵀ𝒜 (KKT cold start) built in mixed mode agrees
+    with the FP64 build to the split tolerance, and the guarded solve refined
+    against the FP64 operator 𝒜ᵀ𝒜 reaches the FP64 solve's direction."""
+    prob = G.sdpa_dense(m=120, blocks=[30, 7, 2], lp=5, seed=8)
+    with cuda(prob) as be:
+        be.schur_build(identity=True)
+        S64 = be.schur_matrix()
+        assert be.factorize()["ok"]
+        be.set_rhs("cold_dual")
+        be.solve_direction()
+        dx64 = be.get_direction()[0].copy()
+        be._set_mode("mixed")
+        be.schur_build(identity=True)
+        Smix = be.schur_matrix()
+        assert be.factorize()["ok"]
+        be.set_rhs("cold_dual")
+        be.solve_direction()
+        steps, res = be.refine("auto", 0.0, 8, 0)
+        dxm = be.get_direction()[0].copy()
+        residual, rnorm = be.direction_residual()
+        assert be.counters()["operator_applications"] > 0
+    scale = np.max(np.abs(S64))
+    assert np.max(np.abs(Smix - S64)) / scale <= SPLIT_TOL
+    assert residual <= 1e-10 * max(rnorm, 1.0)
+    assert np.allclose(dxm, dx64, rtol=1e-9, atol=1e-9 * np.max(np.abs(dx64)))
