@@ -57,6 +57,18 @@ def schur_flops(m, blocks, lp):
     return f
 
 
+def metric_name(wl):
+    return f"time-to-1e-8 relative duality gap, m={wl['m']} dense SDP"
+
+
+def workload_config(wl):
+    """`config` of both arms (the same workload and metric)."""
+    return {"workload": wl["label"], "m": wl["m"], "blocks": wl["blocks"], "lp": wl["lp"],
+            "tolerance": TOL, "seed": "rank (instance seed; the reference arm runs rank 0's)",
+            "l2": "inputs (constraint data 3.2 GB) larger than L2; not flushed",
+            "parallelism": "replicas (independent instance per GPU)"}
+
+
 def syrk_units(m, Kp, sm_count=148):
     """CTAs (lower 128×128 tiles × K chunks) of the split SYRK, as the library plans them."""
     nt = (m + 127) // 128
@@ -99,7 +111,8 @@ def max_over_ranks(v, world):
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -226,12 +239,11 @@ def run_reference(args, world, rank):
     n_it = iters or 20
     value = t_it * n_it
     line = {
-        "impl": "reference", "metric": "time-to-1e-8 relative duality gap, m=2000 dense SDP",
+        "impl": "reference", "metric": metric_name(wl),
         "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t_it * 1000.0, "higher_is_better": False, "scaling": "weak",
+        "ms_per_step": value * 1000.0, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl["label"], "m": wl["m"], "blocks": wl["blocks"], "lp": wl["lp"],
-                   "tolerance": TOL},
+        "config": workload_config(wl),
         "cpu_baseline": {"value": value, "unit": "s", "cores": cpu_threads(), "kind": "port",
                          "sample": (f"one Newton iteration (residuals, Schur, Cholesky, predictor/"
                                     f"corrector, refinement, line search) of the same instance per "
@@ -461,16 +473,14 @@ def run_ours(args, world, rank, local):
                               f"restatement (NumPy/OpenBLAS), {t_it:.2f} s, × the "
                               f"{last.iterations} iterations of the GPU solve")}
         line = {
-            "metric": "time-to-1e-8 relative duality gap (mixed-precision B200 path), m=2000 dense SDP",
+            "metric": metric_name(wl),
+            "path": "mixed precision (split-BF16 Schur, FP32 factor, FP64 refinement, FP64 tail)",
             "value": ms_per_step / 1000.0, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 in/out; Schur assembly mode per precision_trace, FP32 factor, FP64 refinement",
             "data": "synthetic",
-            "config": {"workload": wl["label"], "m": wl["m"], "blocks": wl["blocks"],
-                       "lp": wl["lp"], "tolerance": TOL, "seed": "rank",
-                       "l2": "inputs (constraint data 3.2 GB) larger than L2; not flushed",
-                       "parallelism": "replicas (independent instance per GPU)"},
+            "config": workload_config(wl),
             "status": last.status.value, "iterations": last.iterations,
             "objective": last.pObj, "relative_gap": last.relative_gap,
             "precision_trace": "".join("m" if p == "mixed" else "d" for p in last.precision_trace),
