@@ -97,6 +97,7 @@ struct Handle {
   DBuf<double> gemv_part;
   int gemv_chunks = 8;
   DBuf<double> S, Sf, Dinv;
+  DBuf<double> Linv, tmp_mm;       // explicit inverse of the FP64 factor, its scratch
   DBuf<double> partial;
   SyrkPlan syrk;
   DBuf<double> red;                // small reduction scratch
@@ -898,7 +899,18 @@ struct Handle {
     *ok = info[0] == 0 ? 1 : 0;
     double hi = dmx[0], lo = dmn[0];
     *quality = (*ok && hi > 0 && std::isfinite(hi)) ? std::min(1.0, std::max(0.0, lo / hi)) : 0.0;
-    if (*ok) factor_diag_inverses<double, 64>(Sf.p, m, m, Dinv.p, st);
+    if (*ok) {
+      // Solves with the FP64 factor are applied 3-5 times per iteration
+      // (predictor, corrector, refinement corrections), so L is inverted once
+      // (recursive doubling on the DMMA tiles) and each solve is two GEMVs
+      // instead of 2·ceil(m/64) dependent substitution launches; the FP64
+      // refinement against S follows as before.
+      if (Linv.n < (size_t)m * m) {
+        Linv.alloc((size_t)m * m);
+        tmp_mm.alloc((size_t)m * m);
+      }
+      trinv_recursive_f64(Sf.p, m, Linv.p, Dinv.p, tmp_mm.p, st);
+    }
   }
 
   // ------------------------------------------------------------- solves ----
@@ -907,7 +919,8 @@ struct Handle {
       mixed_solve(vec);
       return;
     }
-    cholesky_solve<double, 64>(Sf.p, m, m, Dinv.p, vec, work_m2.p, st);
+    gemv_n(Linv.p, m, m, vec, work_m2.p, gemv_part.p, gemv_chunks, st);
+    gemv_t(Linv.p, m, m, work_m2.p, 1.0, nullptr, 0.0, vec, st);
   }
   void solve() {
     PhaseScope ps(this, 3);
