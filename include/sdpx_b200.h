@@ -230,6 +230,13 @@ int sdpx_b200_certificate(sdpx_b200_handle* h, const double* x, const double* X,
                           double eps_primal, double eps_dual, double eps_gap, int32_t legacy_gap,
                           sdpx_b200_certificate_result* out);
 
+/* Engine of the FP64 Schur Gram S = P̂ᵀP̂ (no counterpart in the reference,
+ * whose Float64 SYRK is BLAS): 0 = FP64 DMMA tiles (default), 1 = exact int8
+ * digit products on the tensor cores — every P̂ column scaled by a power of two
+ * and cut into seven int8 digits (48 significant bits), digit products
+ * accumulated exactly in int32 and the levels summed in FP64. */
+int sdpx_b200_set_gram_engine(sdpx_b200_handle* h, int engine);
+
 /* Instrumentation (no counterpart in the reference): device time (ms) of the
  * most recent launch of the Schur kernels, measured with events on the
  * handle's stream: [0] split-BF16 SYRK kernel, [1] split-BF16 block products

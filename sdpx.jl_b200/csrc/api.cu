@@ -25,6 +25,7 @@
 #include "chol.h"
 #include "dbuf.h"
 #include "mixed.h"
+#include "ozaki.h"
 #include "schur_bf16.h"
 #include "vec_kernels.h"
 
@@ -98,6 +99,13 @@ struct Handle {
   int gemv_chunks = 8;
   DBuf<double> S, Sf, Dinv;
   DBuf<double> Linv, tmp_mm;       // explicit inverse of the FP64 factor, its scratch
+  // FP64 Gram engine of the Schur SYRK: 0 = FP64 DMMA tiles, 1 = exact int8
+  // digit products (48-bit digits, int32 accumulation, FP64 level sums).
+  int gram_engine = 0;
+  OzakiPlan oz_plan;
+  DBuf<int8_t> oz_digits;
+  DBuf<int> oz_exps, oz_err;
+  DBuf<double> oz_partial;
   DBuf<double> partial;
   SyrkPlan syrk;
   DBuf<double> red;                // small reduction scratch
@@ -856,8 +864,25 @@ struct Handle {
     Pd.mn_extent = m;
     Pd.k_extent = (int)K;
     kt_begin(2);
-    syrk_lower_f64(Pd, syrk, partial.p, S.p, m, m, 0.0, st);
-    kt_end(2);
+    if (gram_engine == 1) {
+      if (oz_plan.m != m || oz_plan.K != K) {
+        oz_plan = plan_ozaki_syrk(m, K, sms);
+        oz_digits.alloc(oz_plan.digit_bytes);
+        oz_exps.alloc(m);
+        oz_err.alloc(1);
+        oz_err.zero(st);
+        oz_partial.alloc(oz_plan.partial_alloc_doubles);
+      }
+      ozaki_syrk(panel, oz_plan, oz_digits.p, oz_exps.p, oz_partial.p, S.p, oz_err.p, st);
+      kt_end(2);
+      int e = 0;
+      d2h(&e, oz_err.p, sizeof(int));
+      sync();
+      if (e) throw CudaError("int8 Gram kernel: a bounded wait gave up");
+    } else {
+      syrk_lower_f64(Pd, syrk, partial.p, S.p, m, m, 0.0, st);
+      kt_end(2);
+    }
     mirror_lower(m, S.p, st);
   }
 
@@ -2309,6 +2334,12 @@ int sdpx_b200_gram_noalloc(const double* P, int64_t K, int32_t m, double* S, voi
     g_noalloc_error = ex.what();
     return -2;
   }
+}
+int sdpx_b200_set_gram_engine(sdpx_b200_handle* h, int engine) {
+  GUARD(h, {
+    if (engine != 0 && engine != 1) throw std::invalid_argument("gram engine must be 0 or 1");
+    h->h.gram_engine = engine;
+  });
 }
 int sdpx_b200_kernel_times(sdpx_b200_handle* h, double* ms4) {
   GUARD(h, {

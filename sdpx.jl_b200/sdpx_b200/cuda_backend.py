@@ -95,6 +95,7 @@ _SIGS = {
                               C.c_int32, C.POINTER(CertificateResult)],
     "sdpx_b200_phase_times": [C.c_void_p, _dp, C.c_int],
     "sdpx_b200_kernel_times": [C.c_void_p, _dp],
+    "sdpx_b200_set_gram_engine": [C.c_void_p, C.c_int],
     "sdpx_b200_counters": [C.c_void_p, C.POINTER(C.c_int64)],
     "sdpx_b200_reset": [C.c_void_p],
     "sdpx_b200_get_precision": [C.c_void_p, _ip, _ip, _dp],
@@ -487,6 +488,11 @@ class CudaBackend:
         self._in_loop = False
         self._history = []
         self._switch_reason = None
+
+    def set_gram_engine(self, engine: str):
+        """FP64 Schur Gram engine: "dmma" (FP64 tensor tiles) or "int8" (exact
+        int8 digit products, 48-bit digits)."""
+        self._call("sdpx_b200_set_gram_engine", {"dmma": 0, "int8": 1}[engine])
 
     def kernel_times(self) -> dict:
         """Device ms of the latest Schur kernel launches (see sdpx_b200_kernel_times)."""
