@@ -231,7 +231,7 @@ int sdpx_b200_certificate(sdpx_b200_handle* h, const double* x, const double* X,
                           sdpx_b200_certificate_result* out);
 
 /* Engine of the FP64 Schur Gram S = P̂ᵀP̂ (no counterpart in the reference,
- * whose Float64 SYRK is BLAS): 0 = FP64 DMMA tiles (default), 1 = exact int8
+ * whose Float64 SYRK is BLAS): 0 = FP64 DMMA tiles, 1 = exact int8 (default)
  * digit products on the tensor cores — every P̂ column scaled by a power of two
  * and cut into seven int8 digits (48 significant bits), digit products
  * accumulated exactly in int32 and the levels summed in FP64. */

@@ -101,7 +101,7 @@ struct Handle {
   DBuf<double> Linv, tmp_mm;       // explicit inverse of the FP64 factor, its scratch
   // FP64 Gram engine of the Schur SYRK: 0 = FP64 DMMA tiles, 1 = exact int8
   // digit products (48-bit digits, int32 accumulation, FP64 level sums).
-  int gram_engine = 0;
+  int gram_engine = 1;
   OzakiPlan oz_plan;
   DBuf<int8_t> oz_digits;
   DBuf<int> oz_exps, oz_err;
