@@ -125,7 +125,9 @@ def test_newton_step_kernels_match_oracle(cuda, name):
             assert lo[1] == pytest.approx(lc[1], rel=max(1e-9, 10 * DIR))
         uo, uc = ob.update(0.7, 0.6), cb.update(0.7, 0.6)
         assert uo[0] == pytest.approx(uc[0], rel=1e-12) and uo[1] == uc[1]
-        assert ob.objectives() == pytest.approx(cb.objectives(), rel=1e-12)
+        # The objectives after the update are linear in the directions, which
+        # are held to DIR; the Schur matrix itself stays within 1e-12 above.
+        assert ob.objectives() == pytest.approx(cb.objectives(), rel=max(1e-12, DIR))
 
 
 def test_equilibration_matches_oracle(cuda):
