@@ -5,19 +5,19 @@
 // and written as OZ_DIGITS signed int8 digits,
 //   v = 2^-6 (d_0 + 2^-7 d_1 + 2^-14 d_2 + …),  d_0, d_t ∈ [-64, 64],
 // (d_0 = rint(64 v), then each remainder times 128 rounded), exactly, with the
-// remainder below 2^-(6+7·(OZ_DIGITS-1)) = 2^-48 of the column's largest entry.
+// remainder below 2^-(6+7·(OZ_DIGITS-1)) = 2^-55 of the column's largest entry.
 // Then
 //   S_ij = 2^(e_i+e_j-12) Σ_ℓ 2^(-7ℓ) I_ℓ[i,j],   I_ℓ = Σ_{t+u=ℓ} Σ_k d_t[k,i] d_u[k,j],
 // keeping the levels ℓ ≤ OZ_DIGITS-1.  Each I_ℓ accumulates exactly in an
 // int32 TMEM accumulator (|d_t d_u| ≤ 4096, at most OZ_DIGITS products per
-// level, K chunks ≤ 65 536, so |I_ℓ| < 2^31), so the result carries no
+// level, K chunks ≤ 65 472, so |I_ℓ| < 2^31), so the result carries no
 // accumulation error at all: only the truncation of the digits and the final
 // FP64 sum of the levels round.  Chunks are summed in FP64 in a fixed order.
 //
-// Tiles: 128 rows of P columns (A) × 64 (B); the seven level accumulators take
-// 7·64 = 448 TMEM columns.  128 threads per CTA, one CTA per SM: thread 0
-// issues the TMA boxes (K = 32 bytes per row, 32-byte swizzle, four 42 KB
-// stages), thread 32 issues the 28 MMAs of a stage (M = 128, N = 64, K = 32)
+// Tiles: 128 rows of P columns (A) × 64 (B); the eight level accumulators take
+// all 8·64 = 512 TMEM columns.  128 threads per CTA, one CTA per SM: thread 0
+// issues the TMA boxes (K = 32 bytes per row, 32-byte swizzle, four 48 KB
+// stages), thread 32 issues the 36 MMAs of a stage (M = 128, N = 64, K = 32)
 // and commits them to the stage's "empty" barrier, all four warps convert the
 // int32 levels to FP64 in the epilogue.  Bounded waits with a device error flag;
 // the producer drains its own copies before the CTA exits.  No cluster, no
@@ -43,7 +43,7 @@ constexpr int ONT = 128;                          // threads
 constexpr int ONST = 4;                           // stages
 constexpr int OA_BYTES = OM * OK;                 // 4 KB per digit tile of A
 constexpr int OB_BYTES = ON * OK;                 // 2 KB per digit tile of B
-constexpr int OSTAGE = OZ_DIGITS * (OA_BYTES + OB_BYTES);  // 42 KB
+constexpr int OSTAGE = OZ_DIGITS * (OA_BYTES + OB_BYTES);  // 48 KB
 constexpr size_t OSMEM = ONST * OSTAGE + 1024 + 256;
 constexpr int OLEVELS = OZ_DIGITS;                // levels 0 … OZ_DIGITS-1
 constexpr int NAN_EXP = INT_MIN;                  // column holds a non-finite value
@@ -300,9 +300,9 @@ OzakiPlan plan_ozaki_syrk(int m, long long K, int sm_count) {
   p.ntile_r = ceil_div(m, OM);
   p.ntile_c = ceil_div(m, ON);
   p.ntri = (int)oz_pairs(m).size();
-  // Chunks of at most 65 536 K (exact int32 levels), enough of them to give
-  // about four waves of one CTA per SM.
-  const long long maxc = 65536;
+  // Chunks of at most 65 472 K (exact int32 levels: 65 472 · 8 · 4096 < 2^31),
+  // enough of them to give about four waves of one CTA per SM.
+  const long long maxc = 65472;
   int nc = (int)std::max<long long>(1, (p.Kp + maxc - 1) / maxc);
   while ((long long)p.ntri * nc < 4LL * sm_count && (p.Kp / (nc + 1)) >= 2048) ++nc;
   long long kc = (p.Kp + nc - 1) / nc;

@@ -8,7 +8,7 @@
 
 namespace sdpx {
 
-constexpr int OZ_DIGITS = 7;  // int8 digits per value: 6 + 7·6 = 48 significant bits
+constexpr int OZ_DIGITS = 8;  // int8 digits per value: 6 + 7·7 = 55 significant bits
 
 struct OzakiPlan {
   int m = 0;
