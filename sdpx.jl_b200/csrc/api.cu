@@ -97,6 +97,44 @@ struct Handle {
   DBuf<double> X, Y, P, R, Z, dX, dY, LX, MY, W, T1, T2, Xbest, Ybest, tmpK, tmpK2;
   DBuf<double> gemv_part;
   int gemv_chunks = 8;
+  // Lower-triangle copy of 𝒜 for the memory-bound operator passes (𝒜v and
+  // 𝒜ᵀz read half the bytes): every dense A_i keeps its entries p ≥ c, column
+  // by column, the 1×1 group follows.  ap_lo[q] / ap_up[q] are the stacked rows
+  // of (p, c) and (c, p), equal on the diagonal and in the 1×1 group.  a_ver
+  // counts changes of 𝒜 (equilibration, reset); the copy is rebuilt when stale.
+  DBuf<double> Ap, kt_fold;
+  DBuf<long long> ap_lo, ap_up;
+  long long Kt = 0;
+  unsigned long long a_ver = 1, ap_ver = 0;
+  // adx = 𝒜·dx of the dx version adx_ver (the mixed operator computes it; the
+  // block directions reuse it when dx has not changed since).
+  DBuf<double> adx;
+  unsigned long long dx_ver = 1, adx_ver = 0;
+  void a_changed() {
+    ++a_ver;
+    adx_ver = 0;
+  }
+  void dx_written() { ++dx_ver; }
+  void amul(const double* xv, double* out) {  // out = 𝒜·xv (stacked, symmetric blocks)
+    ensure_packed();
+    gemv_n_sym(Ap.p, Kt, m, xv, ap_lo.p, ap_up.p, out, gemv_part.p, gemv_chunks, st);
+  }
+  // out = alpha·𝒜ᵀz + beta·base; z need not be symmetric (⟨A_i, Z⟩ = ⟨A_i, sym Z⟩).
+  void atmul(const double* z, double alpha, const double* base, double beta, double* out) {
+    ensure_packed();
+    fold_sym(Kt, z, ap_lo.p, ap_up.p, kt_fold.p, st);
+    gemv_t(Ap.p, Kt, m, kt_fold.p, alpha, base, beta, out, st);
+  }
+  void ensure_packed() {
+    if (ap_ver == a_ver) return;
+    pack_rows(A.p, K, m, ap_lo.p, Kt, Ap.p, st);
+    ap_ver = a_ver;
+  }
+  void adx_current() {  // adx ← 𝒜·dx unless it already holds it
+    if (adx_ver == dx_ver) return;
+    amul(dx.p, adx.p);
+    adx_ver = dx_ver;
+  }
   DBuf<double> S, Sf, Dinv;
   DBuf<double> Linv, tmp_mm;       // explicit inverse of the FP64 factor, its scratch
   // FP64 Gram engine of the Schur SYRK: 0 = FP64 DMMA tiles, 1 = exact int8
@@ -464,6 +502,31 @@ struct Handle {
       b->alloc(K), b->zero(st);
     gemv_chunks = std::max(1, std::min(16, m / 64));
     gemv_part.alloc((size_t)gemv_chunks * std::max<long long>(K, m));
+    {
+      std::vector<long long> lo, up;
+      for (auto& b : dense)
+        for (int cc = 0; cc < b.k; ++cc)
+          for (int pp = cc; pp < b.k; ++pp) {
+            lo.push_back(b.off + pp + (long long)cc * b.k);
+            up.push_back(b.off + cc + (long long)pp * b.k);
+          }
+      for (int j = 0; j < nd; ++j) {
+        lo.push_back(od + j);
+        up.push_back(od + j);
+      }
+      Kt = (long long)lo.size();
+      ap_lo.alloc(std::max<long long>(Kt, 1));
+      ap_up.alloc(std::max<long long>(Kt, 1));
+      if (Kt) {
+        h2d(ap_lo.p, lo.data(), Kt * sizeof(long long));
+        h2d(ap_up.p, up.data(), Kt * sizeof(long long));
+      }
+      Ap.alloc((size_t)std::max<long long>(Kt, 1) * m);
+      kt_fold.alloc(std::max<long long>(Kt, 1));
+      adx.alloc(K);
+      adx.zero(st);
+      sync();  // lo/up are host temporaries
+    }
     Pc.alloc((size_t)K * m);
     S.alloc((size_t)m * m);
     Sf.alloc((size_t)m * m);
@@ -630,6 +693,7 @@ struct Handle {
     if (objscale) *objscale = osc;
     if (passes)
       for (int l = 0; l < L; ++l) passes[l] = used[l];
+    a_changed();
   }
 
   void reset() {
@@ -640,6 +704,7 @@ struct Handle {
     operator_applications = 0;
     schur_builds = 0;
     mixed_predicted_steps = 32;
+    a_changed();
     if (have_original) {
       d2d(A.p, A0.p, sizeof(double) * K * m);
       d2d(Cst.p, C0st.p, sizeof(double) * K);
@@ -764,10 +829,10 @@ struct Handle {
                  int* ok) {
     PhaseScope ps(this, 0);
     // P = 𝒜x − X − C
-    gemv_n(A.p, K, m, x.p, tmpK.p, gemv_part.p, gemv_chunks, st);
+    amul(x.p, tmpK.p);
     axpbypcz(K, 1.0, tmpK.p, -1.0, X.p, -1.0, Cst.p, P.p, st);
     // d = c − 𝒜ᵀ vec(Y)
-    gemv_t(A.p, K, m, Y.p, -1.0, c.p, 1.0, d.p, st);
+    atmul(Y.p, -1.0, c.p, 1.0, d.p);
     clear_red(0, 2);
     absmax(K, P.p, red.p + 0, st);
     absmax(m, d.p, red.p + 1, st);
@@ -951,6 +1016,7 @@ struct Handle {
     PhaseScope ps(this, 3);
     d2d(dx.p, r.p, m * sizeof(double));
     solve_into(dx.p);
+    dx_written();
     if (precision == SDPX_B200_MIXED && mixed) mixed_guard();
   }
   // Mixed-precision solve guard (the reference's `_solve_mixed_kkt_guarded!`,
@@ -976,10 +1042,12 @@ struct Handle {
         d2d(work_m.p, rho.p, m * sizeof(double));
         solve_into(work_m.p);
         combine(m, dx.p, 1.0, work_m.p, st);
+        dx_written();
         double corr = residual_norm_only();
         ++mixed_guard_steps;
         if (!std::isfinite(corr) || corr >= res) {
           d2d(dx.p, dxbest.p, m * sizeof(double));
+          dx_written();
           break;
         }
         res = corr;
@@ -1006,6 +1074,7 @@ struct Handle {
     if (!ok) throw CudaError("FP64 fallback factorisation failed");
     d2d(dx.p, r.p, m * sizeof(double));
     solve_into(dx.p);
+    dx_written();
   }
   // ρ = r − S·dx  (FP64 Newton operator)
   void apply_residual() {
@@ -1044,6 +1113,7 @@ struct Handle {
       d2d(work_m.p, rho.p, m * sizeof(double));
       solve_into(work_m.p);
       combine(m, dx.p, 1.0, work_m.p, st);
+      dx_written();
     };
     int steps = 0;
     double residual;
@@ -1061,6 +1131,7 @@ struct Handle {
         double corr = residual_norm_only();
         if (!std::isfinite(corr) || corr >= residual) {
           d2d(dx.p, dxbest.p, m * sizeof(double));
+          dx_written();
           consistent = false;
           break;
         }
@@ -1080,6 +1151,7 @@ struct Handle {
         double corr = residual_norm_only();
         if (!std::isfinite(corr) || corr > residual) {
           d2d(dx.p, dxbest.p, m * sizeof(double));
+          dx_written();
           consistent = false;
           break;
         }
@@ -1104,6 +1176,7 @@ struct Handle {
         double corr = residual_norm_only();
         if (!std::isfinite(corr) || corr > residual) {
           d2d(dx.p, dxbest.p, m * sizeof(double));
+          dx_written();
           consistent = false;
           break;
         }
@@ -1128,7 +1201,7 @@ struct Handle {
     }
     dense_cholsolve(T1.p, Z.p);
     diag_rhs_Z(nd, od, P.p, Y.p, R.p, LX.p, Z.p, st);
-    gemv_t(A.p, K, m, Z.p, -1.0, d.p, -1.0, r.p, st);  // r = −v − d
+    atmul(Z.p, -1.0, d.p, -1.0, r.p);  // r = −v − d
   }
   void rhs_predictor() {
     PhaseScope ps(this, 4);
@@ -1181,15 +1254,15 @@ struct Handle {
     diag_corrector_R(nd, od, X.p, Y.p, dX.p, dY.p, target_user.p, d_diag_user.p, R.p, st);
   }
   void set_rhs(int which) {
-    if (which == 0) gemv_t(A.p, K, m, Cst.p, 1.0, nullptr, 0.0, r.p, st);
+    if (which == 0) atmul(Cst.p, 1.0, nullptr, 0.0, r.p);
     else d2d(r.p, c.p, m * sizeof(double));
   }
 
   // ---------------------------------------------------------- directions --
   void direction_blocks() {
     PhaseScope ps(this, 4);
-    gemv_n(A.p, K, m, dx.p, tmpK.p, gemv_part.p, gemv_chunks, st);
-    axpbypcz(K, 1.0, tmpK.p, 1.0, P.p, 0.0, nullptr, dX.p, st);  // dX = 𝒜dx + P
+    adx_current();
+    axpbypcz(K, 1.0, adx.p, 1.0, P.p, 0.0, nullptr, dX.p, st);  // dX = 𝒜dx + P
     for (auto& b : dense) {
       d2d(T1.p + b.off, R.p + b.off, sizeof(double) * b.k * b.k);
       blk_gemm(blk_as_A(dX.p, b.off, b.k), false, blk_as_B(Y.p, b.off, b.k), true, T1.p, b, -1.0,
@@ -1638,9 +1711,9 @@ struct Handle {
     *dobj = dd;
   }
   void solution_residuals(double* pr, double* dr) {
-    gemv_n(A.p, K, m, x.p, tmpK.p, gemv_part.p, gemv_chunks, st);
+    amul(x.p, tmpK.p);
     axpbypcz(K, 1.0, tmpK.p, -1.0, X.p, -1.0, Cst.p, tmpK2.p, st);
-    gemv_t(A.p, K, m, Y.p, -1.0, c.p, 1.0, work_m.p, st);
+    atmul(Y.p, -1.0, c.p, 1.0, work_m.p);
     clear_red(0, 2);
     absmax(K, tmpK2.p, red.p + 0, st);
     absmax(m, work_m.p, red.p + 1, st);
@@ -1653,9 +1726,9 @@ struct Handle {
   // ---------------------------------------------------------- cold start --
   void cold_start_iterate() {
     d2d(x.p, keptx.p, m * sizeof(double));
-    gemv_n(A.p, K, m, x.p, tmpK.p, gemv_part.p, gemv_chunks, st);
+    amul(x.p, tmpK.p);
     axpbypcz(K, 1.0, tmpK.p, -1.0, Cst.p, 0.0, nullptr, X.p, st);
-    gemv_n(A.p, K, m, dx.p, Y.p, gemv_part.p, gemv_chunks, st);
+    amul(dx.p, Y.p);
   }
   // Per-block certified shift (src/cold_start.jl:287-308) for all blocks at once.
   void psd_shift(int which, int* ok_out) {

@@ -46,6 +46,61 @@ void gemv_n(const double* A, long long K, int m, const double* x, double* out, d
   SDPX_LAUNCH_CHECK_N(2);
 }
 
+// ------------------------------------------- lower-triangle constraints ---
+// Ap[q + i·Kt] = A[rows[q] + i·K]: the rows kept by the packed copy.
+__global__ void k_pack_rows(const double* __restrict__ A, long long K, int m,
+                            const long long* __restrict__ rows, long long Kt,
+                            double* __restrict__ Ap) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= Kt) return;
+  const long long src = rows[q];
+  for (int i = blockIdx.y; i < m; i += gridDim.y) Ap[q + (long long)i * Kt] = A[src + (long long)i * K];
+}
+void pack_rows(const double* A, long long K, int m, const long long* rows, long long Kt, double* Ap,
+               cudaStream_t st) {
+  if (Kt == 0 || m == 0) return;
+  dim3 g(ceil_div(Kt, 256), std::min(m, 64));
+  k_pack_rows<<<g, 256, 0, st>>>(A, K, m, rows, Kt, Ap);
+  SDPX_LAUNCH_CHECK();
+}
+
+// Row sums of the column-chunk partials, written to both stacked positions.
+__global__ void k_gemv_n_reduce_sym(const double* __restrict__ part, long long Kt, int chunks,
+                                    const long long* __restrict__ lo,
+                                    const long long* __restrict__ up, double* __restrict__ out) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= Kt) return;
+  double s = 0;
+  for (int c = 0; c < chunks; ++c) s += part[(long long)c * Kt + q];
+  out[lo[q]] = s;
+  out[up[q]] = s;
+}
+void gemv_n_sym(const double* Ap, long long Kt, int m, const double* x, const long long* lo,
+                const long long* up, double* out, double* part, int chunks, cudaStream_t st) {
+  if (Kt == 0) return;
+  dim3 g(ceil_div(Kt, 256), chunks);
+  k_gemv_n_part<<<g, 256, 0, st>>>(Ap, Kt, m, x, chunks, part);
+  k_gemv_n_reduce_sym<<<ceil_div(Kt, 256), 256, 0, st>>>(part, Kt, chunks, lo, up, out);
+  SDPX_LAUNCH_CHECK_N(2);
+}
+
+// zf[q] = z[lo] + z[up] off the diagonal, z[lo] on it: ⟨A_i, Z⟩ over the
+// lower triangle of a symmetric A_i.
+__global__ void k_fold_sym(long long Kt, const double* __restrict__ z,
+                           const long long* __restrict__ lo, const long long* __restrict__ up,
+                           double* __restrict__ zf) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= Kt) return;
+  const long long a = lo[q], b = up[q];
+  zf[q] = a == b ? z[a] : z[a] + z[b];
+}
+void fold_sym(long long Kt, const double* z, const long long* lo, const long long* up, double* zf,
+              cudaStream_t st) {
+  if (Kt == 0) return;
+  k_fold_sym<<<ceil_div(Kt, 256), 256, 0, st>>>(Kt, z, lo, up, zf);
+  SDPX_LAUNCH_CHECK();
+}
+
 // out[i] = alpha·(A[:,i] · z) + beta·base[i]   (one CTA per column).
 __global__ void k_gemv_t(const double* __restrict__ A, long long K, int m,
                          const double* __restrict__ z, double alpha, const double* __restrict__ base,

@@ -19,6 +19,16 @@ void gemv_n(const double* A, long long K, int m, const double* x, double* out, d
             int chunks, cudaStream_t st);
 void gemv_t(const double* A, long long K, int m, const double* z, double alpha, const double* base,
             double beta, double* out, cudaStream_t st);
+// Lower-triangle copy of the constraint matrix (Kt kept rows per column):
+// pack_rows gathers it, gemv_n_sym writes Ap·x to both stacked positions
+// lo[q] and up[q] of every kept row, fold_sym folds a stacked vector onto the
+// kept rows (z[lo] + z[up] off the diagonal) for Apᵀ·zf = 𝒜ᵀz.
+void pack_rows(const double* A, long long K, int m, const long long* rows, long long Kt, double* Ap,
+               cudaStream_t st);
+void gemv_n_sym(const double* Ap, long long Kt, int m, const double* x, const long long* lo,
+                const long long* up, double* out, double* part, int chunks, cudaStream_t st);
+void fold_sym(long long Kt, const double* z, const long long* lo, const long long* up, double* zf,
+              cudaStream_t st);
 void axpbypcz(long long n, double a, const double* x, double b, const double* y, double c,
               const double* z, double* out, cudaStream_t st);
 void combine(long long n, double* x, double t, const double* d, cudaStream_t st);
