@@ -144,6 +144,20 @@ struct Handle {
   DBuf<int8_t> oz_digits;
   DBuf<int> oz_exps, oz_err;
   DBuf<double> oz_partial;
+  // FP64 block products on the same digit engine: T_i = W·A_i is written
+  // row-major into Pc's block region, its rows are cut into digits and
+  // P_i = T_i·M_Y overwrites the region column-major (the Gram's layout).  The
+  // digits of the constraint matrices are cut once per version of 𝒜.
+  struct OzBlock {
+    long long kp = 0;
+    size_t dig_off = 0;
+    long long exp_off = 0;
+  };
+  std::vector<OzBlock> ozb;
+  DBuf<int8_t> oz_adig, oz_tdig, oz_wdig;
+  DBuf<int> oz_aexp, oz_texp, oz_wexp;
+  unsigned long long oz_a_ver = 0;
+  int oz_blk_state = 0;  // 0 = not planned, 1 = digit products, -1 = DMMA tiles (memory)
   DBuf<double> partial;
   SyrkPlan syrk;
   DBuf<double> red;                // small reduction scratch
@@ -500,6 +514,8 @@ struct Handle {
       b->alloc(m), b->zero(st);
     for (auto* b : {&X, &Y, &P, &R, &Z, &dX, &dY, &LX, &MY, &W, &T1, &T2, &Xbest, &Ybest, &tmpK2})
       b->alloc(K), b->zero(st);
+    oz_err.alloc(1);
+    oz_err.zero(st);
     gemv_chunks = std::max(1, std::min(16, m / 64));
     gemv_part.alloc((size_t)gemv_chunks * std::max<long long>(K, m));
     {
@@ -868,11 +884,126 @@ struct Handle {
     }
     schur_build_fp64(identity);
   }
+  bool oz_blocks_ready() {
+    if (oz_blk_state == 0) {
+      size_t adig = 0, tdig = 0, wdig = 0;
+      long long aexp = 0, texp = 0, wexp = 0;
+      ozb.clear();
+      for (auto& b : dense) {
+        OzBlock o;
+        o.kp = oz_kpad(b.k);
+        o.dig_off = adig;
+        o.exp_off = aexp;
+        const size_t rows = (size_t)b.k * m;
+        adig += (size_t)OZ_DIGITS * rows * (size_t)o.kp;
+        aexp += (long long)rows;
+        tdig = std::max(tdig, (size_t)OZ_DIGITS * rows * (size_t)o.kp);
+        texp = std::max(texp, (long long)rows);
+        wdig = std::max(wdig, (size_t)2 * OZ_DIGITS * (size_t)b.k * (size_t)o.kp);
+        wexp = std::max(wexp, 2LL * b.k);
+        ozb.push_back(o);
+      }
+      // Room for the cached constraint digits, the per-build scratch and the
+      // Gram's digit planes (same size as the FP64 panel), with 2 GB to spare.
+      size_t freeb = 0, totb = 0;
+      SDPX_CUDA(cudaMemGetInfo(&freeb, &totb));
+      const size_t gram = oz_plan.m == m && oz_plan.K == K ? 0 : (size_t)OZ_DIGITS * m * (K + 64);
+      const size_t need = adig + tdig + wdig + 4 * (size_t)(aexp + texp + wexp) + gram;
+      if (dense.empty() || need + (2ull << 30) > freeb) {
+        oz_blk_state = -1;
+      } else {
+        oz_adig.alloc(adig);
+        oz_tdig.alloc(tdig);
+        oz_wdig.alloc(wdig);
+        oz_aexp.alloc(aexp);
+        oz_texp.alloc(texp);
+        oz_wexp.alloc(wexp);
+        oz_a_ver = 0;
+        oz_blk_state = 1;
+      }
+    }
+    return oz_blk_state == 1;
+  }
+  void oz_block_products() {
+    if (oz_a_ver != a_ver) {
+      for (size_t bi = 0; bi < dense.size(); ++bi) {
+        const DenseBlk& b = dense[bi];
+        const OzBlock& o = ozb[bi];
+        OzRows r;  // row (i, c): A_i[p, c] at off + i·K + c·k + p
+        r.base = A.p + b.off;
+        r.rows = (long long)b.k * m;
+        r.inner = b.k;
+        r.is = b.k;
+        r.os = K;
+        r.len = b.k;
+        ozaki_digits_rows(r, o.kp, r.rows * o.kp, oz_adig.p + o.dig_off, oz_aexp.p + o.exp_off, st);
+      }
+      oz_a_ver = a_ver;
+    }
+    for (size_t bi = 0; bi < dense.size(); ++bi) {
+      const DenseBlk& b = dense[bi];
+      const OzBlock& o = ozb[bi];
+      const long long rows = (long long)b.k * m;
+      const long long aplane = rows * o.kp, wplane = (long long)b.k * o.kp;
+      int8_t* wd = oz_wdig.p;
+      int8_t* yd = oz_wdig.p + OZ_DIGITS * wplane;
+      int* we = oz_wexp.p;
+      int* ye = oz_wexp.p + b.k;
+      OzRows w;  // row r of W: W[r, p] at off + r + p·k, p ≤ r
+      w.base = W.p + b.off;
+      w.rows = b.k;
+      w.is = 1;
+      w.es = b.k;
+      w.len = b.k;
+      w.tri = 1;
+      ozaki_digits_rows(w, o.kp, wplane, wd, we, st);
+      OzRows y;  // column c' of M_Y: M_Y[c, c'] at off + c + c'·k, c ≥ c'
+      y.base = MY.p + b.off;
+      y.rows = b.k;
+      y.is = b.k;
+      y.len = b.k;
+      y.tri = 2;
+      ozaki_digits_rows(y, o.kp, wplane, yd, ye, st);
+      OzGemm g;  // T_i[r, c] = Σ_p A_i[p, c]·W[r, p] → Pc[off + i·K + r·k + c]
+      g.xd = oz_adig.p + o.dig_off;
+      g.x_plane = aplane;
+      g.rows_a = (int)rows;
+      g.ea = oz_aexp.p + o.exp_off;
+      g.yd = wd;
+      g.y_plane = wplane;
+      g.rows_b = b.k;
+      g.eb = we;
+      g.Kp = o.kp;
+      g.kmode = 1;
+      g.out = Pc.p + b.off;
+      g.a_inner = b.k;
+      g.a_is = 1;
+      g.a_os = K;
+      g.b_stride = b.k;
+      ozaki_gemm(g, sms, oz_err.p, st);
+      OzRows t;  // row (i, r) of T: T_i[r, c] at off + i·K + r·k + c
+      t.base = Pc.p + b.off;
+      t.rows = rows;
+      t.inner = b.k;
+      t.is = b.k;
+      t.os = K;
+      t.len = b.k;
+      ozaki_digits_rows(t, o.kp, aplane, oz_tdig.p, oz_texp.p, st);
+      OzGemm h = g;  // P_i[r, c'] = Σ_c T_i[r, c]·M_Y[c, c'] → Pc[off + i·K + c'·k + r]
+      h.xd = oz_tdig.p;
+      h.ea = oz_texp.p;
+      h.yd = yd;
+      h.eb = ye;
+      h.kmode = 2;
+      ozaki_gemm(h, sms, oz_err.p, st);
+    }
+  }
   void schur_build_fp64(int identity) {
     const double* panel = A.p;
     if (!identity) {
       kt_begin(3);
-      for (auto& b : dense) {
+      if (gram_engine == 1 && oz_blocks_ready()) oz_block_products();
+      else for (auto& b : dense) {
         // T = W · [A_1 … A_m]  (W lower ⇒ K range [0, row-tile end))
         Opnd Wd = blk_as_A(W.p, b.off, b.k);
         Opnd Ap;  // (kk = p, nn = (i, c)) → A[off + c·k + p, i]
@@ -934,8 +1065,6 @@ struct Handle {
         oz_plan = plan_ozaki_syrk(m, K, sms);
         oz_digits.alloc(oz_plan.digit_bytes);
         oz_exps.alloc(m);
-        oz_err.alloc(1);
-        oz_err.zero(st);
         oz_partial.alloc(oz_plan.partial_alloc_doubles);
       }
       ozaki_syrk(panel, oz_plan, oz_digits.p, oz_exps.p, oz_partial.p, S.p, oz_err.p, st);

@@ -17,8 +17,8 @@
 // Tiles: 128 rows of P columns (A) × 64 (B); the eight level accumulators take
 // all 8·64 = 512 TMEM columns.  128 threads per CTA, one CTA per SM: thread 0
 // issues the TMA boxes (K = 32 bytes per row, 32-byte swizzle, four 48 KB
-// stages), thread 32 issues the 36 MMAs of a stage (M = 128, N = 64, K = 32)
-// and commits them to the stage's "empty" barrier, all four warps convert the
+// stages), thread 32 issues the 12 MMAs of a stage (M = 128, N ≤ 256, K = 32,
+// all 36 digit products) and commits them to the stage's "empty" barrier, all four warps convert the
 // int32 levels to FP64 in the epilogue.  Bounded waits with a device error flag;
 // the producer drains its own copies before the CTA exits.  No cluster, no
 // multicast.
@@ -47,6 +47,31 @@ constexpr int OSTAGE = OZ_DIGITS * (OA_BYTES + OB_BYTES);  // 48 KB
 constexpr size_t OSMEM = ONST * OSTAGE + 1024 + 256;
 constexpr int OLEVELS = OZ_DIGITS;                // levels 0 … OZ_DIGITS-1
 constexpr int NAN_EXP = INT_MIN;                  // column holds a non-finite value
+
+// Exact helpers on the FP64 pipe (the conversion pipe is the slow one here).
+// (double)x for an int32 x: the double 2^52 + (x + 2^31) has x + 2^31 in its
+// low mantissa bits; subtracting 2^52 + 2^31 is exact.
+__device__ __forceinline__ double i32_to_f64(int x) {
+  return __hiloint2double(0x43300000, x ^ (int)0x80000000) - 4503601774854144.0;
+}
+// v·2^e, identical to ldexp(v, e) (one rounding of the exact product); the
+// power of two is built from its exponent field when it is a normal double.
+__device__ __forceinline__ double scale2(double v, int e) {
+  return (e >= -1022 && e <= 1023) ? v * __longlong_as_double((long long)(e + 1023) << 52)
+                                   : ldexp(v, e);
+}
+// Nearest integer (ties to even, as rint) of |x| < 2^51 by adding and
+// subtracting 1.5·2^52; the low word of the sum is the integer itself.
+// 2^(-7·lv), the weight of digit level lv.
+__device__ __forceinline__ double level_scale(int lv) {
+  return __longlong_as_double((long long)(1023 - 7 * lv) << 52);
+}
+constexpr double kRound = 6755399441055744.0;
+__device__ __forceinline__ double round_digit(double x, int& di) {
+  const double t = x + kRound;
+  di = __double2loint(t);
+  return t - kRound;
+}
 
 // ---------------------------------------------------------------- digits --
 // One CTA per column: largest magnitude → exponent, then the digit planes
@@ -77,11 +102,12 @@ __global__ void k_oz_digits(const double* __restrict__ P, long long K, long long
   const size_t plane = (size_t)m * Kp;
   int8_t* dst = digits + (size_t)i * Kp;
   for (long long k = threadIdx.x; k < Kp; k += blockDim.x) {
-    double r = (k < K && e != NAN_EXP) ? ldexp(col[k], 6 - e) : 0.0;  // 64·v, |v| < 1
+    double r = (k < K && e != NAN_EXP) ? scale2(col[k], 6 - e) : 0.0;  // 64·v, |v| < 1
 #pragma unroll
     for (int t = 0; t < OZ_DIGITS; ++t) {
-      const double d = rint(r);
-      dst[(size_t)t * plane + k] = (int8_t)d;
+      int di;
+      const double d = round_digit(r, di);
+      dst[(size_t)t * plane + k] = (int8_t)di;
       r = (r - d) * 128.0;
     }
   }
@@ -122,6 +148,27 @@ __device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t a, uint64_t b, 
       "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
       "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+// The MMAs of one stage.  Level ℓ = t + u sits in TMEM columns [64ℓ, 64ℓ+64),
+// and the digit tiles of B are contiguous in shared memory (uniform 256-byte
+// swizzle atoms), so for a fixed digit t of A the products with all digits
+// u = 0 … 7-t of B are ONE operand of N = 64·(8-t) rows writing the contiguous
+// columns [64t, 512): 12 MMAs of N ≤ 256 instead of 36 of N = 64, and each A
+// tile is read from shared memory once per MMA instead of once per product.
+// The first stage of a tile writes every level through t = 0 (no accumulate).
+__device__ __forceinline__ void oz_mma_stage(uint32_t tmem, uint32_t base, bool first) {
+#pragma unroll
+  for (int ta = 0; ta < OZ_DIGITS; ++ta) {
+    const uint64_t ad = smem_desc_sw32(base + ta * OA_BYTES);
+#pragma unroll
+    for (int c0 = 0; c0 < (OZ_DIGITS - ta) * ON; c0 += 256) {
+      const int n = (OZ_DIGITS - ta) * ON - c0 < 256 ? (OZ_DIGITS - ta) * ON - c0 : 256;
+      const uint64_t bd = smem_desc_sw32(base + OZ_DIGITS * OA_BYTES + (c0 / ON) * OB_BYTES);
+      mma_s8(tmem + (uint32_t)(ta * ON + c0), ad, bd, idesc_s8_s32(OM, n),
+             (first && ta == 0) ? 0u : 1u);
+    }
+  }
 }
 
 __global__ void __launch_bounds__(ONT, 1)
@@ -174,22 +221,12 @@ __global__ void __launch_bounds__(ONT, 1)
     for (int t = max(0, issued - ONST); t < issued; ++t)
       umma::mbar_wait_bounded(&sh->full[t % ONST], (t / ONST) & 1, err);
   } else if (threadIdx.x == 32) {
-    constexpr uint32_t IDESC = idesc_s8_s32(OM, ON);
     for (int t = 0; t < ntiles; ++t) {
       const int s = t % ONST;
       if (!umma::mbar_wait_bounded(&sh->full[s], (t / ONST) & 1, err)) break;
       umma::fence_after_sync();
       const uint32_t base = umma::smem_u32(smem + s * OSTAGE);
-#pragma unroll
-      for (int ta = 0; ta < OZ_DIGITS; ++ta)
-#pragma unroll
-        for (int tb = 0; tb < OZ_DIGITS - ta; ++tb) {
-          const uint64_t ad = smem_desc_sw32(base + ta * OA_BYTES);
-          const uint64_t bd = smem_desc_sw32(base + OZ_DIGITS * OA_BYTES + tb * OB_BYTES);
-          // level ta+tb; its first product (ta = 0) of the first tile starts it
-          const uint32_t acc = (t > 0 || ta > 0) ? 1u : 0u;
-          mma_s8(tmem + (uint32_t)((ta + tb) * ON), ad, bd, IDESC, acc);
-        }
+      oz_mma_stage(tmem, base, t == 0);
       umma::commit(&sh->empty[s]);
     }
     umma::commit(&sh->done);
@@ -215,7 +252,7 @@ __global__ void __launch_bounds__(ONT, 1)
         umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(lv * ON + cb), raw);
 #pragma unroll
         for (int q = 0; q < 32; ++q)
-          acc[q] += ldexp((double)__float_as_int(raw[q]), -7 * lv);
+          acc[q] = fma(i32_to_f64(__float_as_int(raw[q])), level_scale(lv), acc[q]);
       }
 #pragma unroll
       for (int q = 0; q < 32; ++q) {
@@ -225,7 +262,7 @@ __global__ void __launch_bounds__(ONT, 1)
         if (ei == NAN_EXP || ej == NAN_EXP)
           v = __longlong_as_double(0x7ff8000000000000ll);
         else
-          v = ldexp(acc[q], ei + ej - 12);
+          v = scale2(acc[q], ei + ej - 12);
         dst[cb + q] = v;
       }
     }
@@ -249,6 +286,238 @@ __global__ void k_oz_reduce(const double* __restrict__ partial, const int2* __re
     for (int ch = 0; ch < nchunk; ++ch) s += partial[((size_t)ch * npairs + pr) * OM * ON + e];
     S[gi + (size_t)gj * m] = s;
   }
+}
+
+// ------------------------------------------------------------ row digits --
+// One warp per row vector: largest magnitude over the kept elements, then the
+// digit planes, four consecutive elements per lane (char4 stores).
+struct OzRowsDev {
+  const double* base;
+  long long rows, is, os, es;
+  int inner, len, tri;
+};
+
+__global__ void k_oz_digits_rows(const OzRowsDev r, long long Kp, long long plane,
+                                 int8_t* __restrict__ digits, int* __restrict__ exps) {
+  const int lane = threadIdx.x & 31;
+  const long long n = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (n >= r.rows) return;
+  const double* v = r.base + (n / r.inner) * r.os + (n % r.inner) * r.is;
+  int jlo = 0, jhi = r.len;
+  if (r.tri == 1) jhi = (int)(n + 1 < (long long)r.len ? n + 1 : (long long)r.len);
+  if (r.tri == 2) jlo = (int)(n < (long long)r.len ? n : (long long)r.len);
+  double mx = 0.0;
+  bool finite = true;
+  for (int j = jlo + lane; j < jhi; j += 32) {
+    const double a = fabs(v[(long long)j * r.es]);
+    finite = finite && isfinite(a);
+    mx = fmax(mx, a);
+  }
+  const bool all_finite = __all_sync(0xffffffffu, finite);
+  mx = warp_max(mx);
+  int e = 0;
+  if (all_finite && mx > 0.0) frexp(mx, &e);
+  if (!all_finite) e = NAN_EXP;
+  if (lane == 0) exps[n] = e;
+  int8_t* dst = digits + n * Kp;
+  for (long long j0 = 4 * lane; j0 < Kp; j0 += 128) {
+    double x[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const long long j = j0 + q;
+      x[q] = (j >= jlo && j < jhi && e != NAN_EXP) ? scale2(v[j * r.es], 6 - e) : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < OZ_DIGITS; ++t) {
+      char4 c;
+      double d;
+      int di;
+      d = round_digit(x[0], di); c.x = (signed char)di; x[0] = (x[0] - d) * 128.0;
+      d = round_digit(x[1], di); c.y = (signed char)di; x[1] = (x[1] - d) * 128.0;
+      d = round_digit(x[2], di); c.z = (signed char)di; x[2] = (x[2] - d) * 128.0;
+      d = round_digit(x[3], di); c.w = (signed char)di; x[3] = (x[3] - d) * 128.0;
+      *reinterpret_cast<char4*>(dst + t * plane + j0) = c;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- GEMM ----
+// Persistent CTAs over the (128-row X tile, 64-row Y tile) tasks, Y tiles
+// fastest so that concurrent tasks share X tiles in L2.  Warp 16 (one thread)
+// streams the digit boxes through the four stages and runs ahead into the
+// next task; warp 17 (one thread) issues the 12 MMAs of a stage and, at the
+// end of a task, commits the eight level accumulators to `tfull`; warps 0-15
+// (TMEM lane quarter w % 4, 16-column group w / 4) read the levels, hand the
+// accumulator back through `tempty` and then scale and store while the next
+// task's MMAs run.  Sixteen epilogue warps keep every scheduler busy: the
+// level sums are chains of dependent FP64 operations.
+constexpr int GEPI = 16;              // epilogue warps: 4 TMEM lane quarters × 4 column groups
+constexpr int GNT = (GEPI + 2) * 32;  // + the TMA warp and the MMA warp
+
+struct OzGemmDev {
+  const int* ea;
+  const int* eb;
+  double* out;
+  long long ntask, a_is, a_os, b_stride;
+  int rows_a, rows_b, kext, kmode, ntile_b, a_inner;
+};
+
+struct OzGemmShared {
+  uint64_t full[ONST], empty[ONST], tfull, tempty, mdone;
+  uint32_t tmem;
+  int abort;
+};
+
+// Bounded wait that also gives up as soon as another role of the CTA has.
+__device__ __forceinline__ bool oz_wait(uint64_t* mbar, uint32_t parity, int* err,
+                                        volatile int* abort) {
+  const long long t0 = clock64();
+  while (!umma::mbar_test(mbar, parity)) {
+    if (*abort) return false;
+    if (clock64() - t0 > (1LL << 32)) {
+      atomicExch(err, 1);
+      *abort = 1;
+      return false;
+    }
+    __nanosleep(32);
+  }
+  return true;
+}
+
+__device__ __forceinline__ void oz_task(const OzGemmDev& g, long long u, int& mt, int& nt, int& kb,
+                                        int& nk) {
+  mt = (int)(u / g.ntile_b);
+  nt = (int)(u % g.ntile_b);
+  kb = 0;
+  int ke = g.kext;
+  const int n0 = nt * ON;
+  if (g.kmode == 1) ke = min(g.kext, n0 + ON);
+  if (g.kmode == 2) kb = min(g.kext, n0) / OK * OK;
+  nk = ke > kb ? (ke - kb + OK - 1) / OK : 0;
+}
+
+__global__ void __launch_bounds__(GNT, 1)
+    k_oz_gemm(const __grid_constant__ OzMaps maps, const OzGemmDev g, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  OzGemmShared* sh = reinterpret_cast<OzGemmShared*>(smem + ONST * OSTAGE);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ONST; ++s) {
+      umma::mbar_init(&sh->full[s], 1);
+      umma::mbar_init(&sh->empty[s], 1);
+    }
+    umma::mbar_init(&sh->tfull, 1);
+    umma::mbar_init(&sh->tempty, GEPI);
+    umma::mbar_init(&sh->mdone, 1);
+    sh->abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  if (warp == 0) umma::tmem_alloc(&sh->tmem, 512);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = sh->tmem;
+  volatile int* abort = &sh->abort;
+
+  if (warp == GEPI) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (long long u = blockIdx.x; u < g.ntask && !*abort; u += gridDim.x) {
+        int mt, nt, kb, nk;
+        oz_task(g, u, mt, nt, kb, nk);
+        bool ok = true;
+        for (int t = 0; t < nk; ++t, ++it) {
+          const int s = it % ONST;
+          if (it >= ONST && !oz_wait(&sh->empty[s], ((it / ONST) - 1) & 1, err, abort)) {
+            ok = false;
+            break;
+          }
+          umma::mbar_expect_tx(&sh->full[s], OSTAGE);
+          const uint32_t base = umma::smem_u32(smem + s * OSTAGE);
+          const int k = kb + t * OK;
+#pragma unroll
+          for (int d = 0; d < OZ_DIGITS; ++d) {
+            umma::tma_load_2d(base + d * OA_BYTES, &maps.a[d], k, mt * OM, &sh->full[s]);
+            umma::tma_load_2d(base + OZ_DIGITS * OA_BYTES + d * OB_BYTES, &maps.b[d], k, nt * ON,
+                              &sh->full[s]);
+          }
+        }
+        if (!ok) break;
+      }
+      // Drain this thread's copies in flight before the CTA may exit.
+      for (uint32_t t = it > (uint32_t)ONST ? it - ONST : 0; t < it; ++t)
+        umma::mbar_wait_bounded(&sh->full[t % ONST], (t / ONST) & 1, err);
+    }
+  } else if (warp == GEPI + 1) {
+    if (lane == 0) {
+        uint32_t it = 0, j = 0;
+      bool ok = true;
+      for (long long u = blockIdx.x; u < g.ntask && ok; u += gridDim.x, ++j) {
+        int mt, nt, kb, nk;
+        oz_task(g, u, mt, nt, kb, nk);
+        if (j > 0 && !oz_wait(&sh->tempty, (j - 1) & 1, err, abort)) break;
+        umma::fence_after_sync();
+        for (int t = 0; t < nk; ++t, ++it) {
+          const int s = it % ONST;
+          if (!oz_wait(&sh->full[s], (it / ONST) & 1, err, abort)) {
+            ok = false;
+            break;
+          }
+          umma::fence_after_sync();
+          const uint32_t base = umma::smem_u32(smem + s * OSTAGE);
+          oz_mma_stage(tmem, base, t == 0);
+          umma::commit(&sh->empty[s]);
+        }
+        if (ok) umma::commit(&sh->tfull);
+      }
+      // Every MMA of this thread completes before the accumulator is freed.
+      umma::commit(&sh->mdone);
+      umma::mbar_wait_bounded(&sh->mdone, 0, err);
+    }
+  } else {
+    // Epilogue: warp w reads TMEM lanes 32·(w % 4) … (one X row per thread) and
+    // the 16 Y columns of group w / 4.
+    const int quarter = warp & 3, cgrp = warp >> 2;
+    uint32_t j = 0;
+    for (long long u = blockIdx.x; u < g.ntask; u += gridDim.x, ++j) {
+      if (!oz_wait(&sh->tfull, j & 1, err, abort)) break;
+      umma::fence_after_sync();
+      const int mt = (int)(u / g.ntile_b), nt = (int)(u % g.ntile_b);
+      double acc[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+#pragma unroll
+      for (int lv = OLEVELS - 1; lv >= 0; --lv) {
+        uint32_t raw[16];
+        umma::tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(lv * ON + cgrp * 16), raw);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] = fma(i32_to_f64((int)raw[q]), level_scale(lv), acc[q]);
+      }
+      umma::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) umma::mbar_arrive(&sh->tempty);
+      const int ga = mt * OM + quarter * 32 + lane;
+      if (ga < g.rows_a) {
+        const int ea = g.ea[ga];
+        double* row = g.out + (long long)(ga / g.a_inner) * g.a_os + (long long)(ga % g.a_inner) * g.a_is;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int gb = nt * ON + cgrp * 16 + q;
+          if (gb < g.rows_b) {
+            const int eb = g.eb[gb];
+            row[(long long)gb * g.b_stride] = (ea == NAN_EXP || eb == NAN_EXP)
+                                                  ? __longlong_as_double(0x7ff8000000000000ll)
+                                                  : scale2(acc[q], ea + eb - 12);
+          }
+        }
+      }
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, 512);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 oz_encoder() {
@@ -342,6 +611,48 @@ void ozaki_syrk(const double* P, const OzakiPlan& plan, int8_t* digits, int* exp
   if (ev_end) SDPX_CUDA(cudaEventRecord(ev_end, st));
   k_oz_reduce<<<plan.ntri, 256, 0, st>>>(partial, d_pairs, plan.ntri, plan.nchunk, m, S);
   SDPX_LAUNCH_CHECK_N(2);
+}
+
+long long oz_kpad(int len) { return std::max<long long>(32, (len + 15LL) / 16 * 16); }
+
+void ozaki_digits_rows(const OzRows& r, long long Kp, long long plane, int8_t* digits, int* exps,
+                       cudaStream_t st) {
+  if (r.rows <= 0) return;
+  if (Kp % 16 != 0 || Kp < r.len || plane < r.rows * Kp)
+    throw std::invalid_argument("ozaki: digit rows do not fit the planes");
+  OzRowsDev d{r.base, r.rows, r.is, r.os, r.es, r.inner, r.len, r.tri};
+  constexpr int WARPS = 8;
+  const long long blocks = (r.rows + WARPS - 1) / WARPS;
+  k_oz_digits_rows<<<(unsigned)blocks, WARPS * 32, 0, st>>>(d, Kp, plane, digits, exps);
+  SDPX_LAUNCH_CHECK();
+}
+
+void ozaki_gemm(const OzGemm& g, int sm_count, int* err, cudaStream_t st) {
+  if (g.rows_a <= 0 || g.rows_b <= 0) return;
+  if (g.Kp % 16 != 0 || g.Kp < OK) throw std::invalid_argument("ozaki: contraction width");
+  OzMaps maps;
+  for (int d = 0; d < OZ_DIGITS; ++d) {
+    encode_digit_map(&maps.a[d], g.xd + d * g.x_plane, g.rows_a, g.Kp, OM);
+    encode_digit_map(&maps.b[d], g.yd + d * g.y_plane, g.rows_b, g.Kp, ON);
+  }
+  OzGemmDev dv;
+  dv.ea = g.ea;
+  dv.eb = g.eb;
+  dv.out = g.out;
+  dv.rows_a = g.rows_a;
+  dv.rows_b = g.rows_b;
+  dv.kext = (int)g.Kp;
+  dv.kmode = g.kmode;
+  dv.ntile_b = ceil_div(g.rows_b, ON);
+  dv.ntask = (long long)ceil_div(g.rows_a, OM) * dv.ntile_b;
+  dv.a_inner = g.a_inner;
+  dv.a_is = g.a_is;
+  dv.a_os = g.a_os;
+  dv.b_stride = g.b_stride;
+  ensure_smem(k_oz_gemm, OSMEM);
+  const long long grid = std::min<long long>(dv.ntask, std::max(1, sm_count));
+  k_oz_gemm<<<(unsigned)grid, GNT, OSMEM, st>>>(maps, dv, err);
+  SDPX_LAUNCH_CHECK();
 }
 
 }  // namespace sdpx

@@ -29,4 +29,49 @@ void ozaki_syrk(const double* P, const OzakiPlan& plan, int8_t* digits, int* exp
                 double* S, int* err, cudaStream_t st, cudaEvent_t ev_begin = nullptr,
                 cudaEvent_t ev_end = nullptr);
 
+// ---- general products C[a, b] = Σ_j X[a, j]·Y[b, j] on digit planes --------
+
+// `rows` FP64 row vectors of length `len`: row n starts at
+// base + (n / inner)·os + (n % inner)·is, its element j sits at +j·es.
+// tri = 1 keeps only the elements j ≤ n of row n, tri = 2 only j ≥ n (the
+// others read as zero: triangular factors whose other half is not stored).
+struct OzRows {
+  const double* base = nullptr;
+  long long rows = 0;
+  int inner = 1 << 30;
+  long long is = 0, os = 0, es = 1;
+  int len = 0;
+  int tri = 0;
+};
+
+// Padded digit-row width for a contraction length (multiple of 16, ≥ 32).
+long long oz_kpad(int len);
+
+// Digit planes of the rows: digit t of row n at digits[t·plane + n·Kp + j]
+// (zero for j ≥ len), the row's power-of-two exponent at exps[n].
+// plane ≥ rows·Kp.
+void ozaki_digits_rows(const OzRows& r, long long Kp, long long plane, int8_t* digits, int* exps,
+                       cudaStream_t st);
+
+// out[(a / a_inner)·a_os + (a % a_inner)·a_is + b·b_stride] = Σ_j X[a, j]·Y[b, j]
+// for the digit planes of X (rows_a rows) and Y (rows_b rows), both Kp wide.
+// kmode 1: row b of Y is zero beyond j = b, kmode 2: before j = b (the
+// contraction of a tile of Y rows is cut to where they can be nonzero).
+struct OzGemm {
+  const int8_t* xd = nullptr;
+  long long x_plane = 0;
+  int rows_a = 0;
+  const int* ea = nullptr;
+  const int8_t* yd = nullptr;
+  long long y_plane = 0;
+  int rows_b = 0;
+  const int* eb = nullptr;
+  long long Kp = 0;
+  int kmode = 0;
+  double* out = nullptr;
+  int a_inner = 1 << 30;
+  long long a_is = 0, a_os = 0, b_stride = 0;
+};
+void ozaki_gemm(const OzGemm& g, int sm_count, int* err, cudaStream_t st);
+
 }  // namespace sdpx
