@@ -436,7 +436,7 @@ def run_ours(args, world, rank, local):
     be.close()
     torch.cuda.synchronize()
     e2e_times, e2e_create = [], []
-    for _ in range(max(1, min(args.steps, 2))):
+    for _ in range(max(1, min(args.steps, 3))):
         t0 = time.perf_counter()
         with CudaBackend(prob_p, precision="mixed", device=local) as be2:
             t1 = time.perf_counter()

@@ -388,8 +388,11 @@ struct Handle {
   }
 
   // Batched Cholesky of host-described matrices; fills info/dmin/dmax (host).
+  // zero_upper = false for positive-definiteness tests that read only
+  // info/dmin/dmax (the factor's strict upper triangle is then left as is).
   void potrf_host_list(const std::vector<MatDesc<double>>& mats, std::vector<int>& info,
-                       std::vector<double>& dmin, std::vector<double>& dmax) {
+                       std::vector<double>& dmin, std::vector<double>& dmax,
+                       bool zero_upper = true) {
     size_t n = mats.size();
     info.assign(n, 0);
     dmin.assign(n, 0.0);
@@ -400,9 +403,11 @@ struct Handle {
     for (auto& q : mats) nmax = std::max(nmax, q.n);
     h2d(d_descs.p, mats.data(), n * sizeof(MatDesc<double>));
     if (nmax >= 192)
-      potrf_batched<double, 64>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p, st);
+      potrf_batched<double, 64>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p, st,
+                                zero_upper);
     else
-      potrf_batched<double, 32>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p, st);
+      potrf_batched<double, 32>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p, st,
+                                zero_upper);
     d2h(info.data(), d_info.p, n * sizeof(int));
     d2h(dmin.data(), d_dmin.p, n * sizeof(double));
     d2h(dmax.data(), d_dmax.p, n * sizeof(double));
@@ -1502,7 +1507,7 @@ struct Handle {
                         dense[b].k});
     std::vector<int> info;
     std::vector<double> dmn, dmx;
-    potrf_host_list(mats, info, dmn, dmx);
+    potrf_host_list(mats, info, dmn, dmx, false);
     size_t q = 0;
     for (size_t bi = 0; bi < idx.size(); ++bi)
       for (size_t c2 = 0; c2 < t.size(); ++c2, ++q) {
@@ -1576,7 +1581,7 @@ struct Handle {
     make_trials_list(d_trial_desc.p, (int)n, nmax, st);
     std::vector<MatDesc<double>> mats(n);
     for (size_t q = 0; q < n; ++q) mats[q] = {trials.p + off[q], dense[reqs[q].b].k, dense[reqs[q].b].k};
-    potrf_host_list(mats, info, dmn, dmx);
+    potrf_host_list(mats, info, dmn, dmx, false);
   }
 
   // Fraction-to-boundary bounds of both sides (src/kernels/generic.jl:350-422):
@@ -2102,7 +2107,7 @@ struct Handle {
       std::vector<MatDesc<double>> mats;
       for (size_t b : sel) mats.push_back({cert_sym.p + dense[b].off, dense[b].k, dense[b].k});
       std::vector<double> dmn, dmx;
-      potrf_host_list(mats, info, dmn, dmx);
+      potrf_host_list(mats, info, dmn, dmx, false);
     };
     std::vector<int> info;
     factor_with(chol0, std::vector<double>(chol0.size(), 0.0), info);

@@ -211,18 +211,35 @@ __global__ void __launch_bounds__(512) k_potrf_panel_smem(const MatDesc<T>* mats
   const int w = min(NB, M.n - c0);
   const int rows = M.n - c0;
   const int ld = rows | 1;  // odd stride: conflict-free column walks
-  for (int e = threadIdx.x; e < rows * w; e += blockDim.x) {
-    int r = e % rows, c = e / rows;
-    Pn[c * ld + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
+  // A warp per column, lanes along the rows; each lane issues its PU loads of
+  // a batch before storing any, so a column costs one memory round trip per
+  // 32·PU rows instead of one per element.
+  constexpr int PU = 8;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int c = warp; c < w; c += nwarp) {
+    const T* src = M.a + (size_t)(c0 + c) * M.ld + c0;
+    for (int rb = 0; rb < rows; rb += 32 * PU) {
+      T v[PU];
+#pragma unroll
+      for (int u = 0; u < PU; ++u) {
+        const int r = rb + lane + 32 * u;
+        v[u] = (r < rows && r >= c) ? src[r] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < PU; ++u) {
+        const int r = rb + lane + 32 * u;
+        if (r < rows) Pn[c * ld + r] = v[u];
+      }
+    }
   }
   const int fail = factor_panel_smem<T>(Pn, ld, rows, w);
   if (fail >= 0) {
     if (threadIdx.x == 0) info[b] = c0 + fail + 1;
     return;
   }
-  for (int e = threadIdx.x; e < rows * w; e += blockDim.x) {
-    int r = e % rows, c = e / rows;
-    M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] = (r >= c) ? Pn[c * ld + r] : T(0);
+  for (int c = warp; c < w; c += nwarp) {
+    T* dst = M.a + (size_t)(c0 + c) * M.ld + c0;
+    for (int r = lane; r < rows; r += 32) dst[r] = (r >= c) ? Pn[c * ld + r] : T(0);
   }
   note_pivots(Pn, ld, w, dmin, dmax, b);
 }
@@ -248,10 +265,24 @@ __global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info) {
   const int i = j + 1 + a, q = j + 1 + bq;
   const int c0 = j * NB, r0 = i * NB, q0 = q * NB;
   const int w = min(NB, M.n - c0), h = min(NB, M.n - r0), hq = min(NB, M.n - q0);
-  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
-    int r = e % NB, c = e / NB;
-    La[c * LD + r] = (r < h && c < w) ? M.a[(size_t)(c0 + c) * M.ld + (r0 + r)] : T(0);
-    Lb[c * LD + r] = (r < hq && c < w) ? M.a[(size_t)(c0 + c) * M.ld + (q0 + r)] : T(0);
+  {
+    // All loads of the two tiles are issued before the shared stores (one
+    // memory round trip per tile instead of one per loop trip).
+    constexpr int PER = NB * NB / 256;
+    static_assert(NB * NB % 256 == 0, "tile load split");
+    T va[PER], vb[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int e = threadIdx.x + k * 256, r = e % NB, c = e / NB;
+      va[k] = (r < h && c < w) ? M.a[(size_t)(c0 + c) * M.ld + (r0 + r)] : T(0);
+      vb[k] = (r < hq && c < w) ? M.a[(size_t)(c0 + c) * M.ld + (q0 + r)] : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int e = threadIdx.x + k * 256, r = e % NB, c = e / NB;
+      La[c * LD + r] = va[k];
+      Lb[c * LD + r] = vb[k];
+    }
   }
   __syncthreads();
   // Each thread owns a 4×4 block of outputs (NB=64: 256 threads; NB=32: 64 active).
@@ -281,14 +312,15 @@ __global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info) {
   }
 }
 
+// Strict upper triangle set to zero: a warp per column (rows 0 … c-1).
 template <class T>
 __global__ void k_zero_upper(const MatDesc<T>* mats) {
   const MatDesc<T> M = mats[blockIdx.y];
-  long long total = (long long)M.n * M.n;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    int r = (int)(e % M.n), c = (int)(e / M.n);
-    if (r < c) M.a[(size_t)c * M.ld + r] = T(0);
+  const int lane = threadIdx.x & 31;
+  for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < M.n;
+       c += gridDim.x * (blockDim.x >> 5)) {
+    T* col = M.a + (size_t)c * M.ld;
+    for (int r = lane; r < c; r += 32) col[r] = T(0);
   }
 }
 
@@ -304,7 +336,7 @@ __global__ void k_init_stats(int n, int* info, T* dmin, T* dmax) {
 
 template <class T, int NB>
 void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* dmin, T* dmax,
-                   cudaStream_t st) {
+                   cudaStream_t st, bool zero_upper) {
   if (nmat == 0 || nmax == 0) return;
   const size_t smem = 2 * sizeof(T) * NB * (NB + 1);
   ensure_smem(k_potrf_update<T, NB>, smem);
@@ -314,7 +346,7 @@ void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* d
   const size_t panel_smem = sizeof(T) * (size_t)rows_pad * NB;
   const bool whole_panel = panel_smem <= 224 * 1024;
   if (whole_panel) ensure_smem(k_potrf_panel_smem<T, NB>, panel_smem);
-  int launches = 2;
+  int launches = 1;  // k_init_stats
   for (int j = 0; j < nt; ++j) {
     int rem = nt - j - 1;
     if (whole_panel) {
@@ -336,17 +368,20 @@ void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* d
       ++launches;
     }
   }
-  dim3 gz(std::max(1, std::min(1024, ceil_div((long long)nmax * nmax, 256))), nmat);
-  k_zero_upper<T><<<gz, 256, 0, st>>>(d_mats);
+  if (zero_upper) {
+    dim3 gz(std::max(1, ceil_div(nmax, 8)), nmat);
+    k_zero_upper<T><<<gz, 256, 0, st>>>(d_mats);
+    ++launches;
+  }
   SDPX_LAUNCH_CHECK_N(launches);
 }
 
 template void potrf_batched<double, 32>(const MatDesc<double>*, int, int, int*, double*, double*,
-                                        cudaStream_t);
+                                        cudaStream_t, bool);
 template void potrf_batched<double, 64>(const MatDesc<double>*, int, int, int*, double*, double*,
-                                        cudaStream_t);
+                                        cudaStream_t, bool);
 template void potrf_batched<float, 64>(const MatDesc<float>*, int, int, int*, float*, float*,
-                                       cudaStream_t);
+                                       cudaStream_t, bool);
 
 // ---------------------------------------------------------------------------
 // Triangular inverse W = L^{-1} (lower), blocked by NB.  Step 0 inverts every

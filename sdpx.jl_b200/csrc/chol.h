@@ -16,10 +16,11 @@ struct MatDesc {
 // Lower Cholesky in place of every matrix in d_mats (device array of nmat
 // descriptors, largest order nmax).  info[b] = 0 on success, else the 1-based
 // index of the first non-positive pivot.  dmin/dmax receive min/max |L_ii|.
-// The strict upper triangle is zeroed.
+// The strict upper triangle is zeroed unless zero_upper is false (positive-
+// definiteness tests that only read info/dmin/dmax).
 template <class T, int NB>
 void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* dmin, T* dmax,
-                   cudaStream_t st);
+                   cudaStream_t st, bool zero_upper = true);
 
 // W_b = L_b^{-1} for lower-triangular L_b (W zero-initialised by the caller).
 template <class T, int NB>
