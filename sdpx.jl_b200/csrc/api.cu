@@ -156,6 +156,7 @@ struct Handle {
   std::vector<OzBlock> ozb;
   DBuf<int8_t> oz_adig, oz_tdig, oz_wdig;
   DBuf<int> oz_aexp, oz_texp, oz_wexp;
+  DBuf<unsigned> oz_colmax;  // per Schur column: largest high word of |P| over the dense rows
   unsigned long long oz_a_ver = 0;
   int oz_blk_state = 0;  // 0 = not planned, 1 = digit products, -1 = DMMA tiles (memory)
   DBuf<double> partial;
@@ -923,6 +924,7 @@ struct Handle {
         oz_aexp.alloc(aexp);
         oz_texp.alloc(texp);
         oz_wexp.alloc(wexp);
+        oz_colmax.alloc(m);
         oz_a_ver = 0;
         oz_blk_state = 1;
       }
@@ -945,6 +947,7 @@ struct Handle {
       }
       oz_a_ver = a_ver;
     }
+    SDPX_CUDA(cudaMemsetAsync(oz_colmax.p, 0, sizeof(unsigned) * m, st));
     for (size_t bi = 0; bi < dense.size(); ++bi) {
       const DenseBlk& b = dense[bi];
       const OzBlock& o = ozb[bi];
@@ -1000,6 +1003,7 @@ struct Handle {
       h.yd = yd;
       h.eb = ye;
       h.kmode = 2;
+      h.colmax = oz_colmax.p;  // the Gram's column exponents over the dense rows
       ozaki_gemm(h, sms, oz_err.p, st);
     }
   }
@@ -1072,7 +1076,11 @@ struct Handle {
         oz_exps.alloc(m);
         oz_partial.alloc(oz_plan.partial_alloc_doubles);
       }
-      ozaki_syrk(panel, oz_plan, oz_digits.p, oz_exps.p, oz_partial.p, S.p, oz_err.p, st);
+      // After the digit block products every dense row of P̂ carries its column
+      // maximum already; the Gram's digit pass scans only the 1×1 rows for it.
+      const bool known = !identity && oz_blk_state == 1;
+      ozaki_syrk(panel, oz_plan, oz_digits.p, oz_exps.p, oz_partial.p, S.p, oz_err.p, st, nullptr,
+                 nullptr, known ? oz_colmax.p : nullptr, od);
       kt_end(2);
       int e = 0;
       d2h(&e, oz_err.p, sizeof(int));

@@ -129,9 +129,30 @@ __device__ void note_pivots(const T* P, int ld, int w, T* dmin, T* dmax, int b) 
   dmax[b] = hi;
 }
 
+// The lower part of the w×w diagonal tile at (c0, c0) into shared D (column
+// c at D[c·LD + …], zeros above the diagonal and outside w).  NT threads; each
+// issues all of its NB·NB/NT loads before any shared store, so the tile costs
+// one memory round trip.
+template <class T, int NB, int NT>
+__device__ __forceinline__ void load_diag_tile(T* D, int LD, const MatDesc<T>& M, int c0, int w) {
+  constexpr int PER = NB * NB / NT;
+  static_assert(NB * NB % NT == 0, "tile split");
+  T v[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * NT, r = e % NB, c = e / NB;
+    v[k] = (r < w && c < w && r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
+  }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * NT, r = e % NB, c = e / NB;
+    if (r < w && c < w) D[c * LD + r] = v[k];
+  }
+}
+
 // Tiled path, step 1: factor the diagonal tile of panel j (one CTA per matrix).
 template <class T, int NB>
-__global__ void k_potrf_diag(const MatDesc<T>* mats, int j, int* info, T* dmin, T* dmax) {
+__global__ void __launch_bounds__(256) k_potrf_diag(const MatDesc<T>* mats, int j, int* info, T* dmin, T* dmax) {
   __shared__ T D[NB * (NB + 1)];
   constexpr int LD = NB + 1;
   const int b = blockIdx.x;
@@ -139,18 +160,15 @@ __global__ void k_potrf_diag(const MatDesc<T>* mats, int j, int* info, T* dmin, 
   const int c0 = j * NB;
   if (c0 >= M.n || info[b] != 0) return;
   const int w = min(NB, M.n - c0);
-  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-    int r = e % w, c = e / w;
-    D[c * LD + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
-  }
+  load_diag_tile<T, NB, 256>(D, LD, M, c0, w);
   const int fail = factor_panel_smem<T>(D, LD, w, w);
   if (fail >= 0) {
     if (threadIdx.x == 0) info[b] = c0 + fail + 1;
     return;
   }
-  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-    int r = e % w, c = e / w;
-    if (r >= c) M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] = D[c * LD + r];
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    const int r = e % NB, c = e / NB;
+    if (r < w && c < w && r >= c) M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] = D[c * LD + r];
   }
   note_pivots(D, LD, w, dmin, dmax, b);
 }
@@ -171,10 +189,7 @@ __global__ void __launch_bounds__(128) k_potrf_trsm_rows(const MatDesc<T>* mats,
   const int w = min(NB, M.n - c0);
   const int first = c0 + w + blockIdx.x * blockDim.x;
   if (first >= M.n) return;
-  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-    int r = e % w, c = e / w;
-    D[c * LD + r] = (r >= c) ? M.a[(size_t)(c0 + c) * M.ld + (c0 + r)] : T(0);
-  }
+  load_diag_tile<T, NB, 128>(D, LD, M, c0, w);
   __shared__ T inv[NB];
   __syncthreads();  // the diagonal tile is loaded
   for (int c = threadIdx.x; c < w; c += blockDim.x) inv[c] = T(1) / D[c * LD + c];

@@ -18,8 +18,8 @@
 // all 8·64 = 512 TMEM columns.  128 threads per CTA, one CTA per SM: thread 0
 // issues the TMA boxes (K = 32 bytes per row, 32-byte swizzle, four 48 KB
 // stages), thread 32 issues the 12 MMAs of a stage (M = 128, N ≤ 256, K = 32,
-// all 36 digit products) and commits them to the stage's "empty" barrier, all four warps convert the
-// int32 levels to FP64 in the epilogue.  Bounded waits with a device error flag;
+// all 36 digit products) and commits them to the stage's "empty" barrier, all
+// four warps convert the int32 levels to FP64 in the epilogue.  Bounded waits with a device error flag;
 // the producer drains its own copies before the CTA exits.  No cluster, no
 // multicast.
 #include <cuda.h>
@@ -60,12 +60,12 @@ __device__ __forceinline__ double scale2(double v, int e) {
   return (e >= -1022 && e <= 1023) ? v * __longlong_as_double((long long)(e + 1023) << 52)
                                    : ldexp(v, e);
 }
-// Nearest integer (ties to even, as rint) of |x| < 2^51 by adding and
-// subtracting 1.5·2^52; the low word of the sum is the integer itself.
 // 2^(-7·lv), the weight of digit level lv.
 __device__ __forceinline__ double level_scale(int lv) {
   return __longlong_as_double((long long)(1023 - 7 * lv) << 52);
 }
+// Nearest integer (ties to even, as rint) of |x| < 2^51 by adding and
+// subtracting 1.5·2^52; the low word of the sum is the integer itself.
 constexpr double kRound = 6755399441055744.0;
 __device__ __forceinline__ double round_digit(double x, int& di) {
   const double t = x + kRound;
@@ -76,15 +76,21 @@ __device__ __forceinline__ double round_digit(double x, int& di) {
 // ---------------------------------------------------------------- digits --
 // One CTA per column: largest magnitude → exponent, then the digit planes
 // (digit t of column i at digits[t·m·Kp + i·Kp + k], zero for k ≥ K).
+// When dense_hi is given, the rows [0, tail_off) were written by a producer
+// that recorded the largest high word of |P_ki| per column (dense_hi[i]); only
+// the tail rows are scanned here and the exponent follows from the combined
+// high word (the exponent field of the largest magnitude: the same e as frexp
+// for a normal maximum).
 __global__ void k_oz_digits(const double* __restrict__ P, long long K, long long Kp, int m,
-                            int8_t* __restrict__ digits, int* __restrict__ exps) {
+                            int8_t* __restrict__ digits, int* __restrict__ exps,
+                            const unsigned* __restrict__ dense_hi, long long tail_off) {
   __shared__ double red[32];
   __shared__ int s_exp;
   const int i = blockIdx.x;
   const double* col = P + (long long)i * K;
   double mx = 0.0;
   bool finite = true;
-  for (long long k = threadIdx.x; k < K; k += blockDim.x) {
+  for (long long k = (dense_hi ? tail_off : 0) + threadIdx.x; k < K; k += blockDim.x) {
     const double a = fabs(col[k]);
     if (!isfinite(a)) finite = false;
     mx = fmax(mx, a);
@@ -93,22 +99,42 @@ __global__ void k_oz_digits(const double* __restrict__ P, long long K, long long
   mx = block_max(mx, red);
   if (threadIdx.x == 0) {
     int e = 0;
-    if (all_finite && mx > 0.0) frexp(mx, &e);  // mx = f·2^e, f ∈ [0.5, 1)
-    s_exp = all_finite ? e : NAN_EXP;
-    exps[i] = s_exp;
+    if (dense_hi) {
+      const unsigned hw = max(dense_hi[i], (unsigned)__double2hiint(mx) & 0x7fffffffu);
+      if (!all_finite || hw >= 0x7ff00000u) e = NAN_EXP;
+      else if (hw >= 0x00100000u) e = (int)(hw >> 20) - 1022;
+      else e = -1021;  // subnormal or zero maximum: 2^-e still bounds the column
+    } else {
+      if (all_finite && mx > 0.0) frexp(mx, &e);  // mx = f·2^e, f ∈ [0.5, 1)
+      if (!all_finite) e = NAN_EXP;
+    }
+    s_exp = e;
+    exps[i] = e;
   }
   __syncthreads();
   const int e = s_exp;
   const size_t plane = (size_t)m * Kp;
   int8_t* dst = digits + (size_t)i * Kp;
-  for (long long k = threadIdx.x; k < Kp; k += blockDim.x) {
-    double r = (k < K && e != NAN_EXP) ? scale2(col[k], 6 - e) : 0.0;  // 64·v, |v| < 1
+  // Four consecutive rows per thread: one char4 store per digit plane (Kp is a
+  // multiple of 64).
+  for (long long k0 = 4 * (long long)threadIdx.x; k0 < Kp; k0 += 4 * blockDim.x) {
+    double r[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const long long k = k0 + q;
+      r[q] = (k < K && e != NAN_EXP) ? scale2(col[k], 6 - e) : 0.0;  // 64·v, |v| < 1
+    }
 #pragma unroll
     for (int t = 0; t < OZ_DIGITS; ++t) {
-      int di;
-      const double d = round_digit(r, di);
-      dst[(size_t)t * plane + k] = (int8_t)di;
-      r = (r - d) * 128.0;
+      int d0, d1, d2, d3;
+      const double a0 = round_digit(r[0], d0), a1 = round_digit(r[1], d1);
+      const double a2 = round_digit(r[2], d2), a3 = round_digit(r[3], d3);
+      *reinterpret_cast<char4*>(dst + (size_t)t * plane + k0) =
+          make_char4((signed char)d0, (signed char)d1, (signed char)d2, (signed char)d3);
+      r[0] = (r[0] - a0) * 128.0;
+      r[1] = (r[1] - a1) * 128.0;
+      r[2] = (r[2] - a2) * 128.0;
+      r[3] = (r[3] - a3) * 128.0;
     }
   }
 }
@@ -358,6 +384,7 @@ struct OzGemmDev {
   const int* ea;
   const int* eb;
   double* out;
+  unsigned* colmax;  // optional: largest high word of |out| per group a / a_inner
   long long ntask, a_is, a_os, b_stride;
   int rows_a, rows_b, kext, kmode, ntile_b, a_inner;
 };
@@ -499,6 +526,7 @@ __global__ void __launch_bounds__(GNT, 1)
       __syncwarp();
       if (lane == 0) umma::mbar_arrive(&sh->tempty);
       const int ga = mt * OM + quarter * 32 + lane;
+      unsigned hw = 0;
       if (ga < g.rows_a) {
         const int ea = g.ea[ga];
         double* row = g.out + (long long)(ga / g.a_inner) * g.a_os + (long long)(ga % g.a_inner) * g.a_is;
@@ -507,11 +535,19 @@ __global__ void __launch_bounds__(GNT, 1)
           const int gb = nt * ON + cgrp * 16 + q;
           if (gb < g.rows_b) {
             const int eb = g.eb[gb];
-            row[(long long)gb * g.b_stride] = (ea == NAN_EXP || eb == NAN_EXP)
-                                                  ? __longlong_as_double(0x7ff8000000000000ll)
-                                                  : scale2(acc[q], ea + eb - 12);
+            const double v = (ea == NAN_EXP || eb == NAN_EXP)
+                                 ? __longlong_as_double(0x7ff8000000000000ll)
+                                 : scale2(acc[q], ea + eb - 12);
+            row[(long long)gb * g.b_stride] = v;
+            hw = max(hw, (unsigned)__double2hiint(v) & 0x7fffffffu);
           }
         }
+      }
+      if (g.colmax) {  // one atomic per group of lanes that share a / a_inner
+        const int grp = ga < g.rows_a ? ga / g.a_inner : -1;
+        const unsigned same = __match_any_sync(0xffffffffu, grp);
+        const unsigned mx = __reduce_max_sync(same, hw);
+        if (grp >= 0 && lane == __ffs(same) - 1) atomicMax(&g.colmax[grp], mx);
       }
     }
   }
@@ -585,10 +621,11 @@ OzakiPlan plan_ozaki_syrk(int m, long long K, int sm_count) {
 }
 
 void ozaki_syrk(const double* P, const OzakiPlan& plan, int8_t* digits, int* exps, double* partial,
-                double* S, int* err, cudaStream_t st, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
+                double* S, int* err, cudaStream_t st, cudaEvent_t ev_begin, cudaEvent_t ev_end,
+                const unsigned* dense_hi, long long tail_off) {
   const int m = plan.m;
   if (m <= 0) return;
-  k_oz_digits<<<m, 256, 0, st>>>(P, plan.K, plan.Kp, m, digits, exps);
+  k_oz_digits<<<m, 256, 0, st>>>(P, plan.K, plan.Kp, m, digits, exps, dense_hi, tail_off);
   SDPX_LAUNCH_CHECK();
   // The tile-pair table follows the partial tiles in the same buffer
   // (plan.partial_alloc_doubles).  A copy from pageable memory returns once the
@@ -639,6 +676,7 @@ void ozaki_gemm(const OzGemm& g, int sm_count, int* err, cudaStream_t st) {
   dv.ea = g.ea;
   dv.eb = g.eb;
   dv.out = g.out;
+  dv.colmax = g.colmax;
   dv.rows_a = g.rows_a;
   dv.rows_b = g.rows_b;
   dv.kext = (int)g.Kp;

@@ -25,9 +25,13 @@ OzakiPlan plan_ozaki_syrk(int m, long long K, int sm_count);
 // (K×m, column-major, ld = K).  digits: plan.digit_bytes of scratch, exps: m
 // ints, partial: plan.partial_alloc_doubles.  err: device flag set when a bounded
 // wait gave up.  ev_begin/ev_end (optional) bracket the tensor-core kernel.
+// dense_hi (optional, m entries): the rows [0, tail_off) of P were written by
+// ozaki_gemm with OzGemm::colmax = dense_hi, so their per-column maxima are
+// known and only the rows [tail_off, K) are scanned for the column exponents.
 void ozaki_syrk(const double* P, const OzakiPlan& plan, int8_t* digits, int* exps, double* partial,
                 double* S, int* err, cudaStream_t st, cudaEvent_t ev_begin = nullptr,
-                cudaEvent_t ev_end = nullptr);
+                cudaEvent_t ev_end = nullptr, const unsigned* dense_hi = nullptr,
+                long long tail_off = 0);
 
 // ---- general products C[a, b] = Σ_j X[a, j]·Y[b, j] on digit planes --------
 
@@ -71,6 +75,9 @@ struct OzGemm {
   double* out = nullptr;
   int a_inner = 1 << 30;
   long long a_is = 0, a_os = 0, b_stride = 0;
+  // Optional: colmax[a / a_inner] = max(colmax[...], high word of |out|) — the
+  // exponent field of each group's largest written magnitude (caller zeroes it).
+  unsigned* colmax = nullptr;
 };
 void ozaki_gemm(const OzGemm& g, int sm_count, int* err, cudaStream_t st);
 
