@@ -247,6 +247,7 @@ struct Handle {
     }
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (h_red) cudaFreeHost(h_red);
+    if (h_pin) cudaFreeHost(h_pin);
     mixed.reset();
     if (st) cudaStreamDestroy(st);
   }
@@ -386,6 +387,23 @@ struct Handle {
     d_info.alloc(desc_cap);
     d_dmin.alloc(desc_cap);
     d_dmax.alloc(desc_cap);
+    d_stats.alloc(3 * desc_cap);
+  }
+  // Pinned staging for the per-round uploads (descriptor lists) and the
+  // packed read-back of the batched Cholesky results: asynchronous copies
+  // instead of staged pageable ones.  Only grown right after a sync.
+  DBuf<double> d_stats;  // one round's dmin | dmax | info, contiguous
+  unsigned char* h_pin = nullptr;
+  size_t pin_cap = 0;
+  unsigned char* pinned(size_t bytes) {
+    if (bytes > pin_cap) {
+      sync();
+      if (h_pin) cudaFreeHost(h_pin);
+      h_pin = nullptr;
+      pin_cap = std::max<size_t>(bytes, 2 * pin_cap);
+      SDPX_CUDA(cudaMallocHost(&h_pin, pin_cap));
+    }
+    return h_pin;
   }
 
   // Batched Cholesky of host-described matrices; fills info/dmin/dmax (host).
@@ -402,17 +420,26 @@ struct Handle {
     ensure_descs(n);
     int nmax = 0;
     for (auto& q : mats) nmax = std::max(nmax, q.n);
-    h2d(d_descs.p, mats.data(), n * sizeof(MatDesc<double>));
+    // Pinned layout: [descriptors | dmin (n) | dmax (n) | info (n)], the last
+    // three read back in one copy from d_stats.
+    const size_t dbytes = (n * sizeof(MatDesc<double>) + 15) / 16 * 16;
+    const size_t sbytes = 2 * n * sizeof(double) + n * sizeof(int);
+    unsigned char* hp = pinned(dbytes + sbytes);
+    std::memcpy(hp, mats.data(), n * sizeof(MatDesc<double>));
+    h2d(d_descs.p, hp, n * sizeof(MatDesc<double>));
+    double* sdmin = d_stats.p;
+    double* sdmax = d_stats.p + n;
+    int* sinfo = reinterpret_cast<int*>(d_stats.p + 2 * n);
     if (nmax >= 192)
-      potrf_batched<double, 64>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p, st,
-                                zero_upper);
+      potrf_batched<double, 64>(d_descs.p, (int)n, nmax, sinfo, sdmin, sdmax, st, zero_upper);
     else
-      potrf_batched<double, 32>(d_descs.p, (int)n, nmax, d_info.p, d_dmin.p, d_dmax.p, st,
-                                zero_upper);
-    d2h(info.data(), d_info.p, n * sizeof(int));
-    d2h(dmin.data(), d_dmin.p, n * sizeof(double));
-    d2h(dmax.data(), d_dmax.p, n * sizeof(double));
+      potrf_batched<double, 32>(d_descs.p, (int)n, nmax, sinfo, sdmin, sdmax, st, zero_upper);
+    d2h(hp + dbytes, d_stats.p, sbytes);
     sync();
+    const double* hs = reinterpret_cast<const double*>(hp + dbytes);
+    std::memcpy(dmin.data(), hs, n * sizeof(double));
+    std::memcpy(dmax.data(), hs + n, n * sizeof(double));
+    std::memcpy(info.data(), hs + 2 * n, n * sizeof(int));
   }
 
   // ------------------------------------------------------------ create ----
@@ -559,7 +586,7 @@ struct Handle {
     SDPX_CUDA(cudaMallocHost(&h_red, 64 * sizeof(double)));
     mu_user.alloc(L);
     target_user.alloc(L);
-    work_L.alloc(std::max<size_t>((size_t)L, dense.size()) + 1);
+    work_L.alloc(2 * std::max<size_t>((size_t)L, dense.size()) + 2);
     seg_parts = 8;
     seg_part.alloc((size_t)seg_parts * L);
     ensure_descs(std::max<size_t>(16, 2 * dense.size()));
@@ -1585,7 +1612,12 @@ struct Handle {
       td[q] = {reqs[q].M + B.off, reqs[q].dM + B.off, trials.p + off[q], reqs[q].t, B.k};
     }
     if (d_trial_desc.n < n) d_trial_desc.alloc(std::max<size_t>(n, 2 * d_trial_desc.n));
-    h2d(d_trial_desc.p, td.data(), n * sizeof(TrialDesc));
+    // Staged at the end of the pinned area: potrf_host_list below uses its
+    // start, and this copy is ordered before that call's final sync.
+    const size_t tail = (n * (sizeof(MatDesc<double>) + 2 * sizeof(double) + sizeof(int)) + 64 + 15) / 16 * 16;
+    unsigned char* hp = pinned(tail + n * sizeof(TrialDesc)) + tail;
+    std::memcpy(hp, td.data(), n * sizeof(TrialDesc));
+    h2d(d_trial_desc.p, hp, n * sizeof(TrialDesc));
     make_trials_list(d_trial_desc.p, (int)n, nmax, st);
     std::vector<MatDesc<double>> mats(n);
     for (size_t q = 0; q < n; ++q) mats[q] = {trials.p + off[q], dense[reqs[q].b].k, dense[reqs[q].b].k};
@@ -1715,22 +1747,22 @@ struct Handle {
       tX = bX < 1 ? bX : 1.0;
       tY = bY < 1 ? bY : 1.0;
     }
-    std::vector<double> c1(L), c2(L);
+    std::vector<double> c12(2 * (size_t)L);
     seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, nullptr, 0.0, Y.p, nullptr, 0.0, seg_part.p,
             work_L.p, st);
-    d2h(c1.data(), work_L.p, L * sizeof(double));
+    seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, dX.p, tX, Y.p, dY.p, tY, seg_part.p,
+            work_L.p + L, st);
+    d2h(c12.data(), work_L.p, 2 * L * sizeof(double));  // both in one read-back
     sync();
-    seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, dX.p, tX, Y.p, dY.p, tY, seg_part.p, work_L.p,
-            st);
-    d2h(c2.data(), work_L.p, L * sizeof(double));
-    sync();
+    const double* c1 = c12.data();
+    const double* c2 = c12.data() + L;
     double s1 = 0, s2 = 0;
     for (int l = 0; l < L; ++l) s1 += c1[l], s2 += c2[l];
     out[0] = s1;
     out[1] = s2;
     out[2] = tX;
     out[3] = tY;
-    if (block_compl) std::memcpy(block_compl, c1.data(), L * sizeof(double));
+    if (block_compl) std::memcpy(block_compl, c1, L * sizeof(double));
   }
 
   void line_search(int rule, double fp, double fd, double gamma, double min_step, double margin,

@@ -4,6 +4,7 @@
 #include "blas_f64.h"
 #include "gemm_f64.cuh"
 
+#include <atomic>
 #include <mutex>
 #include <stdexcept>
 
@@ -17,6 +18,12 @@ using CfgSmMK = F64Cfg<64, 64, 2, 2, false, true>;
 using CfgSmKK = F64Cfg<64, 64, 2, 2, true, true>;
 using CfgSmMM = F64Cfg<64, 64, 2, 2, false, false>;
 using CfgSmKM = F64Cfg<64, 64, 2, 2, true, false>;
+// 32×32 / 4 warps when the 64×64 grid would not fill the GPU (the k×k block
+// products of the Newton step: 400×400 is 49 tiles of 64 but 169 of 32).
+using CfgTnMK = F64Cfg<32, 32, 2, 2, false, true>;
+using CfgTnKK = F64Cfg<32, 32, 2, 2, true, true>;
+using CfgTnMM = F64Cfg<32, 32, 2, 2, false, false>;
+using CfgTnKM = F64Cfg<32, 32, 2, 2, true, false>;
 
 // Grid: the fast index runs over the dimension with fewer tiles (rows_fast: x
 // over row tiles), so CTAs sharing a tile of the larger operand run together.
@@ -95,6 +102,21 @@ __global__ void k_syrk_reduce(const double* partial, int ntri, int nchunk, int m
   }
 }
 
+// SM count of the current device (cached per device).
+static int gemm_sm_count() {
+  static std::atomic<int> cached[64];
+  int dev = 0;
+  SDPX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return 148;
+  int v = cached[dev].load(std::memory_order_relaxed);
+  if (v == 0) {
+    SDPX_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    if (v <= 0) v = 148;
+    cached[dev].store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
+
 template <class Cfg>
 static void launch_gemm_cfg(const Opnd& A, const Opnd& B, const OutDesc& C, double alpha,
                             double beta, int mode, cudaStream_t st) {
@@ -112,6 +134,12 @@ void gemm_f64(const Opnd& A, bool a_kcontig, const Opnd& B, bool b_kcontig, cons
               double alpha, double beta, int mode, bool big, cudaStream_t st) {
   if (big && !a_kcontig && b_kcontig) return launch_gemm_cfg<CfgBigMK>(A, B, C, alpha, beta, mode, st);
   if (big && a_kcontig && b_kcontig) return launch_gemm_cfg<CfgBigKT>(A, B, C, alpha, beta, mode, st);
+  if (!big && (long long)ceil_div(C.rows, 64) * ceil_div(C.cols, 64) < gemm_sm_count()) {
+    if (!a_kcontig && b_kcontig) return launch_gemm_cfg<CfgTnMK>(A, B, C, alpha, beta, mode, st);
+    if (a_kcontig && b_kcontig) return launch_gemm_cfg<CfgTnKK>(A, B, C, alpha, beta, mode, st);
+    if (!a_kcontig && !b_kcontig) return launch_gemm_cfg<CfgTnMM>(A, B, C, alpha, beta, mode, st);
+    return launch_gemm_cfg<CfgTnKM>(A, B, C, alpha, beta, mode, st);
+  }
   if (!a_kcontig && b_kcontig) return launch_gemm_cfg<CfgSmMK>(A, B, C, alpha, beta, mode, st);
   if (a_kcontig && b_kcontig) return launch_gemm_cfg<CfgSmKK>(A, B, C, alpha, beta, mode, st);
   if (!a_kcontig && !b_kcontig) return launch_gemm_cfg<CfgSmMM>(A, B, C, alpha, beta, mode, st);
