@@ -230,11 +230,13 @@ int sdpx_b200_certificate(sdpx_b200_handle* h, const double* x, const double* X,
                           double eps_primal, double eps_dual, double eps_gap, int32_t legacy_gap,
                           sdpx_b200_certificate_result* out);
 
-/* Engine of the FP64 Schur Gram S = P̂ᵀP̂ (no counterpart in the reference,
- * whose Float64 SYRK is BLAS): 0 = FP64 DMMA tiles, 1 = exact int8 (default)
- * digit products on the tensor cores — every P̂ column scaled by a power of two
- * and cut into seven int8 digits (48 significant bits), digit products
- * accumulated exactly in int32 and the levels summed in FP64. */
+/* Engine of the FP64 Schur assembly — the Gram S = P̂ᵀP̂ and the block
+ * products T_i = L_X⁻¹·A_i, P_i = T_i·L_Y (no counterpart in the reference,
+ * whose Float64 products are BLAS): 0 = FP64 DMMA tiles, 1 = exact int8
+ * (default) digit products on the tensor cores — every operand row or column
+ * scaled by a power of two and cut into eight int8 digits (55 significant
+ * bits), digit products accumulated exactly in int32 and the levels summed in
+ * FP64. */
 int sdpx_b200_set_gram_engine(sdpx_b200_handle* h, int engine);
 
 /* Instrumentation (no counterpart in the reference): device time (ms) of the

@@ -430,7 +430,7 @@ struct Handle {
     double* sdmin = d_stats.p;
     double* sdmax = d_stats.p + n;
     int* sinfo = reinterpret_cast<int*>(d_stats.p + 2 * n);
-    if (nmax >= 192)
+    if (nmax >= 192 && zero_upper)
       potrf_batched<double, 64>(d_descs.p, (int)n, nmax, sinfo, sdmin, sdmax, st, zero_upper);
     else
       potrf_batched<double, 32>(d_descs.p, (int)n, nmax, sinfo, sdmin, sdmax, st, zero_upper);

@@ -300,8 +300,9 @@ __global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info) {
     }
   }
   __syncthreads();
-  // Each thread owns a 4×4 block of outputs (NB=64: 256 threads; NB=32: 64 active).
-  constexpr int RB = 4;
+  // Each thread owns an RB×RB block of outputs, RB = NB/16: 256 threads for
+  // NB = 64 (4×4) and NB = 32 (2×2).
+  constexpr int RB = NB / 16;
   constexpr int TPR = NB / RB;
   const int tr = threadIdx.x % TPR, tc = threadIdx.x / TPR;
   if (tc < TPR) {

@@ -490,8 +490,8 @@ class CudaBackend:
         self._switch_reason = None
 
     def set_gram_engine(self, engine: str):
-        """FP64 Schur Gram engine: "dmma" (FP64 tensor tiles) or "int8" (exact
-        int8 digit products, 48-bit digits)."""
+        """FP64 Schur engine (Gram and block products): "dmma" (FP64 tensor
+        tiles) or "int8" (exact int8 digit products, eight digits = 55 bits)."""
         self._call("sdpx_b200_set_gram_engine", {"dmma": 0, "int8": 1}[engine])
 
     def kernel_times(self) -> dict:
