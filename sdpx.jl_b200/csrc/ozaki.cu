@@ -369,7 +369,8 @@ __global__ void k_oz_digits_rows(const OzRowsDev r, long long Kp, long long plan
 
 // ---------------------------------------------------------------- GEMM ----
 // Persistent CTAs over the (128-row X tile, 64-row Y tile) tasks, Y tiles
-// fastest so that concurrent tasks share X tiles in L2.  Warp 16 (one thread)
+// fastest (rotated per X tile, see oz_tile) so that concurrent tasks share X
+// tiles in L2.  Warp 16 (one thread)
 // streams the digit boxes through the four stages and runs ahead into the
 // next task; warp 17 (one thread) issues the 12 MMAs of a stage and, at the
 // end of a task, commits the eight level accumulators to `tfull`; warps 0-15
@@ -411,10 +412,19 @@ __device__ __forceinline__ bool oz_wait(uint64_t* mbar, uint32_t parity, int* er
   return true;
 }
 
+// Task u → (X tile mt, Y tile nt).  The Y tiles of one X tile are consecutive
+// tasks (they share the X tile in L2), rotated by mt: a persistent CTA takes
+// every gridDim-th task, and without the rotation a grid that is a multiple
+// of ntile_b would give each CTA one fixed Y tile — one fixed K length under
+// the triangular ranges, so some CTAs would run several times longer.
+__device__ __forceinline__ void oz_tile(const OzGemmDev& g, long long u, int& mt, int& nt) {
+  mt = (int)(u / g.ntile_b);
+  nt = (int)((u % g.ntile_b + mt) % g.ntile_b);
+}
+
 __device__ __forceinline__ void oz_task(const OzGemmDev& g, long long u, int& mt, int& nt, int& kb,
                                         int& nk) {
-  mt = (int)(u / g.ntile_b);
-  nt = (int)(u % g.ntile_b);
+  oz_tile(g, u, mt, nt);
   kb = 0;
   int ke = g.kext;
   const int n0 = nt * ON;
@@ -511,20 +521,43 @@ __global__ void __launch_bounds__(GNT, 1)
     for (long long u = blockIdx.x; u < g.ntask; u += gridDim.x, ++j) {
       if (!oz_wait(&sh->tfull, j & 1, err, abort)) break;
       umma::fence_after_sync();
-      const int mt = (int)(u / g.ntile_b), nt = (int)(u % g.ntile_b);
+      int mt, nt;
+      oz_tile(g, u, mt, nt);
+      // Levels in two batches of four loads in flight, summed smallest first;
+      // the accumulator goes back to the MMA warp as soon as the second batch
+      // is in registers, before its conversion.
+      static_assert(OLEVELS == 8, "two batches of four levels");
+      const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(cgrp * 16);
       double acc[16];
 #pragma unroll
       for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+      {
+        uint32_t raw[4][16];
 #pragma unroll
-      for (int lv = OLEVELS - 1; lv >= 0; --lv) {
-        uint32_t raw[16];
-        umma::tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(lv * ON + cgrp * 16), raw);
+        for (int b = 0; b < 4; ++b) umma::tmem_ld16_async(tbase + (uint32_t)((7 - b) * ON), raw[b]);
+        umma::tmem_wait_ld();
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = fma(i32_to_f64((int)raw[q]), level_scale(lv), acc[q]);
+        for (int b = 0; b < 4; ++b) umma::tmem_regs_ready(raw[b]);
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            acc[q] = fma(i32_to_f64((int)raw[b][q]), level_scale(7 - b), acc[q]);
       }
+      uint32_t raw[4][16];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) umma::tmem_ld16_async(tbase + (uint32_t)((3 - b) * ON), raw[b]);
+      umma::tmem_wait_ld();
+#pragma unroll
+      for (int b = 0; b < 4; ++b) umma::tmem_regs_ready(raw[b]);
       umma::fence_before_sync();
       __syncwarp();
       if (lane == 0) umma::mbar_arrive(&sh->tempty);
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          acc[q] = fma(i32_to_f64((int)raw[b][q]), level_scale(3 - b), acc[q]);
       const int ga = mt * OM + quarter * 32 + lane;
       unsigned hw = 0;
       if (ga < g.rows_a) {
