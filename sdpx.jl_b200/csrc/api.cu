@@ -432,6 +432,8 @@ struct Handle {
     int* sinfo = reinterpret_cast<int*>(d_stats.p + 2 * n);
     if (nmax >= 192 && zero_upper)
       potrf_batched<double, 64>(d_descs.p, (int)n, nmax, sinfo, sdmin, sdmax, st, zero_upper);
+    else if (nmax >= 192)
+      potrf_batched<double, 48>(d_descs.p, (int)n, nmax, sinfo, sdmin, sdmax, st, zero_upper);
     else
       potrf_batched<double, 32>(d_descs.p, (int)n, nmax, sinfo, sdmin, sdmax, st, zero_upper);
     d2h(hp + dbytes, d_stats.p, sbytes);

@@ -394,6 +394,8 @@ void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* d
 
 template void potrf_batched<double, 32>(const MatDesc<double>*, int, int, int*, double*, double*,
                                         cudaStream_t, bool);
+template void potrf_batched<double, 48>(const MatDesc<double>*, int, int, int*, double*, double*,
+                                        cudaStream_t, bool);
 template void potrf_batched<double, 64>(const MatDesc<double>*, int, int, int*, double*, double*,
                                         cudaStream_t, bool);
 template void potrf_batched<float, 64>(const MatDesc<float>*, int, int, int*, float*, float*,
