@@ -942,6 +942,7 @@ struct Handle {
       // Gram's digit planes (same size as the FP64 panel), with 2 GB to spare.
       size_t freeb = 0, totb = 0;
       SDPX_CUDA(cudaMemGetInfo(&freeb, &totb));
+      freeb += dcache::idle_bytes(dev);  // idle cached blocks are ours to reuse
       const size_t gram = oz_plan.m == m && oz_plan.K == K ? 0 : (size_t)OZ_DIGITS * m * (K + 64);
       const size_t need = adig + tdig + wdig + 4 * (size_t)(aexp + texp + wexp) + gram;
       if (dense.empty() || need + (2ull << 30) > freeb) {
@@ -2562,6 +2563,10 @@ int sdpx_b200_counters(sdpx_b200_handle* h, int64_t* out4) {
   });
 }
 int sdpx_b200_get_stream(sdpx_b200_handle* h, void** stream) { GUARD(h, *stream = (void*)h->h.st); }
+int sdpx_b200_trim_device_cache(void) {
+  sdpx::dcache::trim(-1);
+  return 0;
+}
 int sdpx_b200_launch_count(uint64_t* count) {
   if (!count) return -1;
   *count = sdpx::launch_count();
