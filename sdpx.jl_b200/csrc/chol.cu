@@ -19,66 +19,48 @@ namespace sdpx {
 // column-major, leading dimension ld; rows ≥ w).  Returns the failing column
 // or -1.  All threads of the CTA take part.
 //
-// Blocked by 8 columns: thread 0 factors the 8×8 diagonal block (l_cc =
-// sqrt(a_cc), column below scaled by 1/l_cc, as LAPACK's unblocked dpotf2
-// does) and publishes it with the reciprocal pivots; each row below the block
-// is solved in registers (x = a · L_bb^{-T}); the trailing columns of the panel
-// receive the rank-8 update with the block's rows read as warp broadcasts.
-// Every element sees its updates in increasing column order.
+// Blocked by 8 columns: every thread factors the 8×8 diagonal block in its
+// registers (l_cc = sqrt(a_cc), column below scaled by 1/l_cc, as LAPACK's
+// unblocked dpotf2 does) — the same arithmetic in every thread, so the factor
+// needs no publication and no barrier of its own; each row below the block is
+// solved in registers (x = a · L_bb^{-T}); after one barrier the trailing
+// columns of the panel receive the rank-8 update (the block's rows read as
+// warp broadcasts) while thread 0 writes the factored block back.  Two
+// barriers per 8 columns.  Every element sees its updates in increasing column
+// order.
 template <class T>
 __device__ int factor_panel_smem(T* P, int ld, int rows, int w) {
-  __shared__ T sD[8][8];
-  __shared__ T sInv[8];
-  __shared__ int s_fail;
   __syncthreads();
   for (int kb = 0; kb < w; kb += 8) {
     const int kw = min(8, w - kb);
-    if (threadIdx.x == 0) {
-      T D[8][8];
-#pragma unroll
-      for (int c = 0; c < 8; ++c)
-#pragma unroll
-        for (int r = 0; r < 8; ++r)
-          D[c][r] = (c < kw && r < kw && r >= c) ? P[(kb + c) * ld + kb + r] : T(0);
-      int fail = -1;
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        if (c < kw && fail < 0) {
-          const T piv = D[c][c];
-          if (!(piv > T(0))) {
-            fail = c;
-          } else {
-            const T lc = sqrt(piv);
-            const T inv = T(1) / lc;
-            D[c][c] = lc;
-            sInv[c] = inv;
-#pragma unroll
-            for (int r = c + 1; r < 8; ++r) D[c][r] *= inv;
-#pragma unroll
-            for (int q = c + 1; q < 8; ++q)
-#pragma unroll
-              for (int r = q; r < 8; ++r) D[q][r] -= D[c][r] * D[c][q];
-          }
-        }
-      }
-      s_fail = fail;
-#pragma unroll
-      for (int c = 0; c < 8; ++c)
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          sD[c][r] = D[c][r];
-          if (c < kw && r < kw && r >= c) P[(kb + c) * ld + kb + r] = D[c][r];
-        }
-    }
-    __syncthreads();
-    if (s_fail >= 0) return kb + s_fail;  // uniform after the barrier
     T D[8][8], inv[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      inv[c] = sInv[c];
+    for (int c = 0; c < 8; ++c)
 #pragma unroll
-      for (int r = c + 1; r < 8; ++r) D[c][r] = sD[c][r];
+      for (int r = 0; r < 8; ++r)
+        D[c][r] = (c < kw && r < kw && r >= c) ? P[(kb + c) * ld + kb + r] : T(0);
+    int fail = -1;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      inv[c] = T(0);
+      if (c < kw && fail < 0) {
+        const T piv = D[c][c];
+        if (!(piv > T(0))) {
+          fail = c;
+        } else {
+          const T lc = sqrt(piv);
+          inv[c] = T(1) / lc;
+          D[c][c] = lc;
+#pragma unroll
+          for (int r = c + 1; r < 8; ++r) D[c][r] *= inv[c];
+#pragma unroll
+          for (int q = c + 1; q < 8; ++q)
+#pragma unroll
+            for (int r = q; r < 8; ++r) D[q][r] -= D[c][r] * D[c][q];
+        }
+      }
     }
+    if (fail >= 0) return kb + fail;  // the same in every thread
     // rows below the block: x = a · L_bb^{-T}
     for (int r = kb + kw + threadIdx.x; r < rows; r += blockDim.x) {
       T x[8];
@@ -97,6 +79,13 @@ __device__ int factor_panel_smem(T* P, int ld, int rows, int w) {
         if (c < kw) P[(kb + c) * ld + r] = x[c];
     }
     __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+          if (c < kw && r < kw && r >= c) P[(kb + c) * ld + kb + r] = D[c][r];
+    }
     // trailing panel columns q ∈ [kb+kw, w), rows r ≥ q
     for (int r = kb + kw + threadIdx.x; r < rows; r += blockDim.x) {
       T x[8];
