@@ -200,56 +200,208 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   pipe_release(tmem);
 }
 
-// out = A·Bᵀ split into three BF16 output planes.  The grid's fast index runs
-// over the operand with fewer tiles (a_fast: x over A rows, y over B rows;
-// otherwise the reverse), so the CTAs that share a tile of the large operand
-// run together and read it from L2.  kmode 0 full K, 1 A lower-triangular
-// (k ≤ row), 2 B lower-triangular (k ≥ col).
-__global__ void __launch_bounds__(NTHREADS, 1)
-    k_split_gemm_tma(const __grid_constant__ TmaMaps maps, OutMap out, int kmode, int Ktot,
-                     int a_fast, int* err) {
+// Block products, persistent and warp-specialised.  With K at most
+// ceil(k/32) stages per output tile, a CTA per tile spends much of its time
+// filling the pipeline and draining the accumulator.  Here one CTA per SM walks
+// its tiles: warp 4 (one thread) streams the six plane boxes of each stage and
+// runs ahead into the next tile, warp 5 (one thread) issues the MMAs into one
+// of two TMEM accumulator buffers (columns [256·b, 256·b + 256): leading
+// product at +0, lower-order products at +128) and commits the tile to
+// tfull[b]; warps 0-3 drain buffer b, hand it back through tempty[b], and split
+// and store while the MMAs of the next tile run into the other buffer.  Tiles
+// run the operand with fewer tiles fastest (they share the other operand's
+// tile in L2), rotated by the slow index so each CTA sees every K length of the
+// triangular ranges.  out = A·Bᵀ split into three BF16 output planes; kmode 0
+// contracts the full K, 1 stops at the end of the A tile (A lower-triangular,
+// rows of L_X⁻¹), 2 starts at the B tile (B rows are columns of L_Y, zero
+// above the diagonal).
+constexpr int PG_THREADS = 6 * 32;
+
+struct PGemmShared {
+  uint64_t full[SNST], empty[SNST], tfull[2], tempty[2], mdone;
+  uint32_t tmem;
+  int abort;
+};
+
+struct PGemmTiles {
+  long long ntask;
+  int ta, tb, a_fast, kmode, Ktot;
+};
+
+__device__ __forceinline__ bool pg_wait(uint64_t* mbar, uint32_t parity, int* err,
+                                        volatile int* abort) {
+  const long long t0 = clock64();
+  while (!umma::mbar_test(mbar, parity)) {
+    if (*abort) return false;
+    if (clock64() - t0 > (1LL << 32)) {
+      atomicExch(err, 1);
+      *abort = 1;
+      return false;
+    }
+    __nanosleep(32);
+  }
+  return true;
+}
+
+__device__ __forceinline__ void pg_task(const PGemmTiles& g, long long u, int& r0, int& c0, int& kb,
+                                        int& nk) {
+  if (g.a_fast) {
+    const int slow = (int)(u / g.ta);
+    r0 = (int)((u % g.ta + slow) % g.ta) * TM;
+    c0 = slow * TN;
+  } else {
+    const int slow = (int)(u / g.tb);
+    c0 = (int)((u % g.tb + slow) % g.tb) * TN;
+    r0 = slow * TM;
+  }
+  kb = 0;
+  int ke = g.Ktot;
+  if (g.kmode == 1) ke = min(g.Ktot, r0 + TM);
+  if (g.kmode == 2) kb = (c0 / SK) * SK;
+  nk = ke > kb ? (ke - kb + SK - 1) / SK : 0;
+}
+
+__global__ void __launch_bounds__(PG_THREADS, 1)
+    k_split_gemm_persistent(const __grid_constant__ TmaMaps maps, OutMap out, PGemmTiles g,
+                            int* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = aligned_smem(smem_raw);
-  PipeShared* sh = reinterpret_cast<PipeShared*>(smem + SNST * SSTAGE_BYTES);
-  const uint32_t tmem = pipe_init(sh);
+  PGemmShared* sh = reinterpret_cast<PGemmShared*>(smem + SNST * SSTAGE_BYTES);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int r0 = (a_fast ? blockIdx.x : blockIdx.y) * TM;
-  const int c0 = (a_fast ? blockIdx.y : blockIdx.x) * TN;
-  int kb = 0, ke = Ktot;
-  if (kmode == 1) ke = min(Ktot, r0 + TM);
-  if (kmode == 2) kb = (c0 / SK) * SK;
-  const int ntiles = ke > kb ? (ke - kb + SK - 1) / SK : 0;
-  const bool ok = pipe_mainloop(maps, r0, c0, kb, ntiles, smem, sh, tmem, err);
-  const int row = warp * 32 + lane;
-  const int grow = r0 + row;
-  if (ok) {  // CTA-uniform: tcgen05.ld is warp-collective, only the stores are per row
-    const bool live = grow < out.rows.extent;
-    const long long ro = live ? row_off(out.rows, grow) : 0;
-    for (int cb = 0; cb < TN; cb += 32) {
-      float v[32];
-      if (ntiles > 0) {
-        tile_ld32(tmem, warp, cb, v);
-      } else {
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < SNST; ++s) {
+      umma::mbar_init(&sh->full[s], 1);
+      umma::mbar_init(&sh->empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      umma::mbar_init(&sh->tfull[b], 1);
+      umma::mbar_init(&sh->tempty[b], 4);
+    }
+    umma::mbar_init(&sh->mdone, 1);
+    sh->abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  if (warp == 0) umma::tmem_alloc(&sh->tmem, 512);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = sh->tmem;
+  volatile int* abort = &sh->abort;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (long long u = blockIdx.x; u < g.ntask && !*abort; u += gridDim.x) {
+        int r0, c0, kb, nk;
+        pg_task(g, u, r0, c0, kb, nk);
+        bool ok = true;
+        for (int t = 0; t < nk; ++t, ++it) {
+          const int s = it % SNST;
+          if (it >= SNST && !pg_wait(&sh->empty[s], ((it / SNST) - 1) & 1, err, abort)) {
+            ok = false;
+            break;
+          }
+          umma::mbar_expect_tx(&sh->full[s], SSTAGE_BYTES);
+          const uint32_t base = umma::smem_u32(smem + s * SSTAGE_BYTES);
+          const int k = kb + t * SK;
 #pragma unroll
-        for (int q = 0; q < 32; ++q) v[q] = 0.f;
+          for (int p = 0; p < 3; ++p) {
+            umma::tma_load_2d(base + p * SPLANE_BYTES, &maps.a[p], k, r0, &sh->full[s]);
+            umma::tma_load_2d(base + (3 + p) * SPLANE_BYTES, &maps.b[p], k, c0, &sh->full[s]);
+          }
+        }
+        if (!ok) break;
       }
-      if (!live) continue;
+      // every issued stage lands before the CTA may leave
+      for (uint32_t t = it > (uint32_t)SNST ? it - SNST : 0; t < it; ++t)
+        umma::mbar_wait_bounded(&sh->full[t % SNST], (t / SNST) & 1, err);
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {
+      constexpr uint32_t IDESC = umma::idesc_bf16_f32(TM, TN);
+      const int pa[6] = {0, 0, 1, 0, 1, 2};
+      const int pb[6] = {0, 1, 0, 2, 1, 0};
+      uint32_t it = 0, j = 0;
+      bool ok = true;
+      for (long long u = blockIdx.x; u < g.ntask && ok; u += gridDim.x, ++j) {
+        int r0, c0, kb, nk;
+        pg_task(g, u, r0, c0, kb, nk);
+        const int b = j & 1;
+        if (j >= 2 && !pg_wait(&sh->tempty[b], ((j >> 1) - 1) & 1, err, abort)) break;
+        umma::fence_after_sync();
+        const uint32_t acc0 = tmem + (uint32_t)(b * 256);
+        for (int t = 0; t < nk; ++t, ++it) {
+          const int s = it % SNST;
+          if (!pg_wait(&sh->full[s], (it / SNST) & 1, err, abort)) {
+            ok = false;
+            break;
+          }
+          umma::fence_after_sync();
+          const uint32_t base = umma::smem_u32(smem + s * SSTAGE_BYTES);
 #pragma unroll
-      for (int q = 0; q < 32; q += 8) {
-        const int gcol = c0 + cb + q;
-        if (gcol >= out.col_extent) continue;
-        const long long co = (long long)(gcol / out.col_inner) * out.col_os +
-                             (long long)(gcol % out.col_inner);
-        __align__(16) __nv_bfloat16 h[3][8];
+          for (int ks = 0; ks < SK / 16; ++ks) {
 #pragma unroll
-        for (int e = 0; e < 8; ++e) split3(v[q + e], h[0][e], h[1][e], h[2][e]);
+            for (int q = 0; q < 6; ++q) {
+              const uint64_t ad = umma::smem_desc_sw64(base + pa[q] * SPLANE_BYTES + ks * 32);
+              const uint64_t bd = umma::smem_desc_sw64(base + (3 + pb[q]) * SPLANE_BYTES + ks * 32);
+              const uint32_t acc = (t > 0 || ks > 0 || q > 1) ? 1u : 0u;
+              umma::mma_bf16(q == 0 ? acc0 : acc0 + 128, ad, bd, IDESC, acc);
+            }
+          }
+          umma::commit(&sh->empty[s]);
+        }
+        if (ok) umma::commit(&sh->tfull[b]);
+      }
+      umma::commit(&sh->mdone);  // every MMA completes before the accumulators are freed
+      umma::mbar_wait_bounded(&sh->mdone, 0, err);
+    }
+  } else {
+    // Epilogue: warps 0-3, TMEM lane quarter = warp, one output row per thread.
+    const int row = warp * 32 + lane;
+    uint32_t j = 0;
+    for (long long u = blockIdx.x; u < g.ntask; u += gridDim.x, ++j) {
+      int r0, c0, kb, nk;
+      pg_task(g, u, r0, c0, kb, nk);
+      const int b = j & 1;
+      if (!pg_wait(&sh->tfull[b], (j >> 1) & 1, err, abort)) break;
+      umma::fence_after_sync();
+      const int grow = r0 + row;
+      const bool live = grow < out.rows.extent;
+      const long long ro = live ? row_off(out.rows, grow) : 0;
+      const uint32_t acc0 = tmem + (uint32_t)(b * 256);
+      for (int cb = 0; cb < TN; cb += 32) {
+        float v[32];
+        if (nk > 0) {
+          tile_ld32(acc0, warp, cb, v);
+        } else {
 #pragma unroll
-        for (int p = 0; p < 3; ++p)
-          *reinterpret_cast<uint4*>(out.plane[p] + ro + co) = *reinterpret_cast<uint4*>(h[p]);
+          for (int q = 0; q < 32; ++q) v[q] = 0.f;
+        }
+        if (cb + 32 == TN) {  // every read of buffer b is complete: hand it back
+          umma::fence_before_sync();
+          __syncwarp();
+          if (lane == 0) umma::mbar_arrive(&sh->tempty[b]);
+        }
+        if (!live) continue;
+#pragma unroll
+        for (int q = 0; q < 32; q += 8) {
+          const int gcol = c0 + cb + q;
+          if (gcol >= out.col_extent) continue;
+          const long long co = (long long)(gcol / out.col_inner) * out.col_os +
+                               (long long)(gcol % out.col_inner);
+          __align__(16) __nv_bfloat16 h[3][8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) split3(v[q + e], h[0][e], h[1][e], h[2][e]);
+#pragma unroll
+          for (int p = 0; p < 3; ++p)
+            *reinterpret_cast<uint4*>(out.plane[p] + ro + co) = *reinterpret_cast<uint4*>(h[p]);
+        }
       }
     }
   }
-  pipe_release(tmem);
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, 512);
 }
 
 __global__ void k_reduce_partials(const float* partial, int ntri, int nchunk, int m, double* S) {
@@ -388,12 +540,19 @@ void split_gemm_planes(const Plane2D& A, const Plane2D& B, int Ktot, const OutMa
     encode_plane_map(&maps.a[p], A.plane[p], A.rows, Ktot, A.pitch);
     encode_plane_map(&maps.b[p], B.plane[p], B.rows, Ktot, B.pitch);
   }
-  ensure_smem(k_split_gemm_tma, SSMEM_BYTES);
-  const int ta = ceil_div(out.rows.extent, TM), tb = ceil_div(out.col_extent, TN);
-  const int a_fast = (ta < tb && tb <= 65535) ? 1 : 0;  // grid.y is limited to 65535
-  if (!a_fast && ta > 65535) throw std::invalid_argument("split GEMM: too many tiles");
-  dim3 grid(a_fast ? ta : tb, a_fast ? tb : ta);
-  k_split_gemm_tma<<<grid, NTHREADS, SSMEM_BYTES, st>>>(maps, out, kmode, Ktot, a_fast, err);
+  ensure_smem(k_split_gemm_persistent, SSMEM_BYTES);
+  PGemmTiles g;
+  g.ta = ceil_div(out.rows.extent, TM);
+  g.tb = ceil_div(out.col_extent, TN);
+  g.a_fast = g.ta < g.tb ? 1 : 0;
+  g.kmode = kmode;
+  g.Ktot = Ktot;
+  g.ntask = (long long)g.ta * g.tb;
+  int dev = 0, sms = 148;
+  SDPX_CUDA(cudaGetDevice(&dev));
+  SDPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const long long grid = std::min<long long>(g.ntask, sms);
+  k_split_gemm_persistent<<<(unsigned)grid, PG_THREADS, SSMEM_BYTES, st>>>(maps, out, g, err);
   SDPX_LAUNCH_CHECK();
 }
 
