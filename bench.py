@@ -446,14 +446,16 @@ def run_ours(args, world, rank, local):
     be.close()
     torch.cuda.synchronize()
     e2e_times, e2e_create = [], []
-    for _ in range(max(1, min(args.steps, 3))):
+    e2e_warmup = 1  # one untimed end-to-end run, as the timed steps above have warm-up
+    for rep in range(e2e_warmup + max(1, min(args.steps, 3))):
         t0 = time.perf_counter()
         with CudaBackend(prob_p, precision="mixed", device=local) as be2:
             t1 = time.perf_counter()
             r_e2e = solve_with_backend(be2, opts_mixed)
         torch.cuda.synchronize()
-        e2e_times.append(time.perf_counter() - t0)
-        e2e_create.append(t1 - t0)
+        if rep >= e2e_warmup:
+            e2e_times.append(time.perf_counter() - t0)
+            e2e_create.append(t1 - t0)
     e2e_s = max_over_ranks(statistics.median(e2e_times), world)
 
     normal = bench_normal(args, world, rank, local, dgemm_tflops)
@@ -528,7 +530,8 @@ def run_ours(args, world, rank, local):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "status": r_e2e.status.value,
-                    "runs_s": e2e_times, "upload_and_allocate_s": e2e_create},
+                    "runs_s": e2e_times, "upload_and_allocate_s": e2e_create,
+                    "warmup": e2e_warmup},
             "gpu_launches": launches,
             "clocks": clock_info,
             "normal_lp_soc": normal,
