@@ -269,6 +269,21 @@ __global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info) {
   const int i = j + 1 + a, q = j + 1 + bq;
   const int c0 = j * NB, r0 = i * NB, q0 = q * NB;
   const int w = min(NB, M.n - c0), h = min(NB, M.n - r0), hq = min(NB, M.n - q0);
+  // Each thread owns an RB×RB block of outputs, RB = NB/16: 256 threads for
+  // NB = 64 (4×4), 48 (3×3) and 32 (2×2).  Its outputs are read together with
+  // the two operand tiles (each output tile belongs to this CTA alone), so the
+  // read-modify-write at the end waits for no memory.
+  constexpr int RB = NB / 16;
+  constexpr int TPR = NB / RB;
+  const int tr = threadIdx.x % TPR, tc = threadIdx.x / TPR;
+  T cur[RB][RB];
+#pragma unroll
+  for (int x = 0; x < RB; ++x)
+#pragma unroll
+    for (int y = 0; y < RB; ++y) {
+      const int r = tr + x * TPR, c = tc + y * TPR;
+      cur[x][y] = (tc < TPR && r < h && c < hq) ? M.a[(size_t)(q0 + c) * M.ld + (r0 + r)] : T(0);
+    }
   {
     // All loads of the two tiles are issued before the shared stores (one
     // memory round trip per tile instead of one per loop trip).
@@ -289,11 +304,6 @@ __global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info) {
     }
   }
   __syncthreads();
-  // Each thread owns an RB×RB block of outputs, RB = NB/16: 256 threads for
-  // NB = 64 (4×4) and NB = 32 (2×2).
-  constexpr int RB = NB / 16;
-  constexpr int TPR = NB / RB;
-  const int tr = threadIdx.x % TPR, tc = threadIdx.x / TPR;
   if (tc < TPR) {
     T acc[RB][RB] = {};
     for (int p = 0; p < w; ++p) {
@@ -312,7 +322,7 @@ __global__ void k_potrf_update(const MatDesc<T>* mats, int j, const int* info) {
 #pragma unroll
       for (int y = 0; y < RB; ++y) {
         int r = tr + x * TPR, c = tc + y * TPR;
-        if (r < h && c < hq) M.a[(size_t)(q0 + c) * M.ld + (r0 + r)] -= acc[x][y];
+        if (r < h && c < hq) M.a[(size_t)(q0 + c) * M.ld + (r0 + r)] = cur[x][y] - acc[x][y];
       }
   }
 }
