@@ -115,12 +115,15 @@ struct Handle {
     adx_ver = 0;
   }
   void dx_written() { ++dx_ver; }
+  bool use_packed = true;  // false when the copy did not fit: passes read 𝒜 itself
   void amul(const double* xv, double* out) {  // out = 𝒜·xv (stacked, symmetric blocks)
+    if (!use_packed) return gemv_n(A.p, K, m, xv, out, gemv_part.p, gemv_chunks, st);
     ensure_packed();
     gemv_n_sym(Ap.p, Kt, m, xv, ap_lo.p, ap_up.p, out, gemv_part.p, gemv_chunks, st);
   }
   // out = alpha·𝒜ᵀz + beta·base; z need not be symmetric (⟨A_i, Z⟩ = ⟨A_i, sym Z⟩).
   void atmul(const double* z, double alpha, const double* base, double beta, double* out) {
+    if (!use_packed) return gemv_t(A.p, K, m, z, alpha, base, beta, out, st);
     ensure_packed();
     fold_sym(Kt, z, ap_lo.p, ap_up.p, kt_fold.p, st);
     gemv_t(Ap.p, Kt, m, kt_fold.p, alpha, base, beta, out, st);
@@ -572,7 +575,14 @@ struct Handle {
         h2d(ap_lo.p, lo.data(), Kt * sizeof(long long));
         h2d(ap_up.p, up.data(), Kt * sizeof(long long));
       }
-      Ap.alloc((size_t)std::max<long long>(Kt, 1) * m);
+      // The copy is an accelerator: it is made only when it fits beside 4 GB of
+      // headroom (the solve's remaining buffers are allocated later).
+      size_t freeb = 0, totb = 0;
+      SDPX_CUDA(cudaMemGetInfo(&freeb, &totb));
+      freeb += dcache::idle_bytes(dev);
+      const size_t apb = sizeof(double) * (size_t)std::max<long long>(Kt, 1) * m;
+      use_packed = apb + (4ull << 30) <= freeb;
+      if (use_packed) Ap.alloc((size_t)std::max<long long>(Kt, 1) * m);
       kt_fold.alloc(std::max<long long>(Kt, 1));
       adx.alloc(K);
       adx.zero(st);
@@ -924,6 +934,8 @@ struct Handle {
       size_t adig = 0, tdig = 0, wdig = 0;
       long long aexp = 0, texp = 0, wexp = 0;
       ozb.clear();
+      bool fits_int = true;  // the digit GEMM indexes k·m rows with 32-bit ints
+      for (auto& b : dense) fits_int = fits_int && (long long)b.k * m < (1LL << 31) - 128;
       for (auto& b : dense) {
         OzBlock o;
         o.kp = oz_kpad(b.k);
@@ -945,7 +957,7 @@ struct Handle {
       freeb += dcache::idle_bytes(dev);  // idle cached blocks are ours to reuse
       const size_t gram = oz_plan.m == m && oz_plan.K == K ? 0 : (size_t)OZ_DIGITS * m * (K + 64);
       const size_t need = adig + tdig + wdig + 4 * (size_t)(aexp + texp + wexp) + gram;
-      if (dense.empty() || need + (2ull << 30) > freeb) {
+      if (dense.empty() || !fits_int || need + (2ull << 30) > freeb) {
         oz_blk_state = -1;
       } else {
         oz_adig.alloc(adig);
