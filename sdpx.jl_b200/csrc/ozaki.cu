@@ -16,8 +16,8 @@
 //
 // Tiles: 128 rows of P columns (A) × 64 (B); the eight level accumulators take
 // all 8·64 = 512 TMEM columns.  128 threads per CTA, one CTA per SM: thread 0
-// issues the TMA boxes (K = 32 bytes per row, 32-byte swizzle, four 48 KB
-// stages), thread 32 issues the 12 MMAs of a stage (M = 128, N ≤ 256, K = 32,
+// issues the TMA boxes (digit pairs (t, t+4): 64 bytes per box row = 32 K
+// positions of two digits, 64-byte swizzle, four 48 KB stages), thread 32 issues the 12 MMAs of a stage (M = 128, N ≤ 256, K = 32,
 // all 36 digit products) and commits them to the stage's "empty" barrier, all
 // four warps convert the int32 levels to FP64 in the epilogue.  Bounded waits with a device error flag;
 // the producer drains its own copies before the CTA exits.  No cluster, no
@@ -41,9 +41,15 @@ namespace {
 constexpr int OM = 128, ON = 64, OK = 32;        // tile rows (A), cols (B), K bytes per stage
 constexpr int ONT = 128;                          // threads
 constexpr int ONST = 4;                           // stages
-constexpr int OA_BYTES = OM * OK;                 // 4 KB per digit tile of A
-constexpr int OB_BYTES = ON * OK;                 // 2 KB per digit tile of B
-constexpr int OSTAGE = OZ_DIGITS * (OA_BYTES + OB_BYTES);  // 48 KB
+// Digit planes are stored in pairs: pair p = t mod 4 holds digits p and p + 4
+// of every value, interleaved in 32-byte chunks along K, so one 64-byte TMA
+// box row carries two digits (half the box rows of one plane per box: the TMA
+// unit issues one request per box row).
+constexpr int OPAIRS = OZ_DIGITS / 2;
+constexpr int OA_BYTES = OM * 2 * OK;             // 8 KB per digit-pair tile of A
+constexpr int OB_BYTES = ON * 2 * OK;             // 4 KB per digit-pair tile of B
+constexpr int OSTAGE = OPAIRS * (OA_BYTES + OB_BYTES);  // 48 KB
+static_assert(OZ_DIGITS == 8, "digit pairs (t, t + 4)");
 constexpr size_t OSMEM = ONST * OSTAGE + 1024 + 256;
 constexpr int OLEVELS = OZ_DIGITS;                // levels 0 … OZ_DIGITS-1
 constexpr int NAN_EXP = INT_MIN;                  // column holds a non-finite value
@@ -74,8 +80,9 @@ __device__ __forceinline__ double round_digit(double x, int& di) {
 }
 
 // ---------------------------------------------------------------- digits --
-// One CTA per column: largest magnitude → exponent, then the digit planes
-// (digit t of column i at digits[t·m·Kp + i·Kp + k], zero for k ≥ K).
+// One CTA per column: largest magnitude → exponent, then the digit planes.
+// Digit t of column i, row k, sits in pair plane t mod 4 (2·m·Kp bytes each) at
+// i·2·Kp + 64·(k div 32) + 32·(t div 4) + (k mod 32); zero for k ≥ K.
 // When dense_hi is given, the rows [0, tail_off) were written by a producer
 // that recorded the largest high word of |P_ki| per column (dense_hi[i]); only
 // the tail rows are scanned here and the exponent follows from the combined
@@ -113,9 +120,9 @@ __global__ void k_oz_digits(const double* __restrict__ P, long long K, long long
   }
   __syncthreads();
   const int e = s_exp;
-  const size_t plane = (size_t)m * Kp;
-  int8_t* dst = digits + (size_t)i * Kp;
-  // Four consecutive rows per thread: one char4 store per digit plane (Kp is a
+  const size_t plane = (size_t)m * Kp;        // bytes per digit; a pair plane is 2·plane
+  int8_t* dst = digits + (size_t)i * 2 * Kp;  // row i of every pair plane
+  // Four consecutive rows per thread: one char4 store per digit (Kp is a
   // multiple of 64).
   for (long long k0 = 4 * (long long)threadIdx.x; k0 < Kp; k0 += 4 * blockDim.x) {
     double r[4];
@@ -129,7 +136,8 @@ __global__ void k_oz_digits(const double* __restrict__ P, long long K, long long
       int d0, d1, d2, d3;
       const double a0 = round_digit(r[0], d0), a1 = round_digit(r[1], d1);
       const double a2 = round_digit(r[2], d2), a3 = round_digit(r[3], d3);
-      *reinterpret_cast<char4*>(dst + (size_t)t * plane + k0) =
+      *reinterpret_cast<char4*>(dst + (size_t)(t & 3) * 2 * plane + (k0 >> 5) * 64 + (t >> 2) * 32 +
+                                (k0 & 31)) =
           make_char4((signed char)d0, (signed char)d1, (signed char)d2, (signed char)d3);
       r[0] = (r[0] - a0) * 128.0;
       r[1] = (r[1] - a1) * 128.0;
@@ -141,25 +149,13 @@ __global__ void k_oz_digits(const double* __restrict__ P, long long K, long long
 
 // ------------------------------------------------------------------ SYRK --
 struct OzMaps {
-  CUtensorMap a[OZ_DIGITS], b[OZ_DIGITS];
+  CUtensorMap a[OPAIRS], b[OPAIRS];
 };
 
 struct OzShared {
   uint64_t full[ONST], empty[ONST], done;
   uint32_t tmem;
 };
-
-// Shared-memory descriptor, K-major 32-byte swizzle (rows of 32 bytes, 8-row
-// atoms of 256 bytes: SBO 256, LBO field 1, layout type 6).
-__device__ __forceinline__ uint64_t smem_desc_sw32(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1 << 16;
-  d |= (uint64_t)(256 >> 4) << 32;
-  d |= (uint64_t)1 << 46;
-  d |= (uint64_t)6 << 61;
-  return d;
-}
 
 // Instruction descriptor, kind::i8: D = S32 (bits 4-5 = 2), A = B = signed 8-bit
 // (bits 7-9, 10-12 = 1), both K-major, N>>3 at bits 17-22, M>>4 at bits 24-28.
@@ -176,24 +172,27 @@ __device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t a, uint64_t b, 
       "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
-// The MMAs of one stage.  Level ℓ = t + u sits in TMEM columns [64ℓ, 64ℓ+64),
-// and the digit tiles of B are contiguous in shared memory (uniform 256-byte
-// swizzle atoms), so for a fixed digit t of A the products with all digits
-// u = 0 … 7-t of B are ONE operand of N = 64·(8-t) rows writing the contiguous
-// columns [64t, 512): 12 MMAs of N ≤ 256 instead of 36 of N = 64, and each A
-// tile is read from shared memory once per MMA instead of once per product.
+// The MMAs of one stage.  Level ℓ = t + u sits in TMEM columns [64ℓ, 64ℓ+64).
+// In shared memory the four pair tiles of B follow each other with uniform
+// 512-byte swizzle atoms (64-byte rows), digit u at pair u mod 4 and byte
+// offset 32·(u div 4) of each row.  So for a fixed digit t of A, the products
+// with the digits u = 0 … min(3, 7-t) are ONE operand of N = 64·(count) rows
+// (pairs 0 …, offset 0) writing the contiguous columns [64t, …), and those with
+// u = 4 … 7-t another (offset 32) writing [64(t+4), …): 12 MMAs of N ≤ 256 for
+// all 36 digit products, each A tile read from shared memory once per MMA.
 // The first stage of a tile writes every level through t = 0 (no accumulate).
 __device__ __forceinline__ void oz_mma_stage(uint32_t tmem, uint32_t base, bool first) {
+  const uint32_t bbase = base + OPAIRS * OA_BYTES;
 #pragma unroll
   for (int ta = 0; ta < OZ_DIGITS; ++ta) {
-    const uint64_t ad = smem_desc_sw32(base + ta * OA_BYTES);
-#pragma unroll
-    for (int c0 = 0; c0 < (OZ_DIGITS - ta) * ON; c0 += 256) {
-      const int n = (OZ_DIGITS - ta) * ON - c0 < 256 ? (OZ_DIGITS - ta) * ON - c0 : 256;
-      const uint64_t bd = smem_desc_sw32(base + OZ_DIGITS * OA_BYTES + (c0 / ON) * OB_BYTES);
-      mma_s8(tmem + (uint32_t)(ta * ON + c0), ad, bd, idesc_s8_s32(OM, n),
-             (first && ta == 0) ? 0u : 1u);
-    }
+    const uint64_t ad = umma::smem_desc_sw64(base + (ta & 3) * OA_BYTES + (ta >> 2) * 32);
+    const uint32_t acc = (first && ta == 0) ? 0u : 1u;
+    const int lo = (OZ_DIGITS - ta) < 4 ? (OZ_DIGITS - ta) : 4;  // u = 0 … lo-1
+    mma_s8(tmem + (uint32_t)(ta * ON), ad, umma::smem_desc_sw64(bbase), idesc_s8_s32(OM, lo * ON),
+           acc);
+    if (OZ_DIGITS - ta > 4)  // u = 4 … 7-ta
+      mma_s8(tmem + (uint32_t)((ta + 4) * ON), ad, umma::smem_desc_sw64(bbase + 32),
+             idesc_s8_s32(OM, (OZ_DIGITS - ta - 4) * ON), acc);
   }
 }
 
@@ -237,9 +236,9 @@ __global__ void __launch_bounds__(ONT, 1)
       const uint32_t base = umma::smem_u32(smem + s * OSTAGE);
       const int k = (int)(kb + (long long)t * OK);
 #pragma unroll
-      for (int d = 0; d < OZ_DIGITS; ++d) {
-        umma::tma_load_2d(base + d * OA_BYTES, &maps.a[d], k, ra, &sh->full[s]);
-        umma::tma_load_2d(base + OZ_DIGITS * OA_BYTES + d * OB_BYTES, &maps.b[d], k, rb,
+      for (int d = 0; d < OPAIRS; ++d) {
+        umma::tma_load_2d(base + d * OA_BYTES, &maps.a[d], 2 * k, ra, &sh->full[s]);
+        umma::tma_load_2d(base + OPAIRS * OA_BYTES + d * OB_BYTES, &maps.b[d], 2 * k, rb,
                           &sh->full[s]);
       }
       ++issued;
@@ -345,7 +344,7 @@ __global__ void k_oz_digits_rows(const OzRowsDev r, long long Kp, long long plan
   if (all_finite && mx > 0.0) frexp(mx, &e);
   if (!all_finite) e = NAN_EXP;
   if (lane == 0) exps[n] = e;
-  int8_t* dst = digits + n * Kp;
+  int8_t* dst = digits + n * 2 * Kp;  // row n of every pair plane (2·plane bytes apart)
   for (long long j0 = 4 * lane; j0 < Kp; j0 += 128) {
     double x[4];
 #pragma unroll
@@ -362,7 +361,8 @@ __global__ void k_oz_digits_rows(const OzRowsDev r, long long Kp, long long plan
       d = round_digit(x[1], di); c.y = (signed char)di; x[1] = (x[1] - d) * 128.0;
       d = round_digit(x[2], di); c.z = (signed char)di; x[2] = (x[2] - d) * 128.0;
       d = round_digit(x[3], di); c.w = (signed char)di; x[3] = (x[3] - d) * 128.0;
-      *reinterpret_cast<char4*>(dst + t * plane + j0) = c;
+      *reinterpret_cast<char4*>(dst + (t & 3) * 2 * plane + (j0 >> 5) * 64 + (t >> 2) * 32 +
+                                (j0 & 31)) = c;
     }
   }
 }
@@ -475,9 +475,9 @@ __global__ void __launch_bounds__(GNT, 1)
           const uint32_t base = umma::smem_u32(smem + s * OSTAGE);
           const int k = kb + t * OK;
 #pragma unroll
-          for (int d = 0; d < OZ_DIGITS; ++d) {
-            umma::tma_load_2d(base + d * OA_BYTES, &maps.a[d], k, mt * OM, &sh->full[s]);
-            umma::tma_load_2d(base + OZ_DIGITS * OA_BYTES + d * OB_BYTES, &maps.b[d], k, nt * ON,
+          for (int d = 0; d < OPAIRS; ++d) {
+            umma::tma_load_2d(base + d * OA_BYTES, &maps.a[d], 2 * k, mt * OM, &sh->full[s]);
+            umma::tma_load_2d(base + OPAIRS * OA_BYTES + d * OB_BYTES, &maps.b[d], 2 * k, nt * ON,
                               &sh->full[s]);
           }
         }
@@ -604,16 +604,19 @@ PFN_cuTensorMapEncodeTiled_v12000 oz_encoder() {
   return fn;
 }
 
-void encode_digit_map(CUtensorMap* map, const int8_t* plane, int rows, long long Kp, int box_rows) {
-  if ((reinterpret_cast<uintptr_t>(plane) & 15) != 0 || Kp % 16 != 0)
-    throw std::invalid_argument("ozaki: digit plane not 16-byte aligned");
-  cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)Kp};
-  cuuint32_t box[2] = {(cuuint32_t)OK, (cuuint32_t)box_rows};
+// TMA map of one digit-pair plane: rows × 2·Kp bytes (row-major), boxes of
+// 64 bytes (32 K positions of two digits) × box_rows, 64-byte swizzle.
+void encode_digit_map(CUtensorMap* map, const int8_t* pair_plane, int rows, long long Kp,
+                      int box_rows) {
+  if ((reinterpret_cast<uintptr_t>(pair_plane) & 15) != 0 || Kp % 32 != 0)
+    throw std::invalid_argument("ozaki: digit plane not 16-byte aligned or Kp not a multiple of 32");
+  cuuint64_t dims[2] = {(cuuint64_t)(2 * Kp), (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(2 * Kp)};
+  cuuint32_t box[2] = {(cuuint32_t)(2 * OK), (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
-  CUresult r = oz_encoder()(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(plane),
+  CUresult r = oz_encoder()(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(pair_plane),
                             dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                            CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
@@ -669,9 +672,9 @@ void ozaki_syrk(const double* P, const OzakiPlan& plan, int8_t* digits, int* exp
                             cudaMemcpyHostToDevice, st));
   OzMaps maps;
   const size_t plane = (size_t)m * plan.Kp;
-  for (int d = 0; d < OZ_DIGITS; ++d) {
-    encode_digit_map(&maps.a[d], digits + d * plane, m, plan.Kp, OM);
-    encode_digit_map(&maps.b[d], digits + d * plane, m, plan.Kp, ON);
+  for (int d = 0; d < OPAIRS; ++d) {
+    encode_digit_map(&maps.a[d], digits + d * 2 * plane, m, plan.Kp, OM);
+    encode_digit_map(&maps.b[d], digits + d * 2 * plane, m, plan.Kp, ON);
   }
   ensure_smem(k_oz_syrk, OSMEM);
   const int units = plan.ntri * plan.nchunk;
@@ -683,12 +686,12 @@ void ozaki_syrk(const double* P, const OzakiPlan& plan, int8_t* digits, int* exp
   SDPX_LAUNCH_CHECK_N(2);
 }
 
-long long oz_kpad(int len) { return std::max<long long>(32, (len + 15LL) / 16 * 16); }
+long long oz_kpad(int len) { return std::max<long long>(32, (len + 31LL) / 32 * 32); }
 
 void ozaki_digits_rows(const OzRows& r, long long Kp, long long plane, int8_t* digits, int* exps,
                        cudaStream_t st) {
   if (r.rows <= 0) return;
-  if (Kp % 16 != 0 || Kp < r.len || plane < r.rows * Kp)
+  if (Kp % 32 != 0 || Kp < r.len || plane < r.rows * Kp)
     throw std::invalid_argument("ozaki: digit rows do not fit the planes");
   OzRowsDev d{r.base, r.rows, r.is, r.os, r.es, r.inner, r.len, r.tri};
   constexpr int WARPS = 8;
@@ -699,11 +702,11 @@ void ozaki_digits_rows(const OzRows& r, long long Kp, long long plane, int8_t* d
 
 void ozaki_gemm(const OzGemm& g, int sm_count, int* err, cudaStream_t st) {
   if (g.rows_a <= 0 || g.rows_b <= 0) return;
-  if (g.Kp % 16 != 0 || g.Kp < OK) throw std::invalid_argument("ozaki: contraction width");
+  if (g.Kp % 32 != 0 || g.Kp < OK) throw std::invalid_argument("ozaki: contraction width");
   OzMaps maps;
-  for (int d = 0; d < OZ_DIGITS; ++d) {
-    encode_digit_map(&maps.a[d], g.xd + d * g.x_plane, g.rows_a, g.Kp, OM);
-    encode_digit_map(&maps.b[d], g.yd + d * g.y_plane, g.rows_b, g.Kp, ON);
+  for (int d = 0; d < OPAIRS; ++d) {
+    encode_digit_map(&maps.a[d], g.xd + d * 2 * g.x_plane, g.rows_a, g.Kp, OM);
+    encode_digit_map(&maps.b[d], g.yd + d * 2 * g.y_plane, g.rows_b, g.Kp, ON);
   }
   OzGemmDev dv;
   dv.ea = g.ea;

@@ -48,17 +48,19 @@ struct OzRows {
   int tri = 0;
 };
 
-// Padded digit-row width for a contraction length (multiple of 16, ≥ 32).
+// Padded digit-row width for a contraction length (multiple of 32, ≥ 32).
 long long oz_kpad(int len);
 
-// Digit planes of the rows: digit t of row n at digits[t·plane + n·Kp + j]
-// (zero for j ≥ len), the row's power-of-two exponent at exps[n].
-// plane ≥ rows·Kp.
+// Digit planes of the rows, stored in pairs (t, t + 4): digit t of row n,
+// position j, at digits[(t mod 4)·2·plane + n·2·Kp + 64·(j div 32) +
+// 32·(t div 4) + (j mod 32)] (zero for j ≥ len), the row's power-of-two
+// exponent at exps[n].  plane ≥ rows·Kp (8·plane bytes in all).
 void ozaki_digits_rows(const OzRows& r, long long Kp, long long plane, int8_t* digits, int* exps,
                        cudaStream_t st);
 
 // out[(a / a_inner)·a_os + (a % a_inner)·a_is + b·b_stride] = Σ_j X[a, j]·Y[b, j]
-// for the digit planes of X (rows_a rows) and Y (rows_b rows), both Kp wide.
+// for the digit planes of X (rows_a rows) and Y (rows_b rows), both Kp wide, in
+// the pair layout of ozaki_digits_rows (x_plane, y_plane: its `plane`).
 // kmode 1: row b of Y is zero beyond j = b, kmode 2: before j = b (the
 // contraction of a tile of Y rows is cut to where they can be nonzero).
 struct OzGemm {
