@@ -11,8 +11,10 @@ kernels of the reference's hot path so that
   * the CUDA backend can be compared kernel-by-kernel (Schur matrix, KKT
     direction, residuals, step lengths) on the same iterate.
 
-Parity pins: the gate problems `sdp_closed_form` and `sdp_dense` and the
-fixed-policy T1 toy problem; see tests/test_oracle_gates.py.
+Parity pins: the gate problems `sdp_closed_form` and `sdp_dense`, the
+fixed-policy T1 toy problem and the equality-row problems T2 (15 ± 2
+iterations) and T3 (rank-deficient, rank-revealing QR) of
+test/correctness.jl; see tests/test_oracle_gates.py.
 
 Every method cites the reference function it follows (paths inside SDPX.jl).
 """
@@ -56,6 +58,16 @@ def kchol(A: np.ndarray) -> Tuple[bool, np.ndarray]:
         return True, np.array([[l11, 0.0], [l21, math.sqrt(d22)]])
     c, info = lapack.dpotrf(A, lower=1, clean=1)
     return info == 0, c
+
+
+def kchol_lapack(A: np.ndarray) -> Tuple[bool, np.ndarray]:
+    """`LinearAlgebra.cholesky!(Symmetric(A, :L); check=false)` (LAPACK potrf,
+    every size) as the standard provider's `la_cholesky_factor!` calls it
+    (src/la_backend.jl:686-698)."""
+    if A.shape[0] == 0:
+        return True, A.copy()
+    c, info = lapack.dpotrf(A, lower=1, clean=1)
+    return info == 0 and bool(np.all(np.isfinite(np.diag(c)))), c
 
 
 def kcholsolve(L: np.ndarray, M: np.ndarray) -> np.ndarray:
@@ -217,6 +229,115 @@ def equilibrate_problem(Av: List[np.ndarray], C: List[np.ndarray], c: np.ndarray
 
 
 # ---------------------------------------------------------------------------
+#   Equality block of the KKT system (src/kkt.jl)
+# ---------------------------------------------------------------------------
+
+QR_MAX_COLUMNS = 2048          # `_equality_qr_allowed`, Float64 (src/kkt.jl:553-576)
+QR_MAX_ELEMENTS = 50_000_000   # `_equality_qr_maximum_elements`, Float64 (src/kkt.jl:540-551)
+
+
+def equality_rank_tau(rows: int, cols: int, requested: float) -> float:
+    """`_equality_cholesky_rank_tau`, Float64 branch (src/kkt.jl:76-112):
+    max(max(rows, cols)·eps, min(√eps, requested accuracy))."""
+    if not requested > 0:
+        requested = SQRT_EPS
+    requested = min(SQRT_EPS, requested)
+    return max(float(max(rows, cols)) * EPS, min(SQRT_EPS, requested))
+
+
+def normalize_equality_columns(Bt: np.ndarray):
+    """`_normalize_equality_panel_columns!` (src/kkt.jl:281-304): column j is
+    multiplied by 1/‖B̃[:, j]‖∞ (zero columns, and reciprocals that overflow,
+    keep scale one).  Returns (B̂, scale)."""
+    n = Bt.shape[1]
+    scale = np.ones(n)
+    out = Bt.copy()
+    for j in range(n):
+        norm = float(np.max(np.abs(Bt[:, j]))) if Bt.shape[0] else 0.0
+        s = 1.0 if norm == 0.0 else 1.0 / norm
+        if not math.isfinite(s):
+            s = 1.0
+        scale[j] = s
+        if s != 1.0:
+            out[:, j] = Bt[:, j] * s
+    return out, scale
+
+
+def has_exact_duplicate_columns(M: np.ndarray) -> bool:
+    """`_has_exact_duplicate_columns` (src/kkt.jl:411-440): two columns equal
+    entry by entry (signed zeros equal, NaN never equal)."""
+    n = M.shape[1]
+    for i in range(n - 1):
+        for j in range(i + 1, n):
+            if np.array_equal(M[:, i], M[:, j]):
+                return True
+    return False
+
+
+def cholesky_has_numerical_rank(Lq: np.ndarray, Bt: np.ndarray, tau: float) -> bool:
+    """`_cholesky_has_numerical_rank` (src/kkt.jl:114-178) on the factor's
+    diagonal: min|L_jj| > τ·max|L_jj|, and in the suspicious band
+    min ≤ √τ·max no two columns of B̂ may be exactly equal."""
+    if Lq.shape[0] == 0:
+        return True
+    d = np.abs(np.diag(Lq))
+    if not np.all(np.isfinite(d)):
+        return False
+    lo, hi = float(d.min()), float(d.max())
+    if not hi > 0:
+        return False
+    if not lo > tau * hi:
+        return False
+    if lo <= math.sqrt(tau) * hi and has_exact_duplicate_columns(Bt):
+        return False
+    return True
+
+
+def equality_qr_allowed(rows: int, cols: int) -> bool:
+    """Dimension gates of `_equality_qr_allowed` (src/kkt.jl:553-576)."""
+    return 0 < cols <= QR_MAX_COLUMNS and rows * cols <= QR_MAX_ELEMENTS
+
+
+def equality_qr(Bt: np.ndarray, tau: float):
+    """`la_qr_factor!(…; pivoted=true)` (src/la_backend.jl:823-850: LAPACK
+    geqp3, column-norm pivoting) and `_equality_qr_factor_handle`
+    (src/la_backend.jl:956-1024): rank = leading count of |R_jj| > τ·max|R_jj|,
+    quality = min/max over those diagonals.  Returns (R, perm, rank, quality)."""
+    R, perm = sla.qr(Bt, mode="r", pivoting=True, check_finite=False)
+    d = np.abs(np.diag(R))
+    largest = float(d.max()) if d.size else 0.0
+    threshold = tau * largest
+    rank, smallest = 0, largest
+    for v in d:
+        if not v > threshold:
+            break
+        rank += 1
+        smallest = min(smallest, float(v))
+    quality = min(max(smallest / largest, 0.0), 1.0) if rank > 0 and largest > 0 else 0.0
+    return R, np.asarray(perm, dtype=np.int64), rank, quality
+
+
+def equality_qr_solve(R: np.ndarray, perm: np.ndarray, rank: int, rhs: np.ndarray) -> np.ndarray:
+    """`la_factor_solve!(::EqualityQRFactor)` (src/la_backend.jl:1425-1455):
+    RᵀR z = rhs[perm] on the leading rank×rank block, dependent directions
+    zero, scattered back through the permutation."""
+    z = np.array(rhs[perm[:rank]], dtype=np.float64)
+    for row in range(rank):
+        v = z[row]
+        for col in range(row):
+            v -= R[col, row] * z[col]
+        z[row] = v / R[row, row]
+    for row in range(rank - 1, -1, -1):
+        v = z[row]
+        for col in range(row + 1, rank):
+            v -= R[row, col] * z[col]
+        z[row] = v / R[row, row]
+    out = np.zeros(rhs.shape[0])
+    out[perm[:rank]] = z
+    return out
+
+
+# ---------------------------------------------------------------------------
 #   Backend: the driver seam (see sdpx_b200.driver)
 # ---------------------------------------------------------------------------
 
@@ -232,9 +353,18 @@ class OracleBackend:
         self.Av = [a.copy() for a in prob.Av]
         self.C = [x.copy() for x in prob.C]
         self.c = prob.c.copy()
+        self.B = np.array(prob.B, dtype=np.float64).reshape(self.m, self.n)
+        self.b = np.array(prob.b, dtype=np.float64).reshape(self.n)
         L = len(self.k)
         self.x = np.zeros(self.m)
-        self.y = np.zeros(0)
+        self.y = np.zeros(self.n)
+        self.p = np.zeros(self.n)          # b − Bᵀx
+        self.dy = np.zeros(self.n)
+        self.rho_p = np.zeros(self.n)      # p − Bᵀdx
+        self.eq = None                     # current equality factor
+        self.eq_qr_sticky = False
+        self.requested_accuracy = SQRT_EPS
+        self.equality_solver = "auto"
         self.X = [np.eye(kl) for kl in self.k]
         self.Y = [np.eye(kl) for kl in self.k]
         self.P = [None] * L
@@ -265,6 +395,14 @@ class OracleBackend:
     def _accumulate(self, l, M):      # src/schur.jl:41-44 (⟨A_i, M⟩ for all i)
         return self.Av[l] @ M.reshape(-1)
 
+    def configure_equality(self, requested_accuracy, solver):
+        """Options the equality factor reads: `_requested_accuracy`
+        (src/kkt.jl:518-521) and `equality_solver` (src/types/workspaces.jl:181)."""
+        if solver not in ("auto", "qr"):
+            raise NotImplementedError(f"equality_solver={solver!r}")
+        self.requested_accuracy = float(requested_accuracy)
+        self.equality_solver = solver
+
     def precision_label(self):
         return "fp64"
 
@@ -282,15 +420,18 @@ class OracleBackend:
         from sdpx_b200.problem import Equilibration
         Av2, C2, cc, E, s, objscale, passes = equilibrate_problem(self.Av, self.C, self.c, self.k)
         self.Av, self.C, self.c = Av2, C2, cc
+        self.B = self.B / s[:, None]       # `_scale_equality_rows!` (src/ingest.jl:1176-1184)
         self.eq_applied = True
         return Equilibration(E, s, objscale, passes)
 
     def data_norms(self):
         maxC = max((float(np.max(np.abs(Cl))) for Cl in self.C), default=0.0)
-        return maxC, float(np.max(np.abs(self.c))) if self.m else 0.0, 0.0
+        bn = float(np.max(np.abs(self.b))) if self.n else 0.0
+        return maxC, float(np.max(np.abs(self.c))) if self.m else 0.0, bn
 
     def fixed_start(self, omega_p, omega_d):
         self.x = np.zeros(self.m)
+        self.y = np.zeros(self.n)
         self.X = [omega_p * np.eye(kl) for kl in self.k]
         self.Y = [omega_d * np.eye(kl) for kl in self.k]
 
@@ -302,8 +443,13 @@ class OracleBackend:
             self.P[l] = P
             self.block_norms[l] = np.max(np.abs(P)) if P.size else 0.0
             d -= self._accumulate(l, self.Y[l])
+        if self.n:
+            d -= self.B @ self.y                      # src/step.jl:41
+            self.p = self.b - self.B.T @ self.x       # src/step.jl:43-45
         self.d = d
         p_res = float(np.max(self.block_norms)) if len(self.k) else 0.0
+        if self.n:
+            p_res = max(p_res, float(np.max(np.abs(self.p))))   # src/step.jl:51
         d_res = float(np.max(np.abs(d))) if d.size else 0.0
         ok = True
         for l in range(len(self.k)):
@@ -358,22 +504,90 @@ class OracleBackend:
             return dict(ok=False, reg_attempts=attempts, quality=0.0)
         dg = np.abs(np.diag(Lf))
         q = float(np.clip(dg.min() / dg.max(), 0, 1)) if dg.max() > 0 and np.isfinite(dg.max()) else 0.0
+        rank_deficient = False
+        if self.n:
+            ok_eq, rank_deficient = self._factor_equality()
+            if not ok_eq:
+                return dict(ok=False, reg_attempts=attempts, quality=0.0)
+            if self.eq[0] == "qr":
+                q = min(q, self.eq[4])       # `_kkt_factorization_quality` (src/step.jl:338-345)
+        if rank_deficient:
+            q = 0.0                          # src/step.jl:797-801
         return dict(ok=True, reg_attempts=attempts, quality=q)
 
-    def _solve(self, rhs):
-        y = sla.solve_triangular(self.Sfac, rhs, lower=True, check_finite=False)
-        return sla.solve_triangular(self.Sfac, y, lower=True, trans="T", check_finite=False)
+    def _factor_equality(self):
+        """Equality part of `_factor_dense_kkt_native!` (src/kkt.jl:1466-1680)
+        for the standard Float64 provider: B̃ = L_S⁻¹B with unit-∞-norm columns,
+        then Q = B̃ᵀB̃ by Cholesky with the rank test, or the column-pivoted QR
+        of B̃ when that test fails (`:standard_compatibility`) or QR was
+        already in use.  Returns (ok, rank_deficient)."""
+        Bt = sla.solve_triangular(self.Sfac, self.B, lower=True, check_finite=False)
+        Bt, scale = normalize_equality_columns(Bt)
+        tau = equality_rank_tau(Bt.shape[0], Bt.shape[1], self.requested_accuracy)
+        direct_qr = self.equality_solver == "qr" or self.eq_qr_sticky
+        self.eq = None
+        if not direct_qr:
+            Q = Bt.T @ Bt
+            ok, Lq = kchol_lapack(Q)
+            if ok and cholesky_has_numerical_rank(Lq, Bt, tau):
+                self.eq = ("chol", Bt, scale, Lq)
+                return True, False
+            if not equality_qr_allowed(*Bt.shape):
+                return False, False
+        R, perm, rank, quality = equality_qr(Bt, tau)
+        self.eq = ("qr", Bt, scale, (R, perm, rank), quality)
+        self.eq_qr_sticky = True
+        return True, rank < self.n
+
+    def _solve_Q(self, rhs):
+        """`_solve_Q!` (src/kkt.jl:2407-2486) for the current equality factor."""
+        if self.eq[0] == "chol":
+            Lq = self.eq[3]
+            z = sla.solve_triangular(Lq, rhs, lower=True, check_finite=False)
+            return sla.solve_triangular(Lq, z, lower=True, trans="T", check_finite=False)
+        R, perm, rank = self.eq[3]
+        return equality_qr_solve(R, perm, rank, rhs)
+
+    def _solve(self, rhs, prhs=None):
+        """`_solve_dense_kkt_owned!` (src/kkt.jl:2570-2595).  Returns (dx, dy)."""
+        rt = sla.solve_triangular(self.Sfac, rhs, lower=True, check_finite=False)
+        if not self.n:
+            return sla.solve_triangular(self.Sfac, rt, lower=True, trans="T",
+                                        check_finite=False), np.zeros(0)
+        _, Bt, scale = self.eq[:3]
+        q = scale * prhs - Bt.T @ rt                 # `_form_scaled_equality_rhs!`
+        dyh = self._solve_Q(q)
+        dx = sla.solve_triangular(self.Sfac, rt + Bt @ dyh, lower=True, trans="T",
+                                  check_finite=False)
+        return dx, dyh * scale                       # `_recover_original_equality_multiplier!`
 
     def solve_direction(self):
-        self.dx = self._solve(self.r)
+        self.dx, self.dy = self._solve(self.r, self.p if self.n else None)
 
     def _schur_mul(self, v):
         return self.schur_matrix() @ v
 
     def direction_residual(self):
-        """`_kkt_direction_residual!` (src/kkt.jl:3689-3708): ρ = r − S·dx."""
+        """`_kkt_direction_residual!` (src/kkt.jl:3689-3708): ρ = r − S·dx + B·dy,
+        ρ_p = p − Bᵀdx.  Returns (max(‖ρ‖∞, ‖ρ_p‖∞), max(‖r‖∞, ‖p‖∞)); the second
+        value is the scale of the acceptance and cold-start gates
+        (src/kkt.jl:3670-3687, src/solver/interior_point.jl:785-789)."""
         self.rho = self.r - self._schur_mul(self.dx)
-        return float(np.max(np.abs(self.rho))), float(np.max(np.abs(self.r)))
+        res = float(np.max(np.abs(self.rho)))
+        rn = float(np.max(np.abs(self.r)))
+        if self.n:
+            self.rho = self.rho + self.B @ self.dy
+            self.rho_p = self.p - self.B.T @ self.dx
+            res = max(float(np.max(np.abs(self.rho))), float(np.max(np.abs(self.rho_p))))
+            rn = max(rn, float(np.max(np.abs(self.p))))
+        return res, rn
+
+    def _correct(self):
+        """`_apply_kkt_correction!` (src/kkt.jl:3762-3780)."""
+        ddx, ddy = self._solve(self.rho, self.rho_p if self.n else None)
+        self.dx = self.dx + ddx
+        if self.n:
+            self.dy = self.dy + ddy
 
     def refine(self, policy, tol, cap, fixed_steps):
         """`_refine_native_direction!` (src/kkt.jl:3891-3963)."""
@@ -381,11 +595,11 @@ class OracleBackend:
             steps = 0
             residual, _ = self.direction_residual()
             for _ in range(fixed_steps):
-                best = self.dx.copy()
-                self.dx = self.dx + self._solve(self.rho)
+                best = (self.dx.copy(), self.dy.copy())
+                self._correct()
                 corrected, _ = self.direction_residual()
                 if not math.isfinite(corrected) or corrected > residual:
-                    self.dx = best
+                    self.dx, self.dy = best
                     break
                 steps += 1
                 residual = corrected
@@ -399,11 +613,11 @@ class OracleBackend:
         for _ in range(cap):
             if residual <= abstol:
                 break
-            best = self.dx.copy()
-            self.dx = self.dx + self._solve(self.rho)
+            best = (self.dx.copy(), self.dy.copy())
+            self._correct()
             corrected, _ = self.direction_residual()
             if not math.isfinite(corrected) or corrected > residual:
-                self.dx = best
+                self.dx, self.dy = best
                 break
             steps += 1
             small = corrected > residual * REFINE_MIN_DECREASE
@@ -535,16 +749,24 @@ class OracleBackend:
             finite = finite and bool(np.all(np.isfinite(self.X[l])) and np.all(np.isfinite(self.Y[l])))
         self.x = self.x + tX * self.dx
         finite = finite and bool(np.all(np.isfinite(self.x)))
+        if self.n:                       # src/solver/interior_point.jl:2228-2229
+            self.y = self.y + tY * self.dy
+            finite = finite and bool(np.all(np.isfinite(self.y)))
         return float(sum(dots)), finite, dots
 
     def accepted_trial_residuals(self, block_primal_residual, tX, tY):
         p_after = abs(1.0 - tX) * block_primal_residual
+        if self.n:                       # p+ = (1 − tX)p + tX·ρ_p
+            self.p = (1.0 - tX) * self.p + tX * self.rho_p
+            p_after = max(p_after, float(np.max(np.abs(self.p))))
         self.d = (1.0 - tY) * self.d - tY * self.rho
         return p_after, float(np.max(np.abs(self.d))) if self.d.size else 0.0
 
     def objectives(self):
         pObj = float(self.c @ self.x)
         dObj = float(sum(np.sum(Cl * Yl) for Cl, Yl in zip(self.C, self.Y)))
+        if self.n:                       # src/kernels/threaded.jl:833
+            dObj += float(self.b @ self.y)
         return pObj, dObj
 
     def solution_residuals(self):
@@ -555,6 +777,9 @@ class OracleBackend:
             P = self._buildP(l, self.x) - self.X[l] - self.C[l]
             p = max(p, float(np.max(np.abs(P))))
             d -= self._accumulate(l, self.Y[l])
+        if self.n:
+            d -= self.B @ self.y
+            p = max(p, float(np.max(np.abs(self.b - self.B.T @ self.x))))
         return p, float(np.max(np.abs(d))) if d.size else 0.0
 
     # -- cold start helpers ----------------------------------------------------
@@ -564,8 +789,10 @@ class OracleBackend:
             for l in range(len(self.k)):
                 r += self._accumulate(l, self.C[l])
             self.r = r
+            self.p = self.b.copy()       # src/solver/interior_point.jl:820
         elif which == "cold_dual":
             self.r = self.c.copy()
+            self.p = np.zeros(self.n)    # src/solver/interior_point.jl:860-861
         else:
             raise ValueError(which)
 
@@ -578,7 +805,7 @@ class OracleBackend:
         self.x = x.copy()
         self.X = [self._buildP(l, x) - self.C[l] for l in range(len(self.k))]
         self.Y = [self._buildP(l, v) for l in range(len(self.k))]
-        self.y = np.zeros(0)
+        self.y = -self.dy                # src/solver/interior_point.jl:920-923
 
     def _psd_stats(self, M):
         low = np.tril(M)
@@ -630,20 +857,34 @@ class OracleBackend:
             self.Y = [factor * Y for Y in self.Y]
 
     def store_best(self):
-        self.best = (self.x.copy(), [X.copy() for X in self.X], [Y.copy() for Y in self.Y])
+        self.best = (self.x.copy(), [X.copy() for X in self.X], [Y.copy() for Y in self.Y],
+                     self.y.copy())
 
     def restore_best(self):
         if self.best is not None:
             self.x, self.X, self.Y = self.best[0].copy(), [X.copy() for X in self.best[1]], \
                 [Y.copy() for Y in self.best[2]]
+            self.y = self.best[3].copy()
 
-    def set_iterate(self, x, X, Y):
+    def set_iterate(self, x, X, Y, y=None):
         self.x = np.array(x, dtype=np.float64)
+        self.y = np.zeros(self.n) if y is None else np.array(y, dtype=np.float64).reshape(self.n)
         self.X = [np.array(M, dtype=np.float64) for M in X]
         self.Y = [np.array(M, dtype=np.float64) for M in Y]
 
     def get_direction(self):
         return self.dx.copy(), [M.copy() for M in self.dX], [M.copy() for M in self.dY]
+
+    def get_equality_direction(self):
+        return self.dy.copy()
+
+    def equality_info(self):
+        """(kind, rank, quality) of the current equality factor."""
+        if self.eq is None:
+            return "none", 0, 0.0
+        if self.eq[0] == "chol":
+            return "normal_equations", self.n, 1.0
+        return "rank_revealing_qr", int(self.eq[3][2]), float(self.eq[4])
 
     def get_rhs(self):
         return self.r.copy()
@@ -661,6 +902,9 @@ class OracleBackend:
     def original_C(self):
         return self.prob0.C
 
+    def original_b(self):
+        return self.prob0.b
+
     def rebuild_slack(self, x):
         p = self.prob0
         return [(x @ p.Av[l]).reshape(p.k[l], p.k[l]) - p.C[l] for l in range(p.L)]
@@ -673,6 +917,10 @@ class OracleBackend:
             P = (x @ p.Av[l]).reshape(p.k[l], p.k[l]) - X[l] - p.C[l]
             pr = max(pr, float(np.max(np.abs(P))))
             d -= p.Av[l] @ Y[l].reshape(-1)
+        if p.n:
+            B = np.asarray(p.B, dtype=np.float64).reshape(p.m, p.n)
+            d -= B @ np.asarray(y, dtype=np.float64)
+            pr = max(pr, float(np.max(np.abs(np.asarray(p.b) - B.T @ np.asarray(x)))))
         return pr, float(np.max(np.abs(d))) if d.size else 0.0
 
 

@@ -58,6 +58,10 @@ class SolverOptions:
     parameter_strategy: str = "adaptive"  # fixed | adaptive
     adaptive_sigma_max: float = 0.0
     scaling: str = "auto"                # auto | none | equilibrate
+    # Equality block of the KKT system (src/types/workspaces.jl:181):
+    # "auto" = normal equations, rank-revealing QR once they lose rank;
+    # "qr" = rank-revealing QR from the first factorization.
+    equality_solver: str = "auto"
     verbosity: int = 0
     # B200 precision mode: "fp64" (plain FP64 device path) or "mixed"
     # (split-BF16 Schur assembly + FP32 factor + FP64 refinement, FP64 switch).

@@ -471,9 +471,12 @@ def solve_with_backend(be, opts: SolverOptions, *, trace=None) -> SDPResult:
     (src/solver/interior_point.jl:3131-3571): Ruiz scaling (plan.scaling ===
     :sdp_ruiz for `scaling=:auto`), the core loop, unscaling, slack rebuild and
     original-coordinate residuals."""
-    if be.n > 0:
-        raise NotImplementedError("equality rows (n > 0) are not supported by the B200 dense core")
     t0 = time.perf_counter()
+    if be.n > 0:
+        # `_requested_accuracy` (src/kkt.jl:518-521) sets the rank tolerance of
+        # the equality factor; `equality_solver` picks its first method.
+        requested = min(opts.eps_gap, opts.eps_primal, opts.eps_dual)
+        be.configure_equality(requested if requested > 0 else SQRT_EPS, opts.equality_solver)
     eq: Optional[Equilibration] = None
     if opts.scaling in ("auto", "equilibrate"):
         eq = be.equilibrate()
@@ -488,6 +491,8 @@ def solve_with_backend(be, opts: SolverOptions, *, trace=None) -> SDPResult:
     X = be.rebuild_slack(x)
     pObj = float(be.original_c() @ x)
     dObj = float(sum(np.sum(Cl * Yl) for Cl, Yl in zip(be.original_C(), Y)))
+    if be.n > 0:
+        dObj += float(np.asarray(be.original_b()) @ np.asarray(y))
     p_res, d_res = be.original_residuals(x, X, y, Y)
     return SDPResult(status=core["status"], message=core["message"], x=x, X=X, y=y, Y=Y,
                      pObj=pObj, dObj=dObj, p_res=p_res, d_res=d_res,

@@ -56,6 +56,34 @@ def toy_t1() -> SDPProblem:
     return ingest([2.0, 3.0], [A], [C])
 
 
+def toy_t2() -> SDPProblem:
+    """T2 of test/correctness.jl:97-106: T1 plus the equality x₁ = 2
+    (B = [1; 0], b = [2]); optimum x₂ = 1/2, p* = 11/2."""
+    t1 = toy_t1()
+    return ingest(t1.c, [t1.Av[0].reshape(2, 2, 2)], t1.C, np.array([[1.0], [0.0]]), [2.0])
+
+
+def toy_t3() -> SDPProblem:
+    """T3 of test/correctness.jl:124-135: the T2 equality row duplicated
+    (B = [1 1; 0 0], b = [2, 2]: n = 2, rank 1)."""
+    t1 = toy_t1()
+    return ingest(t1.c, [t1.Av[0].reshape(2, 2, 2)], t1.C, np.array([[1.0, 1.0], [0.0, 0.0]]),
+                  [2.0, 2.0])
+
+
+def readme_moment_equalities() -> SDPProblem:
+    """The README quick-start moment SDP (README.md:44-75) with its two
+    equality rows kept: variables (W0, W2, W4), maximize W2, i.e.
+    min −W2 s.t. W0 = 1, W0 − W2 − W4 = 0 and [[W0, W2], [W2, W4]] ⪰ 0
+    (C = 0).  Optimum W2 = (√5 − 1)/2."""
+    A = np.zeros((3, 2, 2))
+    A[0, 0, 0] = 1.0
+    A[1, 0, 1] = A[1, 1, 0] = 1.0
+    A[2, 1, 1] = 1.0
+    B = np.array([[1.0, 1.0], [0.0, -1.0], [0.0, -1.0]])
+    return ingest([0.0, -1.0, 0.0], [A], [np.zeros((2, 2))], B, [1.0, 0.0])
+
+
 def readme_moment() -> SDPProblem:
     """The quick-start moment SDP of the reference's README (README.md:44-75):
     maximize W2 s.t. W0 = 1, W0 − W2 − W4 = 0, [[W0, W2], [W2, W4]] ⪰ 0.

@@ -17,4 +17,9 @@ out["compare"] = {"iterations": 1, "objective_rel": 1e-9, "residual_factor": 10.
                   "absolute_floor": 1e-10}       # benchmark/gates.jl:58-77
 out["T1_fixed_policy"] = {"iterations": 19, "iteration_slack": 2,
                           "objective": 4.898979485566356, "objective_abs": 1e-8}
+# T2 / T3 (test/correctness.jl:97-135, T6 pin :T2_Float64 => 15 at :230-233):
+# the equality x1 = 2 (once, then duplicated), optimum 11/2, tolerance 1e-6.
+out["T2_fixed_policy"] = {"iterations": 15, "iteration_slack": 2, "objective": 5.5,
+                          "objective_abs": 1e-6}
+out["T3_fixed_policy"] = {"objective": 5.5, "objective_abs": 1e-6}
 Path(__file__).with_name("gates.json").write_text(json.dumps(out, indent=1, sort_keys=True) + "\n")

@@ -94,3 +94,93 @@ def test_dense_gate_iteration_count_is_summation_order_sensitive():
     assert a.status.value == b.status.value == "Optimal"
     assert abs(a.pObj - b.pObj) / abs(a.pObj) < 1e-10
     assert abs(a.iterations - b.iterations) <= 2
+
+
+# ---- equality rows (n > 0): test/correctness.jl:97-135, T6 pin :230-242 ----
+
+def _fixed():
+    return SolverOptions(parameter_policy="fixed", parameter_strategy="fixed", scaling="none")
+
+
+def _dual_residual(prob, r):
+    import numpy as np
+    d = prob.c.copy()
+    for l in range(prob.L):
+        d -= prob.Av[l] @ r.Y[l].reshape(-1)
+    return float(np.max(np.abs(d - prob.B @ r.y)))
+
+
+def test_t2_equality_fixed_policy():
+    """T2: T1 plus x₁ = 2 — optimum 11/2, 15 ± 2 iterations (T6 pin),
+    Bᵀx = b and the dual residual recomputed here within 1e-6."""
+    import numpy as np
+    pin = GOLD["T2_fixed_policy"]
+    prob = G.toy_t2()
+    r = oracle_solve(prob, _fixed())
+    assert r.status.value == "Optimal"
+    assert abs(r.iterations - pin["iterations"]) <= pin["iteration_slack"]
+    assert abs(r.pObj - pin["objective"]) < pin["objective_abs"]
+    assert float(np.max(np.abs(prob.B.T @ r.x - prob.b))) < 1e-6
+    assert _dual_residual(prob, r) < 1e-6
+    assert np.all(np.isfinite(r.y))
+
+
+def test_t3_duplicated_equality_uses_rank_revealing_qr():
+    """T3: the T2 row duplicated (rank 1).  The normal-equations Cholesky of
+    Q = B̃ᵀB̃ fails, the rank-revealing QR reports rank 1, the dependent
+    multiplier is zero and the optimum is still 11/2."""
+    import numpy as np
+    from sdpx_b200.driver import solve_with_backend
+    from oracle.sdpx_oracle import OracleBackend
+    pin = GOLD["T3_fixed_policy"]
+    prob = G.toy_t3()
+    be = OracleBackend(prob)
+    r = solve_with_backend(be, _fixed())
+    assert r.status.value == "Optimal"
+    assert abs(r.pObj - pin["objective"]) < pin["objective_abs"]
+    assert np.all(np.isfinite(r.x)) and np.all(np.isfinite(r.y))
+    kind, rank, _ = be.equality_info()
+    assert kind == "rank_revealing_qr" and rank == 1
+    assert r.y[1] == 0.0
+
+
+def test_equality_rows_default_options():
+    """T2, T3 and the README moment SDP with its two equality rows, under the
+    default (automatic, equilibrated) options."""
+    for prob, opt in ((G.toy_t2(), 5.5), (G.toy_t3(), 5.5),
+                      (G.readme_moment_equalities(), -(math.sqrt(5) - 1) / 2)):
+        r = oracle_solve(prob, SolverOptions().with_tolerance(1e-8))
+        assert r.status.value == "Optimal"
+        assert abs(r.pObj - opt) < 1e-6
+        assert r.p_res < 1e-6 and r.d_res < 1e-6
+
+
+def test_equality_qr_matches_normal_equations_on_full_rank():
+    """On a full-rank equality block the forced QR route and the
+    normal-equations route solve the same KKT system."""
+    import numpy as np
+    from oracle.sdpx_oracle import OracleBackend
+    prob = G.sdpa_dense(m=24, blocks=[6, 3], lp=2, seed=3)
+    rng = np.random.default_rng(7)
+    B = rng.standard_normal((prob.m, 3))
+    prob = prob.__class__(prob.c, prob.k, prob.Av, prob.C, B, rng.standard_normal(3))
+    out = []
+    for solver in ("auto", "qr"):
+        be = OracleBackend(prob)
+        be.configure_equality(1e-8, solver)
+        x = rng.standard_normal(prob.m) * 0.1 if not out else x0
+        x0 = x
+        X = [np.eye(k) * 2.0 for k in prob.k]
+        Y = [np.eye(k) for k in prob.k]
+        be.set_iterate(x, X, Y, y=np.ones(3) * 0.5)
+        be.compute_residuals([0.1] * prob.L, False, True)
+        be.schur_build()
+        assert be.factorize()["ok"]
+        be.predictor_rhs()
+        be.solve_direction()
+        res, rn = be.direction_residual()
+        assert res <= 1e-10 * max(rn, 1.0)
+        out.append((be.dx.copy(), be.dy.copy(), be.equality_info()[0]))
+    assert out[0][2] == "normal_equations" and out[1][2] == "rank_revealing_qr"
+    assert np.allclose(out[0][0], out[1][0], rtol=1e-9, atol=1e-10)
+    assert np.allclose(out[0][1], out[1][1], rtol=1e-9, atol=1e-10)
