@@ -161,6 +161,39 @@ int sdpx_b200_rebuild_slack(sdpx_b200_handle* h, const double* x, double* X);
 int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const double* X,
                                  const double* Y, double* p_res, double* d_res);
 
+/* ---- Equality rows Bᵀx = b (n > 0) ------------------------------------
+ * SDPX's `SDPProblem.B` (m×n, one column per equality) and `.b`
+ * (src/types/problems.jl) with their multipliers y; the KKT factor and solve
+ * replace the n > 0 branches of `_factor_dense_kkt_native!`
+ * (src/kkt.jl:1466-1680: B̃ = L_S⁻¹B, unit ∞-norm columns, Q = B̃ᵀB̃ by
+ * Cholesky with the rank test, column-pivoted QR of B̃ when it fails) and of
+ * `_solve_dense_kkt_owned!` (src/kkt.jl:2570-2595).  Residuals, refinement,
+ * update, objectives, the cold start and the equilibration carry the B, b, y
+ * terms of src/step.jl:25-72, src/kkt.jl:3689-3708 and
+ * src/solver/interior_point.jl:699-1311 once they are set.  FP64 precision
+ * mode only (sdpx_b200_set_precision refuses the mixed mode while n > 0). */
+
+/* B column-major m×n, b length n; call after create and before
+ * sdpx_b200_equilibrate.  n = 0 removes the equality rows. */
+int sdpx_b200_set_equality(sdpx_b200_handle* h, int32_t n, const double* B, const double* b);
+/* Rank tolerance input min(ϵ_gap, ϵ_primal, ϵ_dual) (`_requested_accuracy`,
+ * src/kkt.jl:518-521) and `equality_solver`: 0 = automatic (normal
+ * equations, rank-revealing QR once they lose rank), 1 = QR from the start. */
+int sdpx_b200_set_equality_options(sdpx_b200_handle* h, double requested_accuracy, int solver);
+/* y, dy and p = b − Bᵀx (p as last updated: residuals, cold-start right-hand
+ * side or accepted-step carry); any pointer may be NULL. */
+int sdpx_b200_get_multipliers(sdpx_b200_handle* h, double* y, double* dy, double* p);
+int sdpx_b200_set_multipliers(sdpx_b200_handle* h, const double* y);
+/* Current equality factor: kind 0 = none, 1 = normal equations (Cholesky of
+ * Q), 2 = rank-revealing QR; its numerical rank and quality (min/max |R_jj|
+ * over the rank for QR, 1 for the normal equations). */
+int sdpx_b200_equality_info(sdpx_b200_handle* h, int* kind, int* rank, double* quality);
+/* sdpx_b200_original_residuals with the equality terms: d −= B·y and
+ * p = b − Bᵀx on the original rows. */
+int sdpx_b200_original_residuals_eq(sdpx_b200_handle* h, const double* x, const double* X,
+                                    const double* y, const double* Y, double* p_res,
+                                    double* d_res);
+
 /* Restore the data as uploaded (undo sdpx_b200_equilibrate) and reset the
  * iterate to x = 0, X = Y = I, so one handle can run repeated solves. */
 int sdpx_b200_reset(sdpx_b200_handle* h);

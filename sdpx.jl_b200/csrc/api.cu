@@ -24,6 +24,7 @@
 #include "certificate.h"
 #include "chol.h"
 #include "dbuf.h"
+#include "equality.h"
 #include "mixed.h"
 #include "ozaki.h"
 #include "schur_bf16.h"
@@ -115,6 +116,11 @@ struct Handle {
     adx_ver = 0;
   }
   void dx_written() { ++dx_ver; }
+  void restore_dx_best() {  // the last accepted direction (dx, and dy with equality rows)
+    d2d(dx.p, dxbest.p, m * sizeof(double));
+    if (n_eq) d2d(dyv.p, dybest.p, n_eq * sizeof(double));
+    dx_written();
+  }
   bool use_packed = true;  // false when the copy did not fit: passes read 𝒜 itself
   void amul(const double* xv, double* out) {  // out = 𝒜·xv (stacked, symmetric blocks)
     if (!use_packed) return gemv_n(A.p, K, m, xv, out, gemv_part.p, gemv_chunks, st);
@@ -743,6 +749,14 @@ struct Handle {
     for (int i = 0; i < m; ++i) ch[i] /= osc;
     h2d(work_m.p, s.data(), m * sizeof(double));
     scale_cols(A.p, K, m, work_m.p, st);
+    if (n_eq) {  // `_scale_equality_rows!` (src/ingest.jl:1176-1184); b is unchanged
+      if (!eq_have_original) {
+        Beq0.alloc((size_t)m * n_eq);
+        d2d(Beq0.p, Beq.p, sizeof(double) * m * n_eq);
+        eq_have_original = true;
+      }
+      eq_scale_rows(m, n_eq, Beq.p, work_m.p, st);
+    }
     h2d(c.p, ch.data(), m * sizeof(double));
     sync();
     if (E_out) {
@@ -771,6 +785,9 @@ struct Handle {
       d2d(Cst.p, C0st.p, sizeof(double) * K);
       d2d(c.p, c0.p, sizeof(double) * m);
     }
+    if (eq_have_original) d2d(Beq.p, Beq0.p, sizeof(double) * m * n_eq);
+    eq_kind = 0;
+    eq_qr_sticky = false;
     precision = SDPX_B200_FP64;
     fixed_start(1.0, 1.0);
     sync();
@@ -808,6 +825,7 @@ struct Handle {
   }
   void fixed_start(double wp, double wd) {
     x.zero(st);
+    if (n_eq) yv.zero(st);
     X.zero(st);
     Y.zero(st);
     if (!dense.empty()) {
@@ -894,7 +912,14 @@ struct Handle {
     axpbypcz(K, 1.0, tmpK.p, -1.0, X.p, -1.0, Cst.p, P.p, st);
     // d = c − 𝒜ᵀ vec(Y)
     atmul(Y.p, -1.0, c.p, 1.0, d.p);
-    clear_red(0, 2);
+    clear_red(0, 3);
+    if (n_eq) {
+      // d −= B·y, p = b − Bᵀx (src/step.jl:41-51)
+      gemv_n(Beq.p, m, n_eq, yv.p, eq_tm.p, gemv_part.p, gemv_chunks, st);
+      axpbypcz(m, 1.0, d.p, -1.0, eq_tm.p, 0.0, nullptr, d.p, st);
+      gemv_t(Beq.p, m, n_eq, x.p, -1.0, beq.p, 1.0, pv.p, st);
+      absmax(n_eq, pv.p, red.p + 2, st);
+    }
     absmax(K, P.p, red.p + 0, st);
     absmax(m, d.p, red.p + 1, st);
     // R = −XY (+ μ I)
@@ -909,9 +934,9 @@ struct Handle {
       add_diag(d_doff.p, d_dk.p, (int)dense.size(), kmax, R.p, work_L.p, 0.0, st);
     }
     diag_residual_R(nd, od, X.p, Y.p, mu_user.p, d_diag_user.p, use_affine, R.p, st);
-    d2h(h_red, red.p, 2 * sizeof(double));
+    d2h(h_red, red.p, 3 * sizeof(double));
     sync();
-    *p_res = h_red[0];
+    *p_res = std::max(h_red[0], h_red[2]);
     *d_res = h_red[1];
     last_bpr = h_red[0];
     *ok = 1;
@@ -1184,6 +1209,17 @@ struct Handle {
         tmp_mm.alloc((size_t)m * m);
       }
       trinv_recursive_f64(Sf.p, m, Linv.p, Dinv.p, tmp_mm.p, st);
+      if (n_eq) {
+        bool rank_deficient = false;
+        if (!factor_equality(&rank_deficient)) {
+          *ok = 0;
+          *quality = 0.0;
+          return;
+        }
+        // `_kkt_factorization_quality` (src/step.jl:338-345, 797-801)
+        if (eq_kind == 2) *quality = std::min(*quality, eq_quality);
+        if (rank_deficient) *quality = 0.0;
+      }
     }
   }
 
@@ -1199,7 +1235,7 @@ struct Handle {
   void solve() {
     PhaseScope ps(this, 3);
     d2d(dx.p, r.p, m * sizeof(double));
-    solve_into(dx.p);
+    solve_kkt_into(dx.p, pv.p, dyv.p);
     dx_written();
     if (precision == SDPX_B200_MIXED && mixed) mixed_guard();
   }
@@ -1267,36 +1303,47 @@ struct Handle {
       return;
     }
     symv_full(m, S.p, dx.p, -1.0, r.p, 1.0, rho.p, st);
+    if (n_eq) eq_residual_terms();
   }
   void direction_residual(double* res, double* rnorm, bool allow_cache = true) {
     PhaseScope ps(this, 3);
     double cached = 0.0;
     const bool hit = allow_cache && take_rho_cache(&cached);
     if (!hit) apply_residual();
-    clear_red(0, 2);
+    clear_red(0, 4);
     if (!hit) absmax(m, rho.p, red.p + 0, st);
     absmax(m, r.p, red.p + 1, st);
-    d2h(h_red, red.p, 2 * sizeof(double));
+    if (n_eq) {  // ρ_p and p enter the residual and the gate scale (src/kkt.jl:3670-3708)
+      if (!hit) absmax(n_eq, rho_p.p, red.p + 2, st);
+      absmax(n_eq, pv.p, red.p + 3, st);
+    }
+    d2h(h_red, red.p, 4 * sizeof(double));
     sync();
-    *res = hit ? cached : h_red[0];
-    *rnorm = h_red[1];
+    *res = hit ? cached : std::max(h_red[0], h_red[2]);
+    *rnorm = std::max(h_red[1], h_red[3]);
     mark_rho_fresh(*res);
   }
   double residual_norm_only(bool allow_cache = false) {
     double cached = 0.0;
     if (allow_cache && take_rho_cache(&cached)) return cached;
     apply_residual();
-    clear_red(0, 1);
+    clear_red(0, 2);
     absmax(m, rho.p, red.p, st);
-    return read_red(0);
+    if (!n_eq) return read_red(0);
+    absmax(n_eq, rho_p.p, red.p + 1, st);
+    d2h(h_red, red.p, 2 * sizeof(double));
+    sync();
+    return std::max(h_red[0], h_red[1]);
   }
   void refine(int policy, double tol, int cap, int fixed_steps, int* steps_out, double* res_out) {
     PhaseScope ps(this, 3);
-    auto correction = [&]() {
+    auto correction = [&]() {  // `_apply_kkt_correction!` (src/kkt.jl:3762-3780)
       d2d(dxbest.p, dx.p, m * sizeof(double));
+      if (n_eq) d2d(dybest.p, dyv.p, n_eq * sizeof(double));
       d2d(work_m.p, rho.p, m * sizeof(double));
-      solve_into(work_m.p);
+      solve_kkt_into(work_m.p, rho_p.p, eq_ddy.p);
       combine(m, dx.p, 1.0, work_m.p, st);
+      if (n_eq) combine(n_eq, dyv.p, 1.0, eq_ddy.p, st);
       dx_written();
     };
     int steps = 0;
@@ -1314,8 +1361,7 @@ struct Handle {
         correction();
         double corr = residual_norm_only();
         if (!std::isfinite(corr) || corr >= residual) {
-          d2d(dx.p, dxbest.p, m * sizeof(double));
-          dx_written();
+          restore_dx_best();
           consistent = false;
           break;
         }
@@ -1334,8 +1380,7 @@ struct Handle {
         correction();
         double corr = residual_norm_only();
         if (!std::isfinite(corr) || corr > residual) {
-          d2d(dx.p, dxbest.p, m * sizeof(double));
-          dx_written();
+          restore_dx_best();
           consistent = false;
           break;
         }
@@ -1359,8 +1404,7 @@ struct Handle {
         correction();
         double corr = residual_norm_only();
         if (!std::isfinite(corr) || corr > residual) {
-          d2d(dx.p, dxbest.p, m * sizeof(double));
-          dx_written();
+          restore_dx_best();
           consistent = false;
           break;
         }
@@ -1440,6 +1484,12 @@ struct Handle {
   void set_rhs(int which) {
     if (which == 0) atmul(Cst.p, 1.0, nullptr, 0.0, r.p);
     else d2d(r.p, c.p, m * sizeof(double));
+    // equality right-hand side: b for the primal solve, 0 for the dual one
+    // (src/solver/interior_point.jl:817-861)
+    if (n_eq) {
+      if (which == 0) d2d(pv.p, beq.p, n_eq * sizeof(double));
+      else pv.zero(st);
+    }
   }
 
   // ---------------------------------------------------------- directions --
@@ -1858,28 +1908,38 @@ struct Handle {
     combine(K, X.p, tX, dX.p, st);
     combine(K, Y.p, tY, dY.p, st);
     combine(m, x.p, tX, dx.p, st);
+    if (n_eq) combine(n_eq, yv.p, tY, dyv.p, st);  // src/solver/interior_point.jl:2228-2229
     std::vector<double> dots(L);
     seg_dot(d_uoff.p, d_ulen.p, L, seg_parts, X.p, nullptr, 0.0, Y.p, nullptr, 0.0, seg_part.p,
             work_L.p, st);
     d2h(dots.data(), work_L.p, L * sizeof(double));
-    clear_red(0, 3);
+    clear_red(0, 4);
     absmax(K, X.p, red.p + 0, st);
     absmax(K, Y.p, red.p + 1, st);
     absmax(m, x.p, red.p + 2, st);
-    d2h(h_red, red.p, 3 * sizeof(double));
+    if (n_eq) absmax(n_eq, yv.p, red.p + 3, st);
+    d2h(h_red, red.p, 4 * sizeof(double));
     sync();
     double s = 0;
     for (int l = 0; l < L; ++l) s += dots[l];
     *compl_total = s;
-    *finite = std::isfinite(h_red[0]) && std::isfinite(h_red[1]) && std::isfinite(h_red[2]);
+    *finite = std::isfinite(h_red[0]) && std::isfinite(h_red[1]) && std::isfinite(h_red[2]) &&
+              std::isfinite(h_red[3]);
     if (block_dots) std::memcpy(block_dots, dots.data(), L * sizeof(double));
   }
   void accepted_residuals(double bpr, double tX, double tY, double* pa, double* da) {
     *pa = std::fabs(1.0 - tX) * bpr;
     axpbypcz(m, 1.0 - tY, d.p, -tY, rho.p, 0.0, nullptr, d.p, st);
-    clear_red(0, 1);
+    clear_red(0, 2);
     absmax(m, d.p, red.p, st);
-    *da = read_red(0);
+    if (n_eq) {  // p+ = (1 − tX)p + tX·ρ_p (src/solver/interior_point.jl:1298-1305)
+      axpbypcz(n_eq, tX, rho_p.p, 1.0 - tX, pv.p, 0.0, nullptr, pv.p, st);
+      absmax(n_eq, pv.p, red.p + 1, st);
+    }
+    d2h(h_red, red.p, 2 * sizeof(double));
+    sync();
+    *da = h_red[0];
+    if (n_eq) *pa = std::max(*pa, h_red[1]);
   }
   void objectives(double* po, double* dobj) {
     std::vector<double> dots(2);
@@ -1896,6 +1956,10 @@ struct Handle {
     for (int i = 0; i < m; ++i) p += hc[i] * hx[i];
     double dd = 0;
     for (int l = 0; l < L; ++l) dd += cy[l];
+    if (n_eq) {  // + bᵀy (src/kernels/threaded.jl:833)
+      eq_dot(n_eq, beq.p, yv.p, red.p, st);
+      dd += read_red(0);
+    }
     *po = p;
     *dobj = dd;
   }
@@ -1903,12 +1967,18 @@ struct Handle {
     amul(x.p, tmpK.p);
     axpbypcz(K, 1.0, tmpK.p, -1.0, X.p, -1.0, Cst.p, tmpK2.p, st);
     atmul(Y.p, -1.0, c.p, 1.0, work_m.p);
-    clear_red(0, 2);
+    clear_red(0, 3);
+    if (n_eq) {
+      gemv_n(Beq.p, m, n_eq, yv.p, eq_tm.p, gemv_part.p, gemv_chunks, st);
+      axpbypcz(m, 1.0, work_m.p, -1.0, eq_tm.p, 0.0, nullptr, work_m.p, st);
+      gemv_t(Beq.p, m, n_eq, x.p, -1.0, beq.p, 1.0, eq_q.p, st);
+      absmax(n_eq, eq_q.p, red.p + 2, st);
+    }
     absmax(K, tmpK2.p, red.p + 0, st);
     absmax(m, work_m.p, red.p + 1, st);
-    d2h(h_red, red.p, 2 * sizeof(double));
+    d2h(h_red, red.p, 3 * sizeof(double));
     sync();
-    *pr = h_red[0];
+    *pr = std::max(h_red[0], h_red[2]);
     *dr = h_red[1];
   }
 
@@ -1918,6 +1988,7 @@ struct Handle {
     amul(x.p, tmpK.p);
     axpbypcz(K, 1.0, tmpK.p, -1.0, Cst.p, 0.0, nullptr, X.p, st);
     amul(dx.p, Y.p);
+    if (n_eq) axpbypcz(n_eq, -1.0, dyv.p, 0.0, nullptr, 0.0, nullptr, yv.p, st);  // y = −q
   }
   // Per-block certified shift (src/cold_start.jl:287-308) for all blocks at once.
   void psd_shift(int which, int* ok_out) {
@@ -2052,7 +2123,7 @@ struct Handle {
     get_stacked(tmpK2.p, hX);
   }
   void original_residuals(const double* hx, const double* hX, const double* hY, double* pr,
-                          double* dr) {
+                          double* dr, const double* hy = nullptr) {
     const double* Ause = have_original ? A0.p : A.p;
     const double* Cuse = have_original ? C0st.p : Cst.p;
     const double* cuse = have_original ? c0.p : c.p;
@@ -2065,12 +2136,21 @@ struct Handle {
     gemv_n(Ause, K, m, work_m.p, tmpK2.p, gemv_part.p, gemv_chunks, st);
     axpbypcz(K, 1.0, tmpK2.p, -1.0, T1.p, -1.0, Cuse, tmpK2.p, st);
     gemv_t(Ause, K, m, T2.p, -1.0, cuse, 1.0, work_m2.p, st);
-    clear_red(0, 2);
+    clear_red(0, 3);
+    if (n_eq) {  // d −= B·y, p = b − Bᵀx on the original equality rows
+      if (!hy) throw std::invalid_argument("equality multipliers y are required when n > 0");
+      const double* Buse = eq_have_original ? Beq0.p : Beq.p;
+      h2d(eq_z.p, hy, n_eq * sizeof(double));
+      gemv_n(Buse, m, n_eq, eq_z.p, eq_tm.p, gemv_part.p, gemv_chunks, st);
+      axpbypcz(m, 1.0, work_m2.p, -1.0, eq_tm.p, 0.0, nullptr, work_m2.p, st);
+      gemv_t(Buse, m, n_eq, work_m.p, -1.0, beq.p, 1.0, eq_q.p, st);
+      absmax(n_eq, eq_q.p, red.p + 2, st);
+    }
     absmax(K, tmpK2.p, red.p + 0, st);
     absmax(m, work_m2.p, red.p + 1, st);
-    d2h(h_red, red.p, 2 * sizeof(double));
+    d2h(h_red, red.p, 3 * sizeof(double));
     sync();
-    *pr = h_red[0];
+    *pr = std::max(h_red[0], h_red[2]);
     *dr = h_red[1];
   }
 
@@ -2333,12 +2413,39 @@ struct Handle {
   void mixed_factorize(int* ok, int* attempts, double* quality);
   void mixed_solve(double* vec);
   void mixed_residual();
+
+  // ------------------------------------------- equality rows (n > 0) ------
+  // Bᵀx = b with B m×n column-major (SDPX's `SDPProblem.B`, `.b`), multipliers
+  // y.  p = b − Bᵀx, ρ_p = p − Bᵀdx.  The equality factor is either the
+  // Cholesky of Q = B̂ᵀB̂ (eq_kind 1) or the column-pivoted QR of B̂ (eq_kind
+  // 2, kept for the rest of the solve once used), B̂ = L_S⁻¹B·D with D the
+  // column scales.  FP64 precision only.
+  int n_eq = 0;
+  DBuf<double> Beq, Beq0, beq;
+  DBuf<double> yv, dyv, pv, rho_p, ybest, dybest, eq_dyh, eq_ddy, eq_q, eq_z, eq_tm;
+  DBuf<double> Bt, Qf, Bqr, eq_scale, eq_rdiag, eq_colnorm, eq_partial;
+  DBuf<int> eq_perm, eq_pairs, eq_equal;
+  DBuf<unsigned long long> eq_fp;
+  SyrkPlan eq_syrk;
+  bool eq_have_original = false;
+  double eq_requested = kSqrtEps;
+  int eq_solver = 0;  // 0 = automatic, 1 = rank-revealing QR from the start
+  int eq_kind = 0;    // 0 = none, 1 = normal equations, 2 = rank-revealing QR
+  int eq_rank = 0;
+  double eq_quality = 0.0;
+  bool eq_qr_sticky = false;
+  void set_equality(int n, const double* hB, const double* hb);
+  bool factor_equality(bool* rank_deficient);
+  void solve_kkt_into(double* vec, const double* prhs, double* dy_out);
+  void eq_residual_terms();
 };
 
 }  // namespace sdpx
 
-// Mixed-precision members live in mixed_api.inc (same translation unit).
+// Mixed-precision members live in mixed_api.inc, the equality block's in
+// equality_api.inc (same translation unit).
 #include "mixed_api.inc"
+#include "equality_api.inc"
 
 // ============================================================================
 //                                   C ABI
@@ -2398,6 +2505,8 @@ const char* sdpx_b200_last_error(const sdpx_b200_handle* h) { return h ? h->h.er
 int sdpx_b200_set_precision(sdpx_b200_handle* h, int mode) {
   GUARD(h, {
     if (mode != SDPX_B200_FP64 && mode != SDPX_B200_MIXED) throw std::invalid_argument("bad precision mode");
+    if (mode == SDPX_B200_MIXED && h->h.n_eq > 0)
+      throw std::invalid_argument("the mixed precision mode needs n == 0 equality rows");
     h->h.precision = mode;
     if (mode == SDPX_B200_MIXED) h->h.mixed_init();
   });
@@ -2531,6 +2640,7 @@ int sdpx_b200_store_best(sdpx_b200_handle* h) {
     H.d2d(H.xbest.p, H.x.p, H.m * sizeof(double));
     H.d2d(H.Xbest.p, H.X.p, H.K * sizeof(double));
     H.d2d(H.Ybest.p, H.Y.p, H.K * sizeof(double));
+    if (H.n_eq) H.d2d(H.ybest.p, H.yv.p, H.n_eq * sizeof(double));
   });
 }
 int sdpx_b200_restore_best(sdpx_b200_handle* h) {
@@ -2539,6 +2649,7 @@ int sdpx_b200_restore_best(sdpx_b200_handle* h) {
     H.d2d(H.x.p, H.xbest.p, H.m * sizeof(double));
     H.d2d(H.X.p, H.Xbest.p, H.K * sizeof(double));
     H.d2d(H.Y.p, H.Ybest.p, H.K * sizeof(double));
+    if (H.n_eq) H.d2d(H.yv.p, H.ybest.p, H.n_eq * sizeof(double));
     H.sync();
   });
 }
@@ -2556,6 +2667,48 @@ int sdpx_b200_certificate(sdpx_b200_handle* h, const double* x, const double* X,
 int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const double* X,
                                  const double* Y, double* p, double* d) {
   GUARD(h, h->h.original_residuals(x, X, Y, p, d));
+}
+int sdpx_b200_original_residuals_eq(sdpx_b200_handle* h, const double* x, const double* X,
+                                    const double* y, const double* Y, double* p, double* d) {
+  GUARD(h, h->h.original_residuals(x, X, Y, p, d, y));
+}
+int sdpx_b200_set_equality(sdpx_b200_handle* h, int32_t n, const double* B, const double* b) {
+  GUARD(h, h->h.set_equality(n, B, b));
+}
+int sdpx_b200_set_equality_options(sdpx_b200_handle* h, double requested_accuracy, int solver) {
+  GUARD(h, {
+    if (solver != 0 && solver != 1) throw std::invalid_argument("bad equality solver");
+    h->h.eq_requested = requested_accuracy;
+    h->h.eq_solver = solver;
+  });
+}
+int sdpx_b200_get_multipliers(sdpx_b200_handle* h, double* y, double* dy, double* p) {
+  GUARD(h, {
+    auto& H = h->h;
+    const size_t bytes = (size_t)H.n_eq * sizeof(double);
+    if (H.n_eq) {
+      if (y) H.d2h(y, H.yv.p, bytes);
+      if (dy) H.d2h(dy, H.dyv.p, bytes);
+      if (p) H.d2h(p, H.pv.p, bytes);
+      H.sync();
+    }
+  });
+}
+int sdpx_b200_set_multipliers(sdpx_b200_handle* h, const double* y) {
+  GUARD(h, {
+    auto& H = h->h;
+    if (H.n_eq && y) {
+      H.h2d(H.yv.p, y, (size_t)H.n_eq * sizeof(double));
+      H.sync();
+    }
+  });
+}
+int sdpx_b200_equality_info(sdpx_b200_handle* h, int* kind, int* rank, double* quality) {
+  GUARD(h, {
+    if (kind) *kind = h->h.eq_kind;
+    if (rank) *rank = h->h.eq_rank;
+    if (quality) *quality = h->h.eq_quality;
+  });
 }
 int sdpx_b200_reset(sdpx_b200_handle* h) { GUARD(h, h->h.reset()); }
 int sdpx_b200_get_precision(sdpx_b200_handle* h, int* mode, int* fallbacks, double* cond_estimate) {

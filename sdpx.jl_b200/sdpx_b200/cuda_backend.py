@@ -101,6 +101,12 @@ _SIGS = {
     "sdpx_b200_get_precision": [C.c_void_p, _ip, _ip, _dp],
     "sdpx_b200_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
     "sdpx_b200_launch_count": [C.POINTER(C.c_uint64)],
+    "sdpx_b200_set_equality": [C.c_void_p, C.c_int32, _dp, _dp],
+    "sdpx_b200_set_equality_options": [C.c_void_p, C.c_double, C.c_int],
+    "sdpx_b200_get_multipliers": [C.c_void_p, _dp, _dp, _dp],
+    "sdpx_b200_set_multipliers": [C.c_void_p, _dp],
+    "sdpx_b200_equality_info": [C.c_void_p, _ip, _ip, _dp],
+    "sdpx_b200_original_residuals_eq": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp],
 }
 
 _lib = None
@@ -173,6 +179,14 @@ class CudaBackend:
                                 self.lib.sdpx_b200_create_error().decode())
         self._keep = []     # host data has been copied to the device
         self.h = h
+        if self.n > 0:
+            # Equality rows (SDPX `SDPProblem.B`, `.b`): FP64 precision mode only.
+            if precision == "mixed":
+                self.close()
+                raise NotImplementedError("the mixed precision mode needs n == 0 equality rows")
+            Bm = np.asfortranarray(np.asarray(prob.B, dtype=np.float64).reshape(self.m, self.n))
+            bv = np.ascontiguousarray(prob.b, dtype=np.float64)
+            self._call("sdpx_b200_set_equality", self.n, _p(Bm), _p(bv))
         self.requested = precision
         self.condition_limit = condition_limit
         self.mode = "fp64"
@@ -267,22 +281,49 @@ class CudaBackend:
     def data_norms(self):
         a, b = C.c_double(), C.c_double()
         self._call("sdpx_b200_data_norms", C.byref(a), C.byref(b))
-        return a.value, b.value, 0.0
+        bn = float(np.max(np.abs(self.prob0.b))) if self.n else 0.0
+        return a.value, b.value, bn
+
+    def configure_equality(self, requested_accuracy, solver):
+        """Rank tolerance input and `equality_solver` of the equality factor."""
+        if solver not in ("auto", "qr"):
+            raise NotImplementedError(f"equality_solver={solver!r}")
+        self._call("sdpx_b200_set_equality_options", float(requested_accuracy),
+                   0 if solver == "auto" else 1)
+
+    def equality_info(self):
+        """(kind, rank, quality) of the current equality factor."""
+        kind, rank, q = C.c_int(), C.c_int(), C.c_double()
+        self._call("sdpx_b200_equality_info", C.byref(kind), C.byref(rank), C.byref(q))
+        return (("none", "normal_equations", "rank_revealing_qr")[kind.value], rank.value,
+                q.value)
+
+    def get_equality_direction(self):
+        dy = np.zeros(self.n)
+        if self.n:
+            self._call("sdpx_b200_get_multipliers", None, _p(dy), None)
+        return dy
 
     def fixed_start(self, omega_p, omega_d):
         self._call("sdpx_b200_fixed_start", omega_p, omega_d)
 
-    def set_iterate(self, x, X, Y):
+    def set_iterate(self, x, X, Y, y=None):
         x = np.ascontiguousarray(x, dtype=np.float64)
         Xs, Ys = self._join(X), self._join(Y)
         self._call("sdpx_b200_set_iterate", _p(x), _p(Xs), _p(Ys))
+        if self.n:
+            yv = np.zeros(self.n) if y is None else np.ascontiguousarray(y, dtype=np.float64)
+            self._call("sdpx_b200_set_multipliers", _p(yv))
 
     def get_iterate(self):
         x = np.zeros(self.m)
         Xs = np.zeros(self.Ku)
         Ys = np.zeros(self.Ku)
         self._call("sdpx_b200_get_iterate", _p(x), _p(Xs), _p(Ys))
-        return x, self._split(Xs), np.zeros(0), self._split(Ys)
+        y = np.zeros(self.n)
+        if self.n:
+            self._call("sdpx_b200_get_multipliers", _p(y), None, None)
+        return x, self._split(Xs), y, self._split(Ys)
 
     def get_direction(self):
         dx = np.zeros(self.m)
@@ -452,6 +493,9 @@ class CudaBackend:
     def original_C(self):
         return self.prob0.C
 
+    def original_b(self):
+        return self.prob0.b
+
     def rebuild_slack(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
         Xs = np.zeros(self.Ku)
@@ -462,13 +506,21 @@ class CudaBackend:
         x = np.ascontiguousarray(x, dtype=np.float64)
         Xs, Ys = self._join(X), self._join(Y)
         a, b = C.c_double(), C.c_double()
-        self._call("sdpx_b200_original_residuals", _p(x), _p(Xs), _p(Ys), C.byref(a), C.byref(b))
+        if self.n:
+            yv = np.ascontiguousarray(y, dtype=np.float64)
+            self._call("sdpx_b200_original_residuals_eq", _p(x), _p(Xs), _p(yv), _p(Ys),
+                       C.byref(a), C.byref(b))
+        else:
+            self._call("sdpx_b200_original_residuals", _p(x), _p(Xs), _p(Ys), C.byref(a),
+                       C.byref(b))
         return a.value, b.value
 
     def certificate(self, x, X, Y, eps_primal=1e-10, eps_dual=1e-10, eps_gap=1e-10,
                     legacy_gap=False) -> dict:
         """Cold-path certificate of (x, X, Y) against the original data
         (`result_certificate`, src/validation.jl:948-1115)."""
+        if self.n:
+            raise NotImplementedError("the device certificate covers problems without equality rows")
         x = np.ascontiguousarray(x, dtype=np.float64)
         Xs, Ys = self._join(X), self._join(Y)
         out = CertificateResult()

@@ -16,7 +16,7 @@ SDPA's Z and SDPX's dual Y is SDPA's X; objectives change sign.
 """
 from __future__ import annotations
 
-from typing import List, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -127,6 +127,28 @@ def gate_dense(variables: int = 180, side: int = 8, blocks: int = 3, seed: int =
 
 def sdpa_dense(m: int, blocks: Sequence[int], lp: int = 0, seed: int = 0,
                dtype=np.float64) -> SDPProblem:
+    """Strictly feasible dense SDP in SDPX core form (construction below)."""
+    return _sdpa_dense(m, blocks, lp, seed)[0]
+
+
+def sdpa_dense_equalities(m: int, blocks: Sequence[int], lp: int = 0, n_eq: int = 1,
+                          seed: int = 0, rank: Optional[int] = None) -> SDPProblem:
+    """`sdpa_dense` plus `n_eq` equality rows Bᵀx = b that keep its strictly
+    feasible point: B (m×n_eq, N(0,1) from `default_rng(seed + 1)`), b = Bᵀy0
+    with y0 the dual point of the generator (x = y0 gives X = Z0 ≻ 0).  With
+    `rank` < n_eq the columns past `rank` are combinations of the first ones
+    (the first of them an exact copy), a rank-deficient equality block."""
+    prob, y0 = _sdpa_dense(m, blocks, lp, seed)
+    rng = np.random.default_rng(seed + 1)
+    r = n_eq if rank is None else rank
+    B = np.zeros((m, n_eq))
+    B[:, :r] = rng.standard_normal((m, r))
+    for j in range(r, n_eq):
+        B[:, j] = B[:, 0] if j == r else B[:, :r] @ rng.standard_normal(r)
+    return SDPProblem(prob.c, prob.k, prob.Av, prob.C, B, B.T @ y0)
+
+
+def _sdpa_dense(m, blocks, lp, seed):
     """Strictly feasible dense SDP (SDPA primal-dual form) in SDPX core form.
 
     Draw order from `numpy.random.default_rng(seed)`, per PSD block of order n:
@@ -171,7 +193,7 @@ def sdpa_dense(m: int, blocks: Sequence[int], lp: int = 0, seed: int = 0,
     if lp > 0:
         A_sdpx.append(-a_lp.reshape(m, lp, 1, 1))
         C_sdpx.append(-c_lp)
-    return _assemble(-b, A_sdpx, C_sdpx, list(blocks), lp)
+    return _assemble(-b, A_sdpx, C_sdpx, list(blocks), lp), y0
 
 
 def _assemble(c, A_sdpx, C_sdpx, blocks, lp) -> SDPProblem:
