@@ -7,6 +7,9 @@ and m = 2000 constraints (generator `sdpx_b200.generators.sdpa_dense`), solved
 with SDPX's dense interior-point algorithm on the B200 in the mixed-precision
 mode; the plain FP64 device path is timed on the same instance for the
 mixed-vs-FP64 ratio.  Inputs (3.2 GB of constraint data) are larger than L2.
+The line also carries `equality_rows`: the same instance with 64 equality rows
+Bᵀx = b solved on the FP64 path, and the device time of the equality factor
+beside the oracle's host time for the same factor work.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -48,6 +51,9 @@ NORMAL_WORKLOAD = dict(m=3000, n_lp=20000, cones=[64] * 100, density=0.1,
 # Iterations of the CPU restatement on sdp_m2000 (seed 0) to 1e-8, used to
 # scale the reference arm's one-iteration samples to a time-to-gap.
 CPU_ITERATIONS_M2000 = 15  # CPU restatement, seed 0, tolerance 1e-8 (measured: Optimal in 15)
+# Equality rows added to the workload for the n > 0 measurement (Bᵀx = b with
+# B ~ N(0,1) and b = Bᵀy0 at the generator's strictly feasible point).
+EQ_ROWS = 64
 
 
 def schur_flops(m, blocks, lp):
@@ -209,6 +215,28 @@ def cpu_sample(prob, blocks, lp, gpu_iterations):
                    p.backtracking_factor, p.minimum_step, math.sqrt(2.220446049250313e-16))
     t_iter = time.perf_counter() - t0
     return t_iter
+
+
+def eq_cpu_sample(m, n, seed=0):
+    """Seconds of the oracle's equality factor (B̃ = L⁻¹B by LAPACK trsm,
+    unit-∞-norm columns, Q = B̂ᵀB̂, potrf, rank test) for an m×m lower factor
+    and n equality rows: the CPU counterpart of the device equality factor."""
+    import numpy as np
+    import scipy.linalg as sla
+    from oracle.sdpx_oracle import (cholesky_has_numerical_rank, equality_rank_tau,
+                                    kchol_lapack, normalize_equality_columns)
+    rng = np.random.default_rng(seed)
+    Lf = np.tril(rng.standard_normal((m, m))) * (0.5 / math.sqrt(m)) + 2.0 * np.eye(m)
+    B = rng.standard_normal((m, n))
+    best = math.inf
+    for _ in range(3):
+        t0 = time.perf_counter()
+        Bt = sla.solve_triangular(Lf, B, lower=True, check_finite=False)
+        Bt, _ = normalize_equality_columns(Bt)
+        ok, Lq = kchol_lapack(Bt.T @ Bt)
+        cholesky_has_numerical_rank(Lq, Bt, equality_rank_tau(m, n, TOL))
+        best = min(best, time.perf_counter() - t0)
+    return best
 
 
 def cpu_threads():
@@ -418,6 +446,44 @@ def run_ours(args, world, rank, local):
     fp64d_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
     be.set_gram_engine("int8")
 
+    # Equality rows (n > 0): the same instance with EQ_ROWS equality rows that
+    # keep its strictly feasible point, on the FP64 path (the equality block is
+    # FP64-only).  The equality factor's device time is the difference of one
+    # factorize (Schur Cholesky + inverse, then B̃ = L⁻¹B, Q, its Cholesky) with
+    # and without the rows at the final iterate.
+    def time_factorize(backend, bstream, reps=3):
+        backend.compute_residuals([0.0] * prob.L, True, True)
+        backend.schur_build()
+        es = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        es[0].record(bstream)
+        for _ in range(reps):
+            backend.factorize()
+        es[1].record(bstream)
+        torch.cuda.synchronize()
+        return es[0].elapsed_time(es[1]) / reps
+
+    fact_ms_plain = time_factorize(be, stream)
+    peq = G.sdpa_dense_equalities(m=wl["m"], blocks=wl["blocks"], lp=wl["lp"], n_eq=EQ_ROWS,
+                                  seed=rank)
+    with CudaBackend(peq, precision="fp64", device=local) as beq:
+        seq = torch.cuda.ExternalStream(beq.stream_handle())
+        solve_with_backend(beq, opts_fp64)
+        beq.reset()
+        e0.record(seq)
+        req = solve_with_backend(beq, opts_fp64)
+        e1.record(seq)
+        torch.cuda.synchronize()
+        eq_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
+        eq_factor = beq.equality_info()
+        fact_ms_eq = time_factorize(beq, seq)
+    equality = {"n": EQ_ROWS, "value": eq_s, "unit": "s", "iterations": req.iterations,
+                "status": req.status.value, "objective": req.pObj,
+                "p_res": req.p_res, "d_res": req.d_res, "path": "fp64",
+                "equality_factor": eq_factor[0], "equality_rank": eq_factor[1],
+                "factorize_ms_with_rows": fact_ms_eq, "factorize_ms_without_rows": fact_ms_plain,
+                "equality_factor_ms": fact_ms_eq - fact_ms_plain,
+                "workload": f"{wl['label']}, plus {EQ_ROWS} equality rows"}
+
     # FP64 reference throughput of this GPU (cuBLAS DGEMM), context for the FP64 roofline.
     a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
     b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
@@ -478,6 +544,10 @@ def run_ours(args, world, rank, local):
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
+            equality["cpu_equality_factor_ms"] = eq_cpu_sample(wl["m"], EQ_ROWS) * 1000.0
+            equality["cpu_kind"] = ("port: the oracle's equality factor (LAPACK trsm of B, "
+                                    "column scaling, Q = B̂ᵀB̂, potrf, rank test) on a "
+                                    "well-conditioned m×m factor, all host cores")
             t_it = cpu_sample(prob, wl["blocks"], wl["lp"], last.iterations)
             cpu = {"value": t_it * last.iterations, "unit": "s", "cores": cpu_threads(),
                    "kind": "port",
@@ -535,6 +605,7 @@ def run_ours(args, world, rank, local):
             "gpu_launches": launches,
             "clocks": clock_info,
             "normal_lp_soc": normal,
+            "equality_rows": equality,
         }
         print(json.dumps(line), flush=True)
     return line

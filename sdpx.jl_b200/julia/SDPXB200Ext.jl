@@ -33,9 +33,9 @@ function _check(h::B200Handle, status::Cint, what)
     error("libsdpx_b200 $what failed ($status): $msg")
 end
 
-"""Upload a dense SDPProblem (DenseCons, n = 0) to the B200 (src/workspace.jl:779)."""
+"""Upload a dense SDPProblem (DenseCons; equality rows B, b when n > 0) to the
+B200 (src/workspace.jl:779)."""
 function B200Handle(prob::SDPX.SDPProblem{Float64}; device::Integer=0)
-    prob.dims.n == 0 || throw(ArgumentError("the B200 core has no equality rows (n = 0)"))
     cons = prob.cons::SDPX.DenseCons{Float64}
     orders = Int32[prob.dims.k[l] for l in 1:prob.dims.L]
     Avs = [Matrix{Float64}(cons.Av[l]) for l in 1:prob.dims.L]   # k² × m, column i = vec(A_i)
@@ -54,7 +54,32 @@ function B200Handle(prob::SDPX.SDPProblem{Float64}; device::Integer=0)
         x.ptr == C_NULL || ccall((:sdpx_b200_destroy, libsdpx), Cvoid, (Ptr{Cvoid},), x.ptr)
         x.ptr = C_NULL
     end
+    if prob.dims.n > 0
+        # SDPProblem.B (m×n, column-major) and .b; the KKT factor then carries the
+        # equality block of src/kkt.jl:1466-1680 (FP64 precision mode only).
+        B = Matrix{Float64}(prob.B)
+        b = Vector{Float64}(prob.b)
+        _check(h, ccall((:sdpx_b200_set_equality, libsdpx), Cint,
+                        (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}), h.ptr,
+                        Int32(prob.dims.n), B, b), "set_equality")
+    end
     return h
+end
+
+"""Rank tolerance input `_requested_accuracy(opts)` (src/kkt.jl:518-521) and
+`opts.equality_solver` (:auto → 0, :qr → 1)."""
+set_equality_options!(h::B200Handle, requested::Float64, solver::Symbol) =
+    _check(h, ccall((:sdpx_b200_set_equality_options, libsdpx), Cint,
+                    (Ptr{Cvoid}, Float64, Cint), h.ptr, requested, solver === :qr ? 1 : 0),
+           "set_equality_options")
+
+"""Multipliers y (and dy, p = b − Bᵀx) of the equality rows."""
+function multipliers(h::B200Handle, n::Integer)
+    y, dy, p = zeros(n), zeros(n), zeros(n)
+    _check(h, ccall((:sdpx_b200_get_multipliers, libsdpx), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}), h.ptr, y, dy, p),
+           "get_multipliers")
+    return y, dy, p
 end
 
 set_precision!(h::B200Handle, mixed::Bool) =
