@@ -13,7 +13,7 @@
  *   - "stacked" host matrices (X, Y, dX, dY, C) concatenate the k_l×k_l
  *     column-major blocks in block order: Σ_l k_l² doubles;
  *   - the core solves SDPX's form min cᵀx s.t. X_l = Σ_i x_i A_i^(l) − C_l ⪰ 0
- *     with no equality rows (n = 0).
+ *     and, when sdpx_b200_set_equality attached them, Bᵀx = b (n > 0).
  *
  * One handle = one solve = one CUDA stream.  A handle is not reentrant; use
  * one handle per concurrent solve (SDPX: "Concurrent factorization must use
@@ -106,9 +106,12 @@ int sdpx_b200_rhs_corrector_mehrotra(sdpx_b200_handle* h, double sigma, double m
 int sdpx_b200_rhs_corrector_fixed(sdpx_b200_handle* h, double beta, const double* mu);
 int sdpx_b200_set_rhs(sdpx_b200_handle* h, int which);
 
-/* dx = S⁻¹ r with the current factor (`_solve_dense_kkt_owned!`, src/kkt.jl:2570-2595). */
+/* dx = S⁻¹ r with the current factor (`_solve_dense_kkt_owned!`, src/kkt.jl:2570-2595);
+ * with equality rows also dy, from S·dx − B·dy = r, Bᵀdx = p. */
 int sdpx_b200_solve(sdpx_b200_handle* h);
-/* ρ = r − S·dx; residual = ‖ρ‖∞, rnorm = ‖r‖∞ (src/kkt.jl:3689-3708). */
+/* ρ = r − S·dx; residual = ‖ρ‖∞, rnorm = ‖r‖∞ (src/kkt.jl:3689-3708).  With
+ * equality rows ρ += B·dy, ρ_p = p − Bᵀdx, residual = max(‖ρ‖∞, ‖ρ_p‖∞) and
+ * rnorm = max(‖r‖∞, ‖p‖∞). */
 int sdpx_b200_direction_residual(sdpx_b200_handle* h, double* residual, double* rnorm);
 /* Residual-driven refinement with rollback (`_refine_native_direction!`,
  * src/kkt.jl:3891-3963).  policy: 0 fixed, 1 adaptive/auto; tol ≤ 0 selects
@@ -241,7 +244,7 @@ typedef struct {
   double primal_affine_residual, dual_affine_residual;
   double primal_cone_violation, dual_cone_violation;
   double primal_residual_scaled, dual_residual_scaled;
-  double equality_backward_error, equality_strict_backward_error; /* 0 (no equality rows) */
+  double equality_backward_error, equality_strict_backward_error; /* 0 when n = 0 */
   double primal_block_backward_error, primal_block_strict_backward_error;
   double dual_backward_error, dual_strict_backward_error;
   double complementarity, complementarity_relative;
@@ -262,6 +265,14 @@ typedef struct {
 int sdpx_b200_certificate(sdpx_b200_handle* h, const double* x, const double* X, const double* Y,
                           double eps_primal, double eps_dual, double eps_gap, int32_t legacy_gap,
                           sdpx_b200_certificate_result* out);
+/* The same certificate with the equality rows' terms (n > 0): y enters the
+ * dual objective (bᵀy), the dual residual and its backward errors (B·y), and
+ * b − Bᵀx the primal residual and the equality backward errors
+ * (src/validation.jl:454-482, 629-644, 666-740). */
+int sdpx_b200_certificate_eq(sdpx_b200_handle* h, const double* x, const double* X,
+                             const double* y, const double* Y, double eps_primal,
+                             double eps_dual, double eps_gap, int32_t legacy_gap,
+                             sdpx_b200_certificate_result* out);
 
 /* Engine of the FP64 Schur assembly — the Gram S = P̂ᵀP̂ and the block
  * products T_i = L_X⁻¹·A_i, P_i = T_i·L_Y (no counterpart in the reference,

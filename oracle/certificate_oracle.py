@@ -1,12 +1,14 @@
 """CPU oracle of SDPX's cold-path result certificate — TEST INFRASTRUCTURE ONLY.
 
 Only `tests/` may import this module.  It restates `result_certificate`
-(src/validation.jl:948-1115) for the optimality kind of a dense SDP without
-equality rows (n = 0), with its helpers:
+(src/validation.jl:948-1115) for the optimality kind of a dense SDP, with
+equality rows Bᵀx = b when they are given, and its helpers:
 
 * `solution_residuals` (src/validation.jl:15-56),
 * `_primal_block_backward_errors` (:526-600, dense branch),
-* `_dual_backward_errors` (:666-740, dense branch),
+* `_dual_backward_errors` (:666-740, dense branch) with the equality terms of
+  `_accumulate_equality_dual_scales!` (:629-644),
+* `_equality_backward_errors` (:454-482, dense B),
 * `_componentwise_backward_errors` / `_componentwise_ratio` (:418-431, :506-513),
 * `_block_psd_certificate`, `_blocks_psd_certificate`, `_psd_violation`
   (:765-932),
@@ -62,7 +64,7 @@ def primal_block_backward_errors(Av, C, k, x, X):
     return mixed, strict
 
 
-def dual_backward_errors(Av, k, c, Y):
+def dual_backward_errors(Av, k, c, Y, B=None, y=None):
     res = c.copy()
     nominal = np.abs(c).copy()
     realized = np.abs(c).copy()
@@ -72,6 +74,10 @@ def dual_backward_errors(Av, k, c, Y):
         absA = np.abs(Av[l])
         nominal = nominal + absA.sum(axis=1)
         realized = realized + absA @ np.abs(yv)
+    if B is not None and B.shape[1]:
+        res = res - B @ y
+        nominal = nominal + np.abs(B).sum(axis=1)
+        realized = realized + np.abs(B) @ np.abs(y)
     mixed = strict = 0.0
     for i in range(res.size):
         a, b = _cw(res[i], nominal[i], realized[i])
@@ -79,13 +85,31 @@ def dual_backward_errors(Av, k, c, Y):
     return mixed, strict, res
 
 
-def solution_residuals(Av, C, k, c, x, X, Y):
+def equality_backward_errors(B, b, x):
+    """`_equality_backward_errors` (src/validation.jl:454-482), row order."""
+    mixed = strict = 0.0
+    for j in range(B.shape[1]):
+        lhs, nominal, realized = 0.0, abs(b[j]), abs(b[j])
+        for i in range(B.shape[0]):
+            lhs += B[i, j] * x[i]
+            nominal += abs(B[i, j])
+            realized += abs(B[i, j]) * abs(x[i])
+        a, s = _cw(abs(lhs - b[j]), nominal, realized)
+        mixed, strict = max(mixed, a), max(strict, s)
+    return mixed, strict
+
+
+def solution_residuals(Av, C, k, c, x, X, Y, B=None, b=None, y=None):
     p = 0.0
     for l, kl in enumerate(k):
         p = max(p, _knrm_inf(_buildP(Av[l], kl, x) - X[l] - C[l]))
+    if B is not None and B.shape[1]:
+        p = max(p, _knrm_inf(b - B.T @ x))
     d = c.copy()
     for l in range(len(k)):
         d = d - Av[l] @ Y[l].reshape(-1, order="F")
+    if B is not None and B.shape[1]:
+        d = d - B @ y
     return p, _knrm_inf(d)
 
 
@@ -165,14 +189,22 @@ def psd_violation(details):
 
 def result_certificate(Av: List[np.ndarray], C: List[np.ndarray], k: List[int], c: np.ndarray,
                        x, X, Y, eps_primal=1e-10, eps_dual=1e-10, eps_gap=1e-10,
-                       legacy=False) -> dict:
-    """`result_certificate` for the optimality kind, n = 0."""
+                       legacy=False, B=None, b=None, y=None) -> dict:
+    """`result_certificate` for the optimality kind (equality rows B, b with
+    multipliers y when n > 0)."""
     x = np.asarray(x, dtype=np.float64)
+    neq = 0 if B is None else np.asarray(B).reshape(x.size, -1).shape[1]
+    if neq:
+        B = np.asarray(B, dtype=np.float64).reshape(x.size, neq)
+        b = np.asarray(b, dtype=np.float64)
+        y = np.asarray(y, dtype=np.float64)
     p_obj = float(c @ x)
     d_obj = 0.0
     for l in range(len(k)):
         d_obj += float(np.sum(C[l] * Y[l]))
-    p_aff, d_aff = solution_residuals(Av, C, k, c, x, X, Y)
+    if neq:
+        d_obj += float(b @ y)
+    p_aff, d_aff = solution_residuals(Av, C, k, c, x, X, Y, B if neq else None, b, y)
     gap = p_obj - d_obj
     oscale = max(1.0, (abs(p_obj) + abs(d_obj)) / 2.0)
     gap_rel = abs(gap) / oscale
@@ -183,21 +215,26 @@ def result_certificate(Av: List[np.ndarray], C: List[np.ndarray], k: List[int], 
     dd = [block_psd_certificate(Y[l], max(eps_dual, eps_gap)) for l in range(len(k))]
     pviol, dviol = psd_violation(pd), psd_violation(dd)
     p_res, d_res = max(p_aff, pviol), max(d_aff, dviol)
-    pscale = 1.0 + max(max((_knrm_inf(Cl) for Cl in C), default=0.0), 0.0)
+    pscale = 1.0 + max(max((_knrm_inf(Cl) for Cl in C), default=0.0),
+                       _knrm_inf(b) if neq else 0.0)
     dscale = 1.0 + _knrm_inf(c)
     pb_mixed, pb_strict = primal_block_backward_errors(Av, C, k, x, X)
-    db_mixed, db_strict, _ = dual_backward_errors(Av, k, c, Y)
+    db_mixed, db_strict, _ = dual_backward_errors(Av, k, c, Y, B if neq else None, y)
+    eq_mixed, eq_strict = equality_backward_errors(B, b, x) if neq else (0.0, 0.0)
     failures = []
     primal_finite = (math.isfinite(p_obj) and math.isfinite(p_res) and
-                     bool(np.all(np.isfinite(x))) and all(np.all(np.isfinite(B)) for B in X))
+                     bool(np.all(np.isfinite(x))) and all(np.all(np.isfinite(M)) for M in X))
     dual_finite = (math.isfinite(d_obj) and math.isfinite(d_res) and
-                   all(np.all(np.isfinite(B)) for B in Y))
+                   all(np.all(np.isfinite(M)) for M in Y) and
+                   (not neq or bool(np.all(np.isfinite(y)))))
     finite = primal_finite and dual_finite and math.isfinite(gap_rel) and math.isfinite(compl)
     gap_ok = (0.0 <= gap <= eps_gap) if legacy else (gap_rel <= eps_gap)
     if not finite:
         failures.append("nonfinite")
     if not p_res / pscale <= eps_primal:
         failures.append("primal_residual")
+    if not eq_mixed <= eps_primal:
+        failures.append("equality_backward_error")
     if not pb_mixed <= eps_primal:
         failures.append("primal_block_backward_error")
     if not d_res / dscale <= eps_dual:
@@ -215,7 +252,7 @@ def result_certificate(Av: List[np.ndarray], C: List[np.ndarray], k: List[int], 
                 dual_residual=d_res, primal_affine_residual=p_aff, dual_affine_residual=d_aff,
                 primal_cone_violation=pviol, dual_cone_violation=dviol,
                 primal_residual_scaled=p_res / pscale, dual_residual_scaled=d_res / dscale,
-                equality_backward_error=0.0, equality_strict_backward_error=0.0,
+                equality_backward_error=eq_mixed, equality_strict_backward_error=eq_strict,
                 primal_block_backward_error=pb_mixed,
                 primal_block_strict_backward_error=pb_strict,
                 dual_backward_error=db_mixed, dual_strict_backward_error=db_strict,

@@ -2321,7 +2321,8 @@ struct Handle {
   }
 
   void certificate(const double* hx, const double* hX, const double* hY, double ep, double ed,
-                   double eg, int legacy, sdpx_b200_certificate_result* out) {
+                   double eg, int legacy, sdpx_b200_certificate_result* out,
+                   const double* hy = nullptr) {
     const double* Ause = have_original ? A0.p : A.p;
     const double* Cuse = have_original ? C0st.p : Cst.p;
     const double* cuse = have_original ? c0.p : c.p;
@@ -2342,8 +2343,26 @@ struct Handle {
     double* cols = cert_cols.p;
     cert_primal_rows(Ause, K, m, work_m.p, T1.p, Cuse, cert_part.p, gemv_chunks, rows, rows + K,
                      rows + 2 * K, st);
-    cert_dual_cols(Ause, K, m, T2.p, cuse, cols, cols + m, cols + 2 * m, st);
-    clear_red(0, 14);
+    // Equality rows (n > 0): their terms of the dual residual and backward
+    // errors, the equality backward errors and bᵀy (src/validation.jl:454-482,
+    // 629-644, 666-740; `dual_objective`, src/solver/interior_point.jl:7-14).
+    const double* Buse = eq_have_original ? Beq0.p : Beq.p;
+    if (n_eq) {
+      if (!hy) throw std::invalid_argument("equality multipliers y are required when n > 0");
+      h2d(eq_z.p, hy, n_eq * sizeof(double));
+    }
+    cert_dual_cols(Ause, K, m, T2.p, cuse, cols, cols + m, cols + 2 * m, st,
+                   n_eq ? Buse : nullptr, n_eq, n_eq ? eq_z.p : nullptr);
+    clear_red(0, 20);
+    if (n_eq) {
+      cert_equality_rows(Buse, m, n_eq, work_m.p, beq.p, eq_cert.p, eq_cert.p + n_eq,
+                         eq_cert.p + 2 * n_eq, st);
+      absmax(n_eq, eq_cert.p, red.p + 14, st);
+      absmax(n_eq, eq_cert.p + n_eq, red.p + 15, st);
+      absmax(n_eq, eq_cert.p + 2 * n_eq, red.p + 16, st);
+      absmax(n_eq, beq.p, red.p + 17, st);
+      cert_dot(n_eq, eq_z.p, beq.p, red.p + 18, st);  // bᵀy, non-finite y
+    }
     absmax(K, rows, red.p + 0, st);
     absmax(K, rows + K, red.p + 1, st);
     absmax(K, rows + 2 * K, red.p + 2, st);
@@ -2355,7 +2374,7 @@ struct Handle {
     cert_dot(m, work_m.p, cuse, red.p + 8, st);  // c·x, non-finite x
     cert_dot(K, T2.p, Cuse, red.p + 10, st);     // Σ⟨C_l, Y_l⟩, non-finite Y
     cert_dot(K, T1.p, T2.p, red.p + 12, st);     // Σ⟨X_l, Y_l⟩, non-finite X
-    double r[14];
+    double r[20];
     d2h(r, red.p, sizeof(r));
     sync();
     int pfail = 0, dfail = 0;
@@ -2364,21 +2383,23 @@ struct Handle {
 
     sdpx_b200_certificate_result cr{};
     cr.primal_objective = r[8];
-    cr.dual_objective = r[10];
+    cr.dual_objective = r[10] + r[18];
     cr.gap = cr.primal_objective - cr.dual_objective;
     double oscale =
         std::max(1.0, (std::fabs(cr.primal_objective) + std::fabs(cr.dual_objective)) / 2.0);
     cr.gap_relative = std::fabs(cr.gap) / oscale;
     cr.complementarity = r[12];
     cr.complementarity_relative = std::fabs(cr.complementarity) / oscale;
-    cr.primal_affine_residual = r[0];
+    cr.primal_affine_residual = std::max(r[0], r[14]);
     cr.dual_affine_residual = r[3];
     cr.primal_cone_violation = pviol;
     cr.dual_cone_violation = dviol;
-    cr.primal_residual = std::max(r[0], pviol);
+    cr.primal_residual = std::max(cr.primal_affine_residual, pviol);
     cr.dual_residual = std::max(r[3], dviol);
-    cr.primal_residual_scaled = cr.primal_residual / (1.0 + r[6]);
+    cr.primal_residual_scaled = cr.primal_residual / (1.0 + std::max(r[6], r[17]));
     cr.dual_residual_scaled = cr.dual_residual / (1.0 + r[7]);
+    cr.equality_backward_error = r[15];
+    cr.equality_strict_backward_error = r[16];
     cr.primal_block_backward_error = r[1];
     cr.primal_block_strict_backward_error = r[2];
     cr.dual_backward_error = r[4];
@@ -2388,13 +2409,14 @@ struct Handle {
     bool primal_finite = std::isfinite(cr.primal_objective) && std::isfinite(cr.primal_residual) &&
                          r[9] == 0.0 && r[13] == 0.0;
     bool dual_finite = std::isfinite(cr.dual_objective) && std::isfinite(cr.dual_residual) &&
-                       r[11] == 0.0;
+                       r[11] == 0.0 && r[19] == 0.0;
     bool finite = primal_finite && dual_finite && std::isfinite(cr.gap_relative) &&
                   std::isfinite(cr.complementarity);
     bool gap_ok = legacy ? (0.0 <= cr.gap && cr.gap <= eg) : (cr.gap_relative <= eg);
     int f = 0;
     if (!finite) f |= SDPX_B200_CERT_NONFINITE;
     if (!(cr.primal_residual_scaled <= ep)) f |= SDPX_B200_CERT_PRIMAL_RESIDUAL;
+    if (!(cr.equality_backward_error <= ep)) f |= SDPX_B200_CERT_EQUALITY_BACKWARD_ERROR;
     if (!(cr.primal_block_backward_error <= ep)) f |= SDPX_B200_CERT_PRIMAL_BLOCK_BACKWARD_ERROR;
     if (!(cr.dual_residual_scaled <= ed)) f |= SDPX_B200_CERT_DUAL_RESIDUAL;
     if (!(cr.dual_backward_error <= ed)) f |= SDPX_B200_CERT_DUAL_BACKWARD_ERROR;
@@ -2423,7 +2445,7 @@ struct Handle {
   int n_eq = 0;
   DBuf<double> Beq, Beq0, beq;
   DBuf<double> yv, dyv, pv, rho_p, ybest, dybest, eq_dyh, eq_ddy, eq_q, eq_z, eq_tm;
-  DBuf<double> Bt, Qf, Bqr, eq_scale, eq_rdiag, eq_colnorm, eq_partial;
+  DBuf<double> Bt, Qf, Bqr, eq_scale, eq_rdiag, eq_colnorm, eq_partial, eq_cert;
   DBuf<int> eq_perm, eq_pairs, eq_equal;
   DBuf<unsigned long long> eq_fp;
   SyrkPlan eq_syrk;
@@ -2671,6 +2693,12 @@ int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const dou
 int sdpx_b200_original_residuals_eq(sdpx_b200_handle* h, const double* x, const double* X,
                                     const double* y, const double* Y, double* p, double* d) {
   GUARD(h, h->h.original_residuals(x, X, Y, p, d, y));
+}
+int sdpx_b200_certificate_eq(sdpx_b200_handle* h, const double* x, const double* X,
+                             const double* y, const double* Y, double eps_primal,
+                             double eps_dual, double eps_gap, int32_t legacy_gap,
+                             sdpx_b200_certificate_result* out) {
+  GUARD(h, h->h.certificate(x, X, Y, eps_primal, eps_dual, eps_gap, legacy_gap, out, y));
 }
 int sdpx_b200_set_equality(sdpx_b200_handle* h, int32_t n, const double* B, const double* b) {
   GUARD(h, h->h.set_equality(n, B, b));

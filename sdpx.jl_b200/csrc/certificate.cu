@@ -58,7 +58,8 @@ __global__ void k_cert_rows_finish(long long K, int chunks, const double* __rest
 
 __global__ void k_cert_cols(const double* __restrict__ A, long long K, int m,
                             const double* __restrict__ Y, const double* __restrict__ c,
-                            double* absv, double* mixed, double* strict) {
+                            double* absv, double* mixed, double* strict,
+                            const double* __restrict__ B, int n, const double* __restrict__ yv) {
   __shared__ double red[32];
   int i = blockIdx.x;
   const double* col = A + (long long)i * K;
@@ -69,15 +70,32 @@ __global__ void k_cert_cols(const double* __restrict__ A, long long K, int m,
     sn += fabs(a);
     sr += fabs(a) * fabs(y);
   }
+  // equality rows: v_i −= Σ_j B[i,j]·y_j with their |B|, |B|·|y| scales
+  // (`_accumulate_equality_dual_scales!`, src/validation.jl:629-644)
+  double bv = 0.0, bn = 0.0, br = 0.0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const double bij = B[i + (long long)j * m];
+    bv += bij * yv[j];
+    bn += fabs(bij);
+    br += fabs(bij) * fabs(yv[j]);
+  }
   sv = block_sum(sv, red);
   __syncthreads();
   sn = block_sum(sn, red);
   __syncthreads();
   sr = block_sum(sr, red);
+  __syncthreads();
+  if (n > 0) {
+    bv = block_sum(bv, red);
+    __syncthreads();
+    bn = block_sum(bn, red);
+    __syncthreads();
+    br = block_sum(br, red);
+  }
   if (threadIdx.x == 0) {
-    double v = c[i] - sv;
-    double nominal = fabs(c[i]) + sn;
-    double realized = fabs(c[i]) + sr;
+    double v = c[i] - sv - bv;
+    double nominal = fabs(c[i]) + sn + bn;
+    double realized = fabs(c[i]) + sr + br;
     absv[i] = fabs(v);
     mixed[i] = cw_ratio(v, nominal + realized);
     strict[i] = cw_ratio(v, realized);
@@ -155,9 +173,46 @@ void cert_primal_rows(const double* A, long long K, int m, const double* x, cons
 }
 
 void cert_dual_cols(const double* A, long long K, int m, const double* Y, const double* c,
-                    double* absv, double* mixed, double* strict, cudaStream_t st) {
+                    double* absv, double* mixed, double* strict, cudaStream_t st, const double* B,
+                    int n, const double* y) {
   if (m == 0) return;
-  k_cert_cols<<<m, 512, 0, st>>>(A, K, m, Y, c, absv, mixed, strict);
+  k_cert_cols<<<m, 512, 0, st>>>(A, K, m, Y, c, absv, mixed, strict, B, n, y);
+  SDPX_LAUNCH_CHECK();
+}
+
+// One CTA per equality j: lhs = Σ_i B[i,j]·x_i, residual |lhs − b_j|,
+// nominal |b_j| + Σ|B[i,j]|, realized |b_j| + Σ|B[i,j]|·|x_i|
+// (`_equality_backward_errors`, src/validation.jl:454-482).
+__global__ void k_cert_equality(const double* __restrict__ B, int m, const double* __restrict__ x,
+                                const double* __restrict__ b, double* absr, double* mixed,
+                                double* strict) {
+  __shared__ double red[32];
+  const int j = blockIdx.x;
+  const double* col = B + (long long)j * m;
+  double lhs = 0.0, sn = 0.0, sr = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const double a = col[i];
+    lhs += a * x[i];
+    sn += fabs(a);
+    sr += fabs(a) * fabs(x[i]);
+  }
+  lhs = block_sum(lhs, red);
+  __syncthreads();
+  sn = block_sum(sn, red);
+  __syncthreads();
+  sr = block_sum(sr, red);
+  if (threadIdx.x == 0) {
+    const double v = lhs - b[j];
+    absr[j] = fabs(v);
+    mixed[j] = cw_ratio(v, fabs(b[j]) + sn + fabs(b[j]) + sr);
+    strict[j] = cw_ratio(v, fabs(b[j]) + sr);
+  }
+}
+
+void cert_equality_rows(const double* B, int m, int n, const double* x, const double* b,
+                        double* absr, double* mixed, double* strict, cudaStream_t st) {
+  if (n == 0) return;
+  k_cert_equality<<<n, 256, 0, st>>>(B, m, x, b, absr, mixed, strict);
   SDPX_LAUNCH_CHECK();
 }
 

@@ -14,10 +14,18 @@ void cert_primal_rows(const double* A, long long K, int m, const double* x, cons
                       double* strict, cudaStream_t st);
 
 // Dual backward errors per variable i:
-//   v_i = c_i − Σ_r A[r,i]·Y_r, nominal_i = |c_i| + Σ_r |A[r,i]|,
-//   realized_i = |c_i| + Σ_r |A[r,i]|·|Y_r|.
+//   v_i = c_i − Σ_r A[r,i]·Y_r − Σ_j B[i,j]·y_j, nominal_i = |c_i| + Σ_r |A[r,i]| + Σ_j |B[i,j]|,
+//   realized_i = |c_i| + Σ_r |A[r,i]|·|Y_r| + Σ_j |B[i,j]|·|y_j|
+// (the B terms only for n > 0 equality rows, B m×n column-major).
 void cert_dual_cols(const double* A, long long K, int m, const double* Y, const double* c,
-                    double* absv, double* mixed, double* strict, cudaStream_t st);
+                    double* absv, double* mixed, double* strict, cudaStream_t st,
+                    const double* B = nullptr, int n = 0, const double* y = nullptr);
+
+// Equality backward errors per row j of Bᵀx = b: |Σ_i B[i,j]x_i − b_j| and its
+// mixed / strict componentwise ratios with nominal |b_j| + Σ|B| and realized
+// |b_j| + Σ|B|·|x|.
+void cert_equality_rows(const double* B, int m, int n, const double* x, const double* b,
+                        double* absr, double* mixed, double* strict, cudaStream_t st);
 
 // out[0] += Σ a·b (single CTA, fixed order within the launch); out[1] += count of
 // non-finite entries of a (as a double).

@@ -39,7 +39,7 @@ def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
         result = solve_with_backend(be, opts, trace=trace)
         if certificate:
             result.certificate = be.certificate(result.x, result.X, result.Y, opts.eps_primal,
-                                                opts.eps_dual, opts.eps_gap)
+                                                opts.eps_dual, opts.eps_gap, y=result.y)
         return result
 
 
@@ -51,4 +51,4 @@ def certificate(prob: SDPProblem, result: SDPResult, *, eps_primal: float = 1e-1
     from .cuda_backend import CudaBackend
     with CudaBackend(prob, device=device) as be:
         return be.certificate(result.x, result.X, result.Y, eps_primal, eps_dual, eps_gap,
-                              legacy_gap)
+                              legacy_gap, y=result.y)

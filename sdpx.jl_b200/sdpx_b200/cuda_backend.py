@@ -107,6 +107,8 @@ _SIGS = {
     "sdpx_b200_set_multipliers": [C.c_void_p, _dp],
     "sdpx_b200_equality_info": [C.c_void_p, _ip, _ip, _dp],
     "sdpx_b200_original_residuals_eq": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp],
+    "sdpx_b200_certificate_eq": [C.c_void_p, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
+                                 C.c_double, C.c_int32, C.POINTER(CertificateResult)],
 }
 
 _lib = None
@@ -516,16 +518,22 @@ class CudaBackend:
         return a.value, b.value
 
     def certificate(self, x, X, Y, eps_primal=1e-10, eps_dual=1e-10, eps_gap=1e-10,
-                    legacy_gap=False) -> dict:
+                    legacy_gap=False, y=None) -> dict:
         """Cold-path certificate of (x, X, Y) against the original data
         (`result_certificate`, src/validation.jl:948-1115)."""
-        if self.n:
-            raise NotImplementedError("the device certificate covers problems without equality rows")
         x = np.ascontiguousarray(x, dtype=np.float64)
         Xs, Ys = self._join(X), self._join(Y)
         out = CertificateResult()
-        self._call("sdpx_b200_certificate", _p(x), _p(Xs), _p(Ys), float(eps_primal),
-                   float(eps_dual), float(eps_gap), 1 if legacy_gap else 0, C.byref(out))
+        if self.n:
+            if y is None:
+                raise ValueError("the equality multipliers y are required when n > 0")
+            yv = np.ascontiguousarray(y, dtype=np.float64)
+            self._call("sdpx_b200_certificate_eq", _p(x), _p(Xs), _p(yv), _p(Ys),
+                       float(eps_primal), float(eps_dual), float(eps_gap),
+                       1 if legacy_gap else 0, C.byref(out))
+        else:
+            self._call("sdpx_b200_certificate", _p(x), _p(Xs), _p(Ys), float(eps_primal),
+                       float(eps_dual), float(eps_gap), 1 if legacy_gap else 0, C.byref(out))
         d = {name: getattr(out, name) for name, _ in CertificateResult._fields_}
         d["valid"] = bool(out.valid)
         d["failures"] = [name for bit, name in CERTIFICATE_FAILURES if out.failures & bit]

@@ -62,3 +62,23 @@ def test_block_psd_shift_resolution():
     # order 6: unresolved, reported at the allowed shift
     d = block_psd_certificate(np.diag([1.0] * 5 + [-1.0]), 1e-10)
     assert not d["ok"] and not d["resolved"] and d["required"] == d["allowed"]
+
+
+def test_equality_rows_certificate_t2():
+    """T2 (test/correctness.jl:97-122) solved by the oracle: its certificate
+    with the equality row is valid; moving x₁ off the row fails it with the
+    equality backward error."""
+    from oracle.sdpx_oracle import oracle_solve
+    from sdpx_b200 import SolverOptions, generators as G
+    prob = G.toy_t2()
+    r = oracle_solve(prob, SolverOptions().with_tolerance(1e-8))
+    c = result_certificate(prob.Av, prob.C, prob.k, prob.c, r.x, r.X, r.Y, 1e-8, 1e-8, 1e-8,
+                           B=prob.B, b=prob.b, y=r.y)
+    assert c["valid"], c["failures"]
+    assert abs(c["dual_objective"] - 5.5) < 1e-7
+    x = r.x.copy()
+    x[0] += 1e-3
+    bad = result_certificate(prob.Av, prob.C, prob.k, prob.c, x, r.X, r.Y, 1e-8, 1e-8, 1e-8,
+                             B=prob.B, b=prob.b, y=r.y)
+    assert "equality_backward_error" in bad["failures"]
+    assert bad["equality_backward_error"] > 1e-5

@@ -87,3 +87,43 @@ def test_readme_moment_on_gpu():
     assert r.status.value == "Optimal"
     assert abs(-r.pObj - (math.sqrt(5.0) - 1.0) / 2.0) < 1e-8
     assert r.certificate["valid"], r.certificate["failures"]
+
+
+# ---- equality rows (n > 0): src/validation.jl:454-482, 629-644, 666-740 ----
+
+@pytest.fixture(scope="module")
+def solved_eq():
+    from sdpx_b200 import generators as G, solve
+    prob = G.sdpa_dense_equalities(m=30, blocks=[8, 4], lp=3, n_eq=4, seed=5)
+    r = solve(prob, tolerance=1e-8, certificate=True)
+    return prob, r
+
+
+def _oracle_eq(prob, r, x=None, y=None):
+    return result_certificate(prob.Av, prob.C, prob.k, prob.c, r.x if x is None else x, r.X,
+                              r.Y, 1e-8, 1e-8, 1e-8, B=prob.B, b=prob.b,
+                              y=r.y if y is None else y)
+
+
+def test_certificate_with_equality_rows(solved_eq):
+    prob, r = solved_eq
+    o = _oracle_eq(prob, r)
+    assert r.status.value == "Optimal"
+    assert r.certificate["valid"] and o["valid"], (r.certificate["failures"], o["failures"])
+    _compare(r.certificate, o, _scale(prob, r.x))
+    assert abs(r.certificate["equality_backward_error"] - o["equality_backward_error"]) <= 1e-12
+    assert math.isclose(r.certificate["dual_objective"], o["dual_objective"], rel_tol=1e-12)
+
+
+def test_certificate_flags_violated_equality(solved_eq):
+    """x moved by 1e-4 along B's first column: the equality backward error
+    (and the primal residual) fail, and the failure set equals the oracle's."""
+    from sdpx_b200 import certificate
+    prob, r = solved_eq
+    x = r.x + 1e-4 * prob.B[:, 0] / np.linalg.norm(prob.B[:, 0])
+    g = certificate(prob, type(r)(**{**r.__dict__, "x": x}), eps_primal=1e-8, eps_dual=1e-8,
+                    eps_gap=1e-8)
+    o = _oracle_eq(prob, r, x=x)
+    assert "equality_backward_error" in o["failures"]
+    assert sorted(g["failures"]) == sorted(o["failures"])
+    assert abs(g["equality_backward_error"] - o["equality_backward_error"]) <= 1e-12
