@@ -476,9 +476,24 @@ def run_ours(args, world, rank, local):
         eq_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
         eq_factor = beq.equality_info()
         fact_ms_eq = time_factorize(beq, seq)
+    # the same instance in the mixed mode (the headline path)
+    with CudaBackend(peq, precision="mixed", device=local) as beq:
+        seq = torch.cuda.ExternalStream(beq.stream_handle())
+        solve_with_backend(beq, opts_mixed)
+        beq.reset()
+        beq.requested = "mixed"
+        e0.record(seq)
+        reqm = solve_with_backend(beq, opts_mixed)
+        e1.record(seq)
+        torch.cuda.synchronize()
+        eqm_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
     equality = {"n": EQ_ROWS, "value": eq_s, "unit": "s", "iterations": req.iterations,
                 "status": req.status.value, "objective": req.pObj,
                 "p_res": req.p_res, "d_res": req.d_res, "path": "fp64",
+                "mixed": {"value": eqm_s, "unit": "s", "iterations": reqm.iterations,
+                          "status": reqm.status.value, "objective": reqm.pObj,
+                          "precision_trace": "".join("m" if p == "mixed" else "d"
+                                                     for p in reqm.precision_trace)},
                 "equality_factor": eq_factor[0], "equality_rank": eq_factor[1],
                 "factorize_ms_with_rows": fact_ms_eq, "factorize_ms_without_rows": fact_ms_plain,
                 "equality_factor_ms": fact_ms_eq - fact_ms_plain,

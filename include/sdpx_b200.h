@@ -173,8 +173,10 @@ int sdpx_b200_original_residuals(sdpx_b200_handle* h, const double* x, const dou
  * `_solve_dense_kkt_owned!` (src/kkt.jl:2570-2595).  Residuals, refinement,
  * update, objectives, the cold start and the equilibration carry the B, b, y
  * terms of src/step.jl:25-72, src/kkt.jl:3689-3708 and
- * src/solver/interior_point.jl:699-1311 once they are set.  FP64 precision
- * mode only (sdpx_b200_set_precision refuses the mixed mode while n > 0). */
+ * src/solver/interior_point.jl:699-1311 once they are set.  In the mixed
+ * precision mode B̃ comes from the FP32 factor and Q is factored in FP64 with
+ * up to 8 diagonal regularisations (src/kernels/mixed_precision_kkt.jl:481-520,
+ * 1045-1082); the guard refines against the FP64 KKT operator with the B terms. */
 
 /* B column-major m×n, b length n; call after create and before
  * sdpx_b200_equilibrate.  n = 0 removes the equality rows. */

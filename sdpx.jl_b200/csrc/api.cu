@@ -59,6 +59,7 @@ struct DenseBlk {
 
 static constexpr double kEps = 2.220446049250313e-16;
 static const double kSqrtEps = std::sqrt(2.220446049250313e-16);
+int mixed_steps_for(double cond);  // mixed_api.inc
 
 struct Handle {
   int dev = 0;
@@ -1165,6 +1166,20 @@ struct Handle {
     PhaseScope ps(this, 2);
     if (precision == SDPX_B200_MIXED && mixed) {
       mixed_factorize(ok, attempts, quality);
+      if (*ok && n_eq) {
+        // Equality block on the low-precision factor (`_try_factor_mixed_kkt!`,
+        // src/kernels/mixed_precision_kkt.jl:1045-1082): its condition estimate
+        // joins the refinement-budget gate; a Q that stays indefinite rejects
+        // the mixed factor for this iteration.
+        double cond_q = INFINITY, quality_q = 0.0;
+        if (factor_equality_mixed(&cond_q, &quality_q)) {
+          mixed->cond_estimate = std::max(mixed->cond_estimate, cond_q);
+          mixed_predicted_steps = mixed_steps_for(mixed->cond_estimate);
+          *quality = std::min(*quality, quality_q);
+        } else {
+          mixed_predicted_steps = 1 << 30;
+        }
+      }
       if (*ok && mixed_predicted_steps <= 32) return;
       // Static rejection: the FP32 factor of the split-assembled S is not
       // predicted to converge in ≤ 32 refinements (or failed) — FP64 from here.
@@ -1259,15 +1274,16 @@ struct Handle {
     if (std::isfinite(res)) {
       for (int s = 0; s < cap; ++s) {
         d2d(dxbest.p, dx.p, m * sizeof(double));
+        if (n_eq) d2d(dybest.p, dyv.p, n_eq * sizeof(double));
         d2d(work_m.p, rho.p, m * sizeof(double));
-        solve_into(work_m.p);
+        solve_kkt_into(work_m.p, rho_p.p, eq_ddy.p);
         combine(m, dx.p, 1.0, work_m.p, st);
+        if (n_eq) combine(n_eq, dyv.p, 1.0, eq_ddy.p, st);
         dx_written();
         double corr = residual_norm_only();
         ++mixed_guard_steps;
         if (!std::isfinite(corr) || corr >= res) {
-          d2d(dx.p, dxbest.p, m * sizeof(double));
-          dx_written();
+          restore_dx_best();
           break;
         }
         res = corr;
@@ -1293,7 +1309,7 @@ struct Handle {
     factorize(&ok, &att, &q);
     if (!ok) throw CudaError("FP64 fallback factorisation failed");
     d2d(dx.p, r.p, m * sizeof(double));
-    solve_into(dx.p);
+    solve_kkt_into(dx.p, pv.p, dyv.p);
     dx_written();
   }
   // ρ = r − S·dx  (FP64 Newton operator)
@@ -2441,7 +2457,8 @@ struct Handle {
   // y.  p = b − Bᵀx, ρ_p = p − Bᵀdx.  The equality factor is either the
   // Cholesky of Q = B̂ᵀB̂ (eq_kind 1) or the column-pivoted QR of B̂ (eq_kind
   // 2, kept for the rest of the solve once used), B̂ = L_S⁻¹B·D with D the
-  // column scales.  FP64 precision only.
+  // column scales.  In mixed mode L_S is the FP32 factor and Q's Cholesky takes
+  // regularisation retries instead of the rank test.
   int n_eq = 0;
   DBuf<double> Beq, Beq0, beq;
   DBuf<double> yv, dyv, pv, rho_p, ybest, dybest, eq_dyh, eq_ddy, eq_q, eq_z, eq_tm;
@@ -2458,6 +2475,9 @@ struct Handle {
   bool eq_qr_sticky = false;
   void set_equality(int n, const double* hB, const double* hb);
   bool factor_equality(bool* rank_deficient);
+  bool factor_equality_mixed(double* cond_q, double* quality_q);
+  void equality_panel(const double* Li);
+  DBuf<double> Qs;
   void solve_kkt_into(double* vec, const double* prhs, double* dy_out);
   void eq_residual_terms();
 };
@@ -2527,8 +2547,6 @@ const char* sdpx_b200_last_error(const sdpx_b200_handle* h) { return h ? h->h.er
 int sdpx_b200_set_precision(sdpx_b200_handle* h, int mode) {
   GUARD(h, {
     if (mode != SDPX_B200_FP64 && mode != SDPX_B200_MIXED) throw std::invalid_argument("bad precision mode");
-    if (mode == SDPX_B200_MIXED && h->h.n_eq > 0)
-      throw std::invalid_argument("the mixed precision mode needs n == 0 equality rows");
     h->h.precision = mode;
     if (mode == SDPX_B200_MIXED) h->h.mixed_init();
   });

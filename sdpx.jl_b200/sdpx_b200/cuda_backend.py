@@ -182,10 +182,7 @@ class CudaBackend:
         self._keep = []     # host data has been copied to the device
         self.h = h
         if self.n > 0:
-            # Equality rows (SDPX `SDPProblem.B`, `.b`): FP64 precision mode only.
-            if precision == "mixed":
-                self.close()
-                raise NotImplementedError("the mixed precision mode needs n == 0 equality rows")
+            # Equality rows (SDPX `SDPProblem.B`, `.b`).
             Bm = np.asfortranarray(np.asarray(prob.B, dtype=np.float64).reshape(self.m, self.n))
             bv = np.ascontiguousarray(prob.b, dtype=np.float64)
             self._call("sdpx_b200_set_equality", self.n, _p(Bm), _p(bv))

@@ -156,6 +156,24 @@ def test_solve_matches_oracle(cuda):
     assert r.p_res < 1e-7 and r.d_res < 1e-7
 
 
-def test_mixed_precision_refuses_equality_rows(cuda):
-    with pytest.raises(NotImplementedError):
-        cuda(G.toy_t2(), precision="mixed")
+@pytest.mark.parametrize("build,opt", [
+    (lambda: G.sdpa_dense_equalities(m=80, blocks=[12, 6], lp=5, n_eq=5, seed=6), None),
+    (G.toy_t2, 5.5),
+])
+def test_mixed_precision_with_equality_rows(cuda, build, opt):
+    """Mixed mode (B̃ from the FP32 factor, Q in FP64 with regularisation
+    retries, guard against the FP64 KKT operator with the B terms) reaches
+    the FP64 path's optimum."""
+    prob = build()
+    opts = SolverOptions().with_tolerance(1e-8)
+    with cuda(prob, precision="fp64") as be:
+        r64 = solve_with_backend(be, opts)
+    with cuda(prob, precision="mixed") as be:
+        rm = solve_with_backend(be, SolverOptions(precision="mixed").with_tolerance(1e-8))
+    assert rm.status.value == r64.status.value == "Optimal"
+    assert abs(rm.pObj - r64.pObj) <= 1e-7 * max(1.0, abs(r64.pObj))
+    assert rm.p_res < 1e-7 and rm.d_res < 1e-7
+    if opt is not None:
+        assert abs(rm.pObj - opt) < 1e-6
+    else:
+        assert "mixed" in rm.precision_trace
