@@ -199,6 +199,23 @@ int sdpx_b200_original_residuals_eq(sdpx_b200_handle* h, const double* x, const 
                                     const double* y, const double* Y, double* p_res,
                                     double* d_res);
 
+/* ---- Adjoint of the solution map -----------------------------------------
+ * Gradient of L = ⟨wx, x⟩ + ⟨wy, y⟩ + Σ_l⟨WX_l, X_l⟩ + Σ_l⟨WY_l, Y_l⟩ at the
+ * current iterate with respect to the data c (m), b (n), C (stacked, Σk_l²)
+ * and the coefficients A_i for the nA indices in A_index (grad_A: nA stacked
+ * layouts, one per index, each Σk_l²).  SDPX has no adjoint: this is the
+ * implicit-function derivative of the HKM-linearised KKT conditions, reusing
+ * the Newton system's factor — call it after sdpx_b200_residuals (factor = 1),
+ * sdpx_b200_schur_build and sdpx_b200_factorize at the iterate, in the FP64
+ * precision mode.  Any seed may be NULL (zero); any output may be NULL.
+ *   λ from one KKT solve with right-hand side (wx + 𝒜ᵀWX − 𝒜ᵀG, −wy),
+ *   G = X⁻¹·sym(WY)·Y;  ∂L/∂c = −λx, ∂L/∂b = λy,
+ *   ∂L/∂C_l = sym(X⁻¹ΛY) − sym(WX_l − G_l) with Λ = mat(𝒜λx),
+ *   ∂L/∂A_i = λx_i·Y − x_i·∂L/∂C. */
+int sdpx_b200_adjoint(sdpx_b200_handle* h, const double* wx, const double* wy, const double* WX,
+                      const double* WY, double* grad_c, double* grad_b, double* grad_C,
+                      int32_t nA, const int32_t* A_index, double* grad_A);
+
 /* Restore the data as uploaded (undo sdpx_b200_equilibrate) and reset the
  * iterate to x = 0, X = Y = I, so one handle can run repeated solves. */
 int sdpx_b200_reset(sdpx_b200_handle* h);

@@ -878,6 +878,49 @@ class OracleBackend:
     def get_equality_direction(self):
         return self.dy.copy()
 
+    def adjoint(self, wx=None, wy=None, WX=None, WY=None, A_index=()):
+        """Gradient of L = ⟨wx, x⟩ + ⟨wy, y⟩ + Σ_l ⟨WX_l, X_l⟩ + Σ_l ⟨WY_l, Y_l⟩
+        at the current iterate with respect to c, b, C_l and the selected A_i,
+        through the Newton system the solver factors (the reference has no
+        adjoint; this restates the implicit-function derivative of the
+        linearised KKT conditions and is pinned by finite differences).
+
+        The HKM-linearised KKT map from data residuals (P, d, p) to (dx, dy) is
+        dX = 𝒜dx + P, dY = −sym(X⁻¹dX·Y), S·dx − B·dy = r with
+        r = −d − 𝒜ᵀ(X⁻¹PY), Bᵀdx = p.  With G = X⁻¹·sym(WY)·Y the seed on dx is
+        w = wx + 𝒜ᵀWX − 𝒜ᵀG, one KKT solve with right-hand side (w, −wy) gives
+        λx = dx and λy = −dy, and with Λ = mat(𝒜λx):
+            ∂L/∂c = −λx,  ∂L/∂b = λy,
+            ∂L/∂C_l = sym(X⁻¹ΛY) − sym(WX − G),
+            ∂L/∂A_i = λx_i·Y − x_i·∂L/∂C  (per block)."""
+        L = len(self.k)
+        w = np.zeros(self.m) if wx is None else np.array(wx, dtype=np.float64)
+        D = []
+        for l in range(L):
+            kl = self.k[l]
+            Dl = np.zeros((kl, kl))
+            if WX is not None:
+                Dl = Dl + WX[l]
+                w = w + self._accumulate(l, WX[l])
+            if WY is not None:
+                Ws = symmetrize(np.asarray(WY[l], dtype=np.float64))
+                Gl = kcholsolve(self.LX[l], Ws @ self.Y[l])
+                Dl = Dl - Gl
+                w = w - self._accumulate(l, Gl)
+            D.append(Dl)
+        pr = None
+        if self.n:
+            pr = -(np.zeros(self.n) if wy is None else np.asarray(wy, dtype=np.float64))
+        lx, mdy = self._solve(w, pr)
+        ly = -mdy if self.n else np.zeros(0)
+        gC = []
+        for l in range(L):
+            Lam = self._buildP(l, lx)
+            Z = kcholsolve(self.LX[l], Lam @ self.Y[l])
+            gC.append(symmetrize(Z) - symmetrize(D[l]))
+        gA = [[lx[i] * self.Y[l] - self.x[i] * gC[l] for l in range(L)] for i in A_index]
+        return dict(grad_c=-lx, grad_b=ly, grad_C=gC, grad_A=gA, lambda_x=lx, lambda_y=ly)
+
     def equality_info(self):
         """(kind, rank, quality) of the current equality factor."""
         if self.eq is None:

@@ -2476,6 +2476,11 @@ struct Handle {
   void set_equality(int n, const double* hB, const double* hb);
   bool factor_equality(bool* rank_deficient);
   bool factor_equality_mixed(double* cond_q, double* quality_q);
+  // ------------------------------------------------ adjoint (adjoint_api.inc)
+  DBuf<double> adj_D, adj_W, adj_G, adj_L, adj_Z, adj_zero, adj_w, adj_p, adj_dy;
+  void adj_xinv_m_y(const double* Mst, double* Zout);
+  void adjoint(const double* hwx, const double* hwy, const double* hWX, const double* hWY,
+               double* gc, double* gb, double* gC, int nA, const int32_t* Aidx, double* gA);
   void equality_panel(const double* Li);
   DBuf<double> Qs;
   void solve_kkt_into(double* vec, const double* prhs, double* dy_out);
@@ -2488,6 +2493,7 @@ struct Handle {
 // equality_api.inc (same translation unit).
 #include "mixed_api.inc"
 #include "equality_api.inc"
+#include "adjoint_api.inc"
 
 // ============================================================================
 //                                   C ABI
@@ -2755,6 +2761,11 @@ int sdpx_b200_equality_info(sdpx_b200_handle* h, int* kind, int* rank, double* q
     if (rank) *rank = h->h.eq_rank;
     if (quality) *quality = h->h.eq_quality;
   });
+}
+int sdpx_b200_adjoint(sdpx_b200_handle* h, const double* wx, const double* wy, const double* WX,
+                      const double* WY, double* grad_c, double* grad_b, double* grad_C,
+                      int32_t nA, const int32_t* A_index, double* grad_A) {
+  GUARD(h, h->h.adjoint(wx, wy, WX, WY, grad_c, grad_b, grad_C, nA, A_index, grad_A));
 }
 int sdpx_b200_reset(sdpx_b200_handle* h) { GUARD(h, h->h.reset()); }
 int sdpx_b200_get_precision(sdpx_b200_handle* h, int* mode, int* fallbacks, double* cond_estimate) {

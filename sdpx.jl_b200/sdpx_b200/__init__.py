@@ -16,7 +16,7 @@ from .driver import SDPResult, Status, solve_with_backend
 from .problem import Equilibration, SDPProblem, ingest, unequilibrate
 
 __all__ = ["SolverOptions", "SDPResult", "Status", "SDPProblem", "Equilibration", "ingest",
-           "unequilibrate", "solve", "solve_with_backend", "certificate"]
+           "unequilibrate", "solve", "solve_with_backend", "certificate", "adjoint"]
 
 
 def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
@@ -41,6 +41,23 @@ def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
             result.certificate = be.certificate(result.x, result.X, result.Y, opts.eps_primal,
                                                 opts.eps_dual, opts.eps_gap, y=result.y)
         return result
+
+
+def adjoint(prob: SDPProblem, result: SDPResult, *, wx=None, wy=None, WX=None, WY=None,
+            A_index=(), device: int = 0) -> dict:
+    """Gradient of L = ⟨wx, x⟩ + ⟨wy, y⟩ + Σ⟨WX_l, X_l⟩ + Σ⟨WY_l, Y_l⟩ at the
+    returned solution with respect to the original data c, b, C and the
+    coefficients A_i of `A_index` (no counterpart in SDPX).  The Newton system
+    is factored once more at the solution, on the original (unscaled) data in
+    FP64, and one KKT solve gives every gradient (sdpx_b200_adjoint)."""
+    from .cuda_backend import CudaBackend
+    with CudaBackend(prob, precision="fp64", device=device) as be:
+        be.set_iterate(result.x, result.X, result.Y, y=result.y)
+        be.compute_residuals([0.0] * prob.L, True, True)
+        be.schur_build()
+        if not be.factorize()["ok"]:
+            raise RuntimeError("the Newton system at the solution could not be factored")
+        return be.adjoint(wx, wy, WX, WY, A_index)
 
 
 def certificate(prob: SDPProblem, result: SDPResult, *, eps_primal: float = 1e-10,

@@ -107,6 +107,8 @@ _SIGS = {
     "sdpx_b200_set_multipliers": [C.c_void_p, _dp],
     "sdpx_b200_equality_info": [C.c_void_p, _ip, _ip, _dp],
     "sdpx_b200_original_residuals_eq": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp],
+    "sdpx_b200_adjoint": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int32,
+                          C.POINTER(C.c_int32), _dp],
     "sdpx_b200_certificate_eq": [C.c_void_p, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
                                  C.c_double, C.c_int32, C.POINTER(CertificateResult)],
 }
@@ -289,6 +291,26 @@ class CudaBackend:
             raise NotImplementedError(f"equality_solver={solver!r}")
         self._call("sdpx_b200_set_equality_options", float(requested_accuracy),
                    0 if solver == "auto" else 1)
+
+    def adjoint(self, wx=None, wy=None, WX=None, WY=None, A_index=()):
+        """Gradient of ⟨wx, x⟩ + ⟨wy, y⟩ + Σ⟨WX_l, X_l⟩ + Σ⟨WY_l, Y_l⟩ at the current
+        iterate (after residuals with factors, schur_build and factorize) with
+        respect to c, b, C and the A_i of `A_index` (see sdpx_b200_adjoint)."""
+        def vec(a, size):
+            return None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(size)
+        wxv, wyv = vec(wx, self.m), (vec(wy, self.n) if self.n else None)
+        WXs = None if WX is None else self._join(WX)
+        WYs = None if WY is None else self._join(WY)
+        idx = np.ascontiguousarray(A_index, dtype=np.int32)
+        gc, gb, gC = np.zeros(self.m), np.zeros(self.n), np.zeros(self.Ku)
+        gA = np.zeros(max(1, idx.size) * self.Ku)
+        ptr = lambda a: None if a is None else _p(a)
+        self._call("sdpx_b200_adjoint", ptr(wxv), ptr(wyv), ptr(WXs), ptr(WYs), _p(gc),
+                   _p(gb) if self.n else None, _p(gC), int(idx.size),
+                   idx.ctypes.data_as(C.POINTER(C.c_int32)), _p(gA))
+        return dict(grad_c=gc, grad_b=gb, grad_C=self._split(gC),
+                    grad_A=[self._split(gA[q * self.Ku:(q + 1) * self.Ku])
+                            for q in range(idx.size)])
 
     def equality_info(self):
         """(kind, rank, quality) of the current equality factor."""
