@@ -9,7 +9,9 @@ mode; the plain FP64 device path is timed on the same instance for the
 mixed-vs-FP64 ratio.  Inputs (3.2 GB of constraint data) are larger than L2.
 The line also carries `equality_rows`: the same instance with 64 equality rows
 Bᵀx = b solved on the FP64 path, and the device time of the equality factor
-beside the oracle's host time for the same factor work.
+beside the oracle's host time for the same factor work, and `adjoint`: forward
+solves to 1e-9 plus gradients on instances of the differentiable-SDP shape
+(m = 500, one block n = 200).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -54,6 +56,10 @@ CPU_ITERATIONS_M2000 = 15  # CPU restatement, seed 0, tolerance 1e-8 (measured: 
 # Equality rows added to the workload for the n > 0 measurement (Bᵀx = b with
 # B ~ N(0,1) and b = Bᵀy0 at the generator's strictly feasible point).
 EQ_ROWS = 64
+# Differentiable parametric SDP (SDPA-form generator, one PSD block n = 200,
+# m = 500, forward solve to 1e-9): gradient of ⟨W, X_sdpa⟩ + ⟨v, y_sdpa⟩,
+# i.e. of ⟨W, Y⟩ + ⟨v, x⟩ in SDPX's form, w.r.t. c, C and A_1..A_10.
+ADJ_WORKLOAD = dict(m=500, blocks=[200], lp=0, instances=4, A_count=10)
 
 
 def schur_flops(m, blocks, lp):
@@ -215,6 +221,71 @@ def cpu_sample(prob, blocks, lp, gpu_iterations):
                    p.backtracking_factor, p.minimum_step, math.sqrt(2.220446049250313e-16))
     t_iter = time.perf_counter() - t0
     return t_iter
+
+
+def bench_adjoint(args, world, rank, local):
+    """Forward solve to 1e-9 plus the adjoint gradient on a few instances of the
+    differentiable-SDP shape; device times with CUDA events, the oracle's
+    adjoint (same factor-at-solution + one KKT solve) timed beside it."""
+    import numpy as np
+    import torch
+    from sdpx_b200 import SolverOptions, adjoint, generators as G
+    from sdpx_b200.cuda_backend import CudaBackend
+    from sdpx_b200.driver import solve_with_backend
+    wl = ADJ_WORKLOAD
+    solve_s, adj_s, iters = [], [], []
+    last = None
+    for inst in range(wl["instances"]):
+        prob = G.sdpa_dense(m=wl["m"], blocks=wl["blocks"], lp=wl["lp"],
+                            seed=1000 + 64 * rank + inst)
+        rng = np.random.default_rng(inst)
+        v = rng.standard_normal(prob.m)
+        Wm = rng.standard_normal((prob.k[0], prob.k[0]))
+        W = [Wm + Wm.T]
+        with CudaBackend(prob, precision="fp64", device=local) as be:
+            st = torch.cuda.ExternalStream(be.stream_handle())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st)
+            r = solve_with_backend(be, SolverOptions(precision="fp64").with_tolerance(1e-9))
+            e1.record(st)
+            torch.cuda.synchronize()
+            solve_s.append(e0.elapsed_time(e1) / 1000.0)
+            iters.append(r.iterations)
+            t0 = time.perf_counter()
+            be.reset()
+            be.set_iterate(r.x, r.X, r.Y)
+            be.compute_residuals([0.0] * prob.L, True, True)
+            be.schur_build()
+            be.factorize()
+            g = be.adjoint(wx=v, WY=W, A_index=tuple(range(wl["A_count"])))
+            torch.cuda.synchronize()
+            adj_s.append(time.perf_counter() - t0)
+        last = (prob, r, v, W, g)
+    out = {"workload": (f"differentiable SDP: {wl['instances']} instances, m={wl['m']}, one PSD "
+                        f"block n={wl['blocks'][0]}, forward to 1e-9, gradient of "
+                        f"<W, X_sdpa> + <v, y_sdpa> w.r.t. c, C, A_1..A_{wl['A_count']}"),
+           "forward_s_per_instance": statistics.median(solve_s),
+           "adjoint_s_per_instance": statistics.median(adj_s),
+           "iterations": iters, "unit": "s",
+           "adjoint_includes": "refactor at the solution (residuals, Schur build, FP64 "
+                               "Cholesky) + one KKT solve + gradient passes + host copies"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.sdpx_oracle import OracleBackend
+        prob, r, v, W, g = last
+        t0 = time.perf_counter()
+        ob = OracleBackend(prob)
+        ob.set_iterate(r.x, r.X, r.Y)
+        ob.compute_residuals([0.0] * prob.L, True, True)
+        ob.schur_build()
+        ob.factorize()
+        go = ob.adjoint(wx=v, WY=W, A_index=tuple(range(wl["A_count"])))
+        out["cpu_adjoint_s"] = time.perf_counter() - t0
+        out["cpu_kind"] = "port: the oracle's adjoint (NumPy/OpenBLAS, all host cores)"
+        out["max_rel_diff_grad_C_vs_cpu"] = float(
+            np.max(np.abs(g["grad_C"][0] - go["grad_C"][0])) /
+            max(1.0, float(np.max(np.abs(go["grad_C"][0])))))
+    return out
 
 
 def eq_cpu_sample(m, n, seed=0):
@@ -487,6 +558,7 @@ def run_ours(args, world, rank, local):
         e1.record(seq)
         torch.cuda.synchronize()
         eqm_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
+    adjoint_line = bench_adjoint(args, world, rank, local)
     equality = {"n": EQ_ROWS, "value": eq_s, "unit": "s", "iterations": req.iterations,
                 "status": req.status.value, "objective": req.pObj,
                 "p_res": req.p_res, "d_res": req.d_res, "path": "fp64",
@@ -621,6 +693,7 @@ def run_ours(args, world, rank, local):
             "clocks": clock_info,
             "normal_lp_soc": normal,
             "equality_rows": equality,
+            "adjoint": adjoint_line,
         }
         print(json.dumps(line), flush=True)
     return line
