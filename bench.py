@@ -65,6 +65,10 @@ EQ_ROWS = 64
 # NumericalBreakdown near a 2e-11 gap with X's smallest eigenvalues at 5e-13,
 # where the linearised KKT system has no meaningful derivative.
 ADJ_WORKLOAD = dict(m=500, blocks=[200], lp=0, instances=4, A_count=10, tol=1e-7)
+# Batch of small SDPs of uneven size (block n ~ U{4..64}, m ~ U{3..min(200,
+# n(n+1)/2)}): a bounded slice of the 4096-instance workload, solved
+# concurrently (one handle and stream per instance) and as a serial loop.
+BATCH_WORKLOAD = dict(instances=256, serial_sample=32, threads=16, tol=1e-8)
 
 
 def schur_flops(m, blocks, lp):
@@ -226,6 +230,36 @@ def cpu_sample(prob, blocks, lp, gpu_iterations):
                    p.backtracking_factor, p.minimum_step, math.sqrt(2.220446049250313e-16))
     t_iter = time.perf_counter() - t0
     return t_iter
+
+
+def bench_batch(args, world, rank, local):
+    """Wall-clock throughput of a concurrent batch (host threads, one device
+    handle and stream per instance) against the per-instance serial loop."""
+    import torch
+    from sdpx_b200 import batch_instances, solve_batch
+    wl = BATCH_WORKLOAD
+    probs = batch_instances(wl["instances"], seed=rank)
+    solve_batch(probs[:wl["threads"]], tolerance=wl["tol"], threads=wl["threads"], device=local)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = solve_batch(probs, tolerance=wl["tol"], threads=wl["threads"], device=local)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ser = solve_batch(probs[:wl["serial_sample"]], tolerance=wl["tol"], threads=1, device=local)
+    torch.cuda.synchronize()
+    t_serial = time.perf_counter() - t0
+    same = all(a.pObj == b.pObj and a.iterations == b.iterations
+               for a, b in zip(res[:wl["serial_sample"]], ser))
+    return {"workload": (f"{wl['instances']} small dense SDPs, block n ~ U{{4..64}}, "
+                         f"m ~ U{{3..min(200, n(n+1)/2)}}, to {wl['tol']:g}"),
+            "value": wl["instances"] / t_batch, "unit": "instances/s",
+            "threads": wl["threads"], "timing": "wall clock (host threads, several streams)",
+            "serial_loop_instances_per_s": wl["serial_sample"] / t_serial,
+            "speedup_vs_serial_loop": (wl["instances"] / t_batch) /
+                                      (wl["serial_sample"] / t_serial),
+            "optimal": sum(r.status.value == "Optimal" for r in res),
+            "serial_results_identical": same}
 
 
 def bench_adjoint(args, world, rank, local):
@@ -584,6 +618,7 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         eqm_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
     adjoint_line = bench_adjoint(args, world, rank, local)
+    batch_line = bench_batch(args, world, rank, local)
     equality = {"n": EQ_ROWS, "value": eq_s, "unit": "s", "iterations": req.iterations,
                 "status": req.status.value, "objective": req.pObj,
                 "p_res": req.p_res, "d_res": req.d_res, "path": "fp64",
@@ -719,6 +754,7 @@ def run_ours(args, world, rank, local):
             "normal_lp_soc": normal,
             "equality_rows": equality,
             "adjoint": adjoint_line,
+            "batch": batch_line,
         }
         print(json.dumps(line), flush=True)
     return line

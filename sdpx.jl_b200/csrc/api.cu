@@ -40,14 +40,17 @@ static std::mutex g_attr_mu;
 static std::map<std::pair<const void*, int>, size_t> g_attr_done;
 // True when `kern` on the current device has not yet been opted in to at
 // least `bytes` of dynamic shared memory (records the new size).
-bool smem_attr_needed(const void* kern, size_t bytes) {
+// Raises the kernel's dynamic shared-memory limit on the current device once.
+// The attribute is set while the lock is held, so a concurrent caller never
+// sees the kernel recorded before the attribute is in place.
+void smem_attr_ensure(const void* kern, size_t bytes) {
   int dev = 0;
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lk(g_attr_mu);
   size_t& have = g_attr_done[{kern, dev}];
-  if (have >= bytes) return false;
+  if (have >= bytes) return;
+  SDPX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   have = bytes;
-  return true;
 }
 
 

@@ -176,12 +176,11 @@ enum KRange : int {
 };
 
 // Per-(kernel, device) one-time opt-in to large dynamic shared memory.
-bool smem_attr_needed(const void* kern, size_t bytes);  // defined in api.cu
+void smem_attr_ensure(const void* kern, size_t bytes);  // defined in api.cu
 template <class Kern>
 inline void ensure_smem(Kern kern, size_t bytes) {
   if (bytes <= 48 * 1024) return;
-  if (smem_attr_needed((const void*)kern, bytes))
-    SDPX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  smem_attr_ensure((const void*)kern, bytes);
 }
 
 }  // namespace sdpx

@@ -7,6 +7,9 @@ Public surface mirrors SDPX's qualified entry points:
 * `certificate(prob, result)` ↔ `result_certificate(prob, result)` (src/validation.jl:948)
 * `normal.NormalSystem`     ↔ the LP standard-form reduced system and Lorentz NT
   scaling (src/lp_solver.jl, src/soc_lorentz_kernels.jl, src/soc_native.jl)
+* `adjoint(prob, result, …)` gradients of a loss of the solution with respect
+  to the data, and `batch.solve_batch` for many independent instances (no
+  counterpart in SDPX)
 
 `solve` runs on the CUDA backend (`libsdpx_b200.so`, sm_100a) and raises if
 the library or a GPU is unavailable; there is no CPU fallback.
@@ -14,9 +17,11 @@ the library or a GPU is unavailable; there is no CPU fallback.
 from .controller import SolverOptions
 from .driver import SDPResult, Status, solve_with_backend
 from .problem import Equilibration, SDPProblem, ingest, unequilibrate
+from .batch import batch_instances, solve_batch
 
 __all__ = ["SolverOptions", "SDPResult", "Status", "SDPProblem", "Equilibration", "ingest",
-           "unequilibrate", "solve", "solve_with_backend", "certificate", "adjoint"]
+           "unequilibrate", "solve", "solve_with_backend", "certificate", "adjoint",
+           "solve_batch", "batch_instances"]
 
 
 def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
