@@ -65,6 +65,7 @@ static const double kSqrtEps = std::sqrt(2.220446049250313e-16);
 int mixed_steps_for(double cond);  // mixed_api.inc
 
 struct Handle {
+  dcache::ReleaseScope release_scope;  // first member: destroyed after every buffer
   int dev = 0;
   cudaStream_t st = nullptr;
   int sms = 148;
@@ -251,6 +252,9 @@ struct Handle {
   }
 
   ~Handle() {
+    // All of the handle's device work runs on st: once st is idle its buffers
+    // can return to the cache without a device-wide synchronisation.
+    if (st && cudaStreamSynchronize(st) == cudaSuccess) release_scope.begin();
     for (auto& row : kt_ev)
       for (auto e : row)
         if (e) cudaEventDestroy(e);

@@ -7,9 +7,13 @@
 // A request takes an idle block of the same device whose size is within
 // [bytes, 1.25·bytes + 1 MB]; otherwise it calls cudaMalloc, and when that
 // fails the device's idle blocks are freed and the call is retried.  A block
-// enters the cache only after a device synchronisation (the same guarantee
-// cudaFree gives: no queued work still uses it).  Idle blocks of a device are
-// capped at kIdleCap bytes; sdpx_b200_trim_device_cache() returns them all.
+// enters the cache only once no queued work still uses it (the guarantee
+// cudaFree gives): after a device synchronisation, or — while an owner that
+// issues all its work on one stream releases its buffers after synchronising
+// that stream (ReleaseScope) — without one, so that tearing down one solve
+// does not wait for the work of concurrent solves on other streams.  Idle
+// blocks of a device are capped at kIdleCap bytes;
+// sdpx_b200_trim_device_cache() returns them all.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -35,6 +39,13 @@ struct Cache {
 inline Cache& cache() {
   static Cache c;
   return c;
+}
+
+// True on this thread while an owner whose only stream is synchronised
+// releases its buffers.
+inline bool& owner_synced() {
+  static thread_local bool flag = false;
+  return flag;
 }
 
 // Frees every idle block of `dev` (all devices when dev < 0).
@@ -98,7 +109,7 @@ inline void put(void* p, size_t bytes, int dev) {
   int cur = 0;
   cudaGetDevice(&cur);
   if (cur != dev) cudaSetDevice(dev);
-  cudaDeviceSynchronize();
+  if (!owner_synced()) cudaDeviceSynchronize();
   Cache& c = cache();
   bool keep = false;
   {
@@ -112,6 +123,15 @@ inline void put(void* p, size_t bytes, int dev) {
   if (!keep) cudaFree(p);
   if (cur != dev) cudaSetDevice(cur);
 }
+
+// Declared as an owner's first member (so destroyed last): the owner's
+// destructor synchronises its stream and calls begin(); the buffers released
+// by the members destroyed after that skip the device synchronisation, and
+// this member's destructor ends the scope.
+struct ReleaseScope {
+  void begin() { owner_synced() = true; }
+  ~ReleaseScope() { owner_synced() = false; }
+};
 
 }  // namespace dcache
 
