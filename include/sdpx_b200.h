@@ -216,6 +216,71 @@ int sdpx_b200_adjoint(sdpx_b200_handle* h, const double* wx, const double* wy, c
                       const double* WY, double* grad_c, double* grad_b, double* grad_C,
                       int32_t nA, const int32_t* A_index, double* grad_A);
 
+/* ---- The whole interior-point solve inside the library -------------------
+ * SDPX's `_solve_pipeline!` for the dense route (src/solver/interior_point.jl:
+ * 3131-3571: Ruiz scaling, KKT cold start :699-1287, core loop :1323-2687 with
+ * `newton_step!` src/step.jl:643-1023, the guarded Mehrotra controller
+ * src/adaptive_parameters.jl and the stagnation detector src/stagnation.jl,
+ * unscaling and original-coordinate residuals) run on the host side of the
+ * library: one call per solve, or begin / one loop pass per newton_step / end. */
+typedef struct {
+  double beta, gamma, omega_p, omega_d, eps_gap, eps_primal, eps_dual;
+  int32_t iter_max, restart;
+  double min_step, omega_step;
+  int32_t max_restarts, max_centering, stall_iterations;
+  double stall_tolerance;
+  int32_t step_rule;         /* 0 auto, 1 backtrack, 2 fraction to boundary      */
+  int32_t refine_steps;
+  int32_t refine_policy;     /* 0 fixed, 1 adaptive, 2 auto                      */
+  int32_t refine_max_steps;
+  double refine_tol, max_time;
+  int32_t parameter_policy;  /* 0 auto (KKT cold start), 1 fixed start           */
+  int32_t parameter_strategy; /* 0 adaptive, 1 fixed                             */
+  double adaptive_sigma_max;
+  int32_t scaling;           /* 0 auto, 1 none, 2 equilibrate                    */
+  int32_t precision;         /* SDPX_B200_FP64 or SDPX_B200_MIXED                */
+  int32_t equality_solver;   /* 0 automatic, 1 rank-revealing QR                 */
+} sdpx_b200_solve_options;
+
+#define SDPX_B200_STATUS_OPTIMAL 1
+#define SDPX_B200_STATUS_ITER_LIMIT 2
+#define SDPX_B200_STATUS_STALLED 3
+#define SDPX_B200_STATUS_INSUFFICIENT_PRECISION 4
+#define SDPX_B200_STATUS_NUMERICAL_BREAKDOWN 5
+#define SDPX_B200_STATUS_MAX_RESTARTS 6
+#define SDPX_B200_STATUS_TIME_LIMIT 7
+
+typedef struct {
+  int32_t status;            /* SDPX_B200_STATUS_*                               */
+  int32_t iterations, restarts;
+  int32_t mixed_iterations, fp64_iterations;
+  double p_obj, d_obj;       /* original data                                    */
+  double p_res, d_res;       /* original data                                    */
+  double seconds;
+  char message[256];
+} sdpx_b200_solve_result;
+
+/* SDPX's SolverOptions{Float64} defaults (src/types/workspaces.jl:101-185),
+ * tolerances 1e-10. */
+void sdpx_b200_default_options(sdpx_b200_solve_options* opts);
+int sdpx_b200_optimize(sdpx_b200_handle* h, const sdpx_b200_solve_options* opts,
+                       sdpx_b200_solve_result* result);
+int sdpx_b200_optimize_begin(sdpx_b200_handle* h, const sdpx_b200_solve_options* opts);
+/* One pass of the loop body: termination tests, then one Newton step with step
+ * length and update (a1–a13), or a restart / centering / FP64-switch pass.
+ * running = 0 once the loop has ended. */
+int sdpx_b200_newton_step(sdpx_b200_handle* h, int32_t* running, int32_t* iteration,
+                          double* p_obj, double* d_obj, double* p_res, double* d_res);
+int sdpx_b200_optimize_end(sdpx_b200_handle* h, sdpx_b200_solve_result* result);
+/* The solution of the last sdpx_b200_optimize(_end), original coordinates
+ * (stacked X, Y; y of length n).  Any pointer may be NULL. */
+int sdpx_b200_get_solution(sdpx_b200_handle* h, double* x, double* X, double* y, double* Y);
+/* Loop state after begin or a step: pObj, dObj, p_res, d_res (working
+ * data), the primal and dual residual scales, the gap tolerance and Σ⟨X_l,Y_l⟩. */
+int sdpx_b200_loop_state(sdpx_b200_handle* h, double* out8);
+/* Precision of each Newton step of the last solve: 1 mixed, 0 FP64. */
+int sdpx_b200_get_trace(sdpx_b200_handle* h, int32_t* modes, int32_t capacity, int32_t* count);
+
 /* Restore the data as uploaded (undo sdpx_b200_equilibrate) and reset the
  * iterate to x = 0, X = Y = I, so one handle can run repeated solves. */
 int sdpx_b200_reset(sdpx_b200_handle* h);

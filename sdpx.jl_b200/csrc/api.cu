@@ -10,6 +10,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <deque>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -2501,6 +2504,7 @@ struct Handle {
 #include "mixed_api.inc"
 #include "equality_api.inc"
 #include "adjoint_api.inc"
+#include "driver_api.inc"
 
 // ============================================================================
 //                                   C ABI
@@ -2509,6 +2513,7 @@ using sdpx::Handle;
 
 struct sdpx_b200_handle {
   Handle h;
+  std::unique_ptr<sdpx::CoreLoop> loop;  // declared after h: destroyed first
 };
 
 static thread_local std::string g_create_error;
@@ -2773,6 +2778,107 @@ int sdpx_b200_adjoint(sdpx_b200_handle* h, const double* wx, const double* wy, c
                       const double* WY, double* grad_c, double* grad_b, double* grad_C,
                       int32_t nA, const int32_t* A_index, double* grad_A) {
   GUARD(h, h->h.adjoint(wx, wy, WX, WY, grad_c, grad_b, grad_C, nA, A_index, grad_A));
+}
+void sdpx_b200_default_options(sdpx_b200_solve_options* o) {
+  if (!o) return;
+  *o = sdpx_b200_solve_options{};
+  o->beta = 0.1;
+  o->gamma = 0.9;
+  o->omega_p = o->omega_d = 1.0;
+  o->eps_gap = o->eps_primal = o->eps_dual = 1e-10;
+  o->iter_max = 200;
+  o->restart = 1;
+  o->min_step = 1e-10;
+  o->omega_step = 1e5;
+  o->max_restarts = 5;
+  o->max_centering = 4;
+  o->stall_iterations = 15;
+  o->stall_tolerance = 1e-3;
+  o->step_rule = 0;
+  o->refine_steps = 1;
+  o->refine_policy = 2;
+  o->refine_max_steps = 8;
+  o->refine_tol = 0.0;
+  o->max_time = INFINITY;
+  o->parameter_policy = 0;
+  o->parameter_strategy = 0;
+  o->adaptive_sigma_max = 0.0;
+  o->scaling = 0;
+  o->precision = SDPX_B200_FP64;
+  o->equality_solver = 0;
+}
+int sdpx_b200_optimize_begin(sdpx_b200_handle* h, const sdpx_b200_solve_options* o) {
+  GUARD(h, {
+    if (!o) throw std::invalid_argument("options are required");
+    h->h.reset();
+    h->loop = std::make_unique<sdpx::CoreLoop>(h->h);
+    h->loop->begin(*o);
+  });
+}
+int sdpx_b200_newton_step(sdpx_b200_handle* h, int32_t* running, int32_t* iteration,
+                          double* p_obj, double* d_obj, double* p_res, double* d_res) {
+  GUARD(h, {
+    if (!h->loop) throw std::logic_error("sdpx_b200_optimize_begin was not called");
+    const bool more = h->loop->step();
+    if (running) *running = more ? 1 : 0;
+    if (iteration) *iteration = h->loop->iter;
+    if (p_obj) *p_obj = h->loop->pObj;
+    if (d_obj) *d_obj = h->loop->dObj;
+    if (p_res) *p_res = h->loop->p_res;
+    if (d_res) *d_res = h->loop->d_res;
+  });
+}
+int sdpx_b200_optimize_end(sdpx_b200_handle* h, sdpx_b200_solve_result* out) {
+  GUARD(h, {
+    if (!h->loop) throw std::logic_error("sdpx_b200_optimize_begin was not called");
+    if (!out) throw std::invalid_argument("result is required");
+    while (h->loop->step()) {
+    }
+    h->loop->end(out);
+  });
+}
+int sdpx_b200_optimize(sdpx_b200_handle* h, const sdpx_b200_solve_options* o,
+                       sdpx_b200_solve_result* out) {
+  GUARD(h, {
+    if (!o || !out) throw std::invalid_argument("options and result are required");
+    h->h.reset();
+    h->loop = std::make_unique<sdpx::CoreLoop>(h->h);
+    h->loop->begin(*o);
+    while (h->loop->step()) {
+    }
+    h->loop->end(out);
+  });
+}
+int sdpx_b200_loop_state(sdpx_b200_handle* h, double* out8) {
+  GUARD(h, {
+    if (!h->loop) throw std::logic_error("sdpx_b200_optimize_begin was not called");
+    auto& L = *h->loop;
+    out8[0] = L.pObj;
+    out8[1] = L.dObj;
+    out8[2] = L.p_res;
+    out8[3] = L.d_res;
+    out8[4] = L.scale_p;
+    out8[5] = L.scale_d;
+    out8[6] = L.term_tol;
+    out8[7] = L.current_compl;
+  });
+}
+int sdpx_b200_get_solution(sdpx_b200_handle* h, double* x, double* X, double* y, double* Y) {
+  GUARD(h, {
+    if (!h->loop || h->loop->sx.empty()) throw std::logic_error("no solution: optimize first");
+    auto& L = *h->loop;
+    if (x) std::memcpy(x, L.sx.data(), L.sx.size() * sizeof(double));
+    if (X) std::memcpy(X, L.sX.data(), L.sX.size() * sizeof(double));
+    if (y && !L.sy.empty()) std::memcpy(y, L.sy.data(), L.sy.size() * sizeof(double));
+    if (Y) std::memcpy(Y, L.sY.data(), L.sY.size() * sizeof(double));
+  });
+}
+int sdpx_b200_get_trace(sdpx_b200_handle* h, int32_t* modes, int32_t cap, int32_t* count) {
+  GUARD(h, {
+    const int n = h->loop ? (int)h->loop->trace.size() : 0;
+    if (count) *count = n;
+    for (int i = 0; i < n && i < cap && modes; ++i) modes[i] = h->loop->trace[i];
+  });
 }
 int sdpx_b200_reset(sdpx_b200_handle* h) { GUARD(h, h->h.reset()); }
 int sdpx_b200_get_precision(sdpx_b200_handle* h, int* mode, int* fallbacks, double* cond_estimate) {

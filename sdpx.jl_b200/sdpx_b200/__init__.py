@@ -26,7 +26,8 @@ __all__ = ["SolverOptions", "SDPResult", "Status", "SDPProblem", "Equilibration"
 
 def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
           maximum_iterations: int = 200, scaling: str = "auto", device: int = 0,
-          trace=None, certificate: bool = False, **kwargs) -> SDPResult:
+          trace=None, certificate: bool = False, driver: str = "native",
+          **kwargs) -> SDPResult:
     """Solve `prob` on the B200 (mirrors `SDPX.solve(prob; tolerance)`).
 
     `precision="fp64"` is the plain FP64 device path; `precision="mixed"`
@@ -34,14 +35,19 @@ def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
     it in FP32 and refines the Newton system in FP64, switching to the FP64 path
     when the condition estimate or the stagnation detector calls for it.
     `certificate=True` attaches the device-computed cold-path certificate
-    (`result.certificate`) before the device data is released.
+    (`result.certificate`) before the device data is released.  The loop runs
+    inside the library (`driver="native"`, sdpx_b200_optimize) unless
+    `driver="python"` or a `trace` list asks for the Python driver.
     """
     from .cuda_backend import CudaBackend
     opts = SolverOptions(iter_max=maximum_iterations, scaling=scaling, precision=precision,
                          **kwargs).with_tolerance(tolerance)
     with CudaBackend(prob, precision=precision, device=device,
                      condition_limit=opts.mixed_condition_limit) as be:
-        result = solve_with_backend(be, opts, trace=trace)
+        if driver == "native" and trace is None:
+            result = be.optimize(opts)
+        else:
+            result = solve_with_backend(be, opts, trace=trace)
         if certificate:
             result.certificate = be.certificate(result.x, result.X, result.Y, opts.eps_primal,
                                                 opts.eps_dual, opts.eps_gap, y=result.y)

@@ -35,15 +35,18 @@ def batch_instances(count: int, seed: int = 0, n_range=(4, 64), m_cap: int = 200
 
 def solve_batch(problems: Sequence[SDPProblem], *, tolerance: float = 1e-8,
                 precision: str = "fp64", threads: int = 8, device: int = 0,
-                **kwargs) -> List[SDPResult]:
+                driver: str = "native", **kwargs) -> List[SDPResult]:
     """Solve every problem (one handle each, `threads` concurrent solves);
-    results in input order."""
+    results in input order.  With the native driver the whole loop runs inside
+    the library, so the threads hold the GIL only to start and collect."""
     from .cuda_backend import CudaBackend
     opts = SolverOptions(precision=precision, **kwargs).with_tolerance(tolerance)
 
     def one(prob):
         with CudaBackend(prob, precision=precision, device=device,
                          condition_limit=opts.mixed_condition_limit) as be:
+            if driver == "native":
+                return be.optimize(opts)
             return solve_with_backend(be, opts)
 
     if threads <= 1:

@@ -48,6 +48,49 @@ CERTIFICATE_FAILURES = (
     (8, "primal_block_backward_error"), (16, "dual_residual"), (32, "dual_backward_error"),
     (64, "duality_gap"), (128, "primal_psd"), (256, "dual_psd"))
 
+class SolveOptions(C.Structure):
+    """`sdpx_b200_solve_options` (include/sdpx_b200.h)."""
+    _fields_ = [("beta", C.c_double), ("gamma", C.c_double), ("omega_p", C.c_double),
+                ("omega_d", C.c_double), ("eps_gap", C.c_double), ("eps_primal", C.c_double),
+                ("eps_dual", C.c_double), ("iter_max", C.c_int32), ("restart", C.c_int32),
+                ("min_step", C.c_double), ("omega_step", C.c_double),
+                ("max_restarts", C.c_int32), ("max_centering", C.c_int32),
+                ("stall_iterations", C.c_int32), ("stall_tolerance", C.c_double),
+                ("step_rule", C.c_int32), ("refine_steps", C.c_int32),
+                ("refine_policy", C.c_int32), ("refine_max_steps", C.c_int32),
+                ("refine_tol", C.c_double), ("max_time", C.c_double),
+                ("parameter_policy", C.c_int32), ("parameter_strategy", C.c_int32),
+                ("adaptive_sigma_max", C.c_double), ("scaling", C.c_int32),
+                ("precision", C.c_int32), ("equality_solver", C.c_int32)]
+
+
+class SolveResult(C.Structure):
+    """`sdpx_b200_solve_result` (include/sdpx_b200.h)."""
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("restarts", C.c_int32),
+                ("mixed_iterations", C.c_int32), ("fp64_iterations", C.c_int32),
+                ("p_obj", C.c_double), ("d_obj", C.c_double), ("p_res", C.c_double),
+                ("d_res", C.c_double), ("seconds", C.c_double), ("message", C.c_char * 256)]
+
+
+STATUS_NAMES = {1: "Optimal", 2: "IterLimit", 3: "Stalled", 4: "InsufficientPrecision",
+                5: "NumericalBreakdown", 6: "MaxRestartsExceeded", 7: "TimeLimit"}
+
+
+def native_options(o) -> SolveOptions:
+    """SolverOptions → sdpx_b200_solve_options."""
+    return SolveOptions(
+        o.beta, o.gamma, o.omega_p, o.omega_d, o.eps_gap, o.eps_primal, o.eps_dual,
+        int(o.iter_max), int(bool(o.restart)), o.min_step, o.omega_step, int(o.max_restarts),
+        int(o.max_centering), int(o.stall_iterations), o.stall_tolerance,
+        {"auto": 0, "backtrack": 1, "fraction_to_boundary": 2}[o.step_rule],
+        int(o.refine_steps), {"fixed": 0, "adaptive": 1, "auto": 2}[o.refine_policy],
+        int(o.refine_max_steps), o.refine_tol, o.max_time,
+        {"auto": 0, "fixed": 1}[o.parameter_policy],
+        {"adaptive": 0, "fixed": 1}[o.parameter_strategy], o.adaptive_sigma_max,
+        {"auto": 0, "none": 1, "equilibrate": 2}[o.scaling],
+        1 if o.precision == "mixed" else 0, {"auto": 0, "qr": 1}[o.equality_solver])
+
+
 # name -> argtypes (restype is int unless noted)
 _SIGS = {
     "sdpx_b200_abi_version": [],
@@ -107,6 +150,15 @@ _SIGS = {
     "sdpx_b200_set_multipliers": [C.c_void_p, _dp],
     "sdpx_b200_equality_info": [C.c_void_p, _ip, _ip, _dp],
     "sdpx_b200_original_residuals_eq": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp],
+    "sdpx_b200_optimize": [C.c_void_p, C.POINTER(SolveOptions), C.POINTER(SolveResult)],
+    "sdpx_b200_optimize_begin": [C.c_void_p, C.POINTER(SolveOptions)],
+    "sdpx_b200_newton_step": [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _dp,
+                              _dp, _dp, _dp],
+    "sdpx_b200_optimize_end": [C.c_void_p, C.POINTER(SolveResult)],
+    "sdpx_b200_get_solution": [C.c_void_p, _dp, _dp, _dp, _dp],
+    "sdpx_b200_loop_state": [C.c_void_p, _dp],
+    "sdpx_b200_get_trace": [C.c_void_p, C.POINTER(C.c_int32), C.c_int32,
+                            C.POINTER(C.c_int32)],
     "sdpx_b200_adjoint": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int32,
                           C.POINTER(C.c_int32), _dp],
     "sdpx_b200_certificate_eq": [C.c_void_p, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
@@ -291,6 +343,37 @@ class CudaBackend:
             raise NotImplementedError(f"equality_solver={solver!r}")
         self._call("sdpx_b200_set_equality_options", float(requested_accuracy),
                    0 if solver == "auto" else 1)
+
+    def optimize(self, opts, steps: bool = False):
+        """The whole solve inside the library (sdpx_b200_optimize: the C++ loop
+        of the same driver); with `steps` the loop is driven one
+        sdpx_b200_newton_step at a time.  Returns an SDPResult in the original
+        coordinates."""
+        from .driver import SDPResult, Status
+        no = native_options(opts)
+        res = SolveResult()
+        if steps:
+            self._call("sdpx_b200_optimize_begin", C.byref(no))
+            running = C.c_int32(1)
+            while running.value:
+                self._call("sdpx_b200_newton_step", C.byref(running), None, None, None, None,
+                           None)
+            self._call("sdpx_b200_optimize_end", C.byref(res))
+        else:
+            self._call("sdpx_b200_optimize", C.byref(no), C.byref(res))
+        x, Xs, Ys = np.zeros(self.m), np.zeros(self.Ku), np.zeros(self.Ku)
+        y = np.zeros(self.n)
+        self._call("sdpx_b200_get_solution", _p(x), _p(Xs), _p(y) if self.n else None, _p(Ys))
+        cnt = C.c_int32()
+        modes = (C.c_int32 * max(1, res.iterations + 8))()
+        self._call("sdpx_b200_get_trace", modes, len(modes), C.byref(cnt))
+        trace = ["mixed" if modes[i] else "fp64" for i in range(min(cnt.value, len(modes)))]
+        self._history = trace
+        return SDPResult(status=Status(STATUS_NAMES[res.status]),
+                         message=res.message.decode(errors="replace"), x=x, X=self._split(Xs),
+                         y=y, Y=self._split(Ys), pObj=res.p_obj, dObj=res.d_obj,
+                         p_res=res.p_res, d_res=res.d_res, iterations=res.iterations,
+                         restarts=res.restarts, precision_trace=trace, seconds=res.seconds)
 
     def adjoint(self, wx=None, wy=None, WX=None, WY=None, A_index=()):
         """Gradient of ⟨wx, x⟩ + ⟨wy, y⟩ + Σ⟨WX_l, X_l⟩ + Σ⟨WY_l, Y_l⟩ at the current

@@ -66,6 +66,17 @@ class SDPResult:
         return abs(self.pObj - self.dObj) / max(1.0, (abs(self.pObj) + abs(self.dObj)) / 2)
 
 
+def _seq_sum(values) -> float:
+    """Left-to-right floating-point sum.  Python's built-in sum() compensates
+    (Neumaier) since 3.12; the host arithmetic of the loop uses the plain
+    order so that it is the same in every interpreter and in the library's
+    own loop (sdpx_b200_optimize)."""
+    total = 0.0
+    for v in values:
+        total += v
+    return total
+
+
 def _relative_regularization(attempts: int) -> float:
     """src/step.jl:383-394."""
     if attempts <= 0:
@@ -217,7 +228,7 @@ def kkt_cold_start(be, opts: SolverOptions, scale_p: float, scale_d: float):
     if not (be.psd_shift("X") and be.psd_shift("Y")):
         return dict(ok=False, reason="cold_start_psd_shift")
     dots, trX, trY = be.block_dots()
-    primal_mass, dual_mass = sum(trX), sum(trY)
+    primal_mass, dual_mass = _seq_sum(trX), _seq_sum(trY)
     # _cold_start_identity_mass_shifts (src/cold_start.jl:338-360)
     if not (total_degree > 0 and math.isfinite(primal_mass) and math.isfinite(dual_mass)):
         return dict(ok=False, reason="cold_start_identity_mass_floor")
@@ -229,8 +240,8 @@ def kkt_cold_start(be, opts: SolverOptions, scale_p: float, scale_d: float):
     if d_floor > 0:
         be.add_identity("Y", d_floor)
     dots, trX, trY = be.block_dots()
-    kappa = sum(dots)
-    pm, dm = sum(trX), sum(trY)
+    kappa = _seq_sum(dots)
+    pm, dm = _seq_sum(trX), _seq_sum(trY)
     # _cold_start_centering_shifts (src/cold_start.jl:407-430)
     ok = (math.isfinite(kappa) and kappa > 0 and math.isfinite(pm) and pm > 0
           and math.isfinite(dm) and dm > 0)
@@ -298,7 +309,7 @@ def solve_core(be, opts: SolverOptions, *, termination_gap_tolerance: Optional[f
     initial_merit = math.inf
     stagnation = StagnationDetector(opts.stall_iterations, opts.stall_tolerance)
     dots, _, _ = be.block_dots()
-    current_compl = sum(dots)
+    current_compl = _seq_sum(dots)
     best = None
     step_rule = resolved_step_rule(k, opts.step_rule)
     adaptive_margin = SQRT_EPS if opts.parameter_strategy == "adaptive" else 0.0
@@ -400,7 +411,7 @@ def solve_core(be, opts: SolverOptions, *, termination_gap_tolerance: Optional[f
                 if rescale_Y:
                     be.scale_iterate("Y", omega_step)
                 dots, _, _ = be.block_dots()
-                current_compl = sum(dots)
+                current_compl = _seq_sum(dots)
                 mu = [ctl.beta * dots[l] / k[l] for l in range(L)]
                 continue
             elif opts.restart and restarts < opts.max_restarts:
