@@ -5,7 +5,7 @@ Workload (one "step" = one complete solve to 1e-8 relative gap): the seeded
 SDPA-form instance with PSD blocks of order 400 and 200 plus 500 nonnegatives
 and m = 2000 constraints (generator `sdpx_b200.generators.sdpa_dense`), solved
 with SDPX's dense interior-point algorithm on the B200 in the mixed-precision
-mode; the plain FP64 device path is timed on the same instance for the
+mode, the whole loop running inside the library (sdpx_b200_optimize); the plain FP64 device path is timed on the same instance for the
 mixed-vs-FP64 ratio.  Inputs (3.2 GB of constraint data) are larger than L2.
 The line also carries `equality_rows`: the same instance with 64 equality rows
 Bᵀx = b solved on the FP64 path, and the device time of the equality factor
@@ -270,7 +270,6 @@ def bench_adjoint(args, world, rank, local):
     import torch
     from sdpx_b200 import SolverOptions, adjoint, generators as G
     from sdpx_b200.cuda_backend import CudaBackend
-    from sdpx_b200.driver import solve_with_backend
     from sdpx_b200.problem import SDPProblem
     wl = ADJ_WORKLOAD
     solve_s, adj_s, iters = [], [], []
@@ -287,7 +286,7 @@ def bench_adjoint(args, world, rank, local):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             e0.record(st)
-            r = solve_with_backend(be, SolverOptions(precision="fp64").with_tolerance(wl["tol"]))
+            r = be.optimize(SolverOptions(precision="fp64").with_tolerance(wl["tol"]))
             e1.record(st)
             torch.cuda.synchronize()
             solve_s.append(e0.elapsed_time(e1) / 1000.0)
@@ -312,7 +311,7 @@ def bench_adjoint(args, world, rank, local):
     def loss_at(C0):
         q = SDPProblem(prob.c, prob.k, prob.Av, [C0], prob.B, prob.b)
         with CudaBackend(q, precision="fp64", device=local) as b2:
-            rr = solve_with_backend(b2, SolverOptions(precision="fp64").with_tolerance(wl["tol"]))
+            rr = b2.optimize(SolverOptions(precision="fp64").with_tolerance(wl["tol"]))
         return float(v @ rr.x + np.sum(W[0] * rr.Y[0]))
 
     h = 1e-3
@@ -500,7 +499,6 @@ def run_ours(args, world, rank, local):
     import torch
     from sdpx_b200 import SolverOptions, generators as G
     from sdpx_b200.cuda_backend import CudaBackend
-    from sdpx_b200.driver import solve_with_backend
     from sdpx_b200.problem import SDPProblem
 
     wl = WORKLOADS[args.workload]
@@ -513,9 +511,8 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.ExternalStream(be.stream_handle())
 
     def one_solve(mode):
-        be.reset()
-        be.requested = mode
-        return solve_with_backend(be, opts_mixed if mode == "mixed" else opts_fp64)
+        # the product path: the whole loop inside the library (sdpx_b200_optimize)
+        return be.optimize(opts_mixed if mode == "mixed" else opts_fp64)
 
     for _ in range(args.warmup):
         one_solve("mixed")
@@ -597,10 +594,9 @@ def run_ours(args, world, rank, local):
                                   seed=rank)
     with CudaBackend(peq, precision="fp64", device=local) as beq:
         seq = torch.cuda.ExternalStream(beq.stream_handle())
-        solve_with_backend(beq, opts_fp64)
-        beq.reset()
+        beq.optimize(opts_fp64)
         e0.record(seq)
-        req = solve_with_backend(beq, opts_fp64)
+        req = beq.optimize(opts_fp64)
         e1.record(seq)
         torch.cuda.synchronize()
         eq_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
@@ -609,11 +605,9 @@ def run_ours(args, world, rank, local):
     # the same instance in the mixed mode (the headline path)
     with CudaBackend(peq, precision="mixed", device=local) as beq:
         seq = torch.cuda.ExternalStream(beq.stream_handle())
-        solve_with_backend(beq, opts_mixed)
-        beq.reset()
-        beq.requested = "mixed"
+        beq.optimize(opts_mixed)
         e0.record(seq)
-        reqm = solve_with_backend(beq, opts_mixed)
+        reqm = beq.optimize(opts_mixed)
         e1.record(seq)
         torch.cuda.synchronize()
         eqm_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
@@ -664,7 +658,7 @@ def run_ours(args, world, rank, local):
         t0 = time.perf_counter()
         with CudaBackend(prob_p, precision="mixed", device=local) as be2:
             t1 = time.perf_counter()
-            r_e2e = solve_with_backend(be2, opts_mixed)
+            r_e2e = be2.optimize(opts_mixed)
         torch.cuda.synchronize()
         if rep >= e2e_warmup:
             e2e_times.append(time.perf_counter() - t0)

@@ -1,11 +1,12 @@
 """Batches of independent dense SDPs (the 4096-instance small-SDP workload).
 
 Every instance gets its own device handle and CUDA stream; `threads` host
-threads drive the solves concurrently (the library calls release the GIL, so
-one instance's device work overlaps the others' host steps).  Results are the
-single-instance solver's: the same kernels in the same order per instance.
-A batched engine that runs one kernel per IPM phase over all instances is not
-part of this module.
+threads drive the solves concurrently.  With the native driver each solve is
+one library call (sdpx_b200_optimize) that releases the GIL for its whole
+duration, so the threads' host loops and device work overlap fully.  Results
+are the single-instance solver's: the same kernels in the same order per
+instance.  A batched engine that runs one kernel per IPM phase over all
+instances is not part of this module.
 """
 from __future__ import annotations
 
