@@ -67,13 +67,21 @@ class SDPResult:
 
 
 def _seq_sum(values) -> float:
-    """Left-to-right floating-point sum.  Python's built-in sum() compensates
-    (Neumaier) since 3.12; the host arithmetic of the loop uses the plain
-    order so that it is the same in every interpreter and in the library's
-    own loop (sdpx_b200_optimize)."""
-    total = 0.0
+    """Compensated (Neumaier) sum of the per-block scalars the loop adds on
+    the host (block traces and ⟨X_l, Y_l⟩ for the cold-start shifts and the
+    stagnation merit), written out so that it is the same in every interpreter
+    and in the library's own loop (sdpx_b200_optimize, `ipm::comp_sum`)."""
+    total, comp = 0.0, 0.0
     for v in values:
-        total += v
+        v = float(v)
+        t = total + v
+        if abs(total) >= abs(v):
+            comp += (total - t) + v
+        else:
+            comp += (v - t) + total
+        total = t
+    if comp and math.isfinite(comp):
+        total += comp
     return total
 
 
