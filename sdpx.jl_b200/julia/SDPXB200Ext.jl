@@ -86,6 +86,51 @@ set_precision!(h::B200Handle, mixed::Bool) =
     _check(h, ccall((:sdpx_b200_set_precision, libsdpx), Cint, (Ptr{Cvoid}, Cint), h.ptr, mixed ? 1 : 0),
            "set_precision")
 
+# ------------------------------------------------- whole solve in one call ---
+"""`sdpx_b200_solve_options`: SDPX's `SolverOptions{Float64}` fields the dense
+core reads (src/types/workspaces.jl:101-185), enums as in include/sdpx_b200.h."""
+mutable struct B200SolveOptions
+    beta::Float64; gamma::Float64; omega_p::Float64; omega_d::Float64
+    eps_gap::Float64; eps_primal::Float64; eps_dual::Float64
+    iter_max::Int32; restart::Int32; min_step::Float64; omega_step::Float64
+    max_restarts::Int32; max_centering::Int32; stall_iterations::Int32
+    stall_tolerance::Float64; step_rule::Int32; refine_steps::Int32
+    refine_policy::Int32; refine_max_steps::Int32; refine_tol::Float64
+    max_time::Float64; parameter_policy::Int32; parameter_strategy::Int32
+    adaptive_sigma_max::Float64; scaling::Int32; precision::Int32
+    equality_solver::Int32
+    B200SolveOptions() = new()
+end
+
+struct B200SolveResult
+    status::Int32; iterations::Int32; restarts::Int32
+    mixed_iterations::Int32; fp64_iterations::Int32
+    p_obj::Float64; d_obj::Float64; p_res::Float64; d_res::Float64; seconds::Float64
+    message::NTuple{256,UInt8}
+end
+
+"""`_solve_pipeline!` for the dense route run inside the library
+(sdpx_b200_optimize): returns the result record and the solution (x, X, y, Y)
+in the original coordinates."""
+function optimize(h::B200Handle, prob::SDPX.SDPProblem{Float64}, tolerance::Float64;
+                  mixed::Bool=false)
+    o = B200SolveOptions()
+    ccall((:sdpx_b200_default_options, libsdpx), Cvoid, (Ref{B200SolveOptions},), o)
+    o.eps_gap = o.eps_primal = o.eps_dual = tolerance
+    o.precision = mixed ? Int32(1) : Int32(0)
+    res = Ref{B200SolveResult}()
+    _check(h, ccall((:sdpx_b200_optimize, libsdpx), Cint,
+                    (Ptr{Cvoid}, Ref{B200SolveOptions}, Ref{B200SolveResult}), h.ptr, o, res),
+           "optimize")
+    m, n = prob.dims.m, prob.dims.n
+    stacked = sum(k -> k * k, prob.dims.k)
+    x, X, y, Y = zeros(m), zeros(stacked), zeros(n), zeros(stacked)
+    _check(h, ccall((:sdpx_b200_get_solution, libsdpx), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                    h.ptr, x, X, n > 0 ? y : C_NULL, Y), "get_solution")
+    return res[], (x, X, y, Y)
+end
+
 # ------------------------------------------------------ KKT backend seam ---
 """`KKTBackend` whose methods run on the B200 (src/kkt_backend.jl:115-552)."""
 struct B200DenseBackend <: SDPX.KKTBackend
