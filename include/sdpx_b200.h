@@ -281,6 +281,10 @@ int sdpx_b200_loop_state(sdpx_b200_handle* h, double* out8);
 /* Precision of each Newton step of the last solve: 1 mixed, 0 FP64. */
 int sdpx_b200_get_trace(sdpx_b200_handle* h, int32_t* modes, int32_t capacity, int32_t* count);
 
+/* Batched trial rounds and trials the fraction-to-boundary bisections
+ * (src/kernels/generic.jl:350-422) have run on this handle. */
+int sdpx_b200_step_stats(sdpx_b200_handle* h, int64_t* rounds, int64_t* trials);
+
 /* Restore the data as uploaded (undo sdpx_b200_equilibrate) and reset the
  * iterate to x = 0, X = Y = I, so one handle can run repeated solves. */
 int sdpx_b200_reset(sdpx_b200_handle* h);

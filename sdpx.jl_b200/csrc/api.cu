@@ -1721,6 +1721,7 @@ struct Handle {
   // the same rounds: each round factors, in one batch, the complete 4-level
   // subtree of midpoints of every unfinished interval, and the sequential
   // bisection path is replayed through it — the result equals the sequential one.
+  long long ftb_rounds = 0, ftb_trials = 0;  // batched trial rounds / trials of the bisections
   void ftb_bounds(double* boundX, double* boundY) {
     double b2[2] = {1.0, 1.0};
     const double* Ms[2] = {X.p, Y.p};
@@ -1788,6 +1789,8 @@ struct Handle {
       std::vector<int> info;
       std::vector<double> dmn, dmx;
       run_trials(reqs, info, dmn, dmx);
+      ++ftb_rounds;
+      ftb_trials += (long long)reqs.size();
       for (size_t q = 0; q < probs.size(); ++q) {
         Bis& P = probs[q];
         if (P.finished) continue;
@@ -2878,6 +2881,12 @@ int sdpx_b200_get_trace(sdpx_b200_handle* h, int32_t* modes, int32_t cap, int32_
     const int n = h->loop ? (int)h->loop->trace.size() : 0;
     if (count) *count = n;
     for (int i = 0; i < n && i < cap && modes; ++i) modes[i] = h->loop->trace[i];
+  });
+}
+int sdpx_b200_step_stats(sdpx_b200_handle* h, int64_t* rounds, int64_t* trials) {
+  GUARD(h, {
+    if (rounds) *rounds = h->h.ftb_rounds;
+    if (trials) *trials = h->h.ftb_trials;
   });
 }
 int sdpx_b200_reset(sdpx_b200_handle* h) { GUARD(h, h->h.reset()); }

@@ -157,6 +157,7 @@ _SIGS = {
     "sdpx_b200_optimize_end": [C.c_void_p, C.POINTER(SolveResult)],
     "sdpx_b200_get_solution": [C.c_void_p, _dp, _dp, _dp, _dp],
     "sdpx_b200_loop_state": [C.c_void_p, _dp],
+    "sdpx_b200_step_stats": [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "sdpx_b200_get_trace": [C.c_void_p, C.POINTER(C.c_int32), C.c_int32,
                             C.POINTER(C.c_int32)],
     "sdpx_b200_adjoint": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int32,
