@@ -27,12 +27,11 @@ def main():
     args = ap.parse_args()
     from sdpx_b200 import SolverOptions, generators as G
     from sdpx_b200.cuda_backend import CudaBackend
-    from sdpx_b200.driver import solve_with_backend
 
     prob = G.sdpa_dense(m=args.m, blocks=args.blocks, lp=args.lp, seed=args.seed)
     opts = SolverOptions(iter_max=args.iterations, precision=args.mode).with_tolerance(1e-8)
     with CudaBackend(prob, precision=args.mode) as be:
-        r = solve_with_backend(be, opts)
+        r = be.optimize(opts)  # the loop inside the library, as the product runs it
         phases = be.phase_times()
     print(json.dumps({"status": r.status.value, "iterations": r.iterations,
                       "precision": r.precision_trace, "phase_ms": phases}))
