@@ -366,9 +366,10 @@ class CudaBackend:
         y = np.zeros(self.n)
         self._call("sdpx_b200_get_solution", _p(x), _p(Xs), _p(y) if self.n else None, _p(Ys))
         cnt = C.c_int32()
-        modes = (C.c_int32 * max(1, res.iterations + 8))()
+        self._call("sdpx_b200_get_trace", None, 0, C.byref(cnt))
+        modes = (C.c_int32 * max(1, cnt.value))()
         self._call("sdpx_b200_get_trace", modes, len(modes), C.byref(cnt))
-        trace = ["mixed" if modes[i] else "fp64" for i in range(min(cnt.value, len(modes)))]
+        trace = ["mixed" if modes[i] else "fp64" for i in range(cnt.value)]
         self._history = trace
         return SDPResult(status=Status(STATUS_NAMES[res.status]),
                          message=res.message.decode(errors="replace"), x=x, X=self._split(Xs),
