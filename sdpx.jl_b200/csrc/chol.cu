@@ -86,18 +86,26 @@ __device__ int factor_panel_smem(T* P, int ld, int rows, int w) {
         for (int r = 0; r < 8; ++r)
           if (c < kw && r < kw && r >= c) P[(kb + c) * ld + kb + r] = D[c][r];
     }
-    // trailing panel columns q ∈ [kb+kw, w), rows r ≥ q
-    for (int r = kb + kw + threadIdx.x; r < rows; r += blockDim.x) {
-      T x[8];
+    // trailing panel columns q ∈ [kb+kw, w), rows r ≥ q.  With fewer rows
+    // than threads (the diagonal tiles, the short last panels) several threads
+    // share a row and take every `slices`-th column of it; each element gets
+    // the same sum in the same order either way.
+    {
+      const int r0 = kb + kw, nrow = rows - r0;
+      const int slices = nrow > 0 ? max(1, (int)blockDim.x / nrow) : 1;
+      for (int idx = threadIdx.x; idx < nrow * slices; idx += blockDim.x) {
+        const int r = r0 + idx % nrow, sl = idx / nrow;
+        T x[8];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) x[c] = (c < kw) ? P[(kb + c) * ld + r] : T(0);
-      const int qe = min(w, r + 1);
-      for (int q = kb + kw; q < qe; ++q) {
-        T a = P[q * ld + r];
+        for (int c = 0; c < 8; ++c) x[c] = (c < kw) ? P[(kb + c) * ld + r] : T(0);
+        const int qe = min(w, r + 1);
+        for (int q = r0 + sl; q < qe; q += slices) {
+          T a = P[q * ld + r];
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (c < kw) a -= x[c] * P[(kb + c) * ld + q];
-        P[q * ld + r] = a;
+          for (int c = 0; c < 8; ++c)
+            if (c < kw) a -= x[c] * P[(kb + c) * ld + q];
+          P[q * ld + r] = a;
+        }
       }
     }
     __syncthreads();
