@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "dbuf.h"
 
 namespace sdpx {
 
@@ -37,14 +38,18 @@ struct MixedWorkspace {
   float* dmax = nullptr;
   void* desc = nullptr;
   double cond_estimate = 1.0;
-  ~MixedWorkspace() {
-    for (void* p : {(void*)Sf, (void*)Dinv, (void*)v32, (void*)w32, (void*)info, (void*)dmin,
-                    (void*)dmax, desc, (void*)partial, (void*)err, (void*)L64,
-                    (void*)Linv, (void*)Dinv64, (void*)tmp64})
-      if (p) cudaFree(p);
-    for (int i = 0; i < 3; ++i)
-      for (void* p : {Apl[i], Ppl[i], Tpl[i], Wpl[i], Lpl[i]})
-        if (p) cudaFree(p);
+  // The device blocks behind the pointers above come from the process-wide
+  // cache of idle device blocks, so a handle created and destroyed per solve
+  // neither allocates them from the driver again nor synchronises the device
+  // to free them.
+  static constexpr int kBlocks = 32;
+  DBuf<unsigned char> blocks[kBlocks];
+  int n_blocks = 0;
+  template <class P>
+  void take(P*& ptr, size_t bytes) {
+    if (n_blocks == kBlocks) throw CudaError("mixed workspace: more device blocks than reserved");
+    blocks[n_blocks].alloc(bytes);
+    ptr = static_cast<P*>(static_cast<void*>(blocks[n_blocks++].p));
   }
 };
 
