@@ -739,7 +739,10 @@ def run_ours(args, world, rank, local):
                              6.0 * wl["m"] * Kp + 4.0 * 128 * 128 * syrk_units(wl["m"], Kp),
                          "hardware_flops_per_launch": hw_flops,
                          "hardware_frac": hw_flops / (syrk_ms / 1000.0) / 1e12 / peak,
-                         "peak_kind": f"bf16_tflops of {peak_kind} MEASURED_PEAKS.json; "
+                         "peak_kind": ("bf16_tflops of MEASURED_PEAKS.json (measured); "
+                                       if peak_kind == "measured" else
+                                       "fallback 1590 TFLOP/s (no MEASURED_PEAKS.json); ")
+                                      + 
                                       f"achieved counts FP64-equivalent algorithmic flops "
                                       f"(6 BF16 products each, so frac <= 1/6)"},
             "cpu_baseline": cpu,
