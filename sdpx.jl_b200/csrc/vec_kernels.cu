@@ -585,69 +585,83 @@ void symv_full(int m, const double* S, const double* x, double alpha, const doub
 }
 
 // --------------------------------------------------------- equilibration ---
-// Row maxima of |A_i| (dense block: rows r of every A_i^(l)) → rn[r] via atomics.
+// Row maxima of |A_i| (dense block: rows r of every A_i^(l)) → rn[r].  CTA i
+// walks A_i's k×k block column by column with thread r holding row r's
+// maximum in a register (each column read coalesced, no index division, no
+// shared-memory atomics), then one atomic per row.  NaN counts as +inf.
 __global__ void k_ruiz_rowmax_dense(const double* A, long long K, int m, long long off, int k,
                                     double* rn) {
-  extern __shared__ double loc[];
-  for (int r = threadIdx.x; r < k; r += blockDim.x) loc[r] = 0.0;
-  __syncthreads();
-  int i = blockIdx.x;
-  const double* col = A + (long long)i * K + off;
-  long long tot = (long long)k * k;
-  for (long long e = threadIdx.x; e < tot; e += blockDim.x) {
-    double v = fabs(col[e]);
-    if (!(v == v)) v = 1.0 / 0.0;
-    int r = (int)(e % k);
-    // shared-memory max via integer atomics on the non-negative bit pattern
-    atomicMax(reinterpret_cast<unsigned long long*>(loc + r), __double_as_longlong(v));
+  const double* blk = A + (long long)blockIdx.x * K + off;
+  for (int r = threadIdx.x; r < k; r += blockDim.x) {
+    double mx = 0.0;
+#pragma unroll 8
+    for (int c = 0; c < k; ++c) {
+      double v = fabs(blk[(long long)c * k + r]);
+      if (!(v == v)) v = 1.0 / 0.0;
+      mx = fmax(mx, v);
+    }
+    atomic_max_nonneg(rn + r, mx);
   }
-  __syncthreads();
-  for (int r = threadIdx.x; r < k; r += blockDim.x) atomic_max_nonneg(rn + r, loc[r]);
 }
 void ruiz_rowmax_dense(const double* A, long long K, int m, long long off, int k, double* rn,
                        cudaStream_t st) {
-  size_t sm = sizeof(double) * k;
-  ensure_smem(k_ruiz_rowmax_dense, sm);
-  k_ruiz_rowmax_dense<<<m, 256, sm, st>>>(A, K, m, off, k, rn);
+  if (m == 0 || k == 0) return;
+  const int threads = std::min(1024, ceil_div(k, 32) * 32);
+  k_ruiz_rowmax_dense<<<m, threads, 0, st>>>(A, K, m, off, k, rn);
   SDPX_LAUNCH_CHECK();
 }
 
-// Row maxima for the 1×1 group: rn[j] = max(rn[j], max_i |A[od+j, i]|).
+// Row maxima for the 1×1 group: rn[j] = max(rn[j], max_i |A[od+j, i]|), the
+// constraints split into chunks of 16 across blockIdx.y (an atomic per chunk)
+// so that the pass is spread over the whole GPU rather than one thread per j.
+constexpr int kRuizDiagChunk = 16;
 __global__ void k_ruiz_rowmax_diag(const double* A, long long K, int m, long long od, int nd,
                                    double* rn) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nd) return;
-  double v = rn[j];
-  for (int i = 0; i < m; ++i) {
-    double a = fabs(A[od + j + (long long)i * K]);
-    if (!(a == a)) a = 1.0 / 0.0;
-    v = fmax(v, a);
+  for (int i0 = blockIdx.y * kRuizDiagChunk; i0 < m; i0 += gridDim.y * kRuizDiagChunk) {
+    const int i1 = min(m, i0 + kRuizDiagChunk);
+    double v = 0.0;
+    for (int i = i0; i < i1; ++i) {
+      double a = fabs(A[od + j + (long long)i * K]);
+      if (!(a == a)) a = 1.0 / 0.0;
+      v = fmax(v, a);
+    }
+    atomic_max_nonneg(rn + j, v);
   }
-  rn[j] = v;
 }
 void ruiz_rowmax_diag(const double* A, long long K, int m, long long od, int nd, double* rn,
                       cudaStream_t st) {
-  if (nd == 0) return;
-  k_ruiz_rowmax_diag<<<ceil_div(nd, 128), 128, 0, st>>>(A, K, m, od, nd, rn);
+  if (nd == 0 || m == 0) return;
+  dim3 grid(ceil_div(nd, 128), std::min(65535, ceil_div(m, kRuizDiagChunk)));
+  k_ruiz_rowmax_diag<<<grid, 128, 0, st>>>(A, K, m, od, nd, rn);
   SDPX_LAUNCH_CHECK();
 }
 
-// A_i[r,c] *= e_r e_c over the rows [off, off+k²) of every column.
-__global__ void k_ruiz_congruence_dense(double* A, long long K, int m, long long off, int k,
-                                        const double* e) {
-  long long tot = (long long)k * k * m;
-  long long kk = (long long)k * k;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
-       t += (long long)gridDim.x * blockDim.x) {
-    long long i = t / kk, q = t % kk;
-    int r = (int)(q % k), c = (int)(q / k);
-    A[i * K + off + q] *= e[r] * e[c];
+// A_i[r,c] *= e_r e_c over the rows [off, off+k²) of every column: one warp
+// per (i, c) column of the block, lanes over r (coalesced, one division per
+// column instead of four per element).
+__global__ void k_ruiz_congruence_dense(double* __restrict__ A, long long K, int m, long long off,
+                                        int k, const double* __restrict__ e) {
+  const long long cols = (long long)m * k;
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long w = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); w < cols;
+       w += warps) {
+    const long long i = w / k;
+    const int c = (int)(w - i * k);
+    const double ec = e[c];
+    double* col = A + i * K + off + (long long)c * k;
+#pragma unroll 4
+    for (int r = lane; r < k; r += 32) col[r] *= e[r] * ec;
   }
 }
 void ruiz_congruence_dense(double* A, long long K, int m, long long off, int k, const double* e,
                            cudaStream_t st) {
-  long long tot = (long long)k * k * m;
-  k_ruiz_congruence_dense<<<std::min(8192, ceil_div(tot, 256)), 256, 0, st>>>(A, K, m, off, k, e);
+  const long long cols = (long long)m * k;
+  if (cols == 0) return;
+  k_ruiz_congruence_dense<<<(int)std::min<long long>(148LL * 8, ceil_div(cols, 8)), 256, 0, st>>>(
+      A, K, m, off, k, e);
   SDPX_LAUNCH_CHECK();
 }
 

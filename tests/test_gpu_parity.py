@@ -130,9 +130,15 @@ def test_newton_step_kernels_match_oracle(cuda, name):
         assert ob.objectives() == pytest.approx(cb.objectives(), rel=max(1e-12, DIR))
 
 
-def test_equilibration_matches_oracle(cuda):
+@pytest.mark.parametrize("m,blocks,lp", [
+    (40, [9, 3], 5),
+    # blocks wider than a warp and not a multiple of 32, two 128-column groups
+    # of 1×1 rows, several 16-constraint chunks of the 1×1 row maxima
+    (60, [45, 70], 150),
+])
+def test_equilibration_matches_oracle(cuda, m, blocks, lp):
     from oracle.sdpx_oracle import OracleBackend
-    prob = G.sdpa_dense(m=40, blocks=[9, 3], lp=5, seed=4)
+    prob = G.sdpa_dense(m=m, blocks=blocks, lp=lp, seed=4)
     ob = OracleBackend(prob)
     with cuda(prob) as cb:
         eo, ec = ob.equilibrate(), cb.equilibrate()
