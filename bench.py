@@ -43,17 +43,19 @@ WORKLOADS = {
                      label="dense SDP (SDPA form), one PSD block n=50, m=100"),
 }
 TOL = 1e-8
-# DRAM bytes (read + write) of one k_split_syrk_tma launch on the sdp_m2000
-# workload, from one ncu capture of dram__bytes_read.sum + dram__bytes_write.sum
-# (a single-pass metric set) on that workload.
-SPLIT_SYRK_DRAM_BYTES = 2.44e9 + 0.6335e9
+# DRAM traffic of one k_split_syrk_tma launch, measured by ncu on the m = 1000
+# instance (profiles/split_bf16_syrk_tma_m1000.md: Kp = 50 688, 36 lower tiles ×
+# 16 K chunks = 576 CTAs): dram__bytes_read.sum = 320.1 MB (the three BF16
+# planes of P̂, read once) and dram__bytes_write.sum = 28.4 MB (FP32 partial
+# tiles).  Other sizes scale the reads by m·Kp and the writes by the CTA count.
+SYRK_CAPTURE = dict(m=1000, Kp=50688, units=576, read=320.1e6, write=28.4e6)
+# Complete CPU oracle solve of the sdp_m2000 instance (seed 0) to 1e-8, with its
+# certificate: the parity record of the headline workload.
+HEADLINE_FIXTURE = os.path.join(ROOT, "tests", "golden", "headline_m2000.json")
 # LP standard form + Lorentz cones: the reduced normal matrix Q = Bᵀ D⁻¹ B + δI.
 NORMAL_WORKLOAD = dict(m=3000, n_lp=20000, cones=[64] * 100, density=0.1,
                        label="LP+SOC reduced normal matrix: 3000 equalities x (20000 LP + "
                              "100 Lorentz cones x 64) variables, 10%-dense N(0,1)")
-# Iterations of the CPU restatement on sdp_m2000 (seed 0) to 1e-8, used to
-# scale the reference arm's one-iteration samples to a time-to-gap.
-CPU_ITERATIONS_M2000 = 15  # CPU restatement, seed 0, tolerance 1e-8 (measured: Optimal in 15)
 # Equality rows added to the workload for the n > 0 measurement (Bᵀx = b with
 # B ~ N(0,1) and b = Bᵀy0 at the generator's strictly feasible point).
 EQ_ROWS = 64
@@ -88,6 +90,17 @@ def workload_config(wl):
             "tolerance": TOL, "seed": "rank (instance seed; the reference arm runs rank 0's)",
             "l2": "inputs (constraint data 3.2 GB) larger than L2; not flushed",
             "parallelism": "replicas (independent instance per GPU)"}
+
+
+def headline_record():
+    with open(HEADLINE_FIXTURE) as f:
+        return json.load(f)
+
+
+def split_syrk_traffic(m, Kp, units):
+    """DRAM bytes per k_split_syrk_tma launch, scaled from the m = 1000 capture."""
+    c = SYRK_CAPTURE
+    return c["read"] * (m * Kp) / (c["m"] * c["Kp"]) + c["write"] * units / c["units"]
 
 
 def syrk_units(m, Kp, sm_count=148):
@@ -380,31 +393,34 @@ def cpu_threads():
 
 
 def run_reference(args, world, rank):
-    """CPU restatement of the reference algorithm (the oracle port)."""
+    """The reference's algorithm on the host cores: one complete solve of the
+    seed-0 instance to 1e-8 by the CPU restatement (the oracle port; SDPX.jl
+    itself is Julia and cannot run here), NumPy/OpenBLAS on every host core.
+    The solve is the step: steps = 1 and warmup = 0 whatever was asked, so the
+    line states exactly what was timed (one solve takes a few minutes)."""
     if rank != 0:
         return
-    from sdpx_b200 import generators as G
+    from oracle.sdpx_oracle import oracle_solve
+    from sdpx_b200 import SolverOptions, generators as G
     wl = WORKLOADS[args.workload]
     prob = G.sdpa_dense(m=wl["m"], blocks=wl["blocks"], lp=wl["lp"], seed=0)
-    iters = CPU_ITERATIONS_M2000 if args.workload == "sdp_m2000" else None
-    samples = []
-    for s in range(args.warmup + args.steps):
-        t_it = cpu_sample(prob, wl["blocks"], wl["lp"], None)
-        if s >= args.warmup:
-            samples.append(t_it)
-    t_it = statistics.median(samples)
-    n_it = iters or 20
-    value = t_it * n_it
+    t0 = time.perf_counter()
+    r = oracle_solve(prob, SolverOptions().with_tolerance(TOL))
+    value = time.perf_counter() - t0
     line = {
         "impl": "reference", "metric": metric_name(wl),
-        "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "value": value, "unit": "s", "n_gpus": world, "steps": 1, "warmup": 0,
         "ms_per_step": value * 1000.0, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(wl),
+        "status": r.status.value, "iterations": r.iterations, "pObj": r.pObj, "dObj": r.dObj,
+        "relative_gap": r.relative_gap,
         "cpu_baseline": {"value": value, "unit": "s", "cores": cpu_threads(), "kind": "port",
-                         "sample": (f"one Newton iteration (residuals, Schur, Cholesky, predictor/"
-                                    f"corrector, refinement, line search) of the same instance per "
-                                    f"step, median of {args.steps}, × {n_it} iterations")},
+                         "sample": ("one complete solve of the seed-0 instance to a 1e-8 "
+                                    "relative gap (equilibration, KKT cold start and every "
+                                    "Newton iteration) by the CPU restatement of SDPX's "
+                                    "Float64 dense path; steps/warmup requested: "
+                                    f"{args.steps}/{args.warmup}, timed: 1/0")},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -562,6 +578,32 @@ def run_ours(args, world, rank, local):
     e1.record(stream)
     torch.cuda.synchronize()
     fp64_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0, world)
+    # Parity of the timed solves with the CPU oracle's complete solve of the same
+    # instance (seed 0 on rank 0), and the original-coordinate certificate of each.
+    parity = None
+    if args.workload == "sdp_m2000":
+        ref = headline_record()
+        opts_c = opts_mixed
+
+        def cert(res):
+            c = be.certificate(res.x, res.X, res.Y, opts_c.eps_primal, opts_c.eps_dual,
+                               opts_c.eps_gap, y=res.y)
+            return {"valid": bool(c["valid"]), "failures": list(c["failures"]),
+                    "gap_relative": c["gap_relative"]}
+
+        def rdiff(a, b):
+            return abs(a - b) / max(abs(b), 1e-300)
+
+        parity = {"oracle": {k: ref[k] for k in ("status", "iterations", "pObj", "dObj",
+                                                 "certificate_valid")},
+                  "instance_seed": rank,
+                  "compared": rank == ref["shape"]["seed"]}
+        for name, res in (("mixed", last), ("fp64", r64)):
+            parity[name] = {"status": res.status.value, "iterations": res.iterations,
+                            "pObj": res.pObj, "dObj": res.dObj,
+                            "rel_obj_diff": max(rdiff(res.pObj, ref["pObj"]),
+                                                rdiff(res.dObj, ref["dObj"])),
+                            "certificate": cert(res)}
     # The same FP64 path with every Schur product on the FP64 DMMA tiles (the
     # plain FP64 tensor-core engine; the default FP64 engine is the exact int8
     # digit product).
@@ -693,12 +735,15 @@ def run_ours(args, world, rank, local):
             equality["cpu_kind"] = ("port: the oracle's equality factor (LAPACK trsm of B, "
                                     "column scaling, Q = B̂ᵀB̂, potrf, rank test) on a "
                                     "well-conditioned m×m factor, all host cores")
-            t_it = cpu_sample(prob, wl["blocks"], wl["lp"], last.iterations)
-            cpu = {"value": t_it * last.iterations, "unit": "s", "cores": cpu_threads(),
+            n_it = headline_record()["iterations"] if args.workload == "sdp_m2000" \
+                else last.iterations
+            t_it = cpu_sample(prob, wl["blocks"], wl["lp"], n_it)
+            cpu = {"value": t_it * n_it, "unit": "s", "cores": cpu_threads(),
                    "kind": "port",
                    "sample": (f"one Newton iteration of the same instance on the CPU "
                               f"restatement (NumPy/OpenBLAS), {t_it:.2f} s, × the "
-                              f"{last.iterations} iterations of the GPU solve")}
+                              f"{n_it} iterations of the oracle's complete solve "
+                              f"(the reference arm times that complete solve)")}
         line = {
             "metric": metric_name(wl),
             "path": "mixed precision (split-BF16 Schur, FP32 factor, FP64 refinement, FP64 tail)",
@@ -728,9 +773,14 @@ def run_ours(args, world, rank, local):
                       "fp64_syrk_tflops": syrk_flops / (kt_fp64["fp64_syrk"] / 1000) / 1e12
                       if kt_fp64["fp64_syrk"] > 0 else None,
                       "dgemm_tflops_measured": dgemm_tflops},
+            "parity_vs_cpu_solve": parity,
             "phase_ms_last_solve": phases_mixed,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": SPLIT_SYRK_DRAM_BYTES,
+                         "frac": achieved / peak,
+                         "traffic": split_syrk_traffic(wl["m"], Kp, syrk_units(wl["m"], Kp)),
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of "
+                                           "the m = 1000 capture (profiles/split_bf16_syrk_tma_"
+                                           "m1000.md), reads scaled by m·Kp, writes by CTAs",
                          "kernel": "k_split_syrk_tma (split-BF16 lower SYRK of the Schur "
                                    "assembly, one launch per build)",
                          "algorithmic_flops_per_launch": syrk_flops,
@@ -762,6 +812,25 @@ def run_ours(args, world, rank, local):
     return line
 
 
+def run_profile(args):
+    """Bounded launch sequence for a kernel profiler: the cold start plus
+    `--profile-iterations` Newton iterations of one seeded instance through the
+    loop inside the library (the solve stops with IterLimit), then the
+    per-phase device time of the run.  Not a bench line."""
+    from sdpx_b200 import SolverOptions, generators as G
+    from sdpx_b200.cuda_backend import CudaBackend
+
+    prob = G.sdpa_dense(m=args.m, blocks=args.blocks, lp=args.lp, seed=args.seed)
+    opts = SolverOptions(iter_max=args.profile_iterations,
+                         precision=args.mode).with_tolerance(TOL)
+    with CudaBackend(prob, precision=args.mode) as be:
+        r = be.optimize(opts)
+        phases = be.phase_times()
+    print(json.dumps({"profile_run": True, "status": r.status.value,
+                      "iterations": r.iterations, "precision": r.precision_trace,
+                      "phase_ms": phases}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -770,7 +839,16 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS), default="sdp_m2000")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # profiling mode (no bench line): a few iterations of one instance
+    ap.add_argument("--profile-iterations", type=int, default=0)
+    ap.add_argument("--m", type=int, default=2000)
+    ap.add_argument("--blocks", type=int, nargs="+", default=[400, 200])
+    ap.add_argument("--lp", type=int, default=500)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--mode", choices=["fp64", "mixed"], default="mixed")
     args = ap.parse_args()
+    if args.profile_iterations > 0:
+        return run_profile(args)
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":

@@ -303,8 +303,9 @@ int sdpx_b200_launch_count(uint64_t* count);
  * call cudaMalloc — runtimes that own all device memory through their own
  * pool (e.g. a Julia or Python caching allocator) or serving loops where an
  * implicit cudaMalloc/cudaFree would synchronise the device.
- *   - m ≤ 2048 (the array holds one K chunk of every lower 128×128 tile);
- *     larger m returns an error and leaves S untouched.
+ *   - m ≤ 2048 (the array holds one K chunk of every lower 128×128 tile) and
+ *     K ≤ 2^30 (the tile loop indexes K in int32); larger m or K, and NULL
+ *     P or S, return -1 with a message and leave S untouched.
  *   - The first call on each device looks up the array's device address with
  *     that device current; make that first call before any stream capture.
  *   - Every call on a device shares the one array: calls that overlap on the

@@ -31,18 +31,26 @@ def nvcc():
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    from concurrent.futures import ThreadPoolExecutor
     BUILD.mkdir(exist_ok=True)
     deps = sorted(CSRC.glob("*")) + sorted((HERE.parent / "include").glob("*.h")) + [Path(__file__)]
     newest_dep = max(p.stat().st_mtime for p in deps)
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         obj = BUILD / (src + ".o")
         objs.append(obj)
         if force or not obj.exists() or obj.stat().st_mtime < newest_dep:
-            cmd = [nvcc(), *ARCH, *FLAGS, *FILE_FLAGS.get(src, []), "-c", str(CSRC / src), "-o", str(obj)]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            cmds.append([nvcc(), *ARCH, *FLAGS, *FILE_FLAGS.get(src, []), "-c", str(CSRC / src),
+                         "-o", str(obj)])
+
+    def compile_one(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+    # one nvcc per translation unit, in parallel (the objects are independent)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(compile_one, cmds))
     if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
         if verbose:

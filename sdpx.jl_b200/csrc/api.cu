@@ -2919,7 +2919,10 @@ int sdpx_b200_launch_count(uint64_t* count) {
 static thread_local std::string g_noalloc_error;
 const char* sdpx_b200_gram_noalloc_error(void) { return g_noalloc_error.c_str(); }
 int sdpx_b200_gram_noalloc(const double* P, int64_t K, int32_t m, double* S, void* stream) {
-  if (!P || !S) return -1;
+  if (!P || !S) {
+    g_noalloc_error = "gram (allocation-free): NULL operand";
+    return -1;
+  }
   try {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     sdpx::syrk_lower_f64_noalloc(P, K, m, S, st);

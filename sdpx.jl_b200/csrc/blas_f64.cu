@@ -202,12 +202,16 @@ void syrk_lower_f64(const Opnd& P, const SyrkPlan& plan, double* partial, double
 // Allocation-free variant of the split-K lower Gram product S = PᵀP.
 //
 // The split-K partial tiles live in a fixed file-scope device array instead of
-// caller- or library-allocated memory.  Its capacity bounds the problem size:
-// one K chunk per lower 128×128 tile must fit, i.e. ntri·128·128 doubles with
-// ntri = t(t+1)/2, t = ceil(m/128), so m ≤ 2048.  Every GPU that loads the
-// library holds the array until the process exits, and all calls share it.
+// caller- or library-allocated memory.  One K chunk of every lower 128×128 tile
+// must fit (ntri·128·128 doubles, ntri = t(t+1)/2, t = ceil(m/128)): the stated
+// limit m ≤ 2048 (t = 16, 2.2 Mi doubles) leaves room for a second chunk.  K is
+// bounded by the int32 K indexing of the tile loop: chunk starts plus a chunk
+// length must stay below 2³¹, which K ≤ 2³⁰ guarantees.  Every GPU that loads
+// the library holds the array until the process exits, and all calls share it.
 // ---------------------------------------------------------------------------
 static constexpr size_t kNoAllocScratchDoubles = (size_t)4 << 20;  // 32 MiB
+static constexpr int kNoAllocMaxM = 2048;
+static constexpr long long kNoAllocMaxK = 1LL << 30;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
 
 static std::mutex g_noalloc_mu;
@@ -239,9 +243,14 @@ void syrk_lower_f64_noalloc(const double* P, long long K, int m, double* S, cuda
   const long long ntri = (long long)nt * (nt + 1) / 2;
   const long long tile = (long long)Cfg::BM * Cfg::BN;
   if (m <= 0 || K <= 0) throw std::invalid_argument("gram: m and K must be positive");
-  if (ntri * tile > (long long)kNoAllocScratchDoubles)
+  if (m > kNoAllocMaxM)
     throw std::invalid_argument("gram (allocation-free): m = " + std::to_string(m) +
                                 " exceeds the fixed scratch (m ≤ 2048)");
+  if (K > kNoAllocMaxK)
+    throw std::invalid_argument("gram (allocation-free): K = " + std::to_string(K) +
+                                " exceeds the int32 K indexing (K ≤ 2^30)");
+  if (ntri * tile > (long long)kNoAllocScratchDoubles)
+    throw std::logic_error("gram (allocation-free): scratch smaller than one chunk");
   double* scratch = noalloc_scratch_address();
   int dev = 0, sms = 148;
   SDPX_CUDA(cudaGetDevice(&dev));

@@ -656,6 +656,7 @@ __global__ void k_ruiz_congruence_dense(double* A, long long K, int m, long long
 void ruiz_congruence_dense(double* A, long long K, int m, long long off, int k, const double* e,
                            cudaStream_t st) {
   long long tot = (long long)k * k * m;
+  if (tot == 0) return;
   k_ruiz_congruence_dense<<<std::min(8192, ceil_div(tot, 256)), 256, 0, st>>>(A, K, m, off, k, e);
   SDPX_LAUNCH_CHECK();
 }
@@ -710,6 +711,7 @@ __global__ void k_scale_cols(double* A, long long K, int m, const double* s) {
 }
 void scale_cols(double* A, long long K, int m, const double* s, cudaStream_t st) {
   long long tot = K * m;
+  if (tot == 0) return;
   k_scale_cols<<<std::min(8192, ceil_div(tot, 256)), 256, 0, st>>>(A, K, m, s);
   SDPX_LAUNCH_CHECK();
 }

@@ -1,7 +1,10 @@
 # SDPX package extension binding libsdpx_b200.so (sm_100a) through ccall.
 #
 # This file is the reference-side glue a maintainer adds as ext/SDPXB200Ext.jl
-# (with `[weakdeps] CUDA` / `[extensions] SDPXB200Ext = "CUDA"` in Project.toml).
+# (with `[weakdeps] CUDA, ChainRulesCore` / `[extensions] SDPXB200Ext =
+# ["CUDA", "ChainRulesCore"]` in Project.toml) together with the small core
+# patch shown in INTEGRATION.md (the `:b200` provider symbol, the plan branch,
+# the instantiate / route / whole-loop hooks this file overloads).
 # It is written against SDPX's seams but is not executed in this repository's
 # tests: the build environment has no Julia.  Every ccall below matches a
 # declaration in include/sdpx_b200.h or include/sdpx_b200_normal.h.
@@ -9,6 +12,7 @@ module SDPXB200Ext
 
 using SDPX
 using LinearAlgebra
+import ChainRulesCore
 
 const libsdpx = get(ENV, "SDPX_B200_LIB", joinpath(@__DIR__, "..", "libsdpx_b200.so"))
 
@@ -161,6 +165,161 @@ function SDPX.refine!(b::B200DenseBackend, ws, prob, opts, r)
                            (Ptr{Cvoid}, Cint, Float64, Cint, Cint, Ref{Cint}, Ref{Float64}),
                            b.handle.ptr, 1, 0.0, 8, 0, steps, resid), "refine")  # auto policy, 64-ulp tol, cap 8
     return resid[]
+end
+
+# ------------------------------------------------------ provider seams ---
+# Capabilities the B200 core executes for the dense Cholesky route
+# (src/la_backend.jl:75-90 `_la_route_requirements(:dense_cholesky, …)`): the
+# Schur Cholesky and its solves, the triangular solves, the Schur SYRK, owned
+# products, iterative refinement against the FP64 operator and (mixed mode)
+# the low-precision factor with higher-precision residuals.
+const _B200_CAPABILITIES = SDPX.LAProviderCapabilities(
+    cholesky=true, rank_revealing_qr=true, factor_solve=true, multi_rhs=true,
+    iterative_refinement=true, higher_precision_residual=true,
+    refinement_correction=true, mixed_precision_residual=true, dot=true,
+    norminf=true, mul=true, mul_owned=true, syrk=true, triangular_solve=true,
+    axpby=true)
+
+_b200_library_ready() =
+    Libc.Libdl.dlopen(libsdpx; throw_error=false) !== nothing
+
+"""`SDPX.la_provider_descriptor` for Float64 (default at src/la_backend.jl:12-16,
+the MultiFloat extension's at ext/SDPXMultiFloatLinearAlgebraExt.jl:743-765):
+the B200 provider advertises the dense-Cholesky route's operations when the
+library loads.  `plan_la_backend` reads it only for `provider = :b200`."""
+function SDPX.la_provider_descriptor(::Type{Float64}, threads::Int=1)
+    _b200_library_ready() || return (available=false, provider=:none, capabilities=(),
+                                     capability_model=SDPX.LAProviderCapabilities(),
+                                     reason=:missing_library)
+    return (available=true, provider=:b200_cuda,
+            capabilities=(:chol, :cholesky_factor!, :solve, :trsm, :trsv_lower,
+                          :trsv_transpose, :syrk, :mul_owned, :rank_revealing_qr),
+            capability_model=_B200_CAPABILITIES)
+end
+
+"""Provider payload of a planned `:b200` backend: the device ordinal and the
+precision mode (`:fp64` or `:mixed`) the handle is created with."""
+struct B200Provider
+    device::Int
+    precision::Symbol
+end
+
+SDPX.la_provider_capability_model(::B200Provider) = _B200_CAPABILITIES
+
+"""Instantiate hook called by the patched `instantiate_la_backend` for
+`config.selected === :b200` (beside `instantiate_multifloat_la_backend`,
+src/la_backend.jl:508-570)."""
+function SDPX.instantiate_b200_la_backend(::Type{Float64}, config::SDPX.LABackendConfiguration,
+                                          threads::Int=1)
+    config.provider === :b200_cuda || return nothing
+    dev = parse(Int, get(ENV, "SDPX_B200_DEVICE", "0"))
+    mode = Symbol(get(ENV, "SDPX_B200_PRECISION", "fp64"))
+    mode in (:fp64, :mixed) || throw(ArgumentError("SDPX_B200_PRECISION must be fp64 or mixed"))
+    return B200Provider(dev, mode)
+end
+
+"""Route hook called by the patched `_backend_from_configuration`
+(src/kkt_backend.jl:86-100): a `DenseNormalEquations` formulation planned on
+the `:b200` provider gets the device backend, with the iterate uploaded once."""
+function SDPX.b200_backend_from_configuration(ws, prob::SDPX.SDPProblem{Float64},
+                                              provider::B200Provider)
+    h = B200Handle(prob; device=provider.device)
+    set_precision!(h, provider.precision === :mixed)
+    return B200DenseBackend(h)
+end
+
+"""Whole-loop hook: the patched `_solve_pipeline!` dense-SDP dispatch
+(src/solver/interior_point.jl:3503-3515) calls this instead of
+`_solve_sdp_core!` when the plan selected the `:b200` provider, so every
+iterate stays in HBM for the whole solve (sdpx_b200_optimize)."""
+function SDPX.b200_solve_sdp_core!(prob::SDPX.SDPProblem{Float64}, opts, provider::B200Provider)
+    h = B200Handle(prob; device=provider.device)
+    tol = min(opts.ϵ_gap, opts.ϵ_primal, opts.ϵ_dual)
+    res, (x, Xs, y, Ys) = optimize(h, prob, tol; mixed=provider.precision === :mixed)
+    return _to_result(prob, res, x, Xs, y, Ys)
+end
+
+# SDPX_B200_STATUS_* (include/sdpx_b200.h), 1-based, in SDPX's status names
+const _STATUS = (:Optimal, :IterLimit, :Stalled, :InsufficientPrecision, :NumericalBreakdown,
+                 :MaxRestarts, :TimeLimit)
+
+function _unstack(prob, v)
+    out, o = Matrix{Float64}[], 0
+    for l in 1:prob.dims.L
+        k = prob.dims.k[l]
+        push!(out, reshape(v[o+1:o+k*k], k, k)); o += k * k
+    end
+    return out
+end
+
+function _to_result(prob, res::B200SolveResult, x, Xs, y, Ys)
+    return (status=_STATUS[res.status], iterations=Int(res.iterations),
+            x=x, X=_unstack(prob, Xs), y=y, Y=_unstack(prob, Ys),
+            pObj=res.p_obj, dObj=res.d_obj, pRes=res.p_res, dRes=res.d_res,
+            mixed_iterations=Int(res.mixed_iterations), seconds=res.seconds)
+end
+
+# ------------------------------------------- differentiation (rrule) ---
+"""Solve on the B200 and return the solution (x, X, y, Y) in original
+coordinates; differentiable through the ChainRulesCore `rrule` below."""
+function b200_solve(prob::SDPX.SDPProblem{Float64}; tolerance::Float64=1e-9, device::Int=0)
+    h = B200Handle(prob; device=device)
+    res, (x, Xs, y, Ys) = optimize(h, prob, tolerance)
+    r = _to_result(prob, res, x, Xs, y, Ys)
+    return (x=r.x, X=r.X, y=r.y, Y=r.Y)
+end
+
+"""`rrule` for `b200_solve` (the Julia counterpart of a torch.autograd.Function):
+the pullback factors the Newton system once more at the solution and calls the
+hand-written adjoint kernel (sdpx_b200_adjoint), one KKT solve with the
+cotangents as right-hand side, for the gradients with respect to c, b, C and
+every A_i.  The tangent of `prob` is returned as a NamedTuple with fields
+`c`, `b`, `C` (per block) and `A` (per variable, per block)."""
+function ChainRulesCore.rrule(::typeof(b200_solve), prob::SDPX.SDPProblem{Float64};
+                              tolerance::Float64=1e-9, device::Int=0)
+    sol = b200_solve(prob; tolerance=tolerance, device=device)
+    function b200_solve_pullback(Δ)
+        Δ = ChainRulesCore.unthunk(Δ)
+        m, n = prob.dims.m, prob.dims.n
+        stacked = sum(k -> k * k, prob.dims.k)
+        seed(v, len) = v isa ChainRulesCore.AbstractZero ? C_NULL : Vector{Float64}(v)
+        seedblocks(v) = v isa ChainRulesCore.AbstractZero ? C_NULL :
+                        reduce(vcat, [vec(Matrix{Float64}(b)) for b in v])
+        wx, wy = seed(Δ.x, m), seed(Δ.y, n)
+        WX, WY = seedblocks(Δ.X), seedblocks(Δ.Y)
+        h = B200Handle(prob; device=device)
+        Xs = reduce(vcat, vec.(sol.X)); Ys = reduce(vcat, vec.(sol.Y))
+        _check(h, ccall((:sdpx_b200_set_iterate, libsdpx), Cint,
+                        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                        h.ptr, sol.x, Xs, Ys), "set_iterate")
+        pres = Ref{Float64}(0); dres = Ref{Float64}(0); okb = Ref{Cint}(0)
+        mu = zeros(prob.dims.L)
+        _check(h, ccall((:sdpx_b200_residuals, libsdpx), Cint,
+                        (Ptr{Cvoid}, Ptr{Float64}, Cint, Cint, Ref{Float64}, Ref{Float64},
+                         Ref{Cint}), h.ptr, mu, 1, 1, pres, dres, okb), "residuals")
+        okb[] == 1 || error("solution blocks are not positive definite")
+        _check(h, ccall((:sdpx_b200_schur_build, libsdpx), Cint, (Ptr{Cvoid}, Cint), h.ptr, 0),
+               "schur_build")
+        ok = Ref{Cint}(0); att = Ref{Cint}(0); q = Ref{Float64}(0)
+        _check(h, ccall((:sdpx_b200_factorize, libsdpx), Cint,
+                        (Ptr{Cvoid}, Ref{Cint}, Ref{Cint}, Ref{Float64}), h.ptr, ok, att, q),
+               "factorize")
+        ok[] == 1 || error("the Newton system at the solution could not be factored")
+        gc, gb, gC = zeros(m), zeros(n), zeros(stacked)
+        idx = Int32.(0:m-1)
+        gA = zeros(stacked * m)
+        _check(h, ccall((:sdpx_b200_adjoint, libsdpx), Cint,
+                        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+                         Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int32, Ptr{Int32},
+                         Ptr{Float64}),
+                        h.ptr, wx, wy, WX, WY, gc, n > 0 ? gb : C_NULL, gC, Int32(m), idx, gA),
+               "adjoint")
+        gA_blocks = [_unstack(prob, view(gA, i*stacked+1:(i+1)*stacked)) for i in 0:m-1]
+        dprob = ChainRulesCore.Tangent{typeof(prob)}(; c=gc, b=gb, C=_unstack(prob, gC),
+                                                     A=gA_blocks)
+        return (ChainRulesCore.NoTangent(), dprob)
+    end
+    return sol, b200_solve_pullback
 end
 
 # ------------------------------------------------------------ certificate ---

@@ -7,7 +7,9 @@ import json
 import sys
 from pathlib import Path
 
-ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_gate_fixture.py <path of the SDPX.jl checkout>")
+ref = Path(sys.argv[1])
 base = json.loads((ref / "benchmark/baselines/gates.json").read_text())
 keep = ("status", "iterations", "objective", "relative_gap", "primal_residual", "dual_residual")
 out = {name: {k: base[name][k] for k in keep} for name in ("sdp_closed_form", "sdp_dense")}
