@@ -37,11 +37,60 @@ __global__ void k_gemv_n_reduce(const double* __restrict__ part, long long K, in
   out[row] = s;
 }
 
+// The same partial sums with 128-bit loads: each thread owns the row pair
+// (2q, 2q+1) and reads one double2 per column (K even and A 16-byte aligned,
+// so every column starts on a 16-byte boundary).  Each row accumulates its
+// columns in exactly the order of k_gemv_n_part, so the results are identical.
+__global__ void k_gemv_n_part2(const double* __restrict__ A, long long K, int m,
+                               const double* __restrict__ x, int chunks, double* __restrict__ part) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long K2 = K >> 1;
+  if (q >= K2) return;
+  const int ch = blockIdx.y;
+  const int per = (m + chunks - 1) / chunks;
+  const int i0 = ch * per, i1 = min(m, i0 + per);
+  const double2* p = reinterpret_cast<const double2*>(A) + q;
+  double2 s0 = {0, 0}, s1 = {0, 0}, s2 = {0, 0}, s3 = {0, 0};
+  int i = i0;
+  for (; i + 3 < i1; i += 4) {
+    const double2 a0 = __ldg(p + (long long)i * K2), a1 = __ldg(p + (long long)(i + 1) * K2);
+    const double2 a2 = __ldg(p + (long long)(i + 2) * K2), a3 = __ldg(p + (long long)(i + 3) * K2);
+    const double x0 = x[i], x1 = x[i + 1], x2 = x[i + 2], x3 = x[i + 3];
+    s0.x += a0.x * x0; s0.y += a0.y * x0;
+    s1.x += a1.x * x1; s1.y += a1.y * x1;
+    s2.x += a2.x * x2; s2.y += a2.y * x2;
+    s3.x += a3.x * x3; s3.y += a3.y * x3;
+  }
+  for (; i < i1; ++i) {
+    const double2 a = __ldg(p + (long long)i * K2);
+    s0.x += a.x * x[i];
+    s0.y += a.y * x[i];
+  }
+  double2 r;
+  r.x = (s0.x + s1.x) + (s2.x + s3.x);
+  r.y = (s0.y + s1.y) + (s2.y + s3.y);
+  reinterpret_cast<double2*>(part + (long long)ch * K)[q] = r;
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Partial sums of 𝒜·x over `chunks` column ranges: the 128-bit variant when
+// the stride allows it, else one row per thread.
+static void gemv_n_partials(const double* A, long long K, int m, const double* x, int chunks,
+                            double* part, cudaStream_t st) {
+  if ((K & 1) == 0 && aligned16(A) && aligned16(part)) {
+    dim3 g(ceil_div(K / 2, 256), chunks);
+    k_gemv_n_part2<<<g, 256, 0, st>>>(A, K, m, x, chunks, part);
+  } else {
+    dim3 g(ceil_div(K, 256), chunks);
+    k_gemv_n_part<<<g, 256, 0, st>>>(A, K, m, x, chunks, part);
+  }
+}
+
 void gemv_n(const double* A, long long K, int m, const double* x, double* out, double* part,
             int chunks, cudaStream_t st) {
   if (K == 0) return;
-  dim3 g(ceil_div(K, 256), chunks);
-  k_gemv_n_part<<<g, 256, 0, st>>>(A, K, m, x, chunks, part);
+  gemv_n_partials(A, K, m, x, chunks, part, st);
   k_gemv_n_reduce<<<ceil_div(K, 256), 256, 0, st>>>(part, K, chunks, out);
   SDPX_LAUNCH_CHECK_N(2);
 }
@@ -78,8 +127,7 @@ __global__ void k_gemv_n_reduce_sym(const double* __restrict__ part, long long K
 void gemv_n_sym(const double* Ap, long long Kt, int m, const double* x, const long long* lo,
                 const long long* up, double* out, double* part, int chunks, cudaStream_t st) {
   if (Kt == 0) return;
-  dim3 g(ceil_div(Kt, 256), chunks);
-  k_gemv_n_part<<<g, 256, 0, st>>>(Ap, Kt, m, x, chunks, part);
+  gemv_n_partials(Ap, Kt, m, x, chunks, part, st);
   k_gemv_n_reduce_sym<<<ceil_div(Kt, 256), 256, 0, st>>>(part, Kt, chunks, lo, up, out);
   SDPX_LAUNCH_CHECK_N(2);
 }
@@ -119,10 +167,42 @@ __global__ void k_gemv_t(const double* __restrict__ A, long long K, int m,
   if (threadIdx.x == 0) out[i] = alpha * s + (base ? beta * base[i] : 0.0);
 }
 
+// 128-bit variant (K even, A and z 16-byte aligned): thread t reads the
+// double2 pairs t, t + 512, …, two accumulators per lane of the pair.
+__global__ void k_gemv_t2(const double* __restrict__ A, long long K, int m,
+                          const double* __restrict__ z, double alpha,
+                          const double* __restrict__ base, double beta, double* __restrict__ out) {
+  __shared__ double red[32];
+  const int i = blockIdx.x;
+  const long long K2 = K >> 1;
+  const double2* col = reinterpret_cast<const double2*>(A + (long long)i * K);
+  const double2* z2 = reinterpret_cast<const double2*>(z);
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  long long r = threadIdx.x;
+  for (; r + blockDim.x < K2; r += 2 * blockDim.x) {
+    const double2 a = __ldg(col + r), b = __ldg(col + r + blockDim.x);
+    const double2 u = __ldg(z2 + r), v = __ldg(z2 + r + blockDim.x);
+    s0 += a.x * u.x;
+    s1 += a.y * u.y;
+    s2 += b.x * v.x;
+    s3 += b.y * v.y;
+  }
+  if (r < K2) {
+    const double2 a = __ldg(col + r), u = __ldg(z2 + r);
+    s0 += a.x * u.x;
+    s1 += a.y * u.y;
+  }
+  const double s = block_sum((s0 + s1) + (s2 + s3), red);
+  if (threadIdx.x == 0) out[i] = alpha * s + (base ? beta * base[i] : 0.0);
+}
+
 void gemv_t(const double* A, long long K, int m, const double* z, double alpha, const double* base,
             double beta, double* out, cudaStream_t st) {
   if (m == 0) return;
-  k_gemv_t<<<m, 512, 0, st>>>(A, K, m, z, alpha, base, beta, out);
+  if ((K & 1) == 0 && aligned16(A) && aligned16(z))
+    k_gemv_t2<<<m, 512, 0, st>>>(A, K, m, z, alpha, base, beta, out);
+  else
+    k_gemv_t<<<m, 512, 0, st>>>(A, K, m, z, alpha, base, beta, out);
   SDPX_LAUNCH_CHECK();
 }
 
@@ -137,11 +217,50 @@ __global__ void k_axpbypcz(long long n, double a, const double* x, double b, con
     out[e] = v;
   }
 }
+// 128-bit variant over element pairs (every operand 16-byte aligned); the odd
+// last element, if any, is done by thread 0 of block 0.  Same arithmetic per
+// element as k_axpbypcz.
+__global__ void k_axpbypcz2(long long n, double a, const double* x, double b, const double* y,
+                            double c, const double* z, double* out) {
+  const long long n2 = n >> 1;
+  const double2* x2 = reinterpret_cast<const double2*>(x);
+  const double2* y2 = reinterpret_cast<const double2*>(y);
+  const double2* z2 = reinterpret_cast<const double2*>(z);
+  double2* o2 = reinterpret_cast<double2*>(out);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n2;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double2 xv = x2[e];
+    double2 v = {a * xv.x, a * xv.y};
+    if (y) {
+      const double2 yv = y2[e];
+      v.x += b * yv.x;
+      v.y += b * yv.y;
+    }
+    if (z) {
+      const double2 zv = z2[e];
+      v.x += c * zv.x;
+      v.y += c * zv.y;
+    }
+    o2[e] = v;
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const long long e = n - 1;
+    double v = a * x[e];
+    if (y) v += b * y[e];
+    if (z) v += c * z[e];
+    out[e] = v;
+  }
+}
 void axpbypcz(long long n, double a, const double* x, double b, const double* y, double c,
               const double* z, double* out, cudaStream_t st) {
   if (n == 0) return;
-  int g = std::min(4096, ceil_div(n, 256));
-  k_axpbypcz<<<g, 256, 0, st>>>(n, a, x, b, y, c, z, out);
+  if (aligned16(x) && aligned16(out) && (!y || aligned16(y)) && (!z || aligned16(z))) {
+    const int g = std::min(4096, (int)std::max<long long>(1, ceil_div(n / 2, 256)));
+    k_axpbypcz2<<<g, 256, 0, st>>>(n, a, x, b, y, c, z, out);
+  } else {
+    const int g = std::min(4096, ceil_div(n, 256));
+    k_axpbypcz<<<g, 256, 0, st>>>(n, a, x, b, y, c, z, out);
+  }
   SDPX_LAUNCH_CHECK();
 }
 
@@ -151,9 +270,27 @@ __global__ void k_combine(long long n, double* x, double t, const double* d) {
        e += (long long)gridDim.x * blockDim.x)
     x[e] = x[e] + t * d[e];
 }
+__global__ void k_combine2(long long n, double* x, double t, const double* d) {
+  const long long n2 = n >> 1;
+  double2* x2 = reinterpret_cast<double2*>(x);
+  const double2* d2 = reinterpret_cast<const double2*>(d);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n2;
+       e += (long long)gridDim.x * blockDim.x) {
+    double2 xv = x2[e];
+    const double2 dv = d2[e];
+    xv.x = xv.x + t * dv.x;
+    xv.y = xv.y + t * dv.y;
+    x2[e] = xv;
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) x[n - 1] = x[n - 1] + t * d[n - 1];
+}
 void combine(long long n, double* x, double t, const double* d, cudaStream_t st) {
   if (n == 0) return;
-  k_combine<<<std::min(4096, ceil_div(n, 256)), 256, 0, st>>>(n, x, t, d);
+  if (aligned16(x) && aligned16(d))
+    k_combine2<<<std::min(4096, (int)std::max<long long>(1, ceil_div(n / 2, 256))), 256, 0, st>>>(
+        n, x, t, d);
+  else
+    k_combine<<<std::min(4096, ceil_div(n, 256)), 256, 0, st>>>(n, x, t, d);
   SDPX_LAUNCH_CHECK();
 }
 
