@@ -293,6 +293,22 @@ int sdpx_b200_get_stream(sdpx_b200_handle* h, void** stream);
 /* Number of kernels this library has launched in this process. */
 int sdpx_b200_launch_count(uint64_t* count);
 
+/* Sparse Schur engine — SDPX's `SparseCons` path (`sparse = :on`,
+ * src/types/constraints.jl:26-101; `sparse_schur_block!` src/schur.jl:936-1032,
+ * `_two_sided_coo_product!` :601-656, `_dot_dense_coo` :566-579, the serial
+ * block-order reduction :1173-1197).  enable = 1 makes every FP64 Schur build
+ * (not the identity-metric one of the cold start, not the mixed mode) take
+ * the coefficients as flat coordinate entries per dense block and active
+ * variable, S_ij += ⟨Y_l·A_i·X_l⁻¹, A_j⟩ over the active pairs, work
+ * Σ_p nnz_p·k² + Σ_{p≤r} nnz_r per block; 1×1 blocks keep their Gram on the
+ * FP64 tiles.  Every dense block order must be ≤ 160 (else -2 and a message).
+ * The entries are extracted from the device copy of 𝒜 (after equilibration)
+ * on the first build. */
+int sdpx_b200_set_sparse_schur(sdpx_b200_handle* h, int enable);
+/* Active (block, variable) positions and stored entries of that form. */
+int sdpx_b200_sparse_schur_info(sdpx_b200_handle* h, int64_t* active_positions,
+                                int64_t* stored_entries);
+
 /* Allocation-free Gram (Schur) product — no counterpart in the reference.
  *
  * S = Pᵀ P for a K×m column-major FP64 matrix P already in device memory

@@ -383,6 +383,7 @@ class OracleBackend:
         self.kept = {}
         self.best = None
         self.eq_applied = False
+        self.sparse_schur = False      # `sparse = :on`: the SparseCons Schur path
 
     # -- helpers -----------------------------------------------------------
     def _mat(self, l, vec):
@@ -469,6 +470,11 @@ class OracleBackend:
     # -- Schur (src/schur.jl:511-562) -----------------------------------------
     def schur_build(self, identity=False):
         m = self.m
+        if self.sparse_schur and not identity:
+            # SparseCons path (src/schur.jl:936-1032, 1173-1197)
+            from oracle.sparse_oracle import sparse_schur_build
+            self.S = sparse_schur_build(self.Av, self.k, self.LX, self.Y, m)
+            return self.S
         S = np.zeros((m, m))
         for l, kl in enumerate(self.k):
             A3 = self.Av[l].reshape(m, kl, kl)

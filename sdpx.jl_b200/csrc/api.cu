@@ -28,6 +28,7 @@
 #include "chol.h"
 #include "dbuf.h"
 #include "equality.h"
+#include "sparse_schur.h"
 #include "mixed.h"
 #include "ozaki.h"
 #include "schur_bf16.h"
@@ -157,6 +158,18 @@ struct Handle {
   // FP64 Gram engine of the Schur SYRK: 0 = FP64 DMMA tiles, 1 = exact int8
   // digit products (48-bit digits, int32 accumulation, FP64 level sums).
   int gram_engine = 1;
+  // Sparse Schur engine (SDPX's SparseCons path): per dense block the active
+  // variables (ascending) and their flat coordinate entries, rebuilt from 𝒜
+  // when 𝒜 changes; the 1×1 group keeps its rank-nd Gram on the FP64 tiles.
+  bool sparse_schur = false;
+  unsigned long long coo_ver = 0;
+  std::vector<int> sp_na;
+  std::vector<long long> sp_act_off;
+  long long sp_active = 0, sp_nnz = 0;
+  DBuf<int> sp_cnt, sp_ids, sp_lin;
+  DBuf<long long> sp_ptr;
+  DBuf<double> sp_val, Xinv, diag_partial;
+  SyrkPlan diag_syrk{};
   OzakiPlan oz_plan;
   DBuf<int8_t> oz_digits;
   DBuf<int> oz_exps, oz_err;
@@ -1085,7 +1098,88 @@ struct Handle {
       ozaki_gemm(h, sms, oz_err.p, st);
     }
   }
+  // Flat coordinate form of every dense block's coefficients (the
+  // `SparseBlockCOO` of src/types/constraints.jl:60-101 with `schur_order`
+  // ascending): count the stored entries of each (block, variable) slab on the
+  // device, scan on the host, compact on the device in linear-index order.
+  void build_coo() {
+    const int nb = (int)dense.size();
+    for (auto& b : dense)
+      if (b.k > kSparseSchurMaxK)
+        throw std::invalid_argument("sparse Schur: block order " + std::to_string(b.k) +
+                                    " exceeds 160");
+    sp_cnt.alloc(std::max<size_t>(1, (size_t)nb * m));
+    for (int b = 0; b < nb; ++b)
+      coo_count(A.p, K, m, dense[b].off, dense[b].k * dense[b].k, sp_cnt.p + (size_t)b * m, st);
+    std::vector<int> cnt((size_t)nb * m);
+    if (!cnt.empty()) d2h(cnt.data(), sp_cnt.p, cnt.size() * sizeof(int));
+    sync();
+    std::vector<int> ids;
+    std::vector<long long> ptr(1, 0);
+    sp_na.assign(nb, 0);
+    sp_act_off.assign(nb, 0);
+    for (int b = 0; b < nb; ++b) {
+      sp_act_off[b] = (long long)ids.size();
+      for (int i = 0; i < m; ++i) {
+        const int c = cnt[(size_t)b * m + i];
+        if (c == 0) continue;
+        ids.push_back(i);
+        ptr.push_back(ptr.back() + c);
+        ++sp_na[b];
+      }
+    }
+    sp_active = (long long)ids.size();
+    sp_nnz = ptr.back();
+    sp_ids.alloc(std::max<long long>(1, sp_active));
+    sp_ptr.alloc(sp_active + 1);
+    sp_lin.alloc(std::max<long long>(1, sp_nnz));
+    sp_val.alloc(std::max<long long>(1, sp_nnz));
+    if (sp_active) h2d(sp_ids.p, ids.data(), ids.size() * sizeof(int));
+    h2d(sp_ptr.p, ptr.data(), ptr.size() * sizeof(long long));
+    for (int b = 0; b < nb; ++b)
+      coo_fill(A.p, K, dense[b].off, dense[b].k * dense[b].k, sp_ids.p + sp_act_off[b],
+               sp_ptr.p + sp_act_off[b], sp_na[b], sp_lin.p, sp_val.p, st);
+    sync();
+    coo_ver = a_ver;
+  }
+  // S from the current block factors by the sparse engine: the 1×1 group's
+  // Gram first, then every dense block's active pairs in block order (one
+  // launch per block, so each entry of S sums its block terms in a fixed order).
+  void schur_sparse() {
+    if (coo_ver != a_ver) build_coo();
+    if (nd) {
+      diag_panel(K, m, nd, od, A.p, LX.p, MY.p, Pc.p, st);
+      if (diag_syrk.ntri == 0 || diag_syrk.bm == 0) {
+        diag_syrk = plan_syrk_f64(m, nd, sms);
+        diag_partial.alloc(diag_syrk.partial_doubles);
+      }
+      Opnd Pd;
+      Pd.base = Pc.p + od;
+      Pd.kstride = 1;
+      Pd.inner = 1 << 30;
+      Pd.inner_stride = K;
+      Pd.outer_stride = 0;
+      Pd.mn_extent = m;
+      Pd.k_extent = nd;
+      syrk_lower_f64(Pd, diag_syrk, diag_partial.p, S.p, m, m, 0.0, st);
+    } else {
+      SDPX_CUDA(cudaMemsetAsync(S.p, 0, sizeof(double) * (size_t)m * m, st));
+    }
+    if (!dense.empty()) {
+      Xinv.alloc(K);
+      for (auto& b : dense)  // X⁻¹ = WᵀW with W = L_X⁻¹
+        blk_gemm(blk_as_At(W.p, b.off, b.k), true, blk_as_B(W.p, b.off, b.k), true, Xinv.p, b,
+                 1.0, 0.0, KR_FULL);
+      for (size_t b = 0; b < dense.size(); ++b)
+        sparse_schur_block(Y.p + dense[b].off, Xinv.p + dense[b].off, dense[b].k,
+                           sp_ptr.p + sp_act_off[b], sp_lin.p, sp_val.p, sp_ids.p + sp_act_off[b],
+                           sp_na[b], S.p, m, st);
+    }
+    mirror_lower(m, S.p, st);
+  }
+
   void schur_build_fp64(int identity) {
+    if (!identity && sparse_schur) return schur_sparse();
     const double* panel = A.p;
     if (!identity) {
       kt_begin(3);
@@ -2935,6 +3029,26 @@ int sdpx_b200_gram_noalloc(const double* P, int64_t K, int32_t m, double* S, voi
     g_noalloc_error = ex.what();
     return -2;
   }
+}
+int sdpx_b200_set_sparse_schur(sdpx_b200_handle* h, int enable) {
+  GUARD(h, {
+    if (enable != 0 && enable != 1) throw std::invalid_argument("enable must be 0 or 1");
+    if (enable) {
+      for (auto& b : h->h.dense)
+        if (b.k > sdpx::kSparseSchurMaxK)
+          throw std::invalid_argument("sparse Schur: block order " + std::to_string(b.k) +
+                                      " exceeds 160");
+    }
+    h->h.sparse_schur = enable == 1;
+  });
+}
+int sdpx_b200_sparse_schur_info(sdpx_b200_handle* h, int64_t* active_positions,
+                                int64_t* stored_entries) {
+  GUARD(h, {
+    if (h->h.coo_ver != h->h.a_ver) h->h.build_coo();
+    if (active_positions) *active_positions = h->h.sp_active;
+    if (stored_entries) *stored_entries = h->h.sp_nnz;
+  });
 }
 int sdpx_b200_set_gram_engine(sdpx_b200_handle* h, int engine) {
   GUARD(h, {

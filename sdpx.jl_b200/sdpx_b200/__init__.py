@@ -27,7 +27,7 @@ __all__ = ["SolverOptions", "SDPResult", "Status", "SDPProblem", "Equilibration"
 def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
           maximum_iterations: int = 200, scaling: str = "auto", device: int = 0,
           trace=None, certificate: bool = False, driver: str = "native",
-          **kwargs) -> SDPResult:
+          sparse_schur: bool = False, **kwargs) -> SDPResult:
     """Solve `prob` on the B200 (mirrors `SDPX.solve(prob; tolerance)`).
 
     `precision="fp64"` is the plain FP64 device path; `precision="mixed"`
@@ -38,12 +38,16 @@ def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
     (`result.certificate`) before the device data is released.  The loop runs
     inside the library (`driver="native"`, sdpx_b200_optimize) unless
     `driver="python"` or a `trace` list asks for the Python driver.
+    `sparse_schur=True` builds the FP64 Schur complement from the coefficients'
+    stored entries (SDPX's `sparse = :on`), for structurally sparse A_i.
     """
     from .cuda_backend import CudaBackend
     opts = SolverOptions(iter_max=maximum_iterations, scaling=scaling, precision=precision,
                          **kwargs).with_tolerance(tolerance)
     with CudaBackend(prob, precision=precision, device=device,
                      condition_limit=opts.mixed_condition_limit) as be:
+        if sparse_schur:
+            be.set_sparse_schur(True)
         if driver == "native" and trace is None:
             result = be.optimize(opts)
         else:

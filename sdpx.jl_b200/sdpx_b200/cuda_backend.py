@@ -139,6 +139,8 @@ _SIGS = {
     "sdpx_b200_phase_times": [C.c_void_p, _dp, C.c_int],
     "sdpx_b200_kernel_times": [C.c_void_p, _dp],
     "sdpx_b200_set_gram_engine": [C.c_void_p, C.c_int],
+    "sdpx_b200_set_sparse_schur": [C.c_void_p, C.c_int],
+    "sdpx_b200_sparse_schur_info": [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "sdpx_b200_counters": [C.c_void_p, C.POINTER(C.c_int64)],
     "sdpx_b200_reset": [C.c_void_p],
     "sdpx_b200_get_precision": [C.c_void_p, _ip, _ip, _dp],
@@ -657,6 +659,17 @@ class CudaBackend:
         """FP64 Schur engine (Gram and block products): "dmma" (FP64 tensor
         tiles) or "int8" (exact int8 digit products, eight digits = 55 bits)."""
         self._call("sdpx_b200_set_gram_engine", {"dmma": 0, "int8": 1}[engine])
+
+    def set_sparse_schur(self, enable: bool = True):
+        """Schur builds from flat coordinate entries per block and active
+        variable (SDPX's `sparse = :on` SparseCons path) instead of the dense
+        block products; FP64 precision mode."""
+        self._call("sdpx_b200_set_sparse_schur", 1 if enable else 0)
+
+    def sparse_schur_info(self) -> dict:
+        a, e = C.c_int64(), C.c_int64()
+        self._call("sdpx_b200_sparse_schur_info", C.byref(a), C.byref(e))
+        return dict(active_positions=int(a.value), stored_entries=int(e.value))
 
     def kernel_times(self) -> dict:
         """Device ms of the latest Schur kernel launches (see sdpx_b200_kernel_times)."""

@@ -4,6 +4,8 @@
   (benchmark/gates.jl:96-199), rebuilt from the same written-out 64-bit LCG so
   they are bit-identical to the ones SDPX records baselines for.
 * `toy_t1`: the 2×2 toy problem of test/correctness.jl:65-80 (optimum 2√6).
+* `sdpa_sparse`: the same construction with structurally sparse coefficients
+  (a few stored entries per A_i and block), the regime of SDPX's SparseCons path.
 * `sdpa_dense`: strictly feasible dense SDPs in SDPA primal-dual form, mapped to
   SDPX's core form.  With `blocks=[50], lp=0, m=100` this is the n=50/m=100
   workload; with `blocks=[400, 200], lp=500, m=2000` it is the two-block plus
@@ -194,6 +196,70 @@ def _sdpa_dense(m, blocks, lp, seed):
         A_sdpx.append(-a_lp.reshape(m, lp, 1, 1))
         C_sdpx.append(-c_lp)
     return _assemble(-b, A_sdpx, C_sdpx, list(blocks), lp), y0
+
+
+def sdpa_sparse(m: int, blocks: Sequence[int], lp: int = 0, active: float = 0.5,
+                pairs: Sequence[int] = (1, 3), seed: int = 0) -> SDPProblem:
+    """Strictly feasible SDP with structurally sparse coefficients (the regime
+    of SDPX's `SparseCons` path: every A_i touches a few entries of a block).
+
+    Draw order from `numpy.random.default_rng(seed)`, per PSD block of order n:
+    the activity mask (m draws U(0,1) < `active`), the pair counts
+    q_i ~ U{pairs[0]..pairs[1]} (m draws), then for the Σq_i pairs their rows,
+    columns (U{0..n−1}) and values (N(0,1)); pair (r, c, v) adds v at (r, c)
+    and (c, r) of A_i (once when r = c), so an active A_i stores 1–2·q_i
+    entries.  A variable active in no block is then made active in block
+    i mod L with one diagonal pair of value 1.  Then, as `sdpa_dense`, per
+    block X0 = I + 0.1·WWᵀ/n, the LP block (aᵢ ~ N(0,1), x0 ~ U(0.5,1.5)),
+    y0 ~ N(0,1)^m, per block Z0 = I + 0.1·VVᵀ/n, LP slack s0 ~ U(0.5,1.5);
+    b_i = Σ⟨A_i, X0⟩ + a_iᵀx0, C = Σ y0_i A_i + Z0, mapped to SDPX's form."""
+    rng = np.random.default_rng(seed)
+    As: List[np.ndarray] = []
+    acts = []
+    for n in blocks:
+        A = np.zeros((m, n, n))
+        act = rng.random(m) < active
+        q = rng.integers(pairs[0], pairs[1] + 1, size=m)
+        q = np.where(act, q, 0)
+        tot = int(q.sum())
+        var = np.repeat(np.arange(m), q)
+        r = rng.integers(0, n, size=tot)
+        c = rng.integers(0, n, size=tot)
+        v = rng.standard_normal(tot)
+        np.add.at(A, (var, r, c), v)
+        off = r != c
+        np.add.at(A, (var[off], c[off], r[off]), v[off])
+        As.append(A)
+        acts.append(act)
+    if blocks:
+        anyact = np.logical_or.reduce(acts)
+        for i in np.nonzero(~anyact)[0]:
+            l = int(i) % len(blocks)
+            As[l][i, 0, 0] = 1.0
+    X0s = []
+    for n in blocks:
+        W = rng.standard_normal((n, n))
+        X0s.append(np.eye(n) + 0.1 * (W @ W.T) / n)
+    if lp > 0:
+        a_lp = rng.standard_normal((m, lp))
+        x0_lp = rng.uniform(0.5, 1.5, lp)
+    b = np.zeros(m)
+    for A, X0 in zip(As, X0s):
+        b += A.reshape(m, -1) @ X0.reshape(-1)
+    if lp > 0:
+        b += a_lp @ x0_lp
+    y0 = rng.standard_normal(m)
+    Cs = []
+    for A, n in zip(As, blocks):
+        V = rng.standard_normal((n, n))
+        Cs.append((y0 @ A.reshape(m, -1)).reshape(n, n) + np.eye(n) + 0.1 * (V @ V.T) / n)
+    A_sdpx = [-A for A in As]
+    C_sdpx = [-C for C in Cs]
+    if lp > 0:
+        s0 = rng.uniform(0.5, 1.5, lp)
+        A_sdpx.append(-a_lp.reshape(m, lp, 1, 1))
+        C_sdpx.append(-(y0 @ a_lp + s0))
+    return _assemble(-b, A_sdpx, C_sdpx, list(blocks), lp)
 
 
 def _assemble(c, A_sdpx, C_sdpx, blocks, lp) -> SDPProblem:
