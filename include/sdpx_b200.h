@@ -216,6 +216,21 @@ int sdpx_b200_adjoint(sdpx_b200_handle* h, const double* wx, const double* wy, c
                       const double* WY, double* grad_c, double* grad_b, double* grad_C,
                       int32_t nA, const int32_t* A_index, double* grad_A);
 
+/* The same gradient (no equality rows: n = 0) with the linear system solved
+ * to double-double (Float64x2) accuracy: X⁻¹ by Newton–Schulz steps from the
+ * FP64 inverse, every product of S·v = 𝒜ᵀ(X⁻¹ mat(𝒜v) Y) and of the seeds in
+ * double-double, and λ refined refine_steps times on the FP64 factor with
+ * double-double residuals (the low-precision factor / high-precision
+ * residual scheme of `_solve_mixed_kkt_guarded!`,
+ * src/kernels/mixed_precision_kkt.jl:1475-1586, one level up).  Near a
+ * solution S is ill-conditioned and the single FP64 solve of
+ * sdpx_b200_adjoint loses κ(S)·eps.  residual (may be NULL) =
+ * ‖w − S·λ‖∞ / ‖w‖∞ after the last step, in double-double. */
+int sdpx_b200_adjoint_refined(sdpx_b200_handle* h, const double* wx, const double* WX,
+                              const double* WY, double* grad_c, double* grad_C, int32_t nA,
+                              const int32_t* A_index, double* grad_A, int32_t refine_steps,
+                              double* residual);
+
 /* ---- The whole interior-point solve inside the library -------------------
  * SDPX's `_solve_pipeline!` for the dense route (src/solver/interior_point.jl:
  * 3131-3571: Ruiz scaling, KKT cold start :699-1287, core loop :1323-2687 with

@@ -17,7 +17,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
 SOURCES = ["api.cu", "blas_f64.cu", "chol.cu", "vec_kernels.cu", "mixed_f32.cu", "schur_bf16.cu",
-           "normal.cu", "certificate.cu", "ozaki.cu", "equality.cu", "sparse_schur.cu"]
+           "normal.cu", "certificate.cu", "ozaki.cu", "equality.cu", "sparse_schur.cu",
+           "dd_kernels.cu"]
 # Per-file flags.  normal.cu evaluates the reference's scalar cone recurrences
 # and must round every product and sum separately (no FMA contraction).
 FILE_FLAGS = {"normal.cu": ["--fmad=false"]}

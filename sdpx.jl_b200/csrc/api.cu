@@ -29,6 +29,7 @@
 #include "dbuf.h"
 #include "equality.h"
 #include "sparse_schur.h"
+#include "dd_kernels.h"
 #include "mixed.h"
 #include "ozaki.h"
 #include "schur_bf16.h"
@@ -2586,6 +2587,16 @@ struct Handle {
   // ------------------------------------------------ adjoint (adjoint_api.inc)
   DBuf<double> adj_D, adj_W, adj_G, adj_L, adj_Z, adj_zero, adj_w, adj_p, adj_dy;
   void adj_xinv_m_y(const double* Mst, double* Zout);
+  // Double-double (Float64x2) workspace of the refined adjoint: pairs
+  // (hi, lo) of stacked K-vectors and m-vectors.
+  DBuf<double> ddXi_h, ddXi_l, ddT_h, ddT_l, ddU_h, ddU_l, ddV_h, ddV_l, ddD_h, ddD_l;
+  DBuf<double> ddp_h, ddp_l, ddw_h, ddw_l, ddlam_h, ddlam_l, ddu_h, ddu_l;
+  void dd_prepare_inverse();
+  void dd_xinv_m_y(const double* Mh, const double* Ml, double* Zh, double* Zl);
+  void dd_schur_apply(const double* vh, const double* vl, double* oh, double* ol);
+  void adjoint_refined(const double* hwx, const double* hWX, const double* hWY, double* gc,
+                       double* gC, int nA, const int32_t* Aidx, double* gA, int steps,
+                       double* residual);
   void adjoint(const double* hwx, const double* hwy, const double* hWX, const double* hWY,
                double* gc, double* gb, double* gC, int nA, const int32_t* Aidx, double* gA);
   void equality_panel(const double* Li);
@@ -2875,6 +2886,13 @@ int sdpx_b200_adjoint(sdpx_b200_handle* h, const double* wx, const double* wy, c
                       const double* WY, double* grad_c, double* grad_b, double* grad_C,
                       int32_t nA, const int32_t* A_index, double* grad_A) {
   GUARD(h, h->h.adjoint(wx, wy, WX, WY, grad_c, grad_b, grad_C, nA, A_index, grad_A));
+}
+int sdpx_b200_adjoint_refined(sdpx_b200_handle* h, const double* wx, const double* WX,
+                              const double* WY, double* grad_c, double* grad_C, int32_t nA,
+                              const int32_t* A_index, double* grad_A, int32_t refine_steps,
+                              double* residual) {
+  GUARD(h, h->h.adjoint_refined(wx, WX, WY, grad_c, grad_C, nA, A_index, grad_A, refine_steps,
+                                residual));
 }
 void sdpx_b200_default_options(sdpx_b200_solve_options* o) {
   if (!o) return;

@@ -59,12 +59,16 @@ def solve(prob: SDPProblem, *, tolerance: float = 1e-8, precision: str = "fp64",
 
 
 def adjoint(prob: SDPProblem, result: SDPResult, *, wx=None, wy=None, WX=None, WY=None,
-            A_index=(), device: int = 0) -> dict:
+            A_index=(), device: int = 0, refine: int = 0) -> dict:
     """Gradient of L = ⟨wx, x⟩ + ⟨wy, y⟩ + Σ⟨WX_l, X_l⟩ + Σ⟨WY_l, Y_l⟩ at the
     returned solution with respect to the original data c, b, C and the
     coefficients A_i of `A_index` (no counterpart in SDPX).  The Newton system
     is factored once more at the solution, on the original (unscaled) data in
-    FP64, and one KKT solve gives every gradient (sdpx_b200_adjoint)."""
+    FP64, and one KKT solve gives every gradient (sdpx_b200_adjoint).  With
+    `refine` > 0 (no equality rows) the system is solved to double-double
+    accuracy with that many refinement steps (sdpx_b200_adjoint_refined): near
+    a solution the Schur matrix is ill-conditioned enough that one FP64 solve
+    is accurate to only ~1e-5."""
     from .cuda_backend import CudaBackend
     with CudaBackend(prob, precision="fp64", device=device) as be:
         be.set_iterate(result.x, result.X, result.Y, y=result.y)
@@ -72,6 +76,10 @@ def adjoint(prob: SDPProblem, result: SDPResult, *, wx=None, wy=None, WX=None, W
         be.schur_build()
         if not be.factorize()["ok"]:
             raise RuntimeError("the Newton system at the solution could not be factored")
+        if refine > 0:
+            if prob.n or wy is not None:
+                raise ValueError("the refined adjoint has no equality rows")
+            return be.adjoint_refined(wx, WX, WY, A_index, steps=refine)
         return be.adjoint(wx, wy, WX, WY, A_index)
 
 

@@ -164,6 +164,8 @@ _SIGS = {
                             C.POINTER(C.c_int32)],
     "sdpx_b200_adjoint": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int32,
                           C.POINTER(C.c_int32), _dp],
+    "sdpx_b200_adjoint_refined": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, C.c_int32,
+                                  C.POINTER(C.c_int32), _dp, C.c_int32, _dp],
     "sdpx_b200_certificate_eq": [C.c_void_p, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
                                  C.c_double, C.c_int32, C.POINTER(CertificateResult)],
 }
@@ -398,6 +400,27 @@ class CudaBackend:
         return dict(grad_c=gc, grad_b=gb, grad_C=self._split(gC),
                     grad_A=[self._split(gA[q * self.Ku:(q + 1) * self.Ku])
                             for q in range(idx.size)])
+
+    def adjoint_refined(self, wx=None, WX=None, WY=None, A_index=(), steps: int = 3):
+        """The adjoint's linear system solved to double-double accuracy
+        (sdpx_b200_adjoint_refined; no equality rows).  Adds `residual`, the
+        relative double-double residual of the refined solve."""
+        def vec(a, size):
+            return None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(size)
+        wxv = vec(wx, self.m)
+        WXs = None if WX is None else self._join(WX)
+        WYs = None if WY is None else self._join(WY)
+        idx = np.ascontiguousarray(A_index, dtype=np.int32)
+        gc, gC = np.zeros(self.m), np.zeros(self.Ku)
+        gA = np.zeros(max(1, idx.size) * self.Ku)
+        res = C.c_double()
+        ptr = lambda a: None if a is None else _p(a)
+        self._call("sdpx_b200_adjoint_refined", ptr(wxv), ptr(WXs), ptr(WYs), _p(gc), _p(gC),
+                   int(idx.size), idx.ctypes.data_as(C.POINTER(C.c_int32)), _p(gA), int(steps),
+                   C.byref(res))
+        return dict(grad_c=gc, grad_C=self._split(gC),
+                    grad_A=[self._split(gA[q * self.Ku:(q + 1) * self.Ku])
+                            for q in range(idx.size)], residual=float(res.value))
 
     def equality_info(self):
         """(kind, rank, quality) of the current equality factor."""
