@@ -239,7 +239,7 @@ def dd_adjoint(prob, x, X, Y, wx=None, WX=None, WY=None, A_index=(), refine=4):
     S = np.zeros((m, m))
     for l, kl in enumerate(prob.k):
         A3 = prob.Av[l].reshape(m, kl, kl)
-        T = np.einsum("ab,ibc,cd->iad", Xi[l].to_float(), A3, np.asarray(Y[l]))
+        T = np.matmul(np.matmul(Xi[l].to_float(), A3), np.asarray(Y[l]))
         S += prob.Av[l] @ T.reshape(m, -1).T
     S = 0.5 * (S + S.T)
     fac = sla.cho_factor(S, lower=True)
