@@ -60,13 +60,13 @@ NORMAL_WORKLOAD = dict(m=3000, n_lp=20000, cones=[64] * 100, density=0.1,
 # B ~ N(0,1) and b = Bᵀy0 at the generator's strictly feasible point).
 EQ_ROWS = 64
 # Differentiable parametric SDP (SDPA-form generator, one PSD block n = 200,
-# m = 500): gradient of ⟨W, X_sdpa⟩ + ⟨v, y_sdpa⟩, i.e. of ⟨W, Y⟩ + ⟨v, x⟩ in
-# SDPX's form, w.r.t. c, C and A_1..A_10.  The forward solve stops at 1e-7:
-# asked for 1e-9, the FP64 path (the CPU restatement too) keeps iterating to
-# the equilibrated tolerance 1e-9/objective_scale and ends in
-# NumericalBreakdown near a 2e-11 gap with X's smallest eigenvalues at 5e-13,
-# where the linearised KKT system has no meaningful derivative.
-ADJ_WORKLOAD = dict(m=500, blocks=[200], lp=0, instances=4, A_count=10, tol=1e-7)
+# m = 500, 64 instances): gradient of ⟨W, X_sdpa⟩ + ⟨v, y_sdpa⟩, i.e. of
+# ⟨W, Y⟩ + ⟨v, x⟩ in SDPX's form, w.r.t. c, C and A_1..A_10, after a forward
+# solve to a 1e-9 gap.  The forward solve runs without equilibration: with it
+# the gap tolerance becomes 1e-9/objective_scale, which the FP64 path (the CPU
+# restatement too) cannot reach on this shape (NumericalBreakdown near 2e-11).
+ADJ_WORKLOAD = dict(m=500, blocks=[200], lp=0, instances=64, A_count=10, tol=1e-9,
+                    scaling="none", refine=3)
 # Structurally sparse SDP in the regime of SDPX's SparseCons path (the lattice
 # bootstrap shape its sparse engine was tuned on: 32 PSD blocks of order
 # 23–74, each coefficient storing 2–6 entries per block it touches).
@@ -280,17 +280,20 @@ def bench_batch(args, world, rank, local):
 
 
 def bench_adjoint(args, world, rank, local):
-    """Forward solve to 1e-9 plus the adjoint gradient on a few instances of the
-    differentiable-SDP shape; device times with CUDA events, the oracle's
-    adjoint (same factor-at-solution + one KKT solve) timed beside it."""
+    """Forward solves plus adjoint gradients on the differentiable-SDP shape
+    (device times with CUDA events on the handle's stream): the FP64 adjoint
+    (one KKT solve on the factor at the solution) and the refined adjoint (the
+    same system solved to double-double accuracy); on one instance both are
+    compared with the double-double CPU implicit-KKT gradient."""
     import numpy as np
     import torch
-    from sdpx_b200 import SolverOptions, adjoint, generators as G
+    from sdpx_b200 import SolverOptions, generators as G
     from sdpx_b200.cuda_backend import CudaBackend
-    from sdpx_b200.problem import SDPProblem
     wl = ADJ_WORKLOAD
-    solve_s, adj_s, iters = [], [], []
-    last = None
+    idx = tuple(range(wl["A_count"]))
+    opts = SolverOptions(precision="fp64", scaling=wl["scaling"]).with_tolerance(wl["tol"])
+    solve_s, adj64_s, adjref_s, statuses, iters, residuals = [], [], [], [], [], []
+    first = None
     for inst in range(wl["instances"]):
         prob = G.sdpa_dense(m=wl["m"], blocks=wl["blocks"], lp=wl["lp"],
                             seed=1000 + 64 * rank + inst)
@@ -300,159 +303,73 @@ def bench_adjoint(args, world, rank, local):
         W = [Wm + Wm.T]
         with CudaBackend(prob, precision="fp64", device=local) as be:
             st = torch.cuda.ExternalStream(be.stream_handle())
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
             torch.cuda.synchronize()
-            e0.record(st)
-            r = be.optimize(SolverOptions(precision="fp64").with_tolerance(wl["tol"]))
-            e1.record(st)
+            ev[0].record(st)
+            r = be.optimize(opts)
+            ev[1].record(st)
             torch.cuda.synchronize()
-            solve_s.append(e0.elapsed_time(e1) / 1000.0)
-            iters.append((r.iterations, r.status.value))
-            t0 = time.perf_counter()
+            solve_s.append(ev[0].elapsed_time(ev[1]) / 1000.0)
+            statuses.append(r.status.value)
+            iters.append(r.iterations)
             be.reset()
+            ev[0].record(st)
             be.set_iterate(r.x, r.X, r.Y)
             be.compute_residuals([0.0] * prob.L, True, True)
             be.schur_build()
             be.factorize()
-            g = be.adjoint(wx=v, WY=W, A_index=tuple(range(wl["A_count"])))
+            g64 = be.adjoint(wx=v, WY=W, A_index=idx)
+            ev[1].record(st)
+            gref = be.adjoint_refined(wx=v, WY=W, A_index=idx, steps=wl["refine"])
+            ev[2].record(st)
             torch.cuda.synchronize()
-            adj_s.append(time.perf_counter() - t0)
-        last = (prob, r, v, W, g)
-    # one directional check of the last instance against central differences
-    # of complete GPU solves (h = 1e-3)
-    prob, r, v, W, g = last
-    rng = np.random.default_rng(99)
-    E = rng.standard_normal((prob.k[0], prob.k[0]))
-    E = E + E.T
-
-    def loss_at(C0):
-        q = SDPProblem(prob.c, prob.k, prob.Av, [C0], prob.B, prob.b)
-        with CudaBackend(q, precision="fp64", device=local) as b2:
-            rr = b2.optimize(SolverOptions(precision="fp64").with_tolerance(wl["tol"]))
-        return float(v @ rr.x + np.sum(W[0] * rr.Y[0]))
-
-    h = 1e-3
-    fd = (loss_at(prob.C[0] + h * E) - loss_at(prob.C[0] - h * E)) / (2 * h)
-    ad = float(np.sum(g["grad_C"][0] * E))
+            adj64_s.append(ev[0].elapsed_time(ev[1]) / 1000.0)
+            adjref_s.append(ev[0].elapsed_time(ev[1]) / 1000.0 + ev[1].elapsed_time(ev[2]) / 1000.0)
+            residuals.append(gref["residual"])
+        if first is None:
+            first = (prob, r, v, W, g64, gref)
     out = {"workload": (f"differentiable SDP: {wl['instances']} instances, m={wl['m']}, one PSD "
-                        f"block n={wl['blocks'][0]}, forward to {wl['tol']:g}, gradient of "
-                        f"<W, X_sdpa> + <v, y_sdpa> w.r.t. c, C, A_1..A_{wl['A_count']}"),
+                        f"block n={wl['blocks'][0]}, forward to {wl['tol']:g} (scaling "
+                        f"{wl['scaling']}), gradient of <W, X_sdpa> + <v, y_sdpa> w.r.t. c, C, "
+                        f"A_1..A_{wl['A_count']}"),
            "forward_s_per_instance": statistics.median(solve_s),
-           "adjoint_s_per_instance": statistics.median(adj_s),
-           "iterations_status": iters, "unit": "s",
-           "fd_check": {"direction": "random symmetric dC, last instance", "adjoint": ad,
-                        "central_difference_h1e-3": fd,
-                        "rel_diff": abs(ad - fd) / max(abs(fd), 1e-12)},
+           "optimal": sum(s == "Optimal" for s in statuses), "instances": wl["instances"],
+           "iterations_median": statistics.median(iters),
+           "adjoint_fp64_s_per_instance": statistics.median(adj64_s),
+           "adjoint_refined_s_per_instance": statistics.median(adjref_s),
+           "refined_residual_max": max(residuals), "unit": "s",
            "adjoint_includes": "refactor at the solution (residuals, Schur build, FP64 "
-                               "Cholesky) + one KKT solve + gradient passes + host copies"}
+                               "Cholesky) + the KKT solve(s) + gradient passes + host copies; "
+                               "refined: + Newton-Schulz X^-1, double-double S·v per step"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.dd_oracle import dd_adjoint
         from oracle.sdpx_oracle import OracleBackend
-        prob, r, v, W, g = last
+        prob, r, v, W, g64, gref = first
         t0 = time.perf_counter()
         ob = OracleBackend(prob)
         ob.set_iterate(r.x, r.X, r.Y)
         ob.compute_residuals([0.0] * prob.L, True, True)
         ob.schur_build()
         ob.factorize()
-        go = ob.adjoint(wx=v, WY=W, A_index=tuple(range(wl["A_count"])))
+        ob.adjoint(wx=v, WY=W, A_index=idx)
         out["cpu_adjoint_s"] = time.perf_counter() - t0
-        out["cpu_kind"] = "port: the oracle's adjoint (NumPy/OpenBLAS, all host cores)"
-        out["max_rel_diff_grad_C_vs_cpu"] = float(
-            np.max(np.abs(g["grad_C"][0] - go["grad_C"][0])) /
-            max(1.0, float(np.max(np.abs(go["grad_C"][0])))))
-    return out
-
-
-def bench_sparse(args, world, rank, local):
-    """Sparse Schur engine against the dense FP64 engines on one structurally
-    sparse instance: the Schur build at the solution iterate (device events,
-    both engines) and complete solves with each; the oracle's sparse assembly
-    of the same iterate is the CPU baseline."""
-    import numpy as np
-    import torch
-    from sdpx_b200 import SolverOptions, generators as G
-    from sdpx_b200.cuda_backend import CudaBackend
-    wl = SPARSE_WORKLOAD
-    ks = np.random.default_rng(wl["seed"]).integers(wl["kmin"], wl["kmax"] + 1, wl["blocks"])
-    prob = G.sdpa_sparse(m=wl["m"], blocks=[int(k) for k in ks], active=wl["active"],
-                         pairs=wl["pairs"], seed=wl["seed"] + rank)
-    opts = SolverOptions(precision="fp64").with_tolerance(TOL)
-    out = {"workload": (f"sparse SDP: m={wl['m']}, {wl['blocks']} PSD blocks of order "
-                        f"{wl['kmin']}-{wl['kmax']}, each variable active in a block with "
-                        f"probability {wl['active']}, {2 * wl['pairs'][0]}-{2 * wl['pairs'][1]} "
-                        f"stored entries per active coefficient")}
-    with CudaBackend(prob, precision="fp64", device=local) as be:
-        st = torch.cuda.ExternalStream(be.stream_handle())
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        solves = {}
-        for name in ("sparse", "dense"):
-            be.set_sparse_schur(name == "sparse")
-            be.reset()
-            be.optimize(opts)                       # warm-up (allocations, digit planes)
-            be.reset()
-            torch.cuda.synchronize()
-            ev[0].record(st)
-            r = be.optimize(opts)
-            ev[1].record(st)
-            torch.cuda.synchronize()
-            solves[name] = (ev[0].elapsed_time(ev[1]) / 1000.0, r)
-        info = be.sparse_schur_info()
-        r = solves["sparse"][1]
-        be.reset()
-        be.set_iterate(r.x, r.X, r.Y)
-        be.compute_residuals([0.0] * prob.L, True, True)
-        build_ms = {}
-        for name in ("sparse", "dense_int8", "dense_dmma"):
-            be.set_sparse_schur(name == "sparse")
-            be.set_gram_engine("dmma" if name == "dense_dmma" else "int8")
-            be.schur_build()
-            ev[0].record(st)
-            for _ in range(3):
-                be.schur_build()
-            ev[1].record(st)
-            torch.cuda.synchronize()
-            build_ms[name] = ev[0].elapsed_time(ev[1]) / 3
-        be.set_gram_engine("int8")
-        be.set_sparse_schur(True)
-        be.schur_build()
-        S_sparse = be.schur_matrix()
-        be.set_sparse_schur(False)
-        be.schur_build()
-        S_dense = be.schur_matrix()
-    pairs = 0
-    from oracle.sparse_oracle import block_coo
-    coo = [block_coo(prob.Av[l], k) for l, k in enumerate(prob.k)]
-    for a, _, _, _ in coo:
-        pairs += a.size * (a.size + 1) // 2
-    out.update({
-        "active_positions": info["active_positions"], "stored_entries": info["stored_entries"],
-        "active_pairs": pairs,
-        "schur_build_ms": build_ms,
-        "speedup_sparse_vs_dense_int8": build_ms["dense_int8"] / build_ms["sparse"],
-        "sparse_vs_dense_schur_rel_diff": float(np.max(np.abs(S_sparse - S_dense)) /
-                                                np.max(np.abs(S_dense))),
-        "solve_sparse": {"value": solves["sparse"][0], "unit": "s",
-                         "status": solves["sparse"][1].status.value,
-                         "iterations": solves["sparse"][1].iterations,
-                         "objective": solves["sparse"][1].pObj},
-        "solve_dense": {"value": solves["dense"][0], "unit": "s",
-                        "status": solves["dense"][1].status.value,
-                        "iterations": solves["dense"][1].iterations,
-                        "objective": solves["dense"][1].pObj},
-        "unit": "ms"})
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle.sdpx_oracle import OracleBackend
-        ob = OracleBackend(prob)
-        ob.sparse_schur = True
-        ob.set_iterate(r.x, r.X, r.Y)
-        ob.compute_residuals([0.0] * prob.L, True, True)
+        out["cpu_kind"] = "port: the oracle's FP64 adjoint (NumPy/OpenBLAS, all host cores)"
         t0 = time.perf_counter()
-        ob.schur_build()
-        out["cpu_baseline"] = {"value": (time.perf_counter() - t0) * 1000.0, "unit": "ms",
-                               "cores": cpu_threads(), "kind": "port",
-                               "sample": "the oracle's sparse Schur assembly (per-position "
-                                         "rank-one products and sparse gathers) of the same "
-                                         "iterate"}
+        gd = dd_adjoint(prob, r.x, r.X, r.Y, wx=v, WY=W, A_index=idx, refine=wl["refine"])
+        out["cpu_float64x2_reference_s"] = time.perf_counter() - t0
+
+        def rel(a, b):
+            return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) /
+                         max(1.0, float(np.max(np.abs(b)))))
+
+        def worst(g):
+            return max([rel(g["grad_c"], gd["grad_c"]), rel(g["grad_C"][0], gd["grad_C"][0])] +
+                       [rel(g["grad_A"][q][0], gd["grad_A"][q][0]) for q in range(len(idx))])
+
+        out["vs_float64x2_reference"] = {
+            "instance": 0, "fp64_max_rel_err": worst(g64), "refined_max_rel_err": worst(gref),
+            "reference": "double-double implicit-KKT gradient of the same iterate "
+                         "(oracle/dd_oracle.py)"}
     return out
 
 

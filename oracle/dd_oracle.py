@@ -196,8 +196,14 @@ def dd_atmul(Av: Sequence[np.ndarray], Z: Sequence[DD]) -> DD:
     tot = DD(np.zeros(m))
     for A, Zl in zip(Av, Z):
         zh, zl = Zl.hi.reshape(-1), Zl.lo.reshape(-1)
-        p, e = two_prod(A, zh[None, :])
-        tot = tot + dd_sum(DD(p, e + A * zl[None, :]), axis=1)
+        rows = max(1, (1 << 22) // max(1, zh.size))     # ≈ 32 MB per temporary
+        part_h, part_l = np.zeros(m), np.zeros(m)
+        for r0 in range(0, m, rows):
+            Ab = A[r0:r0 + rows]
+            p, e = two_prod(Ab, zh[None, :])
+            sb = dd_sum(DD(p, e + Ab * zl[None, :]), axis=1)
+            part_h[r0:r0 + rows], part_l[r0:r0 + rows] = sb.hi, sb.lo
+        tot = tot + DD(part_h, part_l)
     return tot
 
 
