@@ -373,6 +373,99 @@ def bench_adjoint(args, world, rank, local):
     return out
 
 
+def bench_sparse(args, world, rank, local):
+    """Sparse Schur engine against the dense FP64 engines on one structurally
+    sparse instance: the Schur build at the solution iterate (device events,
+    both engines) and complete solves with each; the oracle's sparse assembly
+    of the same iterate is the CPU baseline."""
+    import numpy as np
+    import torch
+    from sdpx_b200 import SolverOptions, generators as G
+    from sdpx_b200.cuda_backend import CudaBackend
+    wl = SPARSE_WORKLOAD
+    ks = np.random.default_rng(wl["seed"]).integers(wl["kmin"], wl["kmax"] + 1, wl["blocks"])
+    prob = G.sdpa_sparse(m=wl["m"], blocks=[int(k) for k in ks], active=wl["active"],
+                         pairs=wl["pairs"], seed=wl["seed"] + rank)
+    opts = SolverOptions(precision="fp64").with_tolerance(TOL)
+    out = {"workload": (f"sparse SDP: m={wl['m']}, {wl['blocks']} PSD blocks of order "
+                        f"{wl['kmin']}-{wl['kmax']}, each variable active in a block with "
+                        f"probability {wl['active']}, {2 * wl['pairs'][0]}-{2 * wl['pairs'][1]} "
+                        f"stored entries per active coefficient")}
+    with CudaBackend(prob, precision="fp64", device=local) as be:
+        st = torch.cuda.ExternalStream(be.stream_handle())
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        solves = {}
+        for name in ("sparse", "dense"):
+            be.set_sparse_schur(name == "sparse")
+            be.reset()
+            be.optimize(opts)                       # warm-up (allocations, digit planes)
+            be.reset()
+            torch.cuda.synchronize()
+            ev[0].record(st)
+            r = be.optimize(opts)
+            ev[1].record(st)
+            torch.cuda.synchronize()
+            solves[name] = (ev[0].elapsed_time(ev[1]) / 1000.0, r)
+        info = be.sparse_schur_info()
+        r = solves["sparse"][1]
+        be.reset()
+        be.set_iterate(r.x, r.X, r.Y)
+        be.compute_residuals([0.0] * prob.L, True, True)
+        build_ms = {}
+        for name in ("sparse", "dense_int8", "dense_dmma"):
+            be.set_sparse_schur(name == "sparse")
+            be.set_gram_engine("dmma" if name == "dense_dmma" else "int8")
+            be.schur_build()
+            ev[0].record(st)
+            for _ in range(3):
+                be.schur_build()
+            ev[1].record(st)
+            torch.cuda.synchronize()
+            build_ms[name] = ev[0].elapsed_time(ev[1]) / 3
+        be.set_gram_engine("int8")
+        be.set_sparse_schur(True)
+        be.schur_build()
+        S_sparse = be.schur_matrix()
+        be.set_sparse_schur(False)
+        be.schur_build()
+        S_dense = be.schur_matrix()
+    pairs = 0
+    from oracle.sparse_oracle import block_coo
+    coo = [block_coo(prob.Av[l], k) for l, k in enumerate(prob.k)]
+    for a, _, _, _ in coo:
+        pairs += a.size * (a.size + 1) // 2
+    out.update({
+        "active_positions": info["active_positions"], "stored_entries": info["stored_entries"],
+        "active_pairs": pairs,
+        "schur_build_ms": build_ms,
+        "speedup_sparse_vs_dense_int8": build_ms["dense_int8"] / build_ms["sparse"],
+        "sparse_vs_dense_schur_rel_diff": float(np.max(np.abs(S_sparse - S_dense)) /
+                                                np.max(np.abs(S_dense))),
+        "solve_sparse": {"value": solves["sparse"][0], "unit": "s",
+                         "status": solves["sparse"][1].status.value,
+                         "iterations": solves["sparse"][1].iterations,
+                         "objective": solves["sparse"][1].pObj},
+        "solve_dense": {"value": solves["dense"][0], "unit": "s",
+                        "status": solves["dense"][1].status.value,
+                        "iterations": solves["dense"][1].iterations,
+                        "objective": solves["dense"][1].pObj},
+        "unit": "ms"})
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.sdpx_oracle import OracleBackend
+        ob = OracleBackend(prob)
+        ob.sparse_schur = True
+        ob.set_iterate(r.x, r.X, r.Y)
+        ob.compute_residuals([0.0] * prob.L, True, True)
+        t0 = time.perf_counter()
+        ob.schur_build()
+        out["cpu_baseline"] = {"value": (time.perf_counter() - t0) * 1000.0, "unit": "ms",
+                               "cores": cpu_threads(), "kind": "port",
+                               "sample": "the oracle's sparse Schur assembly (per-position "
+                                         "rank-one products and sparse gathers) of the same "
+                                         "iterate"}
+    return out
+
+
 def eq_cpu_sample(m, n, seed=0):
     """Seconds of the oracle's equality factor (B̃ = L⁻¹B by LAPACK trsm,
     unit-∞-norm columns, Q = B̂ᵀB̂, potrf, rank test) for an m×m lower factor
