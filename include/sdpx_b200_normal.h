@@ -21,6 +21,8 @@
 
 #include <stdint.h>
 
+#include "sdpx_b200.h" /* sdpx_b200_solve_options, sdpx_b200_solve_result */
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -82,6 +84,24 @@ int sdpx_b200_normal_get_matrix(sdpx_b200_normal* h, int32_t which, double* out)
  * (src/lp_solver.jl:2177-2213): t = D⁻¹rx, dy = Q⁻¹(ry − Bᵀt),
  * dx = t + D⁻¹B·dy.  Returns 1 when no successful factor is held. */
 int sdpx_b200_normal_solve(sdpx_b200_normal* h, double* rhs);
+
+/* Primal-dual interior-point solve of the standard-form LP + Lorentz-cone
+ * problem  min cᵀx  s.t.  Bᵀx = b,  x ∈ R₊^{n_lp} × L^{q_1} × …  (dual
+ * max bᵀy s.t. By + z = c, z in the same cone) on this handle's B, every
+ * vector and matrix operation on the device.  SDPX's LP loop `solve_lp!`
+ * (src/lp_solver.jl:3651-4400: residuals and best snapshot, termination, the
+ * regularised reduced factor with ×10 retries decaying to √(eps·√eps),
+ * Mehrotra predictor-corrector under the adaptive controller of
+ * src/adaptive_parameters.jl, fraction-to-boundary steps, the regularisation-
+ * aware direction gate) with the Lorentz cones entering through their
+ * Nesterov–Todd scaling (src/soc_lorentz_kernels.jl:72-255).  Start x = z = e,
+ * y = 0.  The options' beta, gamma, eps_*, iter_max, max_time and
+ * parameter_strategy apply.  x, z (n) and y (m_eq) receive the solution (the
+ * best iterate when not Optimal; NULL to skip).  Requires the standard LP
+ * layout (identity row_for_variable, g = 1). */
+int sdpx_b200_normal_optimize(sdpx_b200_normal* h, const double* b, const double* c,
+                              const sdpx_b200_solve_options* opts, sdpx_b200_solve_result* result,
+                              double* x, double* y, double* z);
 
 /* Device time (ms) of the last assemble (pack + scale + SYRK) and factor. */
 int sdpx_b200_normal_times(sdpx_b200_normal* h, double* assemble_ms, double* factor_ms);

@@ -18,12 +18,17 @@
 // a sequential IEEE evaluation in the reference's order.
 #include <cuda_runtime.h>
 
+#include <array>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "../../include/sdpx_b200_normal.h"
+#include "ipm_controller.h"
 #include "blas_f64.h"
 #include "chol.h"
 #include "dbuf.h"
@@ -287,6 +292,7 @@ struct NormalHandle {
   SyrkPlan plan;
   int gemv_chunks = 8;
   bool have_scaling = false, have_factor = false, have_assembled = false;
+  bool standard_rows = true;  // row_for_variable = identity, g = 1, one weight per LP variable
   cudaEvent_t ev[4] = {};
   double assemble_ms = 0.0, factor_ms = 0.0;
 
@@ -318,6 +324,8 @@ struct NormalHandle {
     for (int j = 0; j < n_lp; ++j)
       if (row[j] < 0 || row[j] >= n_weights)
         throw std::invalid_argument("row_for_variable out of range at variable " + std::to_string(j));
+    standard_rows = n_weights == n_lp;
+    for (int j = 0; j < n_lp && standard_rows; ++j) standard_rows = row[j] == j && hcoef[j] == 1.0;
     if (n > 0 && m > 0 && !hB) throw std::invalid_argument("B is NULL");
     B.alloc((size_t)n * m);
     Bh.alloc((size_t)n * m);
@@ -525,6 +533,34 @@ struct NormalHandle {
     return 0;
   }
 
+  // One assembly + Cholesky attempt with LP weights already on the device
+  // (one weight per LP variable): 0 on success, 1 when the factor failed.
+  int factorize_dev(const double* dweights, double reg) {
+    require_scaling();
+    have_factor = false;
+    if (n_lp) {
+      k_lp_pack<<<ceil_div(n_lp, 256), 256, 0, st>>>(n_lp, dweights, d_row.p, coef.p, reg, D.p,
+                                                      Dinv.p, Dis.p);
+      SDPX_LAUNCH_CHECK();
+    }
+    scale_cones();
+    assemble_lp_and_syrk(reg);
+    if (m == 0) {
+      have_factor = true;
+      return 0;
+    }
+    MatDesc<double> md{F.p, m, m};
+    h2d(descs.p, &md, sizeof(md));
+    potrf_batched<double, 64>(descs.p, 1, m, d_info.p, dmin.p, dmax.p, st);
+    int info = 1;
+    d2h(&info, d_info.p, sizeof(int));
+    sync();
+    if (info != 0) return 1;
+    factor_diag_inverses<double, 64>(F.p, m, m, Finv_diag.p, st);
+    have_factor = true;
+    return 0;
+  }
+
   void get_matrix(int which, double* hout) {
     if (which == 0) {
       if (!have_assembled) throw std::logic_error("no assembled matrix");
@@ -574,6 +610,8 @@ struct NormalHandle {
 };
 
 }  // namespace sdpx
+
+#include "cone_ipm.inc"
 
 // ============================================================================
 //                                   C ABI
@@ -680,6 +718,23 @@ int sdpx_b200_normal_solve(sdpx_b200_normal* h, double* rhs) {
     if (rc) h->h.err = "no successful factor held (factorize failed or was not called)";
     return rc;
   });
+}
+int sdpx_b200_normal_optimize(sdpx_b200_normal* h, const double* b, const double* c,
+                              const sdpx_b200_solve_options* opts, sdpx_b200_solve_result* result,
+                              double* x, double* y, double* z) {
+  if (!h) return -1;
+  try {
+    SDPX_CUDA(cudaSetDevice(h->h.dev));
+    if (!opts || !c || (h->h.m > 0 && !b)) throw std::invalid_argument("NULL b, c or options");
+    if (!h->h.standard_rows)
+      throw std::invalid_argument("the LP part must be standard form (identity rows, g = 1)");
+    sdpx::ConeIPM ipm(h->h);
+    ipm.run(b, c, *opts, result, x, y, z);
+    return 0;
+  } catch (const std::exception& ex) {
+    h->h.err = ex.what();
+    return -2;
+  }
 }
 int sdpx_b200_normal_times(sdpx_b200_normal* h, double* assemble_ms, double* factor_ms) {
   NGUARD(h, {

@@ -305,3 +305,25 @@ def lp_soc_standard(m: int, n_lp: int, cones: Sequence[int], density: float = 0.
             dst.append(np.concatenate([[1.5 * np.linalg.norm(u) + 1.0], u]))
     cat = (lambda v: np.concatenate(v)) if cones else (lambda v: np.zeros(0))
     return np.asfortranarray(A.T), s_lp / x, cat(sc), cat(zc)
+
+
+def lp_soc_problem(m: int, n_lp: int, cones: Sequence[int], density: float = 0.1,
+                   seed: int = 0):
+    """Standard-form LP + Lorentz-cone problem  min cᵀx s.t. Ax = b, x ∈ K
+    with a strictly feasible primal-dual pair: the draws of `lp_soc_standard`
+    (A, the LP primal and dual points, the cone primal and dual points) and
+    then y0 ~ N(0,1)^m; b = A x0, c = Aᵀy0 + z0.  Returns (B = Aᵀ, b, c)."""
+    B, w, sc, zc = lp_soc_standard(m, n_lp, cones, density, seed)
+    # lp_soc_standard returns the LP weights s/x; redraw the same LP points
+    rng = np.random.default_rng(seed)
+    n = n_lp + int(sum(cones))
+    rng.standard_normal((m, n))
+    rng.random((m, n))
+    x_lp = rng.uniform(0.5, 1.5, n_lp)
+    z_lp = rng.uniform(0.5, 1.5, n_lp)
+    x0 = np.concatenate([x_lp, sc])
+    z0 = np.concatenate([z_lp, zc])
+    y0 = np.random.default_rng(seed + 1).standard_normal(m)
+    b = B.T @ x0
+    c = B @ y0 + z0
+    return B, b, c

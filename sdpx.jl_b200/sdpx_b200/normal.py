@@ -49,6 +49,9 @@ def _lib():
     global _bound
     lib = load_library()
     if not _bound:
+        from .cuda_backend import SolveOptions, SolveResult
+        _SIGS["sdpx_b200_normal_optimize"] = [C.c_void_p, _dp, _dp, C.POINTER(SolveOptions),
+                                              C.POINTER(SolveResult), _dp, _dp, _dp]
         for name, args in _SIGS.items():
             fn = getattr(lib, name)
             fn.argtypes = args
@@ -69,6 +72,20 @@ def _p(a: Optional[np.ndarray]):
 
 def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class ConeSolveResult:
+    """Outcome of `NormalSystem.optimize` (statuses as `SDPResult`)."""
+
+    def __init__(self, status, iterations, x, y, z, pObj, dObj, p_res, d_res, seconds, message):
+        self.status, self.iterations = status, iterations
+        self.x, self.y, self.z = x, y, z
+        self.pObj, self.dObj, self.p_res, self.d_res = pObj, dObj, p_res, d_res
+        self.seconds, self.message = seconds, message
+
+    @property
+    def relative_gap(self) -> float:
+        return abs(self.pObj - self.dObj) / max(1.0, (abs(self.pObj) + abs(self.dObj)) / 2)
 
 
 class PosDefError(np.linalg.LinAlgError):
@@ -222,6 +239,27 @@ class NormalSystem:
         if rc != 0:
             raise PosDefError("no successful factor held")
         return v
+
+    def optimize(self, b, c, *, tolerance: float = 1e-8, **kwargs):
+        """Interior-point solve of  min cᵀx  s.t.  Bᵀx = b,  x ∈ R₊^{n_lp} × cones
+        on the device (sdpx_b200_normal_optimize): SDPX's LP loop with the
+        Lorentz cones through their NT scaling.  Needs the standard LP layout
+        (one weight row per LP variable, g = 1).  Returns a `ConeSolveResult`."""
+        from .controller import SolverOptions
+        from .cuda_backend import STATUS_NAMES, SolveResult, native_options
+        opts = SolverOptions(**kwargs).with_tolerance(tolerance)
+        no = native_options(opts)
+        res = SolveResult()
+        bv, cv = _f64(b), _f64(c)
+        if bv.shape != (self.m,) or cv.shape != (self.n,):
+            raise ValueError("b must have m_eq entries and c n entries")
+        x, y, z = np.zeros(self.n), np.zeros(self.m), np.zeros(self.n)
+        self._check(self.lib.sdpx_b200_normal_optimize(self.h, _p(bv), _p(cv), C.byref(no),
+                                                       C.byref(res), _p(x), _p(y), _p(z)),
+                    "optimize")
+        return ConeSolveResult(STATUS_NAMES[res.status], res.iterations, x, y, z, res.p_obj,
+                               res.d_obj, res.p_res, res.d_res, res.seconds,
+                               res.message.decode(errors="replace"))
 
     def times(self) -> Tuple[float, float]:
         a, f = C.c_double(), C.c_double()
