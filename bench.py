@@ -618,6 +618,7 @@ def bench_lp_soc_solve(args, world, rank, local):
     B, b, c = G.lp_soc_problem(wl["m"], wl["n_lp"], wl["cones"], wl["density"], seed=rank)
     with NormalSystem(B, wl["n_lp"], wl["cones"], device=local) as ns:
         ns.optimize(b, c, tolerance=TOL)          # warm-up (allocations, kernels)
+        ns.optimize(b, c, tolerance=TOL, precision="mixed")
         st = torch.cuda.ExternalStream(ns.stream_handle())
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         torch.cuda.synchronize()
@@ -626,6 +627,11 @@ def bench_lp_soc_solve(args, world, rank, local):
         ev[1].record(st)
         torch.cuda.synchronize()
         dev_s = ev[0].elapsed_time(ev[1]) / 1000.0
+        ev[0].record(st)
+        rm = ns.optimize(b, c, tolerance=TOL, precision="mixed")
+        ev[1].record(st)
+        torch.cuda.synchronize()
+        mixed_s = ev[0].elapsed_time(ev[1]) / 1000.0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     with NormalSystem(B, wl["n_lp"], wl["cones"], device=local) as ns:
@@ -636,6 +642,12 @@ def bench_lp_soc_solve(args, world, rank, local):
            "value": max_over_ranks(dev_s, world), "unit": "s", "status": r.status,
            "iterations": r.iterations, "pObj": r.pObj, "dObj": r.dObj,
            "relative_gap": r.relative_gap,
+           "mixed": {"value": max_over_ranks(mixed_s, world), "unit": "s", "status": rm.status,
+                     "iterations": rm.iterations, "split_iterations": rm.split_iterations,
+                     "fp64_iterations": rm.fp64_iterations, "pObj": rm.pObj, "dObj": rm.dObj,
+                     "rel_obj_diff_vs_fp64": abs(rm.pObj - r.pObj) / max(1.0, abs(r.pObj)),
+                     "path": "A·D·Aᵀ from split-BF16 planes (tcgen05 SYRK), FP64 factor, Δy "
+                             "refined against the FP64 operator, FP64 assembly after a stall"},
            "kkt": {"primal_residual": float(np.max(np.abs(A @ r.x - b))),
                    "dual_residual": float(np.max(np.abs(A.T @ r.y + r.z - c))),
                    "complementarity": float(r.x @ r.z)},

@@ -32,6 +32,7 @@
 #include "blas_f64.h"
 #include "chol.h"
 #include "dbuf.h"
+#include "schur_bf16.h"
 #include "vec_kernels.h"
 
 namespace sdpx {
@@ -293,6 +294,13 @@ struct NormalHandle {
   int gemv_chunks = 8;
   bool have_scaling = false, have_factor = false, have_assembled = false;
   bool standard_rows = true;  // row_for_variable = identity, g = 1, one weight per LP variable
+  // Split-BF16 assembly: three BF16 planes of B̂ (m rows of pitch Kp = n
+  // rounded up to 64) and the tcgen05 SYRK of the Schur path.
+  long long Kp = 0;
+  DBuf<unsigned char> plane_buf[3];
+  SplitSyrkPlan splan;
+  DBuf<float> spartial;
+  DBuf<int> serr;
   cudaEvent_t ev[4] = {};
   double assemble_ms = 0.0, factor_ms = 0.0;
 
@@ -445,15 +453,49 @@ struct NormalHandle {
     SDPX_LAUNCH_CHECK();
   }
 
-  // LP rows of B̂, SYRK, +δ on the diagonal, copy of lower(Q) into F.
-  void assemble_lp_and_syrk(double reg) {
+  // Q = B̂ᵀB̂ from three BF16 planes of B̂ on the tcgen05 split SYRK (FP32
+  // tiles summed in FP64; ≈ 1e-6 relative), +δ and the lower copy into F.
+  void assemble_split(double reg) {
     if (m == 0) return;
-    if (n_lp > 0) {
+    scale_lp_rows();
+    if (Kp == 0) {
+      Kp = (std::max<long long>(n, 1) + 63) / 64 * 64;
+      for (auto& b : plane_buf) b.alloc(sizeof(__nv_bfloat16) * (size_t)m * Kp);
+      splan = plan_split_syrk(m, Kp, sms);
+      spartial.alloc(splan.partial_floats);
+      serr.alloc(1);
+    }
+    __nv_bfloat16* pl[3];
+    for (int i = 0; i < 3; ++i) pl[i] = reinterpret_cast<__nv_bfloat16*>(plane_buf[i].p);
+    split_rows_f64(Bh.p, n, m, n, Kp, pl, st);
+    SDPX_CUDA(cudaMemsetAsync(serr.p, 0, sizeof(int), st));
+    Plane2D P{{pl[0], pl[1], pl[2]}, m, Kp};
+    split_syrk(P, m, (int)Kp, splan, spartial.p, Q.p, serr.p, st);
+    int e = 0;
+    d2h(&e, serr.p, sizeof(int));
+    sync();
+    if (e) throw CudaError("split normal-matrix SYRK: a bounded wait gave up");
+    long long tot = (long long)m * m;
+    k_shift_copy_lower<<<(int)std::min<long long>(ceil_div(tot, 256), (long long)sms * 16), 256, 0,
+                         st>>>(m, Q.p, reg, F.p);
+    SDPX_LAUNCH_CHECK();
+    have_assembled = true;
+  }
+
+  // B̂ = D^{-1/2}B on the LP rows (the cone rows come from scale_cones).
+  void scale_lp_rows() {
+    if (n_lp > 0 && m > 0) {
       long long tot = (long long)n_lp * m;
       int grid = (int)std::min<long long>(ceil_div(tot, 256), (long long)sms * 16);
       k_scale_lp<<<grid, 256, 0, st>>>(n_lp, n, m, B.p, Dis.p, Bh.p);
       SDPX_LAUNCH_CHECK();
     }
+  }
+
+  // LP rows of B̂, SYRK, +δ on the diagonal, copy of lower(Q) into F.
+  void assemble_lp_and_syrk(double reg) {
+    if (m == 0) return;
+    scale_lp_rows();
     if (n > 0) {
       Opnd P;
       P.base = Bh.p;
@@ -535,7 +577,7 @@ struct NormalHandle {
 
   // One assembly + Cholesky attempt with LP weights already on the device
   // (one weight per LP variable): 0 on success, 1 when the factor failed.
-  int factorize_dev(const double* dweights, double reg) {
+  int factorize_dev(const double* dweights, double reg, bool split = false) {
     require_scaling();
     have_factor = false;
     if (n_lp) {
@@ -544,7 +586,8 @@ struct NormalHandle {
       SDPX_LAUNCH_CHECK();
     }
     scale_cones();
-    assemble_lp_and_syrk(reg);
+    if (split) assemble_split(reg);
+    else assemble_lp_and_syrk(reg);
     if (m == 0) {
       have_factor = true;
       return 0;

@@ -427,6 +427,20 @@ __device__ __forceinline__ void split3d(double v, __nv_bfloat16& h0, __nv_bfloat
   h2 = __double2bfloat16(r - (double)__bfloat162float(h1));
 }
 
+// Rows of a column-major FP64 matrix (row r = column r of src, K entries,
+// leading dimension ld) → planes[p][r·Kp + k], zeros for K ≤ k < Kp.
+__global__ void k_split_rows(const double* __restrict__ src, long long ld, int rows, long long K,
+                             long long Kp, __nv_bfloat16* P0, __nv_bfloat16* P1,
+                             __nv_bfloat16* P2) {
+  const long long tot = (long long)rows * Kp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long r = t / Kp, k = t - r * Kp;
+    const double v = k < K ? src[r * ld + k] : 0.0;
+    split3d(v, P0[t], P1[t], P2[t]);
+  }
+}
+
 // Dense block of 𝒜 (rows off + p + c·k of every column i) → planes[i][o + c·kp + p].
 __global__ void k_split_A_dense(const double* A, long long K, int m, long long off, int k, int kp,
                                 __nv_bfloat16* P0, __nv_bfloat16* P1, __nv_bfloat16* P2,
@@ -573,6 +587,15 @@ void split_syrk(const Plane2D& P, int m, int Kp, const SplitSyrkPlan& plan, floa
   if (ev_end) SDPX_CUDA(cudaEventRecord(ev_end, st));
   k_reduce_partials<<<plan.ntri, 256, 0, st>>>(partial, plan.ntri, plan.nchunk, m, S);
   SDPX_LAUNCH_CHECK_N(2);
+}
+
+void split_rows_f64(const double* src, long long ld, int rows, long long K, long long Kp,
+                    __nv_bfloat16* const* planes, cudaStream_t st) {
+  const long long tot = (long long)rows * Kp;
+  if (tot == 0) return;
+  k_split_rows<<<(int)std::min<long long>(ceil_div(tot, 256), 148LL * 32), 256, 0, st>>>(
+      src, ld, rows, K, Kp, planes[0], planes[1], planes[2]);
+  SDPX_LAUNCH_CHECK();
 }
 
 void split_A_dense(const double* A, long long K, int m, long long off, int k, int kp,

@@ -53,6 +53,10 @@ void split_syrk(const Plane2D& P, int m, int Kp, const SplitSyrkPlan& plan, floa
                 double* S, int* err, cudaStream_t st, cudaEvent_t ev_begin = nullptr,
                 cudaEvent_t ev_end = nullptr);
 
+// Rows of a column-major FP64 matrix (rows columns of K entries, leading
+// dimension ld) → three BF16 planes of pitch Kp (zero padded past K).
+void split_rows_f64(const double* src, long long ld, int rows, long long K, long long Kp,
+                    __nv_bfloat16* const* planes, cudaStream_t st);
 void split_A_dense(const double* A, long long K, int m, long long off, int k, int kp,
                    __nv_bfloat16* const* planes, long long Kp, long long o, cudaStream_t st);
 void split_diag_rows(const double* A, long long K, int m, long long od, int nd, const double* LX,

@@ -243,8 +243,11 @@ class NormalSystem:
     def optimize(self, b, c, *, tolerance: float = 1e-8, **kwargs):
         """Interior-point solve of  min cᵀx  s.t.  Bᵀx = b,  x ∈ R₊^{n_lp} × cones
         on the device (sdpx_b200_normal_optimize): SDPX's LP loop with the
-        Lorentz cones through their NT scaling.  Needs the standard LP layout
-        (one weight row per LP variable, g = 1).  Returns a `ConeSolveResult`."""
+        Lorentz cones through their NT scaling.  `precision="mixed"` assembles
+        the normal matrix from split-BF16 planes on the tensor cores and refines
+        Δy against the FP64 operator, switching to the FP64 assembly when the
+        refinement stalls.  Needs the standard LP layout (one weight row per LP
+        variable, g = 1).  Returns a `ConeSolveResult`."""
         from .controller import SolverOptions
         from .cuda_backend import STATUS_NAMES, SolveResult, native_options
         opts = SolverOptions(**kwargs).with_tolerance(tolerance)
@@ -257,9 +260,11 @@ class NormalSystem:
         self._check(self.lib.sdpx_b200_normal_optimize(self.h, _p(bv), _p(cv), C.byref(no),
                                                        C.byref(res), _p(x), _p(y), _p(z)),
                     "optimize")
-        return ConeSolveResult(STATUS_NAMES[res.status], res.iterations, x, y, z, res.p_obj,
-                               res.d_obj, res.p_res, res.d_res, res.seconds,
-                               res.message.decode(errors="replace"))
+        out = ConeSolveResult(STATUS_NAMES[res.status], res.iterations, x, y, z, res.p_obj,
+                              res.d_obj, res.p_res, res.d_res, res.seconds,
+                              res.message.decode(errors="replace"))
+        out.split_iterations, out.fp64_iterations = res.mixed_iterations, res.fp64_iterations
+        return out
 
     def times(self) -> Tuple[float, float]:
         a, f = C.c_double(), C.c_double()

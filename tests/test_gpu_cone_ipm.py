@@ -4,7 +4,10 @@ against its oracle (oracle/cone_ipm_oracle.py).
 On the same instance the device loop reaches the oracle's status, its
 iteration count within ±1 and its objectives within 1e-7 relative; the device
 solution satisfies the KKT conditions to the tolerance; an LP-only instance
-matches an independent LP solver (HiGHS through scipy) to 1e-7.
+matches an independent LP solver (HiGHS through scipy) to 1e-7.  The mixed
+form (split-BF16 A·D·Aᵀ on the tensor cores, Δy refined against the FP64
+operator) reaches the FP64 form's status and objectives (1e-7) with its
+split iterations counted.
 """
 import numpy as np
 import pytest
@@ -54,3 +57,19 @@ def test_device_lp_matches_linprog(gpu):
         got = ns.optimize(b, c, tolerance=TOL)
     assert got.status == "Optimal" and ref.status == 0
     assert abs(got.pObj - ref.fun) <= 1e-7 * max(1.0, abs(ref.fun))
+
+
+@pytest.mark.parametrize("m,n_lp,cones,seed,density", [CASES[1], CASES[3]])
+def test_mixed_assembly_matches_fp64(gpu, m, n_lp, cones, seed, density):
+    B, b, c = G.lp_soc_problem(m, n_lp, cones, density=density, seed=seed)
+    A = np.ascontiguousarray(B.T)
+    with gpu(B, n_lp, cones) as ns:
+        r64 = ns.optimize(b, c, tolerance=TOL)
+        rmx = ns.optimize(b, c, tolerance=TOL, precision="mixed")
+    assert rmx.status == r64.status == "Optimal", rmx.message
+    assert rmx.split_iterations > 0
+    assert rmx.split_iterations + rmx.fp64_iterations == rmx.iterations
+    assert rmx.pObj == pytest.approx(r64.pObj, rel=1e-7)
+    assert rmx.dObj == pytest.approx(r64.dObj, rel=1e-7)
+    assert np.max(np.abs(A @ rmx.x - b)) <= TOL * (1 + np.max(np.abs(b)))
+    assert np.max(np.abs(A.T @ rmx.y + rmx.z - c)) <= TOL * (1 + np.max(np.abs(c)))
