@@ -301,6 +301,24 @@ struct NormalHandle {
   SplitSyrkPlan splan;
   DBuf<float> spartial;
   DBuf<int> serr;
+  // Explicit inverse of the reduced factor for the refined (mixed) solves:
+  // each solve is two GEMVs over L⁻¹ instead of 2·⌈m/64⌉ dependent launches.
+  DBuf<double> Linv, Ltmp, Ldinv;
+  bool have_inverse = false;
+  void make_inverse() {
+    if (Linv.n < (size_t)m * m) {
+      Linv.alloc((size_t)m * m);
+      Ltmp.alloc((size_t)m * m);
+      Ldinv.alloc((size_t)ceil_div(std::max(m, 1), 64) * 64 * 64);
+    }
+    trinv_recursive_f64(F.p, m, Linv.p, Ldinv.p, Ltmp.p, st);
+    have_inverse = true;
+  }
+  // v ← Q⁻¹v = L⁻ᵀ(L⁻¹v) with the explicit inverse (work: m).
+  void solve_inverse(double* v) {
+    gemv_n(Linv.p, m, m, v, work.p, gemv_part.p, gemv_chunks, st);
+    gemv_t(Linv.p, m, m, work.p, 1.0, nullptr, 0.0, v, st);
+  }
   cudaEvent_t ev[4] = {};
   double assemble_ms = 0.0, factor_ms = 0.0;
 
@@ -580,6 +598,7 @@ struct NormalHandle {
   int factorize_dev(const double* dweights, double reg, bool split = false) {
     require_scaling();
     have_factor = false;
+    have_inverse = false;
     if (n_lp) {
       k_lp_pack<<<ceil_div(n_lp, 256), 256, 0, st>>>(n_lp, dweights, d_row.p, coef.p, reg, D.p,
                                                       Dinv.p, Dis.p);
@@ -600,6 +619,7 @@ struct NormalHandle {
     sync();
     if (info != 0) return 1;
     factor_diag_inverses<double, 64>(F.p, m, m, Finv_diag.p, st);
+    if (split) make_inverse();
     have_factor = true;
     return 0;
   }
