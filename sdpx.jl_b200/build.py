@@ -18,7 +18,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxe
          "-Xptxas", "-warn-spills"]
 SOURCES = ["api.cu", "blas_f64.cu", "chol.cu", "vec_kernels.cu", "mixed_f32.cu", "schur_bf16.cu",
            "normal.cu", "certificate.cu", "ozaki.cu", "equality.cu", "sparse_schur.cu",
-           "dd_kernels.cu"]
+           "dd_kernels.cu", "batch.cu"]
 # Per-file flags.  normal.cu evaluates the reference's scalar cone recurrences
 # and must round every product and sum separately (no FMA contraction).
 FILE_FLAGS = {"normal.cu": ["--fmad=false"]}

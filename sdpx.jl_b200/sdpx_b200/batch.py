@@ -1,23 +1,38 @@
 """Batches of independent dense SDPs (the 4096-instance small-SDP workload).
 
-Every instance gets its own device handle and CUDA stream; `threads` host
-threads drive the solves concurrently.  With the native driver each solve is
-one library call (sdpx_b200_optimize) that releases the GIL for its whole
-duration, so the threads' host loops and device work overlap fully.  Results
-are the single-instance solver's: the same kernels in the same order per
-instance.  A batched engine that runs one kernel per IPM phase over all
-instances is not part of this module.
+Two engines:
+
+* ``engine="batched"`` (`BatchSolver`, include/sdpx_b200_batch.h): every
+  instance lives in one pooled device workspace and every interior-point phase
+  is one kernel launch over all instances still running, one CTA per instance
+  (the Schur assembly split into work items of a tuned size).  Each instance
+  keeps its own scalar controller, so its status, iterations and objectives are
+  those of its single solve with the same options.  It runs SDPX's fixed start
+  without equilibration (``parameter_policy="fixed"``, ``scaling="none"``), in
+  FP64, for one PSD block of order 3..64 and m ≤ 256 per instance.
+* ``engine="loop"``: one device handle and CUDA stream per instance
+  (`sdpx_b200_optimize`), driven by ``threads`` host threads — the
+  per-instance loop the batched engine is measured against.
+
+SDPX has no batch solver (its `src/prepared.jl` only reuses structure between
+solves of one problem); both engines run SDPX's dense loop per instance.
 """
 from __future__ import annotations
 
+import ctypes as C
+import json
+import os
 from concurrent.futures import ThreadPoolExecutor
-from typing import List, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
 from .controller import SolverOptions
-from .driver import SDPResult, solve_with_backend
+from .driver import SDPResult, Status, solve_with_backend
 from .problem import SDPProblem
+
+# The options the batched engine serves (fixed start, no equilibration).
+BATCH_OPTIONS = {"parameter_policy": "fixed", "scaling": "none"}
 
 
 def batch_instances(count: int, seed: int = 0, n_range=(4, 64), m_cap: int = 200) -> List[SDPProblem]:
@@ -34,12 +49,191 @@ def batch_instances(count: int, seed: int = 0, n_range=(4, 64), m_cap: int = 200
     return out
 
 
+def batch_options(tolerance: float = 1e-8, **kwargs) -> SolverOptions:
+    """SolverOptions of the batched engine (and of the loop it is compared with)."""
+    kw = dict(BATCH_OPTIONS)
+    kw.update(kwargs)
+    return SolverOptions(**kw).with_tolerance(tolerance)
+
+
+def _tune_cache_path() -> str:
+    return os.environ.get("SDPX_B200_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "sdpx_b200",
+                                       "batch_schur.json"))
+
+
+class BatchSolver:
+    """All instances in one pooled device workspace (sdpx_b200_batch_*).
+
+    Raises if the library or a GPU is unavailable, or if an instance is outside
+    the engine's scope (more than one block, equality rows, k ∉ [3, 64],
+    m ∉ [1, 256])."""
+
+    def __init__(self, problems: Sequence[SDPProblem], device: int = 0):
+        from .cuda_backend import BatchProblem, SDPXB200Error, load_library
+        self._lib = load_library()
+        self._err = SDPXB200Error
+        self.problems = list(problems)
+        if not self.problems:
+            raise ValueError("empty batch")
+        for i, p in enumerate(self.problems):
+            if p.L != 1 or p.n != 0:
+                raise ValueError(f"instance {i}: the batched engine takes one PSD block and "
+                                 f"no equality rows")
+        dp = C.POINTER(C.c_double)
+        n = len(self.problems)
+        self._keep = []
+        ks = (C.c_int32 * n)(*[p.k[0] for p in self.problems])
+        ms = (C.c_int32 * n)(*[p.m for p in self.problems])
+        Avs, Cs, cs = (dp * n)(), (dp * n)(), (dp * n)()
+        for i, p in enumerate(self.problems):
+            a = np.ascontiguousarray(p.Av[0], dtype=np.float64)
+            cm = np.ascontiguousarray(np.asarray(p.C[0], dtype=np.float64).T)  # column-major
+            cv = np.ascontiguousarray(p.c, dtype=np.float64)
+            self._keep += [a, cm, cv]
+            Avs[i] = a.ctypes.data_as(dp)
+            Cs[i] = cm.ctypes.data_as(dp)
+            cs[i] = cv.ctypes.data_as(dp)
+        prob = BatchProblem(n, ks, ms, Avs, Cs, cs)
+        h = C.c_void_p()
+        rc = self._lib.sdpx_b200_batch_create(C.byref(prob), device, C.byref(h))
+        self._keep = None  # the data is on the device now
+        if rc != 0:
+            raise SDPXB200Error("sdpx_b200_batch_create: " +
+                                self._lib.sdpx_b200_batch_create_error().decode())
+        self._h = h
+        self.shape = None
+
+    def _call(self, name, *args):
+        rc = getattr(self._lib, name)(self._h, *args)
+        if rc != 0:
+            raise self._err(f"{name}: " + self._lib.sdpx_b200_batch_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sdpx_b200_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def signature(self) -> str:
+        """Workload key of the tuning cache: count and size ranges."""
+        ks = [p.k[0] for p in self.problems]
+        ms = [p.m for p in self.problems]
+        return f"n{len(ks)}-k{min(ks)}..{max(ks)}-m{min(ms)}..{max(ms)}"
+
+    def set_schur_shape(self, threads: int, tile: int, grain: float):
+        self._call("sdpx_b200_batch_set_schur_shape", int(threads), int(tile), float(grain))
+        self.shape = (int(threads), int(tile), float(grain))
+
+    def autotune(self, opts: Optional[SolverOptions] = None, cache: bool = True) -> List[tuple]:
+        """Time every Schur launch shape on the device and keep the fastest;
+        with `cache`, a choice stored for this workload signature is reused
+        and a new one is stored (JSON at $SDPX_B200_TUNE_CACHE, default
+        ~/.cache/sdpx_b200/batch_schur.json).  Returns the timing table
+        [(threads, tile, grain, ms)] (empty when the cache answered)."""
+        from .cuda_backend import native_options
+        path = _tune_cache_path()
+        key = self.signature()
+        if cache and os.path.exists(path):
+            try:
+                with open(path) as f:
+                    stored = json.load(f).get(key)
+            except (OSError, ValueError):
+                stored = None
+            if stored:
+                self.set_schur_shape(*stored)
+                return []
+        no = native_options(opts or batch_options())
+        cap = 64
+        table = np.zeros(4 * cap)
+        cnt = C.c_int32()
+        self._call("sdpx_b200_batch_autotune", C.byref(no),
+                   table.ctypes.data_as(C.POINTER(C.c_double)), cap, C.byref(cnt))
+        rows = [tuple(table[4 * i:4 * i + 4]) for i in range(min(cnt.value, cap))]
+        best = min(rows, key=lambda r: r[3])
+        self.shape = (int(best[0]), int(best[1]), float(best[2]))
+        if cache:
+            try:
+                os.makedirs(os.path.dirname(path), exist_ok=True)
+                data = {}
+                if os.path.exists(path):
+                    with open(path) as f:
+                        data = json.load(f)
+                data[key] = list(self.shape)
+                with open(path, "w") as f:
+                    json.dump(data, f, indent=1)
+            except (OSError, ValueError):
+                pass
+        return rows
+
+    def optimize(self, opts: Optional[SolverOptions] = None,
+                 solutions: bool = True) -> List[SDPResult]:
+        """Solve every instance; results in input order (objectives and
+        residuals on the original data, as `sdpx_b200_optimize` reports them)."""
+        from .cuda_backend import STATUS_NAMES, SolveResult, native_options
+        no = native_options(opts or batch_options())
+        n = len(self.problems)
+        res = (SolveResult * n)()
+        self._call("sdpx_b200_batch_optimize", C.byref(no), res)
+        dp = C.POINTER(C.c_double)
+        out = []
+        for i, p in enumerate(self.problems):
+            k = p.k[0]
+            x, X, Y = np.zeros(p.m), np.zeros(k * k), np.zeros(k * k)
+            if solutions:
+                self._call("sdpx_b200_batch_get_solution", i, x.ctypes.data_as(dp),
+                           X.ctypes.data_as(dp), Y.ctypes.data_as(dp))
+            r = res[i]
+            out.append(SDPResult(
+                status=Status(STATUS_NAMES[r.status]), message=r.message.decode(errors="replace"),
+                x=x, X=[X.reshape(k, k).T.copy()], y=np.zeros(0), Y=[Y.reshape(k, k).T.copy()],
+                pObj=r.p_obj, dObj=r.d_obj, p_res=r.p_res, d_res=r.d_res,
+                iterations=r.iterations, restarts=r.restarts,
+                precision_trace=["fp64"] * r.fp64_iterations, seconds=r.seconds))
+        return out
+
+    def stats(self) -> Dict[str, float]:
+        """Counters of the last optimize (sdpx_b200_batch_stats)."""
+        v = np.zeros(8)
+        self._call("sdpx_b200_batch_stats", v.ctypes.data_as(C.POINTER(C.c_double)))
+        keys = ("passes", "launches", "seconds", "schur_seconds", "factor_seconds",
+                "step_seconds", "instance_iterations", "schur_flops")
+        return dict(zip(keys, v.tolist()))
+
+
 def solve_batch(problems: Sequence[SDPProblem], *, tolerance: float = 1e-8,
-                precision: str = "fp64", threads: int = 8, device: int = 0,
-                driver: str = "native", **kwargs) -> List[SDPResult]:
-    """Solve every problem (one handle each, `threads` concurrent solves);
-    results in input order.  With the native driver the whole loop runs inside
-    the library, so the threads hold the GIL only to start and collect."""
+                engine: str = "batched", precision: str = "fp64", threads: int = 8,
+                device: int = 0, driver: str = "native", autotune: bool = False,
+                **kwargs) -> List[SDPResult]:
+    """Solve every problem; results in input order.
+
+    ``engine="batched"``: one `BatchSolver` over all problems with the
+    batched engine's options (`BATCH_OPTIONS` plus `kwargs`; FP64).
+    ``engine="loop"``: one handle per problem, ``threads`` concurrent solves
+    with `SolverOptions(precision, **kwargs)`; with the native driver the whole
+    loop runs inside the library, so the threads hold the GIL only to start and
+    collect."""
+    if engine == "batched":
+        if precision != "fp64":
+            raise ValueError("the batched engine runs in FP64")
+        opts = batch_options(tolerance, **kwargs)
+        with BatchSolver(problems, device=device) as bs:
+            if autotune:
+                bs.autotune(opts)
+            return bs.optimize(opts)
+    if engine != "loop":
+        raise ValueError(f"unknown engine {engine!r}")
     from .cuda_backend import CudaBackend
     opts = SolverOptions(precision=precision, **kwargs).with_tolerance(tolerance)
 

@@ -28,6 +28,13 @@ class _Problem(C.Structure):
                 ("Av", C.POINTER(_dp)), ("C", C.POINTER(_dp)), ("c", _dp)]
 
 
+class BatchProblem(C.Structure):
+    """`sdpx_b200_batch_problem` (include/sdpx_b200_batch.h)."""
+    _fields_ = [("count", C.c_int32), ("block_order", C.POINTER(C.c_int32)),
+                ("m", C.POINTER(C.c_int32)), ("Av", C.POINTER(_dp)), ("C", C.POINTER(_dp)),
+                ("c", C.POINTER(_dp))]
+
+
 class CertificateResult(C.Structure):
     """Mirror of sdpx_b200_certificate_result (include/sdpx_b200.h)."""
     _fields_ = [("valid", C.c_int32), ("failures", C.c_int32),
@@ -168,6 +175,14 @@ _SIGS = {
                                   C.POINTER(C.c_int32), _dp, C.c_int32, _dp],
     "sdpx_b200_certificate_eq": [C.c_void_p, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
                                  C.c_double, C.c_int32, C.POINTER(CertificateResult)],
+    # batched small-SDP engine (include/sdpx_b200_batch.h)
+    "sdpx_b200_batch_create": [C.POINTER(BatchProblem), C.c_int, C.POINTER(C.c_void_p)],
+    "sdpx_b200_batch_optimize": [C.c_void_p, C.POINTER(SolveOptions), C.POINTER(SolveResult)],
+    "sdpx_b200_batch_get_solution": [C.c_void_p, C.c_int32, _dp, _dp, _dp],
+    "sdpx_b200_batch_stats": [C.c_void_p, _dp],
+    "sdpx_b200_batch_set_schur_shape": [C.c_void_p, C.c_int32, C.c_int32, C.c_double],
+    "sdpx_b200_batch_autotune": [C.c_void_p, C.POINTER(SolveOptions), _dp, C.c_int32,
+                                 C.POINTER(C.c_int32)],
 }
 
 _lib = None
@@ -191,6 +206,12 @@ def load_library(path: str = LIB_PATH):
     lib.sdpx_b200_last_error.restype = C.c_char_p
     lib.sdpx_b200_create_error.argtypes = []
     lib.sdpx_b200_create_error.restype = C.c_char_p
+    lib.sdpx_b200_batch_destroy.argtypes = [C.c_void_p]
+    lib.sdpx_b200_batch_destroy.restype = None
+    lib.sdpx_b200_batch_last_error.argtypes = [C.c_void_p]
+    lib.sdpx_b200_batch_last_error.restype = C.c_char_p
+    lib.sdpx_b200_batch_create_error.argtypes = []
+    lib.sdpx_b200_batch_create_error.restype = C.c_char_p
     _lib = lib
     return lib
 

@@ -32,7 +32,8 @@ def test_header_declares_core_entry_points():
     for must in ("sdpx_b200_create", "sdpx_b200_schur_build", "sdpx_b200_factorize",
                  "sdpx_b200_solve", "sdpx_b200_refine", "sdpx_b200_line_search",
                  "sdpx_b200_normal_nt_scaling", "sdpx_b200_normal_factorize",
-                 "sdpx_b200_normal_solve"):
+                 "sdpx_b200_normal_solve", "sdpx_b200_batch_create",
+                 "sdpx_b200_batch_optimize", "sdpx_b200_batch_autotune"):
         assert must in names
 
 

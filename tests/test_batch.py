@@ -1,10 +1,15 @@
 """Batches of independent instances (the 4096 small-SDP workload's shape).
 
-CPU: the instance generator's size distribution.  GPU: a concurrent batch
-(one handle and stream per instance, host threads) reproduces each instance's
-single solve exactly — same status, iterations and objectives — because each
-instance runs the same deterministic kernels in the same order.
+CPU: the instance generator's size distribution, the batched engine's scope
+checks (made before any device call) and the oracle on the batched engine's
+options.  GPU: the per-instance loop (one handle and stream per instance,
+host threads) reproduces each instance's single solve exactly — same status,
+iterations and objectives — because each instance runs the same
+deterministic kernels in the same order.  The batched engine's parity tests
+are in test_gpu_batch_engine.py.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -22,6 +27,58 @@ def test_batch_instance_sizes():
     assert all(np.array_equal(a.c, b.c) for a, b in zip(probs[:4], again))
 
 
+def _batch_problem(ks, ms):
+    from sdpx_b200.cuda_backend import BatchProblem
+    dp = C.POINTER(C.c_double)
+    n = len(ks)
+    keep = [np.zeros(k * k * m) for k, m in zip(ks, ms)] + [np.zeros(k * k) for k in ks] + \
+        [np.zeros(m) for m in ms]
+    Av, Cs, cs = (dp * n)(), (dp * n)(), (dp * n)()
+    for i in range(n):
+        Av[i] = keep[i].ctypes.data_as(dp)
+        Cs[i] = keep[n + i].ctypes.data_as(dp)
+        cs[i] = keep[2 * n + i].ctypes.data_as(dp)
+    prob = BatchProblem(n, (C.c_int32 * n)(*ks), (C.c_int32 * n)(*ms), Av, Cs, cs)
+    return prob, keep
+
+
+@pytest.mark.parametrize("ks, ms, msg", [
+    ([5, 2], [4, 3], "block order 2 outside [3, 64]"),
+    ([65], [4], "block order 65 outside [3, 64]"),
+    ([8, 9], [3, 257], "m = 257 outside [1, 256]"),
+    ([8], [0], "m = 0 outside [1, 256]"),
+])
+def test_batch_create_rejects_out_of_scope_instances(ks, ms, msg):
+    """Sizes are checked before the device is touched (runs without a GPU)."""
+    from sdpx_b200.cuda_backend import load_library
+    lib = load_library()
+    prob, keep = _batch_problem(ks, ms)
+    h = C.c_void_p()
+    assert lib.sdpx_b200_batch_create(C.byref(prob), 0, C.byref(h)) == -2
+    assert not h.value
+    assert msg in lib.sdpx_b200_batch_create_error().decode()
+
+
+def test_batch_solver_rejects_multi_block_problems():
+    from sdpx_b200 import generators as G
+    from sdpx_b200.batch import BatchSolver
+    with pytest.raises(ValueError, match="one PSD block"):
+        BatchSolver([G.sdpa_dense(m=10, blocks=[5, 4], lp=0, seed=1)])
+
+
+def test_oracle_solves_batch_instances_with_the_batch_options():
+    """The oracle runs the batched engine's options (fixed start, no
+    equilibration) to Optimal on small instances of the workload."""
+    from oracle.sdpx_oracle import oracle_solve
+    from sdpx_b200.batch import batch_options
+    probs = [p for p in batch_instances(40, seed=0) if p.k[0] <= 16 and p.m <= 60][:4]
+    assert len(probs) >= 2
+    for p in probs:
+        r = oracle_solve(p, batch_options(1e-8))
+        assert r.status.value == "Optimal"
+        assert r.relative_gap <= 1e-8
+
+
 @pytest.mark.gpu
 def test_concurrent_batch_equals_single_solves():
     import torch
@@ -29,7 +86,7 @@ def test_concurrent_batch_equals_single_solves():
         pytest.skip("no CUDA device")
     from sdpx_b200 import solve, solve_batch
     probs = batch_instances(12, seed=5)
-    batch = solve_batch(probs, tolerance=1e-8, threads=4)
+    batch = solve_batch(probs, tolerance=1e-8, threads=4, engine="loop")
     for p, rb in zip(probs, batch):
         rs = solve(p, tolerance=1e-8)
         assert rb.status == rs.status

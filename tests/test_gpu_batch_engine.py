@@ -1,0 +1,113 @@
+"""The batched small-SDP engine (sdpx_b200_batch_*) against single-instance
+solves with the same options and against the oracle.
+
+Every instance keeps its own controller, so the engine must reproduce each
+instance's single solve: same status, objectives within 1e-7 relative (they
+differ only by summation order), iterations within one.  The launch shape of
+the Schur phase changes no result bit (every Schur entry is one thread's sum
+over K in the same order whatever the tiles and work split).
+"""
+import numpy as np
+import pytest
+
+from sdpx_b200 import batch_instances
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cuda_ok():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return True
+
+
+def rel(a, b):
+    return abs(a - b) / max(1.0, abs(b))
+
+
+def test_batched_engine_matches_single_solves(cuda_ok):
+    from sdpx_b200 import solve
+    from sdpx_b200.batch import BATCH_OPTIONS, BatchSolver, batch_options
+    probs = batch_instances(48, seed=7)
+    opts = batch_options(1e-8)
+    with BatchSolver(probs) as bs:
+        batch = bs.optimize(opts)
+        st = bs.stats()
+    assert st["launches"] > 0 and st["instance_iterations"] > 0
+    mismatch = []
+    for i, (p, rb) in enumerate(zip(probs, batch)):
+        rs = solve(p, tolerance=1e-8, **BATCH_OPTIONS)
+        if rb.status != rs.status or abs(rb.iterations - rs.iterations) > 1 or \
+                rel(rb.pObj, rs.pObj) > 1e-7 or rel(rb.dObj, rs.dObj) > 1e-7:
+            mismatch.append((i, rb.status.value, rs.status.value, rb.iterations, rs.iterations,
+                             rb.pObj, rs.pObj))
+    assert not mismatch, mismatch
+    assert sum(r.status.value == "Optimal" for r in batch) == len(probs)
+    for p, rb in zip(probs, batch):
+        assert rb.relative_gap <= 1e-8
+        assert rb.p_res / (1 + np.abs(p.C[0]).max()) <= 1e-8
+        assert rb.d_res / (1 + np.abs(p.c).max()) <= 1e-8
+        # the returned iterate is the solution: X = 𝒜x − C ⪰ 0, Y ⪰ 0
+        X = np.tensordot(rb.x, p.Av[0], axes=1).reshape(p.k[0], p.k[0]) - p.C[0]
+        assert np.allclose(X, rb.X[0], atol=1e-9 * (1 + np.abs(X).max()))
+        assert np.linalg.eigvalsh(rb.Y[0]).min() >= -1e-9 * (1 + np.abs(rb.Y[0]).max())
+
+
+def test_batched_engine_matches_oracle(cuda_ok):
+    from oracle.sdpx_oracle import oracle_solve
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = [p for p in batch_instances(60, seed=11) if p.k[0] <= 24 and p.m <= 80][:6]
+    assert len(probs) >= 4
+    opts = batch_options(1e-8)
+    with BatchSolver(probs) as bs:
+        batch = bs.optimize(opts)
+    for p, rb in zip(probs, batch):
+        ro = oracle_solve(p, opts)
+        assert rb.status == ro.status
+        assert abs(rb.iterations - ro.iterations) <= 1
+        assert rel(rb.pObj, ro.pObj) <= 1e-7 and rel(rb.dObj, ro.dObj) <= 1e-7
+
+
+def test_schur_launch_shape_changes_no_result(cuda_ok):
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = batch_instances(24, seed=2)
+    opts = batch_options(1e-8)
+    with BatchSolver(probs) as bs:
+        ref = bs.optimize(opts, solutions=False)
+        for shape in [(128, 16, 0.0), (512, 32, 1.0e6), (256, 16, 16.0e6)]:
+            bs.set_schur_shape(*shape)
+            out = bs.optimize(opts, solutions=False)
+            for a, b in zip(ref, out):
+                assert a.status == b.status and a.iterations == b.iterations
+                assert a.pObj == b.pObj and a.dObj == b.dObj
+
+
+def test_autotune_picks_a_timed_shape(cuda_ok, tmp_path, monkeypatch):
+    from sdpx_b200.batch import BatchSolver, batch_options
+    monkeypatch.setenv("SDPX_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    probs = batch_instances(32, seed=4)
+    with BatchSolver(probs) as bs:
+        table = bs.autotune(batch_options(1e-8))
+        assert len(table) == 20
+        best = min(table, key=lambda r: r[3])
+        assert bs.shape == (int(best[0]), int(best[1]), float(best[2]))
+        assert all(r[3] > 0 for r in table)
+        res = bs.optimize(batch_options(1e-8), solutions=False)
+        assert sum(r.status.value == "Optimal" for r in res) == len(probs)
+    with BatchSolver(probs) as bs2:  # the stored choice is reused
+        assert bs2.autotune(batch_options(1e-8)) == []
+        assert bs2.shape == (int(best[0]), int(best[1]), float(best[2]))
+
+
+def test_batched_engine_rejects_unsupported_options(cuda_ok):
+    from sdpx_b200.batch import BatchSolver
+    from sdpx_b200 import SolverOptions
+    from sdpx_b200.cuda_backend import SDPXB200Error
+    probs = batch_instances(2, seed=1)
+    with BatchSolver(probs) as bs:
+        with pytest.raises(SDPXB200Error, match="fixed start"):
+            bs.optimize(SolverOptions().with_tolerance(1e-8))
+        with pytest.raises(SDPXB200Error, match="equilibration"):
+            bs.optimize(SolverOptions(parameter_policy="fixed").with_tolerance(1e-8))
