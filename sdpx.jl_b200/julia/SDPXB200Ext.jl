@@ -401,4 +401,97 @@ function solve_factor!(h::B200Normal, rhs::Vector{Float64})
     return rhs
 end
 
+# --------------------------------------------- batched small SDPs ---------
+# include/sdpx_b200_batch.h: many one-block SDPs in one pooled device
+# workspace, one kernel per interior-point phase over all of them.  SDPX has no
+# batch solver; this replaces a loop of `SDPX.solve` calls over instances.
+struct B200BatchProblem
+    count::Int32
+    block_order::Ptr{Int32}
+    m::Ptr{Int32}
+    Av::Ptr{Ptr{Float64}}
+    C::Ptr{Ptr{Float64}}
+    c::Ptr{Ptr{Float64}}
+end
+
+mutable struct B200Batch
+    ptr::Ptr{Cvoid}
+    count::Int
+    dims::Vector{Tuple{Int,Int}}  # (k, m) per instance
+end
+
+"""Upload one-block problems (each `prob.dims.L == 1`, `prob.dims.n == 0`,
+3 ≤ k ≤ 64, m ≤ 256) into one batch workspace."""
+function B200Batch(probs::Vector{<:SDPX.SDPProblem{Float64}}; device::Integer=0)
+    n = length(probs)
+    ks = Int32[p.dims.k[1] for p in probs]
+    ms = Int32[p.dims.m for p in probs]
+    Av = [Matrix{Float64}((p.cons::SDPX.DenseCons{Float64}).Av[1]) for p in probs]  # k²×m
+    Cm = [Matrix{Float64}(p.C[1]) for p in probs]
+    cv = [Vector{Float64}(p.c) for p in probs]
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    GC.@preserve ks ms Av Cm cv begin
+        pA = [pointer(a) for a in Av]; pC = [pointer(a) for a in Cm]; pc = [pointer(a) for a in cv]
+        GC.@preserve pA pC pc begin
+            bp = B200BatchProblem(Int32(n), pointer(ks), pointer(ms), pointer(pA), pointer(pC),
+                                  pointer(pc))
+            status = ccall((:sdpx_b200_batch_create, libsdpx), Cint,
+                           (Ref{B200BatchProblem}, Cint, Ref{Ptr{Cvoid}}), bp, device, out)
+            status == 0 || error(unsafe_string(ccall((:sdpx_b200_batch_create_error, libsdpx),
+                                                     Cstring, ())))
+        end
+    end
+    b = B200Batch(out[], n, [(Int(ks[i]), Int(ms[i])) for i in 1:n])
+    finalizer(x -> (x.ptr == C_NULL || ccall((:sdpx_b200_batch_destroy, libsdpx), Cvoid,
+                                             (Ptr{Cvoid},), x.ptr)), b)
+    return b
+end
+
+function _bcheck(b::B200Batch, status::Cint, what)
+    status == 0 && return nothing
+    msg = unsafe_string(ccall((:sdpx_b200_batch_last_error, libsdpx), Cstring, (Ptr{Cvoid},),
+                              b.ptr))
+    error("sdpx_b200_batch_$(what): $(msg)")
+end
+
+"""Times the Schur launch shapes on the device and keeps the fastest
+(sdpx_b200_batch_autotune); returns rows (threads, tile, grain, ms)."""
+function autotune!(b::B200Batch, o::B200SolveOptions)
+    table = zeros(4 * 64)
+    cnt = Ref{Int32}(0)
+    _bcheck(b, ccall((:sdpx_b200_batch_autotune, libsdpx), Cint,
+                     (Ptr{Cvoid}, Ref{B200SolveOptions}, Ptr{Float64}, Int32, Ref{Int32}),
+                     b.ptr, o, table, Int32(64), cnt), "autotune")
+    return [Tuple(table[4i+1:4i+4]) for i in 0:cnt[]-1]
+end
+
+"""Solve every instance of the batch with the fixed start and no
+equilibration (the options the batched engine serves); per instance the
+status, iterations, objectives and (x, X, Y)."""
+function optimize(b::B200Batch, tolerance::Float64; autotune::Bool=false)
+    o = B200SolveOptions()
+    ccall((:sdpx_b200_default_options, libsdpx), Cvoid, (Ref{B200SolveOptions},), o)
+    o.eps_gap = o.eps_primal = o.eps_dual = tolerance
+    o.parameter_policy = Int32(1)
+    o.scaling = Int32(1)
+    autotune && autotune!(b, o)
+    res = Vector{B200SolveResult}(undef, b.count)
+    _bcheck(b, ccall((:sdpx_b200_batch_optimize, libsdpx), Cint,
+                     (Ptr{Cvoid}, Ref{B200SolveOptions}, Ptr{B200SolveResult}), b.ptr, o, res),
+            "optimize")
+    out = Vector{Any}(undef, b.count)
+    for i in 1:b.count
+        k, m = b.dims[i]
+        x, X, Y = zeros(m), zeros(k * k), zeros(k * k)
+        _bcheck(b, ccall((:sdpx_b200_batch_get_solution, libsdpx), Cint,
+                         (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                         b.ptr, Int32(i - 1), x, X, Y), "get_solution")
+        r = res[i]
+        out[i] = (status=_STATUS[r.status], iterations=Int(r.iterations), x=x,
+                  X=reshape(X, k, k), Y=reshape(Y, k, k), pObj=r.p_obj, dObj=r.d_obj,
+                  pRes=r.p_res, dRes=r.d_res)
+    end
+    return out
+end
+
 end # module
