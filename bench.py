@@ -74,7 +74,7 @@ SPARSE_WORKLOAD = dict(m=3000, blocks=32, kmin=23, kmax=74, active=0.6, pairs=(1
 # Batch of small SDPs of uneven size (block n ~ U{4..64}, m ~ U{3..min(200,
 # n(n+1)/2)}): a bounded slice of the 4096-instance workload, solved
 # concurrently (one handle and stream per instance) and as a serial loop.
-BATCH_WORKLOAD = dict(instances=256, serial_sample=32, threads=16, tol=1e-8)
+BATCH_WORKLOAD = dict(instances=4096, loop_sample=96, tol=1e-8)
 
 
 def schur_flops(m, blocks, lp):
@@ -250,33 +250,68 @@ def cpu_sample(prob, blocks, lp, gpu_iterations):
 
 
 def bench_batch(args, world, rank, local):
-    """Wall-clock throughput of a concurrent batch (host threads, one device
-    handle and stream per instance) against the per-instance serial loop."""
+    """The 4096-instance small-SDP workload on the batched engine (one kernel
+    per interior-point phase over all instances, sdpx_b200_batch_*) against
+    the per-instance plain GPU loop (one handle and sdpx_b200_optimize per
+    instance, serial) with the same options, timed on a bounded sample.
+    Wall-clock times: both loops are host-driven.  The batched solve is timed
+    with the data resident (after one untimed solve and the launch-shape
+    autotune) and end to end (upload from host memory, solve, every
+    solution read back)."""
     import torch
     from sdpx_b200 import batch_instances, solve_batch
+    from sdpx_b200.batch import BATCH_OPTIONS, BatchSolver, batch_options
     wl = BATCH_WORKLOAD
     probs = batch_instances(wl["instances"], seed=rank)
-    solve_batch(probs[:wl["threads"]], tolerance=wl["tol"], threads=wl["threads"], device=local)
-    torch.cuda.synchronize()
+    opts = batch_options(wl["tol"])
+    with BatchSolver(probs, device=local) as bs:
+        table = bs.autotune(opts, cache=False)
+        bs.optimize(opts, solutions=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = bs.optimize(opts, solutions=False)
+        t_batch = time.perf_counter() - t0
+        st = bs.stats()
     t0 = time.perf_counter()
-    res = solve_batch(probs, tolerance=wl["tol"], threads=wl["threads"], device=local)
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
+    with BatchSolver(probs, device=local) as bs2:
+        bs2.set_schur_shape(*bs.shape)
+        res_e2e = bs2.optimize(opts, solutions=True)
+    t_e2e = time.perf_counter() - t0
+    ns = wl["loop_sample"]
+    solve_batch(probs[:2], tolerance=wl["tol"], engine="loop", threads=1, device=local,
+                **BATCH_OPTIONS)
     t0 = time.perf_counter()
-    ser = solve_batch(probs[:wl["serial_sample"]], tolerance=wl["tol"], threads=1, device=local)
-    torch.cuda.synchronize()
-    t_serial = time.perf_counter() - t0
-    same = all(a.pObj == b.pObj and a.iterations == b.iterations
-               for a, b in zip(res[:wl["serial_sample"]], ser))
-    return {"workload": (f"{wl['instances']} small dense SDPs, block n ~ U{{4..64}}, "
-                         f"m ~ U{{3..min(200, n(n+1)/2)}}, to {wl['tol']:g}"),
-            "value": wl["instances"] / t_batch, "unit": "instances/s",
-            "threads": wl["threads"], "timing": "wall clock (host threads, several streams)",
-            "serial_loop_instances_per_s": wl["serial_sample"] / t_serial,
-            "speedup_vs_serial_loop": (wl["instances"] / t_batch) /
-                                      (wl["serial_sample"] / t_serial),
+    loop = solve_batch(probs[:ns], tolerance=wl["tol"], engine="loop", threads=1, device=local,
+                       **BATCH_OPTIONS)
+    t_loop = time.perf_counter() - t0
+    rel = lambda a, b: abs(a - b) / max(1.0, abs(b))
+    agree = sum(a.status == b.status and abs(a.iterations - b.iterations) <= 1 and
+                rel(a.pObj, b.pObj) <= 1e-7 and rel(a.dObj, b.dObj) <= 1e-7
+                for a, b in zip(res[:ns], loop))
+    rate, loop_rate = wl["instances"] / t_batch, ns / t_loop
+    in_bytes = sum(p.Av[0].nbytes + p.C[0].nbytes + p.c.nbytes for p in probs)
+    out_bytes = sum(p.c.nbytes + 2 * p.C[0].nbytes for p in probs)
+    return {"workload": (f"{wl['instances']} small dense SDPs, one block n ~ U{{4..64}}, "
+                         f"m ~ U{{3..min(200, n(n+1)/2)}}, fixed start, to {wl['tol']:g}"),
+            "engine": "batched (sdpx_b200_batch_optimize)",
+            "value": rate, "unit": "instances/s", "seconds": t_batch,
+            "timing": "wall clock of sdpx_b200_batch_optimize, data resident",
             "optimal": sum(r.status.value == "Optimal" for r in res),
-            "serial_results_identical": same}
+            "instances": wl["instances"],
+            "mean_iterations": sum(r.iterations for r in res) / len(res),
+            "passes": st["passes"], "launches": st["launches"],
+            "phase_seconds": {"schur": st["schur_seconds"], "schur_factor": st["factor_seconds"],
+                              "step_length": st["step_seconds"]},
+            "schur_tflops": st["schur_flops"] / max(st["schur_seconds"], 1e-12) / 1e12,
+            "schur_shape": {"threads": bs.shape[0], "tile": bs.shape[1], "grain": bs.shape[2],
+                            "candidates_timed": len(table)},
+            "e2e": {"value": wl["instances"] / t_e2e, "unit": "instances/s", "seconds": t_e2e,
+                    "h2d_bytes": in_bytes, "d2h_bytes": out_bytes,
+                    "optimal": sum(r.status.value == "Optimal" for r in res_e2e)},
+            "loop": {"value": loop_rate, "unit": "instances/s", "sample": ns,
+                     "engine": "one handle per instance, sdpx_b200_optimize, serial"},
+            "speedup_vs_loop": rate / loop_rate,
+            "loop_agreement": f"{agree}/{ns} same status, iterations ±1, objectives 1e-7"}
 
 
 def bench_adjoint(args, world, rank, local):

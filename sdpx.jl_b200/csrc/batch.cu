@@ -467,31 +467,18 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // B7: affine diagnostics: with kMode 1 the fraction-to-boundary bounds of X
-// and Y along dX, dY (`fraction_to_boundary_bound!`), ⟨X, Y⟩,
-// ⟨X + tX·dX, Y + tY·dY⟩ and ⟨X + dX, Y + dY⟩.
+// and Y along dX, dY (`fraction_to_boundary_bound!`, eight trials at a time),
+// ⟨X, Y⟩, ⟨X + tX·dX, Y + tY·dY⟩ and ⟨X + dX, Y + dY⟩.
 __global__ void __launch_bounds__(kThreads)
     k_b_affine(Pool pool, const int* act, const double* par, double* res) {
   INST_PROLOGUE
   extern __shared__ __align__(16) double sm[];
-  double* Ms = sm;
-  double* Xs = Ms + pool.kq;
-  double* Ds = Xs + pool.kq;
-  __shared__ double red[32], sflag[4];
+  __shared__ double red[32];
+  __shared__ int flags[kTrialWarps];
   double tX = 1.0, tY = 1.0;
   if (in[kMode] == 1.0) {
-    for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
-      Xs[e] = pool.X[I.kk_off + e];
-      Ds[e] = pool.dX[I.kk_off + e];
-    }
-    __syncthreads();
-    const double bX = cta_ftb(Xs, Ds, k, Ms, sflag);
-    __syncthreads();
-    for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
-      Xs[e] = pool.Y[I.kk_off + e];
-      Ds[e] = pool.dY[I.kk_off + e];
-    }
-    __syncthreads();
-    const double bY = cta_ftb(Xs, Ds, k, Ms, sflag);
+    const double bX = cta_ftb_tree(pool.X + I.kk_off, pool.dX + I.kk_off, k, sm, pool.kp, flags);
+    const double bY = cta_ftb_tree(pool.Y + I.kk_off, pool.dY + I.kk_off, k, sm, pool.kp, flags);
     tX = bX < 1.0 ? bX : 1.0;
     tY = bY < 1.0 ? bY : 1.0;
   }
@@ -550,39 +537,21 @@ __global__ void k_b_rollback(Pool pool, const int* act, const double* par, doubl
 
 // B10: backtracking line search per side: the first t of 1, γ, γ², … for
 // which M + t·dM has a Cholesky factor with min|L_jj| > kRatio·max|L_jj|, or
-// the first t below kMinStep (src/kernels/threaded.jl:1751-1818).
+// the first t below kMinStep (src/kernels/threaded.jl:1751-1818); eight
+// candidates at a time.
 __global__ void __launch_bounds__(kThreads)
     k_b_linesearch(Pool pool, const int* act, const double* par, double* res) {
   INST_PROLOGUE
   extern __shared__ __align__(16) double sm[];
-  double* Ms = sm;
-  double* Xs = Ms + pool.kq;
-  double* Ds = Xs + pool.kq;
-  __shared__ double sflag[4];
+  __shared__ int flags[kTrialWarps];
   const double gamma = in[kGamma], min_step = in[kMinStep], ratio = in[kRatio];
-  double t[2];
-  for (int side = 0; side < 2; ++side) {
-    const double* Mv = side ? pool.Y + I.kk_off : pool.X + I.kk_off;
-    const double* Dv = side ? pool.dY + I.kk_off : pool.dX + I.kk_off;
-    __syncthreads();
-    for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
-      Xs[e] = Mv[e];
-      Ds[e] = Dv[e];
-    }
-    __syncthreads();
-    double tt = 1.0;
-    // γ ∈ (0, 1) reaches min_step > 0 long before the guard; the guard bounds
-    // the loop for any other input.
-    for (int guard = 0; guard < 4096; ++guard) {
-      const bool ok = cta_trial(Xs, Ds, tt, k, ratio, Ms, sflag);
-      if (ok || tt < min_step) break;
-      tt *= gamma;
-    }
-    t[side] = tt;
-  }
+  const double tX = cta_backtrack(pool.X + I.kk_off, pool.dX + I.kk_off, k, gamma, min_step,
+                                  ratio, sm, pool.kp, flags);
+  const double tY = cta_backtrack(pool.Y + I.kk_off, pool.dY + I.kk_off, k, gamma, min_step,
+                                  ratio, sm, pool.kp, flags);
   if (threadIdx.x == 0) {
-    out[oTX] = t[0];
-    out[oTY] = t[1];
+    out[oTX] = tX;
+    out[oTY] = tY;
   }
 }
 
@@ -817,6 +786,10 @@ struct Engine {
   }
 
   size_t smem_bytes(int mats) const { return (size_t)mats * (size_t)pool.kq * sizeof(double); }
+  // Packed lower triangles of X, dX and kTrialWarps trial slots (the step-length phases).
+  size_t smem_trials() const {
+    return (size_t)(2 + kTrialWarps) * (size_t)pool.kp * sizeof(double);
+  }
 
   void create(const sdpx_b200_batch_problem* prob, int device) {
     if (!prob || prob->count <= 0) throw std::invalid_argument("empty batch");
@@ -895,9 +868,13 @@ struct Engine {
     pool.x = x.p, pool.dx = dx.p, pool.d = d.p, pool.r = r.p, pool.rho = rho.p;
     pool.xb = xb.p, pool.dxb = dxb.p, pool.S = S.p, pool.LS = LS.p;
     pool.kq = (long long)kmax * kmax;
-    for (PhaseKernel kf : {k_b_residuals, k_b_rhs, k_b_dirblocks, k_b_affine, k_b_linesearch})
+    pool.kp = (long long)kmax * (kmax + 1) / 2;
+    for (PhaseKernel kf : {k_b_residuals, k_b_rhs, k_b_dirblocks})
       SDPX_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem_bytes(3)));
+    for (PhaseKernel kf : {k_b_affine, k_b_linesearch})
+      SDPX_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_trials()));
     SDPX_CUDA(cudaFuncSetAttribute(k_b_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem_bytes(4)));
     SDPX_CUDA(cudaStreamSynchronize(st));
@@ -907,7 +884,7 @@ struct Engine {
   // One launch of `kf` over the instances `ids` (one CTA each); `fill` writes
   // each row's inputs.  With `read`, waits and returns the output rows.
   template <class Fill>
-  const double* phase(PhaseKernel kf, const std::vector<int>& ids, int mats, Fill fill,
+  const double* phase(PhaseKernel kf, const std::vector<int>& ids, size_t smem, Fill fill,
                       bool read) {
     const int n = (int)ids.size();
     if (n == 0) return nullptr;
@@ -924,7 +901,7 @@ struct Engine {
     SDPX_CUDA(cudaMemcpyAsync(d_act.p, ha, n * sizeof(int), cudaMemcpyHostToDevice, st));
     SDPX_CUDA(cudaMemcpyAsync(d_par.p, hp, (size_t)n * kNIn * sizeof(double),
                               cudaMemcpyHostToDevice, st));
-    kf<<<n, kThreads, smem_bytes(mats), st>>>(pool, d_act.p, d_par.p, d_res.p);
+    kf<<<n, kThreads, smem, st>>>(pool, d_act.p, d_par.p, d_res.p);
     SDPX_LAUNCH_CHECK();
     ++launches;
     if (!read) return nullptr;
@@ -933,8 +910,8 @@ struct Engine {
     SDPX_CUDA(cudaStreamSynchronize(st));
     return static_cast<const double*>(h_res.p);
   }
-  const double* phase(PhaseKernel kf, const std::vector<int>& ids, int mats, bool read) {
-    return phase(kf, ids, mats, [](int, double*) {}, read);
+  const double* phase(PhaseKernel kf, const std::vector<int>& ids, size_t smem, bool read) {
+    return phase(kf, ids, smem, [](int, double*) {}, read);
   }
 
   // The Schur assembly over `ids`: panel then SYRK work items, largest first.
@@ -1061,7 +1038,7 @@ struct Engine {
       R.scale_p = scale_p[all[q]];
       R.scale_d = scale_d[all[q]];
     }
-    out = phase(k_b_residuals, all, 2, [&](int id, double* in) {
+    out = phase(k_b_residuals, all, smem_bytes(2), [&](int id, double* in) {
       in[kMu] = runs[id].mu;
       in[kUseAffine] = runs[id].ctl.strategy_adaptive() ? 1 : 0;
       in[kFactor] = 0;
@@ -1137,7 +1114,7 @@ struct Engine {
         R.adaptive = R.ctl.strategy_adaptive();  // use_affine
         R.beta0 = R.ctl.beta;
       }
-      out = phase(k_b_residuals, stepping, 2, [&](int id, double* in) {
+      out = phase(k_b_residuals, stepping, smem_bytes(2), [&](int id, double* in) {
         in[kMu] = runs[id].mu;
         in[kUseAffine] = runs[id].adaptive ? 1 : 0;
         in[kFactor] = 1;
@@ -1175,11 +1152,11 @@ struct Engine {
           ok2.push_back(ok1[q]);
       }
       // predictor
-      phase(k_b_rhs, ok2, 3, [](int, double* in) { in[kMode] = 0; }, false);
+      phase(k_b_rhs, ok2, smem_bytes(3), [](int, double* in) { in[kMode] = 0; }, false);
       phase(k_b_solve, ok2, 0, [](int, double* in) { in[kMode] = 0; }, false);
-      phase(k_b_dirblocks, ok2, 3, false);
+      phase(k_b_dirblocks, ok2, smem_bytes(3), false);
       const auto tl0 = std::chrono::steady_clock::now();
-      out = phase(k_b_affine, ok2, 3, [&](int id, double* in) {
+      out = phase(k_b_affine, ok2, smem_trials(), [&](int id, double* in) {
         const Run& R = runs[id];
         in[kMode] = (R.adaptive && !R.ctl.fallback) ? 1 : 0;
       }, true);
@@ -1248,7 +1225,7 @@ struct Engine {
         R.adaptive = adaptive;  // as evaluated before the controller's selection
       }
       // corrector
-      phase(k_b_rhs, ok2, 3, [&](int id, double* in) {
+      phase(k_b_rhs, ok2, smem_bytes(3), [&](int id, double* in) {
         const Run& R = runs[id];
         const Inst& I = inst[id];
         in[kMode] = 1;
@@ -1319,14 +1296,14 @@ struct Engine {
         else
           ok3.push_back(id);
       }
-      phase(k_b_dirblocks, ok3, 3, false);
+      phase(k_b_dirblocks, ok3, smem_bytes(3), false);
       for (int id : ok3) {  // the step succeeded: its residuals become the loop's
         Run& R = runs[id];
         R.p_res = R.sp_res;
         R.d_res = R.sd_res;
       }
       const auto tl1 = std::chrono::steady_clock::now();
-      out = phase(k_b_linesearch, ok3, 3, [&](int id, double* in) {
+      out = phase(k_b_linesearch, ok3, smem_trials(), [&](int id, double* in) {
         const Run& R = runs[id];
         in[kGamma] = R.params.backtracking;
         in[kMinStep] = R.params.minimum_step;
@@ -1508,7 +1485,7 @@ struct Engine {
       }, false);
     }
     const double* out =
-        phase(k_b_residuals, all, 2, [](int, double* in) { in[kFactor] = 1; }, true);
+        phase(k_b_residuals, all, smem_bytes(2), [](int, double* in) { in[kFactor] = 1; }, true);
     std::vector<int> ok;
     for (int q = 0; q < N; ++q)
       if (out[(size_t)q * oNOut + oOk] != 0.0) ok.push_back(q);
