@@ -64,6 +64,23 @@ int sdpx_b200_batch_optimize(sdpx_b200_batch* b, const sdpx_b200_solve_options* 
  * (k² column-major).  Any pointer may be NULL. */
 int sdpx_b200_batch_get_solution(sdpx_b200_batch* b, int32_t i, double* x, double* X, double* Y);
 
+/* Replaces instance i's current iterate with host x (m), X and Y (k²
+ * column-major), e.g. to certify solutions computed elsewhere; NULL keeps
+ * that part.  Certificates need every instance's x, X and Y set (or a solve). */
+int sdpx_b200_batch_set_solution(sdpx_b200_batch* b, int32_t i, const double* x,
+                                 const double* X, const double* Y);
+
+/* Result certificates of every instance's current solution (after
+ * sdpx_b200_batch_optimize: the returned iterate) against its data, computed
+ * for all instances by one kernel and read back once — SDPX's
+ * `result_certificate` (src/validation.jl:948-1115), optimality kind, n = 0,
+ * with the fields and failure bits of sdpx_b200_certificate (results: count
+ * entries; the block counts are 0 or 1).  legacy_gap = 1 selects the
+ * 0 ≤ gap ≤ eps_gap test. */
+int sdpx_b200_batch_certificate(sdpx_b200_batch* b, double eps_primal, double eps_dual,
+                                double eps_gap, int32_t legacy_gap,
+                                sdpx_b200_certificate_result* results);
+
 /* Counters of the last optimize: out[0] loop passes, out[1] phase kernel
  * launches, out[2] seconds in the loop, out[3] seconds in the Schur phase,
  * out[4] seconds in the Schur factorisation phase, out[5] seconds in the step

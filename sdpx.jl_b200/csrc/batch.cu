@@ -690,6 +690,185 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Batched result certificate (SDPX's `result_certificate`, src/validation.jl:
+// 948-1115, optimality kind, n = 0) of every instance's device-resident
+// solution (x, X, Y): one CTA per instance, one row of kCertOut doubles each.
+enum CertOut { cPobj = 0, cDobj, cPaff, cDaff, cCompl, cPbMixed, cPbStrict, cDbMixed, cDbStrict,
+               cBadX, cBadY, cXsym, cXallowed, cXok, cXrequired, cXresolved, cYsym, cYallowed,
+               cYok, cYrequired, cYresolved, kCertOut };
+
+// |r| / scale with 0/0 = 0 and r/0 = inf (`_componentwise_ratio`,
+// src/validation.jl:506-513); NaN reads as inf.
+__device__ __forceinline__ double cert_ratio(double r, double scale) {
+  const double a = abs_nan_inf(r);
+  if (scale == 0.0) return a == 0.0 ? 0.0 : 1.0 / 0.0;
+  const double q = a / scale;
+  return q == q ? q : 1.0 / 0.0;
+}
+
+// `_block_psd_certificate` (src/validation.jl:765-904) for one k×k block,
+// k ≥ 3: symmetry defect, Cholesky of the symmetrised copy, then of the copy
+// shifted by the allowed amount; for k ≤ 4 the shift is resolved by doubling
+// and 48 bisection steps.  Writes sym, allowed, ok, required, resolved to
+// o[0..4] (thread 0); returns the number of non-finite entries.
+__device__ double cta_psd_certificate(const double* M, int k, double tol, double* S, double* red,
+                                      double* sflag, double* o) {
+  const int kk = k * k;
+  double bad = 0.0, mx = 0.0, sym = 0.0;
+  for (int e = threadIdx.x; e < kk; e += blockDim.x) {
+    const int r = e % k, c = e / k;
+    const double v = M[e];
+    if (!isfinite(v)) bad += 1.0;
+    mx = fmax(mx, fabs(v));
+    if (r < c) sym = fmax(sym, fabs(v - M[c + r * k]));
+  }
+  bad = cta_sum(bad, red);
+  mx = cta_max(mx, red);
+  sym = cta_max(sym, red);
+  const double scale = fmax(mx, 1.0);
+  const double allowed = fmax(tol, 128.0 * 2.220446049250313e-16) * scale;
+  double ok = 0.0, required = allowed, resolved = 0.0;
+  auto shifted = [&](double shift) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < kk; e += blockDim.x) {
+      const int r = e % k, c = e / k;
+      double v = (M[e] + M[c + r * k]) / 2.0;
+      if (r == c) v += shift;
+      S[e] = v;
+    }
+    __syncthreads();
+    return cta_chol(S, k, sflag, nullptr, nullptr);
+  };
+  if (bad == 0.0) {
+    if (shifted(0.0)) {
+      ok = sym <= allowed ? 1.0 : 0.0;
+      required = 0.0;
+      resolved = 1.0;
+    } else {
+      const bool allowed_ok = shifted(allowed);
+      ok = (allowed_ok && sym <= allowed) ? 1.0 : 0.0;
+      if (k <= 4) {
+        double lower = 0.0, upper = allowed;
+        bool res = allowed_ok;
+        if (!res) {
+          lower = upper;
+          for (int it = 0; it < 64; ++it) {
+            const double cand = upper + upper;
+            if (!isfinite(cand)) break;
+            upper = cand;
+            if (shifted(upper)) {
+              res = true;
+              break;
+            }
+            lower = upper;
+          }
+        }
+        if (res)
+          for (int it = 0; it < 48; ++it) {
+            const double mid = (lower + upper) / 2.0;
+            if (shifted(mid)) upper = mid;
+            else lower = mid;
+          }
+        required = upper;
+        resolved = res ? 1.0 : 0.0;
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    o[0] = sym;
+    o[1] = allowed;
+    o[2] = ok;
+    o[3] = required;
+    o[4] = resolved;
+  }
+  __syncthreads();
+  return bad;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_b_certificate(Pool pool, double tol_p, double tol_d, double* cert) {
+  const Inst I = pool.inst[blockIdx.x];
+  const int k = I.k, m = I.m;
+  const long long kk = (long long)k * k;
+  extern __shared__ __align__(16) double sm[];
+  __shared__ double red[32], sflag[4];
+  double* out = cert + (long long)blockIdx.x * kCertOut;
+  const double* A = pool.A + I.a_off;
+  const double* X = pool.X + I.kk_off;
+  const double* Y = pool.Y + I.kk_off;
+  const double* C = pool.C + I.kk_off;
+  const double* x = pool.x + I.m_off;
+  const double* c = pool.c + I.m_off;
+  // primal rows: R = (𝒜x − X) − C with its componentwise scales
+  double paff = 0.0, pbm = 0.0, pbs = 0.0, dobj = 0.0, compl_ = 0.0, badx = 0.0;
+  for (long long r = threadIdx.x; r < kk; r += blockDim.x) {
+    double sv = 0.0, sn = 0.0, sr = 0.0;
+    for (int i = 0; i < m; ++i) {
+      const double a = A[(long long)i * kk + r];
+      sv += a * x[i];
+      sn += fabs(a);
+      sr += fabs(a) * fabs(x[i]);
+    }
+    const double R = (sv - X[r]) - C[r];
+    const double nominal = fabs(C[r]) + sn;
+    const double realized = (fabs(X[r]) + fabs(C[r])) + sr;
+    paff = fmax(paff, abs_nan_inf(R));
+    pbm = fmax(pbm, cert_ratio(R, nominal + realized));
+    pbs = fmax(pbs, cert_ratio(R, realized));
+    dobj += C[r] * Y[r];
+    compl_ += X[r] * Y[r];
+  }
+  // dual columns: v_i = c_i − ⟨A_i, Y⟩, one warp per i
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  double daff = 0.0, dbm = 0.0, dbs = 0.0, pobj = 0.0;
+  for (int i = warp; i < m; i += nw) {
+    double sv = 0.0, sn = 0.0, sr = 0.0;
+    for (long long r = lane; r < kk; r += 32) {
+      const double a = A[(long long)i * kk + r];
+      sv += a * Y[r];
+      sn += fabs(a);
+      sr += fabs(a) * fabs(Y[r]);
+    }
+    sv = warp_sum(sv);
+    sn = warp_sum(sn);
+    sr = warp_sum(sr);
+    const double v = c[i] - sv;
+    daff = fmax(daff, abs_nan_inf(v));
+    dbm = fmax(dbm, cert_ratio(v, fabs(c[i]) + sn + fabs(c[i]) + sr));
+    dbs = fmax(dbs, cert_ratio(v, fabs(c[i]) + sr));
+  }
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    pobj += c[i] * x[i];
+    if (!isfinite(x[i])) badx += 1.0;
+  }
+  paff = cta_max(paff, red);
+  pbm = cta_max(pbm, red);
+  pbs = cta_max(pbs, red);
+  daff = cta_max(daff, red);
+  dbm = cta_max(dbm, red);
+  dbs = cta_max(dbs, red);
+  dobj = cta_sum(dobj, red);
+  compl_ = cta_sum(compl_, red);
+  pobj = cta_sum(pobj, red);
+  badx = cta_sum(badx, red);
+  const double bX = cta_psd_certificate(X, k, tol_p, sm, red, sflag, out + cXsym);
+  const double bY = cta_psd_certificate(Y, k, tol_d, sm, red, sflag, out + cYsym);
+  if (threadIdx.x == 0) {
+    out[cPobj] = pobj;
+    out[cDobj] = dobj;
+    out[cPaff] = paff;
+    out[cDaff] = daff;
+    out[cCompl] = compl_;
+    out[cPbMixed] = pbm;
+    out[cPbStrict] = pbs;
+    out[cDbMixed] = dbm;
+    out[cDbStrict] = dbs;
+    out[cBadX] = badx + bX;
+    out[cBadY] = bY;
+  }
+}
+
 using PhaseKernel = void (*)(Pool, const int*, const double*, double*);
 using WorkKernel = void (*)(Pool, const int*, const int4*);
 
@@ -1531,6 +1710,104 @@ struct Engine {
     return row;
   }
 
+  // Certificates of every instance's current solution (after optimize: the
+  // returned iterate, original coordinates); one kernel, one read-back.
+  DBuf<double> d_cert;
+  Pinned h_cert;
+  void certificate(double ep, double ed, double eg, int legacy,
+                   sdpx_b200_certificate_result* results) {
+    if (!solved)
+      throw std::invalid_argument("no solution to certify: run sdpx_b200_batch_optimize or "
+                                  "set every instance's solution first");
+    if (d_cert.n < (size_t)N * kCertOut) d_cert.alloc((size_t)N * kCertOut);
+    h_cert.ensure((size_t)N * kCertOut * sizeof(double));
+    SDPX_CUDA(cudaFuncSetAttribute(k_b_certificate, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem_bytes(1)));
+    k_b_certificate<<<N, kThreads, smem_bytes(1), st>>>(pool, std::max(ep, eg), std::max(ed, eg),
+                                                       d_cert.p);
+    SDPX_LAUNCH_CHECK();
+    ++launches;
+    SDPX_CUDA(cudaMemcpyAsync(h_cert.p, d_cert.p, (size_t)N * kCertOut * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+    SDPX_CUDA(cudaStreamSynchronize(st));
+    const double* all = static_cast<const double*>(h_cert.p);
+    // `_psd_violation` (src/validation.jl:919-932) of one block
+    auto violation = [](const double* o, double bad) {
+      if (o[2] != 0.0) return 0.0;
+      if (bad != 0.0) return (double)INFINITY;
+      const double excess = std::max(0.0, o[0] - o[1]);
+      return std::max(excess, o[4] != 0.0 ? o[3] : o[1]);
+    };
+    for (int i = 0; i < N; ++i) {
+      const double* o = all + (size_t)i * kCertOut;
+      sdpx_b200_certificate_result& r = results[i];
+      r = sdpx_b200_certificate_result{};
+      r.primal_objective = o[cPobj];
+      r.dual_objective = o[cDobj];
+      r.gap = o[cPobj] - o[cDobj];
+      const double oscale = std::max(1.0, (std::fabs(o[cPobj]) + std::fabs(o[cDobj])) / 2.0);
+      r.gap_relative = std::fabs(r.gap) / oscale;
+      r.primal_affine_residual = o[cPaff];
+      r.dual_affine_residual = o[cDaff];
+      r.primal_cone_violation = violation(o + cXsym, o[cBadX]);
+      r.dual_cone_violation = violation(o + cYsym, o[cBadY]);
+      r.primal_residual = std::max(o[cPaff], r.primal_cone_violation);
+      r.dual_residual = std::max(o[cDaff], r.dual_cone_violation);
+      r.primal_residual_scaled = r.primal_residual / scale_p[i];
+      r.dual_residual_scaled = r.dual_residual / scale_d[i];
+      r.primal_block_backward_error = o[cPbMixed];
+      r.primal_block_strict_backward_error = o[cPbStrict];
+      r.dual_backward_error = o[cDbMixed];
+      r.dual_strict_backward_error = o[cDbStrict];
+      r.complementarity = o[cCompl];
+      r.complementarity_relative = std::fabs(o[cCompl]) / oscale;
+      r.primal_psd_failing_blocks = o[cXok] != 0.0 ? 0 : 1;
+      r.dual_psd_failing_blocks = o[cYok] != 0.0 ? 0 : 1;
+      const bool primal_finite = std::isfinite(r.primal_objective) &&
+                                 std::isfinite(r.primal_residual) && o[cBadX] == 0.0;
+      const bool dual_finite = std::isfinite(r.dual_objective) && std::isfinite(r.dual_residual) &&
+                               o[cBadY] == 0.0;
+      const bool finite = primal_finite && dual_finite && std::isfinite(r.gap_relative) &&
+                          std::isfinite(r.complementarity);
+      const bool gap_ok = legacy ? (0.0 <= r.gap && r.gap <= eg) : (r.gap_relative <= eg);
+      int f = 0;
+      if (!finite) f |= SDPX_B200_CERT_NONFINITE;
+      if (!(r.primal_residual_scaled <= ep)) f |= SDPX_B200_CERT_PRIMAL_RESIDUAL;
+      if (!(r.primal_block_backward_error <= ep)) f |= SDPX_B200_CERT_PRIMAL_BLOCK_BACKWARD_ERROR;
+      if (!(r.dual_residual_scaled <= ed)) f |= SDPX_B200_CERT_DUAL_RESIDUAL;
+      if (!(r.dual_backward_error <= ed)) f |= SDPX_B200_CERT_DUAL_BACKWARD_ERROR;
+      if (!gap_ok) f |= SDPX_B200_CERT_DUALITY_GAP;
+      if (r.primal_psd_failing_blocks) f |= SDPX_B200_CERT_PRIMAL_PSD;
+      if (r.dual_psd_failing_blocks) f |= SDPX_B200_CERT_DUAL_PSD;
+      r.failures = f;
+      r.valid = f == 0 ? 1 : 0;
+    }
+  }
+
+  // Replaces instance i's current iterate (x, X, Y; NULL keeps a part).
+  std::vector<char> has_solution;
+  void set_solution(int i, const double* hx, const double* hX, const double* hY) {
+    if (i < 0 || i >= N) throw std::invalid_argument("instance index out of range");
+    const Inst& I = inst[i];
+    const long long kk = (long long)I.k * I.k;
+    SDPX_CUDA(cudaStreamSynchronize(st));
+    if (hx)
+      SDPX_CUDA(cudaMemcpyAsync(x.p + I.m_off, hx, I.m * sizeof(double), cudaMemcpyHostToDevice,
+                                st));
+    if (hX)
+      SDPX_CUDA(cudaMemcpyAsync(X.p + I.kk_off, hX, kk * sizeof(double), cudaMemcpyHostToDevice,
+                                st));
+    if (hY)
+      SDPX_CUDA(cudaMemcpyAsync(Y.p + I.kk_off, hY, kk * sizeof(double), cudaMemcpyHostToDevice,
+                                st));
+    SDPX_CUDA(cudaStreamSynchronize(st));
+    if (has_solution.empty()) has_solution.assign(N, 0);
+    if (hx && hX && hY) has_solution[i] = 1;
+    bool all = true;
+    for (char h : has_solution) all = all && h;
+    if (all) solved = true;
+  }
+
   void get_solution(int i, double* hx, double* hX, double* hY) {
     if (i < 0 || i >= N) throw std::invalid_argument("instance index out of range");
     const Inst& I = inst[i];
@@ -1616,6 +1893,21 @@ int sdpx_b200_batch_optimize(sdpx_b200_batch* b, const sdpx_b200_solve_options* 
     return -1;
   }
   BGUARD(b, b->e.optimize(*opts, results));
+}
+
+int sdpx_b200_batch_certificate(sdpx_b200_batch* b, double eps_primal, double eps_dual,
+                                double eps_gap, int32_t legacy_gap,
+                                sdpx_b200_certificate_result* results) {
+  if (b && !results) {
+    b->e.err = "NULL results";
+    return -1;
+  }
+  BGUARD(b, b->e.certificate(eps_primal, eps_dual, eps_gap, legacy_gap, results));
+}
+
+int sdpx_b200_batch_set_solution(sdpx_b200_batch* b, int32_t i, const double* x,
+                                 const double* X, const double* Y) {
+  BGUARD(b, b->e.set_solution(i, x, X, Y));
 }
 
 int sdpx_b200_batch_get_solution(sdpx_b200_batch* b, int32_t i, double* x, double* X, double* Y) {

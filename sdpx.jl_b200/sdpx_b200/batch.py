@@ -203,6 +203,42 @@ class BatchSolver:
                 precision_trace=["fp64"] * r.fp64_iterations, seconds=r.seconds))
         return out
 
+    def set_solution(self, i: int, x=None, X=None, Y=None):
+        """Replace instance i's current iterate (X, Y as k×k matrices); None
+        keeps that part (sdpx_b200_batch_set_solution)."""
+        dp = C.POINTER(C.c_double)
+        keep = []
+
+        def ptr(a, col_major):
+            if a is None:
+                return None
+            a = np.asarray(a, dtype=np.float64)
+            a = np.ascontiguousarray(a.T if col_major else a).reshape(-1)
+            keep.append(a)
+            return a.ctypes.data_as(dp)
+        self._call("sdpx_b200_batch_set_solution", int(i), ptr(x, False), ptr(X, True),
+                   ptr(Y, True))
+
+    def certificate(self, eps_primal: float = 1e-10, eps_dual: float = 1e-10,
+                    eps_gap: float = 1e-10, legacy_gap: bool = False) -> List[dict]:
+        """`result_certificate` of every instance's current solution, all
+        computed by one device kernel and read back once
+        (sdpx_b200_batch_certificate); dicts as `sdpx_b200.certificate`."""
+        from .cuda_backend import CERTIFICATE_FAILURES, CertificateResult
+        n = len(self.problems)
+        out = (CertificateResult * n)()
+        self._call("sdpx_b200_batch_certificate", float(eps_primal), float(eps_dual),
+                   float(eps_gap), 1 if legacy_gap else 0, out)
+        certs = []
+        for r in out:
+            d = {name: getattr(r, name) for name, _ in CertificateResult._fields_}
+            d["valid"] = bool(r.valid)
+            d["failures"] = [name for bit, name in CERTIFICATE_FAILURES if r.failures & bit]
+            d["available"] = True
+            d["kind"] = "optimality"
+            certs.append(d)
+        return certs
+
     def stats(self) -> Dict[str, float]:
         """Counters of the last optimize (sdpx_b200_batch_stats)."""
         v = np.zeros(8)

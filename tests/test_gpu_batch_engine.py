@@ -111,3 +111,62 @@ def test_batched_engine_rejects_unsupported_options(cuda_ok):
             bs.optimize(SolverOptions().with_tolerance(1e-8))
         with pytest.raises(SDPXB200Error, match="equilibration"):
             bs.optimize(SolverOptions(parameter_policy="fixed").with_tolerance(1e-8))
+
+
+def _cert_compare(g, o, scale):
+    import math
+    assert g["valid"] == o["valid"], (g["failures"], o["failures"])
+    assert sorted(g["failures"]) == sorted(o["failures"])
+    assert g["primal_psd_failing_blocks"] == len(o["primal_psd_failing_blocks"])
+    assert g["dual_psd_failing_blocks"] == len(o["dual_psd_failing_blocks"])
+    for f in ("primal_objective", "dual_objective", "complementarity"):
+        assert math.isclose(g[f], o[f], rel_tol=1e-12, abs_tol=1e-12 * scale), (f, g[f], o[f])
+    for f in ("primal_affine_residual", "dual_affine_residual"):
+        assert abs(g[f] - o[f]) <= 1e-12 * scale, (f, g[f], o[f])
+    for f in ("primal_block_backward_error", "primal_block_strict_backward_error",
+              "dual_backward_error", "dual_strict_backward_error"):
+        assert abs(g[f] - o[f]) <= 1e-12, (f, g[f], o[f])
+    for f in ("primal_cone_violation", "dual_cone_violation"):
+        assert math.isclose(g[f], o[f], rel_tol=1e-9, abs_tol=1e-14), (f, g[f], o[f])
+
+
+def test_batched_certificate_matches_oracle(cuda_ok):
+    """One kernel certifies every instance; each certificate equals the oracle
+    restatement of `result_certificate` on the same solution, also with a
+    planted indefinite X (order 5: unresolved shift; order 4 and 3: the shift
+    bisection) and a non-finite entry."""
+    from oracle.certificate_oracle import result_certificate
+    from sdpx_b200 import generators as G
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = [p for p in batch_instances(40, seed=9) if p.m <= 60][:5]
+    probs += [G.sdpa_dense(m=m, blocks=[k], lp=0, seed=50 + k) for k, m in ((3, 4), (4, 6), (5, 9))]
+    with BatchSolver(probs) as bs:
+        res = bs.optimize(batch_options(1e-8))
+        certs = bs.certificate(1e-8, 1e-8, 1e-8)
+        for p, r, g in zip(probs, res, certs):
+            o = result_certificate(p.Av, p.C, p.k, p.c, r.x, r.X, r.Y, 1e-8, 1e-8, 1e-8)
+            assert g["valid"] and o["valid"], (g["failures"], o["failures"])
+            scale = 1 + np.abs(p.C[0]).max() + np.abs(p.c).max() + \
+                np.abs(p.Av[0]).max() * np.abs(r.x).sum()
+            _cert_compare(g, o, scale)
+        planted = {}
+        for j, shift in ((len(probs) - 1, 2.0), (len(probs) - 2, 1.5), (len(probs) - 3, 0.75)):
+            X = res[j].X[0] - shift * np.eye(probs[j].k[0])
+            bs.set_solution(j, X=X)
+            planted[j] = X
+        x_bad = res[0].x.copy()
+        x_bad[1] = np.inf
+        bs.set_solution(0, x=x_bad)
+        certs = bs.certificate(1e-8, 1e-8, 1e-8)
+        for j, p in enumerate(probs):
+            X = planted.get(j, res[j].X[0])
+            x = x_bad if j == 0 else res[j].x
+            o = result_certificate(p.Av, p.C, p.k, p.c, x, [X], res[j].Y, 1e-8, 1e-8, 1e-8)
+            if j in planted:
+                assert "primal_psd" in certs[j]["failures"]
+            if j == 0:  # as the per-handle certificate: invalid, with "nonfinite"
+                assert "nonfinite" in certs[j]["failures"] and not certs[j]["valid"]
+                continue
+            scale = 1 + np.abs(p.C[0]).max() + np.abs(p.c).max() + \
+                np.abs(p.Av[0]).max() * np.abs(x).sum()
+            _cert_compare(certs[j], o, scale)
