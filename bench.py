@@ -74,7 +74,8 @@ SPARSE_WORKLOAD = dict(m=3000, blocks=32, kmin=23, kmax=74, active=0.6, pairs=(1
 # Batch of small SDPs of uneven size (block n ~ U{4..64}, m ~ U{3..min(200,
 # n(n+1)/2)}): a bounded slice of the 4096-instance workload, solved
 # concurrently (one handle and stream per instance) and as a serial loop.
-BATCH_WORKLOAD = dict(instances=4096, loop_sample=96, tol=1e-8)
+BATCH_WORKLOAD = dict(instances=4096, loop_sample=96, tol=1e-8, dd_instances=256,
+                      dd_tol=1e-12)
 
 
 def schur_flops(m, blocks, lp):
@@ -281,6 +282,26 @@ def bench_batch(args, world, rank, local):
         bs2.set_schur_shape(*bs.shape)
         res_e2e = bs2.optimize(opts, solutions=True)
     t_e2e = time.perf_counter() - t0
+    # the Float64x2 sub-batch: 256 instances to a 1e-12 gap
+    sub = probs[:wl["dd_instances"]]
+    with BatchSolver(sub, device=local) as bdd:
+        bdd.set_schur_shape(*bs.shape)
+        dd_opts = batch_options(wl["dd_tol"], precision="float64x2")
+        bdd.optimize(dd_opts, solutions=False)
+        t0 = time.perf_counter()
+        res_dd = bdd.optimize(dd_opts, solutions=False)
+        t_dd = time.perf_counter() - t0
+        certs_dd = bdd.certificate(wl["dd_tol"], wl["dd_tol"], wl["dd_tol"])
+        res_dd64 = bdd.optimize(batch_options(wl["dd_tol"]), solutions=False)
+    float64x2 = {"instances": len(sub), "tolerance": wl["dd_tol"],
+                 "value": len(sub) / t_dd, "unit": "instances/s", "seconds": t_dd,
+                 "optimal": sum(r.status.value == "Optimal" for r in res_dd),
+                 "certificates_valid": sum(c["valid"] for c in certs_dd),
+                 "max_relative_gap": max(r.relative_gap for r in res_dd),
+                 "mean_iterations": sum(r.iterations for r in res_dd) / len(res_dd),
+                 "fp64_optimal_same_tolerance": sum(r.status.value == "Optimal"
+                                                    for r in res_dd64),
+                 "mode": "Newton system in double-double, FP64 iterate"}
     ns = wl["loop_sample"]
     solve_batch(probs[:2], tolerance=wl["tol"], engine="loop", threads=1, device=local,
                 **BATCH_OPTIONS)
@@ -323,6 +344,7 @@ def bench_batch(args, world, rank, local):
                      "engine": "one handle per instance, sdpx_b200_optimize, serial"},
             "speedup_vs_loop": rate / loop_rate,
             "loop_agreement": agreement,
+            "float64x2_sub_batch": float64x2,
             "certificate": {"valid": sum(c["valid"] for c in certs), "seconds": t_cert,
                             "engine": "one kernel over all instances "
                                       "(sdpx_b200_batch_certificate), one read-back"},

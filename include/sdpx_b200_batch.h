@@ -16,7 +16,8 @@
  * sdpx_b200_create / sdpx_b200_optimize / sdpx_b200_destroy per instance.
  *
  * Supported options: parameter_policy = 1 (fixed start x = 0, X = ω_p·I,
- * Y = ω_d·I), scaling = 1 (none), precision = SDPX_B200_FP64, step_rule 0 or
+ * Y = ω_d·I), scaling = 1 (none), precision = SDPX_B200_FP64 or
+ * SDPX_B200_FLOAT64X2 (below), step_rule 0 or
  * 1 (backtracking; every block has k ≥ 3), max_time = ∞ per batch.  Sizes:
  * 3 ≤ k ≤ 64 and 1 ≤ m ≤ 256 per instance.  Anything else is a usage error
  * (return < 0, message from sdpx_b200_batch_last_error).
@@ -42,6 +43,12 @@ typedef struct {
   const double* const* C;      /* per instance: k² doubles                    */
   const double* const* c;      /* per instance: m doubles                     */
 } sdpx_b200_batch_problem;
+
+/* Precision mode of the batched engine only (sdpx_b200_solve_options.precision):
+ * the Newton system — block residuals, X⁻¹, the Schur matrix and its
+ * Cholesky factor, right-hand sides, solves, refinement residuals and the
+ * direction blocks — in double-double (Float64x2), the iterate in FP64. */
+#define SDPX_B200_FLOAT64X2 2
 
 /* Largest block order and constraint count an instance may have. */
 #define SDPX_B200_BATCH_MAX_K 64

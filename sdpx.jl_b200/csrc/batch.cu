@@ -33,6 +33,7 @@
 #include "../../include/sdpx_b200_batch.h"
 #include "batch_kernels.cuh"
 #include "dbuf.h"
+#include "dd.cuh"
 #include "ipm_controller.h"
 
 namespace sdpx {
@@ -869,6 +870,8 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+#include "batch_dd.cuh"
+
 using PhaseKernel = void (*)(Pool, const int*, const double*, double*);
 using WorkKernel = void (*)(Pool, const int*, const int4*);
 
@@ -941,6 +944,9 @@ struct Engine {
   DBuf<Inst> d_inst;
   DBuf<double> A, Ph, C, c, X, Y, P, R, LX, LY, W, dX, dY, Z, Xb, Yb;
   DBuf<double> x, dx, d, r, rho, xb, dxb, S, LS;
+  DBuf<double> Pl, Rl, Zl, Xih, Xil, dl, rl, dxl, dxbl, rhol, Sl, LSl, Gl;  // Float64x2 mode
+  long long kk_tot = 0, m_tot = 0, mm_tot = 0, a_tot = 0;
+  bool dd = false;  // the current optimize runs the Float64x2 Newton system
   DBuf<int> d_act;
   DBuf<int4> d_work;
   DBuf<double> d_par, d_res;
@@ -978,7 +984,6 @@ struct Engine {
     inst.resize(N);
     scale_p.assign(N, 1.0);
     scale_d.assign(N, 1.0);
-    long long kk_tot = 0, m_tot = 0, mm_tot = 0, a_tot = 0;
     for (int i = 0; i < N; ++i) {
       const int k = prob->block_order[i], m = prob->m[i];
       if (k < 3 || k > kMaxK)
@@ -1059,6 +1064,26 @@ struct Engine {
     SDPX_CUDA(cudaStreamSynchronize(st));
   }
 
+  // Float64x2 arrays, allocated by the first Float64x2 solve.
+  void ensure_dd() {
+    if (Gl.p) return;
+    for (DBuf<double>* b : {&Pl, &Rl, &Zl, &Xih, &Xil}) b->alloc(kk_tot);
+    for (DBuf<double>* b : {&dl, &rl, &dxl, &dxbl, &rhol}) b->alloc(m_tot);
+    Sl.alloc(mm_tot);
+    LSl.alloc(mm_tot);
+    Gl.alloc(a_tot);
+    for (DBuf<double>* b : {&dxl, &dxbl}) b->zero(st);
+    pool.Pl = Pl.p, pool.Rl = Rl.p, pool.Zl = Zl.p, pool.Xih = Xih.p, pool.Xil = Xil.p;
+    pool.dl = dl.p, pool.rl = rl.p, pool.dxl = dxl.p, pool.dxbl = dxbl.p, pool.rhol = rhol.p;
+    pool.Sl = Sl.p, pool.LSl = LSl.p, pool.Gl = Gl.p;
+    for (PhaseKernel kf : {k_dd_resid, k_dd_xinv, k_dd_rhs, k_dd_dirblocks})
+      SDPX_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_bytes(5)));
+    SDPX_CUDA(cudaFuncSetAttribute(k_dd_schur, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem_bytes(5)));
+    SDPX_CUDA(cudaStreamSynchronize(st));
+  }
+
   // ------------------------------------------------------- phase launches --
   // One launch of `kf` over the instances `ids` (one CTA each); `fill` writes
   // each row's inputs.  With `read`, waits and returns the output rows.
@@ -1091,6 +1116,48 @@ struct Engine {
   }
   const double* phase(PhaseKernel kf, const std::vector<int>& ids, size_t smem, bool read) {
     return phase(kf, ids, smem, [](int, double*) {}, read);
+  }
+
+  // The double-double Schur assembly over `ids`: work items of contiguous
+  // constraint ranges (about 2·10⁶ double-double multiply-adds each), largest
+  // instances first.
+  void schur_dd(const std::vector<int>& ids) {
+    const int n = (int)ids.size();
+    if (n == 0) return;
+    SDPX_CUDA(cudaStreamSynchronize(st));
+    int* ha = static_cast<int*>(h_act.p);
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    auto cost = [&](int q) {
+      const Inst& I = inst[ids[q]];
+      return (2.0 * I.k * I.k * I.k + (double)I.k * I.k * I.m) * I.m;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    std::vector<int4> items;
+    for (int q = 0; q < n; ++q) ha[q] = ids[q];
+    for (int q : order) {
+      const Inst& I = inst[ids[q]];
+      const int parts = std::max(1, std::min(I.m, (int)std::ceil(cost(q) / 2.0e6)));
+      for (int p = 0; p < parts; ++p)
+        items.push_back(make_int4(q, (int)((long long)I.m * p / parts),
+                                  (int)((long long)I.m * (p + 1) / parts), 0));
+      schur_flops += 20.0 * cost(q);
+    }
+    if (d_work.n < items.size()) d_work.alloc(items.size() + items.size() / 4);
+    h_work.ensure(items.size() * sizeof(int4));
+    std::copy(items.begin(), items.end(), static_cast<int4*>(h_work.p));
+    SDPX_CUDA(cudaMemcpyAsync(d_act.p, ha, n * sizeof(int), cudaMemcpyHostToDevice, st));
+    SDPX_CUDA(cudaMemcpyAsync(d_work.p, h_work.p, items.size() * sizeof(int4),
+                              cudaMemcpyHostToDevice, st));
+    SDPX_CUDA(cudaEventRecord(ev[0], st));
+    k_dd_schur<<<(int)items.size(), kThreads, smem_bytes(5), st>>>(pool, d_act.p, d_work.p);
+    SDPX_LAUNCH_CHECK();
+    SDPX_CUDA(cudaEventRecord(ev[1], st));
+    ++launches;
+    SDPX_CUDA(cudaEventSynchronize(ev[1]));
+    float ms = 0;
+    SDPX_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    t_schur += ms * 1e-3;
   }
 
   // The Schur assembly over `ids`: panel then SYRK work items, largest first.
@@ -1179,8 +1246,10 @@ struct Engine {
       throw std::invalid_argument("the batched engine runs the fixed start (parameter_policy = 1)");
     if (o.scaling != 1)
       throw std::invalid_argument("the batched engine runs without equilibration (scaling = 1)");
-    if (o.precision != SDPX_B200_FP64)
-      throw std::invalid_argument("the batched engine runs in FP64 (precision = SDPX_B200_FP64)");
+    if (o.precision != SDPX_B200_FP64 && o.precision != SDPX_B200_FLOAT64X2)
+      throw std::invalid_argument(
+          "the batched engine runs in FP64 or Float64x2 (precision = SDPX_B200_FP64 or "
+          "SDPX_B200_FLOAT64X2)");
     if (o.step_rule == 2)
       throw std::invalid_argument("the batched engine runs the backtracking step rule");
   }
@@ -1191,6 +1260,16 @@ struct Engine {
     auto elapsed = [&] {
       return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     };
+    dd = o.precision == SDPX_B200_FLOAT64X2;
+    if (dd) ensure_dd();
+    // Kernels of the Newton system in the chosen arithmetic.
+    const PhaseKernel K_factor = dd ? k_dd_factor : k_b_factor;
+    const PhaseKernel K_rhs = dd ? k_dd_rhs : k_b_rhs;
+    const PhaseKernel K_solve = dd ? k_dd_solve : k_b_solve;
+    const PhaseKernel K_dir = dd ? k_dd_dirblocks : k_b_dirblocks;
+    const PhaseKernel K_rho = dd ? k_dd_rho : k_b_resid;
+    const PhaseKernel K_back = dd ? k_dd_rollback : k_b_rollback;
+    const size_t smem_blk = dd ? smem_bytes(5) : smem_bytes(3);
     passes = launches = inst_iters = 0;
     t_schur = t_factor = t_step = schur_flops = 0;
     runs.assign(N, Run{});
@@ -1222,6 +1301,11 @@ struct Engine {
       in[kUseAffine] = runs[id].ctl.strategy_adaptive() ? 1 : 0;
       in[kFactor] = 0;
     }, true);
+    if (dd)  // the same residuals in double-double
+      out = phase(k_dd_resid, all, smem_bytes(2), [&](int id, double* in) {
+        in[kMu] = runs[id].mu;
+        in[kUseAffine] = runs[id].ctl.strategy_adaptive() ? 1 : 0;
+      }, true);
     for (int q = 0; q < N; ++q) {
       Run& R = runs[all[q]];
       R.p_res = out[(size_t)q * oNOut + oPres];
@@ -1242,7 +1326,9 @@ struct Engine {
         R.gap_ok = R.gap_rel <= term_tol;
         if (R.term_ok && R.gap_ok) need.push_back(id);
       }
-      out = phase(k_b_solres, need, 0, true);
+      out = dd ? phase(k_dd_resid, need, smem_bytes(2), [](int, double* in) { in[kMode] = 1; },
+                       true)
+               : phase(k_b_solres, need, 0, true);
       for (size_t q = 0; q < need.size(); ++q) {
         Run& R = runs[need[q]];
         R.p_res = out[q * oNOut + oPres];
@@ -1313,9 +1399,23 @@ struct Engine {
         else
           ok1.push_back(stepping[q]);
       }
-      schur(ok1, schur_threads, schur_tile, grain);
+      if (dd) {  // P, d, R and X⁻¹ in double-double
+        out = phase(k_dd_resid, ok1, smem_bytes(2), [&](int id, double* in) {
+          in[kMu] = runs[id].mu;
+          in[kUseAffine] = runs[id].adaptive ? 1 : 0;
+        }, true);
+        for (size_t q = 0; q < ok1.size(); ++q) {
+          Run& R = runs[ok1[q]];
+          R.sp_res = R.bpr = out[q * oNOut + oPres];
+          R.sd_res = out[q * oNOut + oDres];
+        }
+        phase(k_dd_xinv, ok1, smem_bytes(5), false);
+        schur_dd(ok1);
+      } else {
+        schur(ok1, schur_threads, schur_tile, grain);
+      }
       const auto tf0 = std::chrono::steady_clock::now();
-      out = phase(k_b_factor, ok1, 0, true);
+      out = phase(K_factor, ok1, 0, true);
       t_factor += std::chrono::duration<double>(std::chrono::steady_clock::now() - tf0).count();
       std::vector<int> ok2;
       for (size_t q = 0; q < ok1.size(); ++q) {
@@ -1331,9 +1431,9 @@ struct Engine {
           ok2.push_back(ok1[q]);
       }
       // predictor
-      phase(k_b_rhs, ok2, smem_bytes(3), [](int, double* in) { in[kMode] = 0; }, false);
-      phase(k_b_solve, ok2, 0, [](int, double* in) { in[kMode] = 0; }, false);
-      phase(k_b_dirblocks, ok2, smem_bytes(3), false);
+      phase(K_rhs, ok2, smem_blk, [](int, double* in) { in[kMode] = 0; }, false);
+      phase(K_solve, ok2, 0, [](int, double* in) { in[kMode] = 0; }, false);
+      phase(K_dir, ok2, smem_blk, false);
       const auto tl0 = std::chrono::steady_clock::now();
       out = phase(k_b_affine, ok2, smem_trials(), [&](int id, double* in) {
         const Run& R = runs[id];
@@ -1404,7 +1504,7 @@ struct Engine {
         R.adaptive = adaptive;  // as evaluated before the controller's selection
       }
       // corrector
-      phase(k_b_rhs, ok2, smem_bytes(3), [&](int id, double* in) {
+      phase(K_rhs, ok2, smem_blk, [&](int id, double* in) {
         const Run& R = runs[id];
         const Inst& I = inst[id];
         in[kMode] = 1;
@@ -1417,8 +1517,8 @@ struct Engine {
           in[kTarget] = gl * R.mu;
         }
       }, false);
-      phase(k_b_solve, ok2, 0, [](int, double* in) { in[kMode] = 0; }, false);
-      out = phase(k_b_resid, ok2, 0, true);
+      phase(K_solve, ok2, 0, [](int, double* in) { in[kMode] = 0; }, false);
+      out = phase(K_rho, ok2, 0, true);
       std::vector<int> refining;
       for (size_t q = 0; q < ok2.size(); ++q) {
         Run& R = runs[ok2[q]];
@@ -1443,8 +1543,8 @@ struct Engine {
           else R.refining = false;
         }
         if (round.empty()) break;
-        phase(k_b_solve, round, 0, [](int, double* in) { in[kMode] = 1; }, false);
-        out = phase(k_b_resid, round, 0, true);
+        phase(K_solve, round, 0, [](int, double* in) { in[kMode] = 1; }, false);
+        out = phase(K_rho, round, 0, true);
         std::vector<int> back;
         for (size_t q = 0; q < round.size(); ++q) {
           Run& R = runs[round[q]];
@@ -1460,8 +1560,8 @@ struct Engine {
           R.residual = corr;
           if (o.refine_policy != 0 && small) R.refining = false;
         }
-        phase(k_b_rollback, back, 0, false);
-        out = phase(k_b_resid, back, 0, true);  // ρ of the restored direction
+        phase(K_back, back, 0, false);
+        out = phase(K_rho, back, 0, true);  // ρ of the restored direction
         for (size_t q = 0; q < back.size(); ++q) runs[back[q]].residual = out[q * oNOut + oRes];
       }
       std::vector<int> ok3;
@@ -1475,7 +1575,7 @@ struct Engine {
         else
           ok3.push_back(id);
       }
-      phase(k_b_dirblocks, ok3, smem_bytes(3), false);
+      phase(K_dir, ok3, smem_blk, false);
       for (int id : ok3) {  // the step succeeded: its residuals become the loop's
         Run& R = runs[id];
         R.p_res = R.sp_res;
@@ -1632,7 +1732,8 @@ struct Engine {
       po[q] = out[(size_t)q * oNOut + oPobj];
       dob[q] = out[(size_t)q * oNOut + oDobj];
     }
-    out = phase(k_b_solres, all, 0, true);
+    out = dd ? phase(k_dd_resid, all, smem_bytes(2), [](int, double* in) { in[kMode] = 1; }, true)
+             : phase(k_b_solres, all, 0, true);
     t_loop = elapsed();
     for (int i = 0; i < N; ++i) {
       const Run& R = runs[i];

@@ -41,6 +41,9 @@ struct Pool {
   double *S, *LS;
   long long kq;  // stride of one k×k matrix slot in shared memory (kmax² of the pool)
   long long kp;  // stride of one packed lower-triangle slot (kmax(kmax+1)/2)
+  // Float64x2 mode: low halves of the double-double arrays (hi halves are the
+  // FP64 arrays above), X⁻¹ in double-double and the low half of the panel.
+  double *Pl, *Rl, *Zl, *dl, *rl, *dxl, *dxbl, *rhol, *Sl, *LSl, *Xih, *Xil, *Gl;
 };
 
 // |v| with NaN read as +inf, so a poisoned value never passes a max-norm test.

@@ -9,7 +9,8 @@ Two engines:
   keeps its own scalar controller, so its status, iterations and objectives are
   those of its single solve with the same options.  It runs SDPX's fixed start
   without equilibration (``parameter_policy="fixed"``, ``scaling="none"``), in
-  FP64, for one PSD block of order 3..64 and m ≤ 256 per instance.
+  FP64 or with the Newton system in double-double (``precision="float64x2"``),
+  for one PSD block of order 3..64 and m ≤ 256 per instance.
 * ``engine="loop"``: one device handle and CUDA stream per instance
   (`sdpx_b200_optimize`), driven by ``threads`` host threads — the
   per-instance loop the batched engine is measured against.
@@ -255,15 +256,17 @@ def solve_batch(problems: Sequence[SDPProblem], *, tolerance: float = 1e-8,
     """Solve every problem; results in input order.
 
     ``engine="batched"``: one `BatchSolver` over all problems with the
-    batched engine's options (`BATCH_OPTIONS` plus `kwargs`; FP64).
+    batched engine's options (`BATCH_OPTIONS` plus `kwargs`); ``precision``
+    "fp64" or "float64x2" (the Newton system in double-double, for tight
+    tolerances such as 1e-12).
     ``engine="loop"``: one handle per problem, ``threads`` concurrent solves
     with `SolverOptions(precision, **kwargs)`; with the native driver the whole
     loop runs inside the library, so the threads hold the GIL only to start and
     collect."""
     if engine == "batched":
-        if precision != "fp64":
-            raise ValueError("the batched engine runs in FP64")
-        opts = batch_options(tolerance, **kwargs)
+        if precision not in ("fp64", "float64x2"):
+            raise ValueError("the batched engine runs in FP64 or Float64x2")
+        opts = batch_options(tolerance, precision=precision, **kwargs)
         with BatchSolver(problems, device=device) as bs:
             if autotune:
                 bs.autotune(opts)

@@ -95,7 +95,8 @@ def native_options(o) -> SolveOptions:
         {"auto": 0, "fixed": 1}[o.parameter_policy],
         {"adaptive": 0, "fixed": 1}[o.parameter_strategy], o.adaptive_sigma_max,
         {"auto": 0, "none": 1, "equilibrate": 2}[o.scaling],
-        1 if o.precision == "mixed" else 0, {"auto": 0, "qr": 1}[o.equality_solver])
+        {"fp64": 0, "mixed": 1, "float64x2": 2}[o.precision],
+        {"auto": 0, "qr": 1}[o.equality_solver])
 
 
 # name -> argtypes (restype is int unless noted)

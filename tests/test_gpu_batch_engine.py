@@ -170,3 +170,33 @@ def test_batched_certificate_matches_oracle(cuda_ok):
             scale = 1 + np.abs(p.C[0]).max() + np.abs(p.c).max() + \
                 np.abs(p.Av[0]).max() * np.abs(x).sum()
             _cert_compare(certs[j], o, scale)
+
+
+def test_float64x2_mode_reaches_1e12_with_valid_certificates(cuda_ok):
+    """The double-double Newton system takes every instance of a sample of the
+    workload to a 1e-12 gap (FP64 stops short on most) and the batched
+    certificate at 1e-12 is valid for all of them."""
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = batch_instances(32, seed=1)
+    with BatchSolver(probs) as bs:
+        res = bs.optimize(batch_options(1e-12, precision="float64x2"))
+        certs = bs.certificate(1e-12, 1e-12, 1e-12)
+        fp64 = bs.optimize(batch_options(1e-12), solutions=False)
+    assert all(r.status.value == "Optimal" for r in res), [r.message for r in res]
+    assert all(r.relative_gap <= 1e-12 for r in res)
+    assert all(c["valid"] for c in certs), [c["failures"] for c in certs if not c["valid"]]
+    assert sum(r.status.value == "Optimal" for r in fp64) < len(probs) // 2
+
+
+def test_float64x2_mode_matches_its_oracle(cuda_ok):
+    from oracle.dd_newton_oracle import dd_newton_solve
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = [p for p in batch_instances(256, seed=1) if p.k[0] <= 12 and p.m <= 30][:3]
+    opts = batch_options(1e-12, precision="float64x2")
+    with BatchSolver(probs) as bs:
+        res = bs.optimize(opts)
+    for p, rb in zip(probs, res):
+        ro = dd_newton_solve(p, opts)
+        assert rb.status == ro.status
+        assert abs(rb.iterations - ro.iterations) <= 1
+        assert rel(rb.pObj, ro.pObj) <= 1e-10 and rel(rb.dObj, ro.dObj) <= 1e-10
