@@ -1086,6 +1086,22 @@ def run_profile(args):
                       "phase_ms": phases}), flush=True)
 
 
+def run_batch_profile(args):
+    """One batched solve of the first N instances of the small-SDP workload
+    (seed = --seed) with the Schur launch shape the autotuner picks on the
+    B200 (512 threads, 32-tile, one item per instance); prints its counters."""
+    from sdpx_b200 import batch_instances
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = batch_instances(args.batch_profile, seed=args.seed)
+    with BatchSolver(probs) as bs:
+        bs.set_schur_shape(512, 32, 0.0)
+        res = bs.optimize(batch_options(args.batch_tol, precision=args.batch_precision),
+                          solutions=False)
+        st = bs.stats()
+    st["optimal"] = sum(r.status.value == "Optimal" for r in res)
+    print(json.dumps(st))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1101,7 +1117,14 @@ def main():
     ap.add_argument("--lp", type=int, default=500)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--mode", choices=["fp64", "mixed"], default="mixed")
+    # profiling mode (no bench line): one batched solve of N workload instances
+    ap.add_argument("--batch-profile", type=int, default=0)
+    ap.add_argument("--batch-precision", choices=["fp64", "float64x2"], default="fp64")
+    ap.add_argument("--batch-tol", type=float, default=1e-8)
     args = ap.parse_args()
+    if args.batch_profile > 0:
+        run_batch_profile(args)
+        return
     if args.profile_iterations > 0:
         return run_profile(args)
     world, rank, local = dist_setup()
