@@ -277,6 +277,12 @@ def bench_batch(args, world, rank, local):
         t0 = time.perf_counter()
         certs = bs.certificate(wl["tol"], wl["tol"], wl["tol"])
         t_cert = time.perf_counter() - t0
+        # the reference's bisection for the affine bounds (the single path's rule)
+        bs.set_step_bounds("bisection")
+        t0 = time.perf_counter()
+        res_bis = bs.optimize(opts, solutions=False)
+        t_bis = time.perf_counter() - t0
+        bs.set_step_bounds("eigen")
     t0 = time.perf_counter()
     with BatchSolver(probs, device=local) as bs2:
         bs2.set_schur_shape(*bs.shape)
@@ -310,16 +316,19 @@ def bench_batch(args, world, rank, local):
                        **BATCH_OPTIONS)
     t_loop = time.perf_counter() - t0
     rel = lambda a, b: abs(a - b) / max(1.0, abs(b))
-    pairs = list(zip(res[:ns], loop))
-    agreement = {
-        "sample": ns,
-        "status": sum(a.status == b.status for a, b in pairs),
-        "objectives_1e-7": sum(rel(a.pObj, b.pObj) <= 1e-7 and rel(a.dObj, b.dObj) <= 1e-7
-                               for a, b in pairs),
-        "iterations_within_1": sum(abs(a.iterations - b.iterations) <= 1 for a, b in pairs),
-        "max_iteration_difference": max(abs(a.iterations - b.iterations) for a, b in pairs),
-        "mean_iterations": [sum(a.iterations for a, _ in pairs) / ns,
-                            sum(b.iterations for _, b in pairs) / ns]}
+
+    def agreement_of(batch):
+        pairs = list(zip(batch[:ns], loop))
+        return {
+            "sample": ns,
+            "status": sum(a.status == b.status for a, b in pairs),
+            "objectives_1e-7": sum(rel(a.pObj, b.pObj) <= 1e-7 and rel(a.dObj, b.dObj) <= 1e-7
+                                   for a, b in pairs),
+            "iterations_within_1": sum(abs(a.iterations - b.iterations) <= 1 for a, b in pairs),
+            "max_iteration_difference": max(abs(a.iterations - b.iterations) for a, b in pairs),
+            "mean_iterations": [sum(a.iterations for a, _ in pairs) / ns,
+                                sum(b.iterations for _, b in pairs) / ns]}
+    agreement = agreement_of(res)
     rate, loop_rate = wl["instances"] / t_batch, ns / t_loop
     in_bytes = sum(p.Av[0].nbytes + p.C[0].nbytes + p.c.nbytes for p in probs)
     out_bytes = sum(p.c.nbytes + 2 * p.C[0].nbytes for p in probs)
@@ -344,6 +353,12 @@ def bench_batch(args, world, rank, local):
                      "engine": "one handle per instance, sdpx_b200_optimize, serial"},
             "speedup_vs_loop": rate / loop_rate,
             "loop_agreement": agreement,
+            "affine_bounds": "eigen: t* = -1/lambda_min(L^-1 dM L^-T)",
+            "bisection_bounds": {
+                "value": wl["instances"] / t_bis, "unit": "instances/s", "seconds": t_bis,
+                "optimal": sum(r.status.value == "Optimal" for r in res_bis),
+                "speedup_vs_loop": (wl["instances"] / t_bis) / loop_rate,
+                "loop_agreement": agreement_of(res_bis)},
             "float64x2_sub_batch": float64x2,
             "certificate": {"valid": sum(c["valid"] for c in certs), "seconds": t_cert,
                             "engine": "one kernel over all instances "

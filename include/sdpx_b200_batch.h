@@ -95,6 +95,16 @@ int sdpx_b200_batch_certificate(sdpx_b200_batch* b, double eps_primal, double ep
  * (Σ per instance-iteration of 2·k³·m + k²·m²). */
 int sdpx_b200_batch_stats(sdpx_b200_batch* b, double* out8);
 
+/* How the affine predictor's fraction-to-boundary bounds (the step lengths
+ * that set σ, `fraction_to_boundary_bound!`, src/kernels/generic.jl:350-422)
+ * are computed: mode 1 (default) t* = −1/λ_min(L⁻¹·dM·L⁻ᵀ) from the block's
+ * Cholesky factor L (1 when the full step stays interior), by a Householder
+ * tridiagonalisation and a Sturm-count multisection; mode 0 the reference's
+ * bisection of Cholesky trials of M + t·dM (up to 64 steps).  The two agree up
+ * to the rounding of the trials near t*.  The backtracking line search always
+ * runs Cholesky trials. */
+int sdpx_b200_batch_set_step_bounds(sdpx_b200_batch* b, int32_t mode);
+
 /* Launch shape of the Schur phase: threads per CTA (128, 256 or 512), the
  * SYRK tile (16 or 32; 512 threads need 32) and the Schur work per CTA in
  * FLOPs (an instance's panel and SYRK are split over ceil(work / grain) CTAs;

@@ -43,7 +43,7 @@ namespace {
 // Scalars per launched CTA row exchanged with the host each phase (row = the
 // instance's position in the launch's list).
 enum In { kMu = 0, kUseAffine, kFactor, kTarget, kMode, kTX, kTY, kRatio, kGamma, kMinStep,
-          kOmega, kNIn };
+          kOmega, kBoundMode, kNIn };
 enum Out { oPres = 0, oDres, oOk, oPmargin, oDmargin, oReg, oQual, oCompl, oAff, oAffFull, oTX,
            oTY, oRes, oRnorm, oPobj, oDobj, oFinite, oDa, oNOut };
 
@@ -476,10 +476,21 @@ __global__ void __launch_bounds__(kThreads)
   extern __shared__ __align__(16) double sm[];
   __shared__ double red[32];
   __shared__ int flags[kTrialWarps];
+  __shared__ double small[4 * kMaxK];
   double tX = 1.0, tY = 1.0;
   if (in[kMode] == 1.0) {
-    const double bX = cta_ftb_tree(pool.X + I.kk_off, pool.dX + I.kk_off, k, sm, pool.kp, flags);
-    const double bY = cta_ftb_tree(pool.Y + I.kk_off, pool.dY + I.kk_off, k, sm, pool.kp, flags);
+    double bX, bY;
+    if (in[kBoundMode] == 1.0) {  // t* = −1/λ_min(L⁻¹·dM·L⁻ᵀ) from the block factors of B1
+      double* S0 = sm;
+      double* S1 = S0 + pool.kq;
+      double* S2 = S1 + pool.kq;
+      bX = cta_ftb_eig(nullptr, pool.W + I.kk_off, pool.dX + I.kk_off, k, S0, S1, S2, small, red);
+      __syncthreads();
+      bY = cta_ftb_eig(pool.LY + I.kk_off, nullptr, pool.dY + I.kk_off, k, S0, S1, S2, small, red);
+    } else {
+      bX = cta_ftb_tree(pool.X + I.kk_off, pool.dX + I.kk_off, k, sm, pool.kp, flags);
+      bY = cta_ftb_tree(pool.Y + I.kk_off, pool.dY + I.kk_off, k, sm, pool.kp, flags);
+    }
     tX = bX < 1.0 ? bX : 1.0;
     tY = bY < 1.0 ? bY : 1.0;
   }
@@ -953,6 +964,9 @@ struct Engine {
   Pinned h_act, h_par, h_res, h_work;
   Pool pool{};
   int schur_threads = 256, schur_tile = 32;
+  // Affine fraction-to-boundary bounds: 0 the bisection of Cholesky trials
+  // (eight at a time), 1 the eigenvalue bound −1/λ_min(L⁻¹·dM·L⁻ᵀ).
+  int bound_mode = 1;
   double grain = 4.0e6;
   std::vector<Run> runs;
   std::string err;
@@ -1058,7 +1072,7 @@ struct Engine {
                                      (int)smem_bytes(3)));
     for (PhaseKernel kf : {k_b_affine, k_b_linesearch})
       SDPX_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem_trials()));
+                                     (int)std::max(smem_trials(), smem_bytes(3))));
     SDPX_CUDA(cudaFuncSetAttribute(k_b_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem_bytes(4)));
     SDPX_CUDA(cudaStreamSynchronize(st));
@@ -1435,9 +1449,11 @@ struct Engine {
       phase(K_solve, ok2, 0, [](int, double* in) { in[kMode] = 0; }, false);
       phase(K_dir, ok2, smem_blk, false);
       const auto tl0 = std::chrono::steady_clock::now();
-      out = phase(k_b_affine, ok2, smem_trials(), [&](int id, double* in) {
+      out = phase(k_b_affine, ok2, bound_mode == 1 ? smem_bytes(3) : smem_trials(),
+                  [&](int id, double* in) {
         const Run& R = runs[id];
         in[kMode] = (R.adaptive && !R.ctl.fallback) ? 1 : 0;
+        in[kBoundMode] = bound_mode;
       }, true);
       t_step += std::chrono::duration<double>(std::chrono::steady_clock::now() - tl0).count();
       for (size_t q = 0; q < ok2.size(); ++q) {
@@ -2026,6 +2042,13 @@ int sdpx_b200_batch_stats(sdpx_b200_batch* b, double* out8) {
     out8[5] = b->e.t_step;
     out8[6] = (double)b->e.inst_iters;
     out8[7] = b->e.schur_flops;
+  });
+}
+
+int sdpx_b200_batch_set_step_bounds(sdpx_b200_batch* b, int32_t mode) {
+  BGUARD(b, {
+    if (mode != 0 && mode != 1) throw std::invalid_argument("step-bound mode must be 0 or 1");
+    b->e.bound_mode = mode;
   });
 }
 

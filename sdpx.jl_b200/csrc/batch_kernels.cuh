@@ -343,5 +343,170 @@ __device__ double cta_backtrack(const double* X, const double* dX, int k, double
   return t_next;
 }
 
+// ------------------------------------- fraction to the boundary by eigenvalue
+// X + t·dX = L(I + t·G)Lᵀ with G = L⁻¹·dX·L⁻ᵀ, so X + t·dX stays positive
+// definite for t < t* = −1/λ_min(G) (every t when λ_min ≥ 0).  The bound is
+// 1 when 1 + λ_min(G) > 0 (the full step stays interior), else t*: the value
+// the bisection of `fraction_to_boundary_bound!` approaches from below, up to
+// the rounding of its Cholesky tests.  λ_min comes from a Householder
+// tridiagonalisation of G and a Sturm-count multisection of the tridiagonal
+// matrix (one shift per thread per round).
+
+namespace eigdetail {
+// Number of eigenvalues of the symmetric tridiagonal (a, b) below x (the
+// negative pivots of the LDLᵀ recurrence of T − x·I, zero pivots nudged).
+__device__ __forceinline__ int sturm_count(const double* a, const double* b, int n, double x,
+                                           double tiny) {
+  int neg = 0;
+  double q = a[0] - x;
+  if (q == 0.0) q = -tiny;
+  if (q < 0.0) ++neg;
+  for (int i = 1; i < n; ++i) {
+    q = (a[i] - x) - b[i - 1] * b[i - 1] / q;
+    if (q == 0.0) q = -tiny;
+    if (q < 0.0) ++neg;
+  }
+  return neg;
+}
+}  // namespace eigdetail
+
+// λ_min of the symmetric k×k G (shared memory, overwritten); v, w: k doubles
+// each, ab: 2k doubles (shared).  Called by the whole CTA.
+__device__ double cta_lambda_min(double* G, int k, double* v, double* w, double* ab,
+                                 double* red) {
+  // Householder tridiagonalisation: column j's subdiagonal part is reduced
+  // to α·e₁ by H = I − β·v·vᵀ applied on both sides of the trailing block.
+  for (int j = 0; j + 2 < k; ++j) {
+    const int n = k - j - 1, o = j + 1;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const double x = G[(o + i) + j * k];
+      v[i] = x;
+      s += x * x;
+    }
+    s = block_sum(s, red);
+    const double norm = sqrt(s);
+    const double x0 = G[o + j * k];
+    const double alpha = x0 > 0.0 ? -norm : norm;
+    if (norm == 0.0) continue;  // column already reduced (uniform)
+    if (threadIdx.x == 0) v[0] = x0 - alpha;
+    __syncthreads();
+    double vv = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) vv += v[i] * v[i];
+    vv = block_sum(vv, red);
+    if (!(vv > 0.0)) continue;
+    const double beta = 2.0 / vv;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {  // p = β·A·v
+      double t = 0.0;
+      for (int c = 0; c < n; ++c) t += G[(o + i) + (o + c) * k] * v[c];
+      w[i] = beta * t;
+    }
+    __syncthreads();
+    double pv = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) pv += w[i] * v[i];
+    pv = block_sum(pv, red);
+    const double K = 0.5 * beta * pv;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] -= K * v[i];  // w = p − K·v
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {  // A −= v·wᵀ + w·vᵀ
+      const int r = e % n, c = e / n;
+      G[(o + r) + (o + c) * k] -= v[r] * w[c] + w[r] * v[c];
+    }
+    if (threadIdx.x == 0) G[o + j * k] = alpha;
+    __syncthreads();
+  }
+  double* a = ab;
+  double* b = ab + k;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) {
+    a[i] = G[i + i * k];
+    if (i + 1 < k) b[i] = G[(i + 1) + i * k];
+  }
+  __syncthreads();
+  // Gershgorin interval, then multisection: each thread counts at one shift
+  double lo = 0.0, hi = 0.0, bmax = 0.0;
+  if (threadIdx.x == 0) {
+    lo = a[0], hi = a[0];
+    for (int i = 0; i < k; ++i) {
+      const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < k ? fabs(b[i]) : 0.0);
+      lo = fmin(lo, a[i] - r);
+      hi = fmax(hi, a[i] + r);
+      if (i + 1 < k) bmax = fmax(bmax, fabs(b[i]));
+    }
+    red[0] = lo;
+    red[1] = hi;
+    red[2] = fmax(bmax, fmax(fabs(lo), fabs(hi)));
+  }
+  __syncthreads();
+  lo = red[0];
+  hi = red[1];
+  const double tiny = 2.2250738585072014e-308 * fmax(1.0, red[2] * red[2]);  // pivot floor
+  __syncthreads();
+  __shared__ int cnt[kThreads];
+  for (int round = 0; round < 12; ++round) {
+    const double step = (hi - lo) / (blockDim.x + 1);
+    if (!(step > 0.0) || hi - lo <= 4.0 * 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)))
+      break;
+    const double x = lo + (threadIdx.x + 1) * step;
+    cnt[threadIdx.x] = eigdetail::sturm_count(a, b, k, x, tiny);
+    __syncthreads();
+    // smallest eigenvalue ∈ (last shift with count 0, first shift with count ≥ 1]
+    int first = blockDim.x;
+    for (int t = 0; t < (int)blockDim.x; ++t)
+      if (cnt[t] > 0) {
+        first = t;
+        break;
+      }
+    const double nlo = first == 0 ? lo : lo + first * step;
+    const double nhi = first == (int)blockDim.x ? hi : lo + (first + 1) * step;
+    __syncthreads();
+    lo = nlo;
+    hi = nhi;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// Fraction-to-boundary bound of M along dM from the factor L of M (lower,
+// global): W = L⁻¹ (given, or computed when Winv is null), G = W·dM·Wᵀ.
+// S0, S1, S2: three k×k shared slots; small: 4k + 32 doubles of shared scratch.
+__device__ double cta_ftb_eig(const double* L, const double* Wg, const double* dM, int k,
+                              double* S0, double* S1, double* S2, double* small, double* red) {
+  const int kk = k * k;
+  if (Wg) {
+    for (int e = threadIdx.x; e < kk; e += blockDim.x) S0[e] = Wg[e];
+  } else {
+    for (int e = threadIdx.x; e < kk; e += blockDim.x) {
+      const int r = e % k, c = e / k;
+      S2[e] = r >= c ? L[e] : 0.0;
+    }
+    __syncthreads();
+    cta_trinv(S2, S0, k);
+  }
+  for (int e = threadIdx.x; e < kk; e += blockDim.x) S1[e] = dM[e];
+  __syncthreads();
+  for (int e = threadIdx.x; e < kk; e += blockDim.x) {  // T = W·dM (W lower)
+    const int r = e % k, c = e / k;
+    double s = 0.0;
+    for (int p = 0; p <= r; ++p) s += S0[r + p * k] * S1[p + c * k];
+    S2[e] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kk; e += blockDim.x) {  // G = T·Wᵀ
+    const int r = e % k, c = e / k;
+    double s = 0.0;
+    for (int p = 0; p <= c; ++p) s += S2[r + p * k] * S0[c + p * k];
+    S1[e] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kk; e += blockDim.x) {  // symmetrise into S2
+    const int r = e % k, c = e / k;
+    S2[e] = 0.5 * (S1[e] + S1[c + r * k]);
+  }
+  __syncthreads();
+  const double lmin = cta_lambda_min(S2, k, small, small + k, small + 2 * k, red);
+  if (!(lmin == lmin)) return 0.0;  // non-finite direction: no step
+  if (1.0 + lmin > 0.0) return 1.0;
+  return -1.0 / lmin;
+}
+
 }  // namespace batch
 }  // namespace sdpx

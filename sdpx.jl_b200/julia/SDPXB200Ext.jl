@@ -467,13 +467,20 @@ end
 
 """Solve every instance of the batch with the fixed start and no
 equilibration (the options the batched engine serves); per instance the
-status, iterations, objectives and (x, X, Y)."""
-function optimize(b::B200Batch, tolerance::Float64; autotune::Bool=false)
+status, iterations, objectives and (x, X, Y).  `float64x2` forms and solves
+the Newton system in double-double (for gaps such as 1e-12); `bisection`
+selects the reference's Cholesky-trial bisection for the affine step bounds
+instead of the eigenvalue bound."""
+function optimize(b::B200Batch, tolerance::Float64; autotune::Bool=false,
+                  float64x2::Bool=false, bisection::Bool=false)
     o = B200SolveOptions()
     ccall((:sdpx_b200_default_options, libsdpx), Cvoid, (Ref{B200SolveOptions},), o)
     o.eps_gap = o.eps_primal = o.eps_dual = tolerance
     o.parameter_policy = Int32(1)
     o.scaling = Int32(1)
+    o.precision = float64x2 ? Int32(2) : Int32(0)
+    _bcheck(b, ccall((:sdpx_b200_batch_set_step_bounds, libsdpx), Cint, (Ptr{Cvoid}, Int32),
+                     b.ptr, bisection ? Int32(0) : Int32(1)), "set_step_bounds")
     autotune && autotune!(b, o)
     res = Vector{B200SolveResult}(undef, b.count)
     _bcheck(b, ccall((:sdpx_b200_batch_optimize, libsdpx), Cint,
@@ -491,6 +498,17 @@ function optimize(b::B200Batch, tolerance::Float64; autotune::Bool=false)
                   X=reshape(X, k, k), Y=reshape(Y, k, k), pObj=r.p_obj, dObj=r.d_obj,
                   pRes=r.p_res, dRes=r.d_res)
     end
+    return out
+end
+
+"""Certificates of every instance's current solution (after `optimize`) in one
+device kernel and one read-back (sdpx_b200_batch_certificate)."""
+function certificate(b::B200Batch, tolerance::Float64; legacy::Bool=false)
+    out = Vector{B200Certificate}(undef, b.count)
+    _bcheck(b, ccall((:sdpx_b200_batch_certificate, libsdpx), Cint,
+                     (Ptr{Cvoid}, Float64, Float64, Float64, Int32, Ptr{B200Certificate}),
+                     b.ptr, tolerance, tolerance, tolerance, legacy ? Int32(1) : Int32(0), out),
+            "certificate")
     return out
 end
 

@@ -133,6 +133,11 @@ class BatchSolver:
         ms = [p.m for p in self.problems]
         return f"n{len(ks)}-k{min(ks)}..{max(ks)}-m{min(ms)}..{max(ms)}"
 
+    def set_step_bounds(self, mode: str):
+        """Affine fraction-to-boundary bounds: "eigen" (default, −1/λ_min of
+        L⁻¹·dM·L⁻ᵀ) or "bisection" (the reference's Cholesky-trial bisection)."""
+        self._call("sdpx_b200_batch_set_step_bounds", {"bisection": 0, "eigen": 1}[mode])
+
     def set_schur_shape(self, threads: int, tile: int, grain: float):
         self._call("sdpx_b200_batch_set_schur_shape", int(threads), int(tile), float(grain))
         self.shape = (int(threads), int(tile), float(grain))

@@ -184,6 +184,7 @@ _SIGS = {
     "sdpx_b200_batch_certificate": [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int32,
                                     C.POINTER(CertificateResult)],
     "sdpx_b200_batch_stats": [C.c_void_p, _dp],
+    "sdpx_b200_batch_set_step_bounds": [C.c_void_p, C.c_int32],
     "sdpx_b200_batch_set_schur_shape": [C.c_void_p, C.c_int32, C.c_int32, C.c_double],
     "sdpx_b200_batch_autotune": [C.c_void_p, C.POINTER(SolveOptions), _dp, C.c_int32,
                                  C.POINTER(C.c_int32)],

@@ -200,3 +200,22 @@ def test_float64x2_mode_matches_its_oracle(cuda_ok):
         assert rb.status == ro.status
         assert abs(rb.iterations - ro.iterations) <= 1
         assert rel(rb.pObj, ro.pObj) <= 1e-10 and rel(rb.dObj, ro.dObj) <= 1e-10
+
+
+def test_eigenvalue_step_bounds_match_the_bisection(cuda_ok):
+    """The affine bounds from −1/λ_min(L⁻¹·dM·L⁻ᵀ) (the default) and from the
+    reference's bisection of Cholesky trials differ only by the trials'
+    rounding near t*: same status, objectives within 1e-7, iterations ±1."""
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = batch_instances(64, seed=12)
+    opts = batch_options(1e-8)
+    with BatchSolver(probs) as bs:
+        eig = bs.optimize(opts, solutions=False)
+        bs.set_step_bounds("bisection")
+        bis = bs.optimize(opts, solutions=False)
+    diff = [(i, a.status.value, b.status.value, a.iterations, b.iterations)
+            for i, (a, b) in enumerate(zip(eig, bis))
+            if a.status != b.status or abs(a.iterations - b.iterations) > 1 or
+            rel(a.pObj, b.pObj) > 1e-7]
+    assert len(diff) <= 1, diff
+    assert sum(r.status.value == "Optimal" for r in eig) >= len(probs) - 1
