@@ -106,13 +106,15 @@ int sdpx_b200_batch_stats(sdpx_b200_batch* b, double* out8);
 int sdpx_b200_batch_set_step_bounds(sdpx_b200_batch* b, int32_t mode);
 
 /* Launch shape of the Schur phase: threads per CTA (128, 256 or 512), the
- * SYRK tile (16 or 32; 512 threads need 32) and the Schur work per CTA in
+ * SYRK tile (16 or 32; 512 threads need 32; tile 64 with 128 threads selects
+ * the FP64 tensor-core (DMMA) products) and the Schur work per CTA in
  * FLOPs (an instance's panel and SYRK are split over ceil(work / grain) CTAs;
  * grain ≤ 0: one CTA per instance). */
 int sdpx_b200_batch_set_schur_shape(sdpx_b200_batch* b, int32_t threads, int32_t tile,
                                     double grain);
 
-/* Times every candidate Schur launch shape on the current iterate of all
+/* Times every candidate Schur launch shape (24: five scalar shapes and the
+ * DMMA path, each at four work grains) on the current iterate of all
  * instances (the fixed start when no solve ran) and keeps the fastest.
  * table (may be NULL) receives `capacity` rows of (threads, tile, grain,
  * milliseconds); *count = number of candidates timed. */

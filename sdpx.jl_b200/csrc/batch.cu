@@ -34,6 +34,7 @@
 #include "batch_kernels.cuh"
 #include "dbuf.h"
 #include "dd.cuh"
+#include "gemm_f64.cuh"
 #include "ipm_controller.h"
 
 namespace sdpx {
@@ -247,6 +248,86 @@ __global__ void __launch_bounds__(NT) k_b_syrk(Pool pool, const int* act, const 
           S[gj + (long long)gi * m] = acc[a][b];
         }
       }
+  }
+}
+
+// ---- B2 on the FP64 tensor cores (DMMA m8n8k4 tiles of gemm_f64.cuh) -----
+// Three grouped products per instance, 64×64 output tiles, 4 warps per CTA:
+//   T  = W·[A_1 … A_m]          (k × k·m; W = L_X⁻¹),
+//   P̂  = T·L_Y, one k×k block per constraint (rows j·k + r of a k·m × k product),
+//   S  = P̂·P̂ᵀ over the lower 64×64 tiles (both triangles written).
+// Work items {row, first tile, end tile} as for the scalar kernels; T lives in
+// pool.T (an m·k² array beside the panel).
+using DmmaCfgKN = F64Cfg<64, 64, 2, 2, false, true>;  // A MN-contiguous, B K-contiguous
+using DmmaCfgKK = F64Cfg<64, 64, 2, 2, true, true>;   // both K-contiguous
+
+__global__ void __launch_bounds__(DmmaCfgKN::NT)
+    k_b_dmma_t(Pool pool, const int* act, const int4* work) {
+  extern __shared__ __align__(16) double smem[];
+  const int4 wi = work[blockIdx.x];
+  const Inst I = pool.inst[act[wi.x]];
+  const int k = I.k, m = I.m;
+  const long long kk = (long long)k * k;
+  // A = W (k×k): element (r, p) at r + p·k;  B = [A_1 … A_m]: (p, j·k + c) at j·k² + c·k + p
+  const Opnd Aw{pool.W + I.kk_off, k, 1, 0, 1 << 30, k, k};
+  const Opnd Ba{pool.A + I.a_off, 1, k, kk, k, k * m, k};
+  double* T = pool.T + I.a_off;
+  for (int tile = wi.y; tile < wi.z; ++tile) {
+    double acc[DmmaCfgKN::FM][DmmaCfgKN::FN][2];
+    zero_acc<DmmaCfgKN>(acc);
+    f64_tile_mainloop<DmmaCfgKN>(acc, Aw, Ba, 0, tile * 64, 0, k, smem);
+    for_each_acc<DmmaCfgKN>(acc, [&](int r, int col, double v) {
+      const int gc = tile * 64 + col;
+      if (r < k && gc < k * m) T[(long long)(gc / k) * kk + (long long)(gc % k) * k + r] = v;
+    });
+  }
+}
+
+__global__ void __launch_bounds__(DmmaCfgKN::NT)
+    k_b_dmma_p(Pool pool, const int* act, const int4* work) {
+  extern __shared__ __align__(16) double smem[];
+  const int4 wi = work[blockIdx.x];
+  const Inst I = pool.inst[act[wi.x]];
+  const int k = I.k, m = I.m;
+  const long long kk = (long long)k * k;
+  // A = T blocks: (j·k + r, q) at j·k² + r + q·k;  B = L_Y: (q, c) at q + c·k
+  const Opnd At{pool.T + I.a_off, k, 1, kk, k, k * m, k};
+  const Opnd Bl{pool.LY + I.kk_off, 1, k, 0, 1 << 30, k, k};
+  double* Ph = pool.Ph + I.a_off;
+  for (int tile = wi.y; tile < wi.z; ++tile) {
+    double acc[DmmaCfgKN::FM][DmmaCfgKN::FN][2];
+    zero_acc<DmmaCfgKN>(acc);
+    f64_tile_mainloop<DmmaCfgKN>(acc, At, Bl, tile * 64, 0, 0, k, smem);
+    for_each_acc<DmmaCfgKN>(acc, [&](int r, int c, double v) {
+      const int gr = tile * 64 + r;
+      if (gr < k * m && c < k)
+        Ph[(long long)(gr / k) * kk + (gr % k) + (long long)c * k] = v;
+    });
+  }
+}
+
+__global__ void __launch_bounds__(DmmaCfgKK::NT)
+    k_b_dmma_syrk(Pool pool, const int* act, const int4* work) {
+  extern __shared__ __align__(16) double smem[];
+  const int4 wi = work[blockIdx.x];
+  const Inst I = pool.inst[act[wi.x]];
+  const int m = I.m;
+  const int kk = I.k * I.k;
+  // P̂ rows j: (j, e) at j·k² + e, for both operands (S = P̂·P̂ᵀ)
+  const Opnd Pp{pool.Ph + I.a_off, 1, kk, 0, 1 << 30, m, kk};
+  double* S = pool.S + I.mm_off;
+  for (int q = wi.y; q < wi.z; ++q) {
+    const int ti = tri_row(q), tj = q - ti * (ti + 1) / 2;
+    double acc[DmmaCfgKK::FM][DmmaCfgKK::FN][2];
+    zero_acc<DmmaCfgKK>(acc);
+    f64_tile_mainloop<DmmaCfgKK>(acc, Pp, Pp, ti * 64, tj * 64, 0, kk, smem);
+    for_each_acc<DmmaCfgKK>(acc, [&](int r, int c, double v) {
+      const int gi = ti * 64 + r, gj = tj * 64 + c;
+      if (gi < m && gj < m && gi >= gj) {
+        S[gi + (long long)gj * m] = v;
+        S[gj + (long long)gi * m] = v;
+      }
+    });
   }
 }
 
@@ -1174,10 +1255,85 @@ struct Engine {
     t_schur += ms * 1e-3;
   }
 
-  // The Schur assembly over `ids`: panel then SYRK work items, largest first.
+  // The Schur assembly on the FP64 tensor cores: three grouped DMMA products
+  // (T = W·A, P̂ = T·L_Y, S = P̂P̂ᵀ), work items of about `g` flops, largest first.
+  DBuf<double> Tbuf;
+  void schur_dmma(const std::vector<int>& ids, double g) {
+    const int n = (int)ids.size();
+    if (n == 0) return;
+    if (!Tbuf.p) {
+      Tbuf.alloc(a_tot);
+      pool.T = Tbuf.p;
+      for (WorkKernel kf : {k_b_dmma_t, k_b_dmma_p})
+        SDPX_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)DmmaCfgKN::SMEM_BYTES));
+      SDPX_CUDA(cudaFuncSetAttribute(k_b_dmma_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)DmmaCfgKK::SMEM_BYTES));
+    }
+    SDPX_CUDA(cudaStreamSynchronize(st));
+    int* ha = static_cast<int*>(h_act.p);
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    auto cost = [&](int q) {
+      const Inst& I = inst[ids[q]];
+      return 4.0 * I.k * I.k * I.k * I.m + (double)I.k * I.k * I.m * I.m;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    std::vector<int4> w1, w2, w3;
+    auto split = [&](std::vector<int4>& w, int q, int tiles, double flops) {
+      int parts = g > 0 ? (int)std::ceil(flops / g) : 1;
+      parts = std::max(1, std::min(parts, tiles));
+      for (int p = 0; p < parts; ++p)
+        w.push_back(make_int4(q, (int)((long long)tiles * p / parts),
+                              (int)((long long)tiles * (p + 1) / parts), 0));
+    };
+    for (int q = 0; q < n; ++q) ha[q] = ids[q];
+    for (int q : order) {
+      const Inst& I = inst[ids[q]];
+      const int ct = (I.k * I.m + 63) / 64;        // 64-column (or row) tiles of the k·m panel
+      const int nt = (I.m + 63) / 64, tri = nt * (nt + 1) / 2;
+      const double pf = 2.0 * I.k * I.k * I.k * I.m;
+      split(w1, q, ct, pf);
+      split(w2, q, ct, pf);
+      split(w3, q, tri, (double)I.k * I.k * I.m * I.m);
+      schur_flops += 2.0 * I.k * I.k * I.k * I.m + (double)I.k * I.k * I.m * I.m;
+    }
+    const size_t nw = w1.size() + w2.size() + w3.size();
+    if (d_work.n < nw) d_work.alloc(nw + nw / 4);
+    h_work.ensure(nw * sizeof(int4));
+    int4* hw = static_cast<int4*>(h_work.p);
+    std::copy(w1.begin(), w1.end(), hw);
+    std::copy(w2.begin(), w2.end(), hw + w1.size());
+    std::copy(w3.begin(), w3.end(), hw + w1.size() + w2.size());
+    SDPX_CUDA(cudaMemcpyAsync(d_act.p, ha, n * sizeof(int), cudaMemcpyHostToDevice, st));
+    SDPX_CUDA(cudaMemcpyAsync(d_work.p, hw, nw * sizeof(int4), cudaMemcpyHostToDevice, st));
+    SDPX_CUDA(cudaEventRecord(ev[0], st));
+    k_b_dmma_t<<<(int)w1.size(), DmmaCfgKN::NT, DmmaCfgKN::SMEM_BYTES, st>>>(pool, d_act.p,
+                                                                            d_work.p);
+    SDPX_LAUNCH_CHECK();
+    k_b_dmma_p<<<(int)w2.size(), DmmaCfgKN::NT, DmmaCfgKN::SMEM_BYTES, st>>>(
+        pool, d_act.p, d_work.p + w1.size());
+    SDPX_LAUNCH_CHECK();
+    k_b_dmma_syrk<<<(int)w3.size(), DmmaCfgKK::NT, DmmaCfgKK::SMEM_BYTES, st>>>(
+        pool, d_act.p, d_work.p + w1.size() + w2.size());
+    SDPX_LAUNCH_CHECK();
+    SDPX_CUDA(cudaEventRecord(ev[1], st));
+    launches += 3;
+    SDPX_CUDA(cudaEventSynchronize(ev[1]));
+    float ms = 0;
+    SDPX_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    t_schur += ms * 1e-3;
+  }
+
+  // The Schur assembly over `ids`: panel then SYRK work items, largest first
+  // (tile 64: the DMMA products of schur_dmma).
   void schur(const std::vector<int>& ids, int threads, int tile, double g) {
     const int n = (int)ids.size();
     if (n == 0) return;
+    if (tile == 64) {
+      schur_dmma(ids, g);
+      return;
+    }
     WorkKernel syrk = syrk_kernel(threads, tile);
     if (!syrk) throw std::invalid_argument("unsupported Schur launch shape");
     SDPX_CUDA(cudaStreamSynchronize(st));
@@ -1791,7 +1947,8 @@ struct Engine {
       double grain;
     };
     std::vector<Cand> cands;
-    const std::pair<int, int> shapes[] = {{128, 16}, {256, 16}, {128, 32}, {256, 32}, {512, 32}};
+    const std::pair<int, int> shapes[] = {{128, 16}, {256, 16}, {128, 32},
+                                          {256, 32}, {512, 32}, {128, 64}};
     for (double g : {0.0, 1.0e6, 4.0e6, 16.0e6})
       for (const auto& tt : shapes) cands.push_back({tt.first, tt.second, g});
     double best = INFINITY;
@@ -2056,7 +2213,7 @@ int sdpx_b200_batch_set_schur_shape(sdpx_b200_batch* b, int32_t threads, int32_t
                                     double grain) {
   BGUARD(b, {
     if (threads != 0) {
-      if (!sdpx::batch::syrk_kernel(threads, tile))
+      if (!(tile == 64 && threads == 128) && !sdpx::batch::syrk_kernel(threads, tile))
         throw std::invalid_argument("unsupported Schur launch shape (threads, tile)");
       b->e.schur_threads = threads;
       b->e.schur_tile = tile;

@@ -34,6 +34,7 @@ struct Pool {
   const Inst* inst;
   const double* A;
   double* Ph;
+  double* T;  // W·A_j of every constraint (the DMMA Schur path)
   const double* C;
   const double* c;
   double *X, *Y, *P, *R, *LX, *LY, *W, *dX, *dY, *Z, *Xb, *Yb;

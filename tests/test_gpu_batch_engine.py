@@ -84,13 +84,34 @@ def test_schur_launch_shape_changes_no_result(cuda_ok):
                 assert a.pObj == b.pObj and a.dObj == b.dObj
 
 
+def test_dmma_schur_matches_the_scalar_kernels(cuda_ok):
+    """The Schur phase on the FP64 tensor cores (three grouped DMMA products)
+    against the scalar kernels: the same solves up to summation order."""
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = batch_instances(48, seed=21)
+    opts = batch_options(1e-8)
+    with BatchSolver(probs) as bs:
+        bs.set_schur_shape(256, 32, 0.0)
+        ref = bs.optimize(opts, solutions=False)
+        bs.set_schur_shape(128, 64, 0.0)
+        dm = bs.optimize(opts, solutions=False)
+        bs.set_schur_shape(128, 64, 1.0e6)
+        dm2 = bs.optimize(opts, solutions=False)
+    diff = [i for i, (a, b) in enumerate(zip(ref, dm))
+            if a.status != b.status or abs(a.iterations - b.iterations) > 1 or
+            rel(a.pObj, b.pObj) > 1e-7 or rel(a.dObj, b.dObj) > 1e-7]
+    assert len(diff) <= 1, diff
+    for a, b in zip(dm, dm2):  # the work split changes no bit
+        assert a.status == b.status and a.iterations == b.iterations and a.pObj == b.pObj
+
+
 def test_autotune_picks_a_timed_shape(cuda_ok, tmp_path, monkeypatch):
     from sdpx_b200.batch import BatchSolver, batch_options
     monkeypatch.setenv("SDPX_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     probs = batch_instances(32, seed=4)
     with BatchSolver(probs) as bs:
         table = bs.autotune(batch_options(1e-8))
-        assert len(table) == 20
+        assert len(table) == 24
         best = min(table, key=lambda r: r[3])
         assert bs.shape == (int(best[0]), int(best[1]), float(best[2]))
         assert all(r[3] > 0 for r in table)
