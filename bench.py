@@ -1104,12 +1104,12 @@ def run_profile(args):
 def run_batch_profile(args):
     """One batched solve of the first N instances of the small-SDP workload
     (seed = --seed) with the Schur launch shape the autotuner picks on the
-    B200 (512 threads, 32-tile, one item per instance); prints its counters."""
+    B200 (the DMMA products, one work item per instance); prints its counters."""
     from sdpx_b200 import batch_instances
     from sdpx_b200.batch import BatchSolver, batch_options
     probs = batch_instances(args.batch_profile, seed=args.seed)
     with BatchSolver(probs) as bs:
-        bs.set_schur_shape(512, 32, 0.0)
+        bs.set_schur_shape(128, 64, 0.0)
         res = bs.optimize(batch_options(args.batch_tol, precision=args.batch_precision),
                           solutions=False)
         st = bs.stats()
