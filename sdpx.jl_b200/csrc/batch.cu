@@ -99,11 +99,10 @@ __global__ void __launch_bounds__(kThreads)
   double* R = pool.R + I.kk_off;
   const double mu = in[kMu];
   const bool add_mu = in[kUseAffine] == 0.0;
+  cta_gemm_dmma(Xs, false, Ys, R, k);  // R = X·Y (global), then −XY (+μI)
   for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
     const int r = (int)(e % k), c = (int)(e / k);
-    double s = 0.0;
-    for (int p = 0; p < k; ++p) s += Xs[r + p * k] * Ys[p + c * k];
-    s = -s;
+    double s = -R[e];
     if (add_mu && r == c) s += mu;
     R[e] = s;
   }
@@ -431,49 +430,30 @@ __global__ void __launch_bounds__(kThreads)
   double* R = pool.R + I.kk_off;
   const double* X = pool.X + I.kk_off;
   const double* Y = pool.Y + I.kk_off;
-  if (in[kMode] == 1.0) {
-    const double* dX = pool.dX + I.kk_off;
-    const double* dY = pool.dY + I.kk_off;
-    for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
-      M1[e] = X[e];
-      M2[e] = Y[e];
-    }
-    __syncthreads();
+  for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
+    M1[e] = X[e];
+    M2[e] = Y[e];
+  }
+  __syncthreads();
+  if (in[kMode] == 1.0) {  // R = target·I − X·Y − dX·dY
+    cta_gemm_dmma(M1, false, M2, M3, k);                                    // X·Y
+    cta_gemm_dmma(pool.dX + I.kk_off, false, pool.dY + I.kk_off, M1, k);  // dX·dY
     for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
       const int r = (int)(e % k), c = (int)(e / k);
-      double s = 0.0, t = 0.0;
-      for (int p = 0; p < k; ++p) {
-        s += M1[r + p * k] * M2[p + c * k];
-        t += dX[r + p * k] * dY[p + c * k];
-      }
-      double v = -s - t;
+      double v = -M3[e] - M1[e];
       if (r == c) v += in[kTarget];
-      M3[e] = v;
+      R[e] = v;
     }
     __syncthreads();
-    for (long long e = threadIdx.x; e < kk; e += blockDim.x) R[e] = M3[e];
-    __syncthreads();
   }
+  // Z = P·Y − R, then X⁻¹Z = Wᵀ·W·Z
   const double* P = pool.P + I.kk_off;
-  const double* W = pool.W + I.kk_off;
-  for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
-    M1[e] = P[e];
-    M2[e] = Y[e];
-    M3[e] = W[e];
-  }
+  cta_gemm_dmma(P, false, M2, M3, k);  // P·Y
+  for (long long e = threadIdx.x; e < kk; e += blockDim.x) M1[e] = M3[e] - R[e];
+  for (long long e = threadIdx.x; e < kk; e += blockDim.x) M3[e] = pool.W[I.kk_off + e];
   __syncthreads();
-  double* Z = pool.Z + I.kk_off;
-  for (long long e = threadIdx.x; e < kk; e += blockDim.x) {  // Z = PY − R
-    const int r = (int)(e % k), c = (int)(e / k);
-    double s = 0.0;
-    for (int p = 0; p < k; ++p) s += M1[r + p * k] * M2[p + c * k];
-    Z[e] = s - R[e];
-  }
-  __syncthreads();
-  for (long long e = threadIdx.x; e < kk; e += blockDim.x) M1[e] = Z[e];
-  __syncthreads();
-  cta_gemm(M3, false, M1, M2, k);  // W·(PY − R)
-  cta_gemm(M3, true, M2, M1, k);   // X⁻¹(PY − R) = Wᵀ·W·(PY − R)
+  cta_gemm_dmma(M3, false, M1, M2, k);  // W·(PY − R)
+  cta_gemm_dmma(M3, true, M2, M1, k);   // X⁻¹(PY − R) = Wᵀ·W·(PY − R)
   const double* A = pool.A + I.a_off;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int j = warp; j < m; j += nw) {
@@ -530,17 +510,11 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   const double* R = pool.R + I.kk_off;
   double* Z = pool.Z + I.kk_off;
-  for (long long e = threadIdx.x; e < kk; e += blockDim.x) {  // R − dX·Y
-    const int r = (int)(e % k), c = (int)(e / k);
-    double s = 0.0;
-    for (int p = 0; p < k; ++p) s += M1[r + p * k] * M2[p + c * k];
-    Z[e] = R[e] - s;
-  }
+  cta_gemm_dmma(M1, false, M2, Z, k);  // dX·Y (global scratch)
+  for (long long e = threadIdx.x; e < kk; e += blockDim.x) M1[e] = R[e] - Z[e];
   __syncthreads();
-  for (long long e = threadIdx.x; e < kk; e += blockDim.x) M1[e] = Z[e];
-  __syncthreads();
-  cta_gemm(M3, false, M1, M2, k);
-  cta_gemm(M3, true, M2, M1, k);
+  cta_gemm_dmma(M3, false, M1, M2, k);
+  cta_gemm_dmma(M3, true, M2, M1, k);
   double* dY = pool.dY + I.kk_off;
   for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
     const int r = (int)(e % k), c = (int)(e / k);

@@ -102,6 +102,34 @@ __device__ bool cta_chol(double* M, int k, double* sflag, double* dmin, double* 
   return true;
 }
 
+// C = op(A)·B for k×k column-major operands (shared or global memory) on the
+// FP64 tensor cores: each warp takes 8×8 output tiles in turn and runs the
+// m8n8k4 DMMA over k in steps of 4 (loads past k read 0).  ta: A transposed.
+// C must not alias A or B.  Ends with a CTA barrier.
+__device__ void cta_gemm_dmma(const double* A, bool ta, const double* B, double* C, int k) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int nb = (k + 7) / 8;
+  for (int tile = warp; tile < nb * nb; tile += nw) {
+    const int i0 = (tile % nb) * 8, j0 = (tile / nb) * 8;
+    const int r = i0 + g, cB = j0 + g;
+    double c0 = 0.0, c1 = 0.0;
+    for (int kk = 0; kk < k; kk += 4) {
+      const int p = kk + t;
+      const bool okp = p < k;
+      const double a = (okp && r < k) ? (ta ? A[p + r * k] : A[r + p * k]) : 0.0;
+      const double b = (okp && cB < k) ? B[p + cB * k] : 0.0;
+      dmma_8x8x4(c0, c1, a, b);
+    }
+    const int cc = j0 + 2 * t;
+    if (r < k) {
+      if (cc < k) C[r + cc * k] = c0;
+      if (cc + 1 < k) C[r + (cc + 1) * k] = c1;
+    }
+  }
+  __syncthreads();
+}
+
 // W = L⁻¹ (lower, k×k): one thread per column, forward substitution.
 __device__ void cta_trinv(const double* L, double* W, int k) {
   for (int e = threadIdx.x; e < k * k; e += blockDim.x) W[e] = 0.0;
@@ -113,20 +141,6 @@ __device__ void cta_trinv(const double* L, double* W, int k) {
       for (int p = c; p < r; ++p) s += L[r + p * k] * W[p + c * k];
       W[r + c * k] = -s / L[r + r * k];
     }
-  }
-  __syncthreads();
-}
-
-// C = op(A)·B for k×k column-major operands; ta: A transposed.
-__device__ void cta_gemm(const double* A, bool ta, const double* B, double* C, int k) {
-  for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
-    const int r = e % k, c = e / k;
-    double s = 0.0;
-    if (ta)
-      for (int p = 0; p < k; ++p) s += A[p + r * k] * B[p + c * k];
-    else
-      for (int p = 0; p < k; ++p) s += A[r + p * k] * B[p + c * k];
-    C[e] = s;
   }
   __syncthreads();
 }
