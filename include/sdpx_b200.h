@@ -224,8 +224,10 @@ int sdpx_b200_adjoint(sdpx_b200_handle* h, const double* wx, const double* wy, c
  * residual scheme of `_solve_mixed_kkt_guarded!`,
  * src/kernels/mixed_precision_kkt.jl:1475-1586, one level up).  Near a
  * solution S is ill-conditioned and the single FP64 solve of
- * sdpx_b200_adjoint loses κ(S)·eps.  residual (may be NULL) =
- * ‖w − S·λ‖∞ / ‖w‖∞ after the last step, in double-double. */
+ * sdpx_b200_adjoint loses κ(S)·eps.  A step that does not reduce the
+ * residual is rolled back and ends the refinement (when κ(S)·eps ≥ 1 the FP64
+ * factor no longer contracts it).  residual (may be NULL) = ‖w − S·λ‖∞ /
+ * ‖w‖∞ of the returned λ, in double-double. */
 int sdpx_b200_adjoint_refined(sdpx_b200_handle* h, const double* wx, const double* WX,
                               const double* WY, double* grad_c, double* grad_C, int32_t nA,
                               const int32_t* A_index, double* grad_A, int32_t refine_steps,

@@ -330,27 +330,62 @@ __global__ void __launch_bounds__(DmmaCfgKK::NT)
   }
 }
 
-// Lower Cholesky of the m×m column-major M in place (global memory, one CTA):
-// false at the first pivot that is not > 0.
-__device__ bool cta_chol_global(double* M, int m, double* sflag) {
-  for (int j = 0; j < m; ++j) {
-    if (threadIdx.x == 0) {
-      const double d = M[j + (long long)j * m];
-      sflag[0] = d;
-      sflag[1] = d > 0.0 ? sqrt(d) : 0.0;
+// Blocked lower Cholesky of the m×m column-major M in place (global memory,
+// one CTA): 16-column panels factored column by column (pivot, scale, rank-1
+// update inside the panel), then the trailing block updated by the panel as a
+// rank-16 SYRK on DMMA m8n8k4 fragments (8×8 lower tiles, one per warp in
+// turn).  False at the first pivot that is not > 0.
+__device__ bool cta_chol_blocked(double* M, int m, double* sflag) {
+  constexpr int NB = 16;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  for (int jb = 0; jb < m; jb += NB) {
+    const int je = min(m, jb + NB);
+    for (int j = jb; j < je; ++j) {
+      if (threadIdx.x == 0) {
+        const double d = M[j + (long long)j * m];
+        sflag[0] = d;
+        sflag[1] = d > 0.0 ? sqrt(d) : 0.0;
+      }
+      __syncthreads();
+      if (!(sflag[0] > 0.0)) return false;
+      const double ljj = sflag[1];
+      const double inv = 1.0 / ljj;
+      for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) M[i + (long long)j * m] *= inv;
+      if (threadIdx.x == 0) M[j + (long long)j * m] = ljj;
+      __syncthreads();
+      const int nc = je - j - 1, rows = m - j - 1;  // panel columns right of j, all rows below j
+      for (long long e = threadIdx.x; e < (long long)nc * rows; e += blockDim.x) {
+        const int ii = j + 1 + (int)(e % rows), ll = j + 1 + (int)(e / rows);
+        if (ii >= ll)
+          M[ii + (long long)ll * m] -= M[ii + (long long)j * m] * M[ll + (long long)j * m];
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    if (!(sflag[0] > 0.0)) return false;
-    const double ljj = sflag[1];
-    const double inv = 1.0 / ljj;
-    for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) M[i + (long long)j * m] *= inv;
-    if (threadIdx.x == 0) M[j + (long long)j * m] = ljj;
-    __syncthreads();
-    const int rem = m - j - 1;
-    for (long long e = threadIdx.x; e < (long long)rem * rem; e += blockDim.x) {
-      const int ii = j + 1 + (int)(e % rem), ll = j + 1 + (int)(e / rem);
-      if (ii >= ll)
-        M[ii + (long long)ll * m] -= M[ii + (long long)j * m] * M[ll + (long long)j * m];
+    // trailing block rows, cols ≥ je:  M −= L_panel · L_panelᵀ (lower 8×8 tiles)
+    const int n = m - je;
+    if (n <= 0) break;
+    const int nb8 = (n + 7) / 8;
+    const int ntile = nb8 * (nb8 + 1) / 2;
+    for (int tile = warp; tile < ntile; tile += nw) {
+      int ti = (int)((sqrt(8.0 * tile + 1.0) - 1.0) * 0.5);
+      while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
+      while (ti * (ti + 1) / 2 > tile) --ti;
+      const int tj = tile - ti * (ti + 1) / 2;
+      const int r = je + ti * 8 + g, cB = je + tj * 8 + g;
+      double c0 = 0.0, c1 = 0.0;
+      for (int kk = jb; kk < je; kk += 4) {
+        const int p = kk + t;
+        const bool okp = p < je;
+        const double a = (okp && r < m) ? M[r + (long long)p * m] : 0.0;
+        const double b = (okp && cB < m) ? M[cB + (long long)p * m] : 0.0;
+        dmma_8x8x4(c0, c1, a, b);
+      }
+      const int cc = je + tj * 8 + 2 * t;
+      if (r < m) {
+        if (cc < m && r >= cc) M[r + (long long)cc * m] -= c0;
+        if (cc + 1 < m && r >= cc + 1) M[r + (long long)(cc + 1) * m] -= c1;
+      }
     }
     __syncthreads();
   }
@@ -377,7 +412,7 @@ __global__ void __launch_bounds__(kThreads)
       L[e] = v;
     }
     __syncthreads();
-    ok = cta_chol_global(L, m, sflag);
+    ok = cta_chol_blocked(L, m, sflag);
     __syncthreads();
     if (ok || attempts >= 6) break;
     ++attempts;

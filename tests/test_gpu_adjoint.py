@@ -207,3 +207,30 @@ def test_refined_adjoint_at_a_solution_matches_double_double(cuda):
     assert _rel(gr["grad_C"][0], gd["grad_C"][0]) <= FD_TOL
     for q in range(len(idx)):
         assert _rel(gr["grad_A"][q][0], gd["grad_A"][q][0]) <= FD_TOL
+
+
+def test_refined_adjoint_residual_never_grows(cuda):
+    """On the differentiable-SDP shape at 1e-9 solutions the double-double
+    refinement keeps its best λ: more steps never leave a larger residual."""
+    from sdpx_b200 import SolverOptions
+    from sdpx_b200.cuda_backend import CudaBackend
+    opts = SolverOptions(scaling="none").with_tolerance(1e-9)
+    tested = 0
+    for inst in range(8):
+        prob = G.sdpa_dense(m=500, blocks=[200], lp=0, seed=1000 + inst)
+        rng = np.random.default_rng(inst)
+        v = rng.standard_normal(prob.m)
+        with CudaBackend(prob) as cb:
+            r = cb.optimize(opts)
+            cb.set_iterate(r.x, r.X, r.Y)
+            if not cb.compute_residuals([0.0] * prob.L, True, True)[2]:
+                continue  # the returned slack is not positive definite
+            cb.schur_build()
+            if not cb.factorize()["ok"]:
+                continue
+            res = [cb.adjoint_refined(v, None, None, (0,), steps=s)["residual"]
+                   for s in (0, 3, 16)]
+        tested += 1
+        assert all(np.isfinite(res)), res
+        assert res[1] <= res[0] and res[2] <= res[1], res
+    assert tested >= 4
