@@ -251,57 +251,42 @@ __global__ void __launch_bounds__(NT) k_b_syrk(Pool pool, const int* act, const 
 }
 
 // ---- B2 on the FP64 tensor cores (DMMA m8n8k4 tiles of gemm_f64.cuh) -----
-// Three grouped products per instance, 64×64 output tiles, 4 warps per CTA:
-//   T  = W·[A_1 … A_m]          (k × k·m; W = L_X⁻¹),
-//   P̂  = T·L_Y, one k×k block per constraint (rows j·k + r of a k·m × k product),
-//   S  = P̂·P̂ᵀ over the lower 64×64 tiles (both triangles written).
-// Work items {row, first tile, end tile} as for the scalar kernels; T lives in
-// pool.T (an m·k² array beside the panel).
+// Per instance P̂_j = W·A_j·L_Y (W = L_X⁻¹) for every constraint, then
+// S = P̂·P̂ᵀ over the lower 64×64 tiles (both triangles written); 4 warps per
+// CTA, work items {row, first, end} as for the scalar kernels.
 using DmmaCfgKN = F64Cfg<64, 64, 2, 2, false, true>;  // A MN-contiguous, B K-contiguous
 using DmmaCfgKK = F64Cfg<64, 64, 2, 2, true, true>;   // both K-contiguous
 
+// T and P̂ fused per constraint: work item {row, first j, end j}; T_j = W·A_j
+// goes to this CTA's k×k scratch (pool.T + blockIdx.x·kq, reused for every j,
+// so it stays in L2), then P̂_j = T_j·L_Y.
 __global__ void __launch_bounds__(DmmaCfgKN::NT)
-    k_b_dmma_t(Pool pool, const int* act, const int4* work) {
+    k_b_dmma_tp(Pool pool, const int* act, const int4* work) {
   extern __shared__ __align__(16) double smem[];
   const int4 wi = work[blockIdx.x];
   const Inst I = pool.inst[act[wi.x]];
-  const int k = I.k, m = I.m;
+  const int k = I.k;
   const long long kk = (long long)k * k;
-  // A = W (k×k): element (r, p) at r + p·k;  B = [A_1 … A_m]: (p, j·k + c) at j·k² + c·k + p
-  const Opnd Aw{pool.W + I.kk_off, k, 1, 0, 1 << 30, k, k};
-  const Opnd Ba{pool.A + I.a_off, 1, k, kk, k, k * m, k};
-  double* T = pool.T + I.a_off;
-  for (int tile = wi.y; tile < wi.z; ++tile) {
+  double* T = pool.T + (long long)blockIdx.x * pool.kq;
+  const Opnd Aw{pool.W + I.kk_off, k, 1, 0, 1 << 30, k, k};     // (r, p) at r + p·k
+  const Opnd At{T, k, 1, 0, 1 << 30, k, k};                      // (r, q) at r + q·k
+  const Opnd Bl{pool.LY + I.kk_off, 1, k, 0, 1 << 30, k, k};    // (q, c) at q + c·k
+  for (int j = wi.y; j < wi.z; ++j) {
+    const Opnd Bj{pool.A + I.a_off + (long long)j * kk, 1, k, 0, 1 << 30, k, k};  // (p, c)
     double acc[DmmaCfgKN::FM][DmmaCfgKN::FN][2];
     zero_acc<DmmaCfgKN>(acc);
-    f64_tile_mainloop<DmmaCfgKN>(acc, Aw, Ba, 0, tile * 64, 0, k, smem);
-    for_each_acc<DmmaCfgKN>(acc, [&](int r, int col, double v) {
-      const int gc = tile * 64 + col;
-      if (r < k && gc < k * m) T[(long long)(gc / k) * kk + (long long)(gc % k) * k + r] = v;
-    });
-  }
-}
-
-__global__ void __launch_bounds__(DmmaCfgKN::NT)
-    k_b_dmma_p(Pool pool, const int* act, const int4* work) {
-  extern __shared__ __align__(16) double smem[];
-  const int4 wi = work[blockIdx.x];
-  const Inst I = pool.inst[act[wi.x]];
-  const int k = I.k, m = I.m;
-  const long long kk = (long long)k * k;
-  // A = T blocks: (j·k + r, q) at j·k² + r + q·k;  B = L_Y: (q, c) at q + c·k
-  const Opnd At{pool.T + I.a_off, k, 1, kk, k, k * m, k};
-  const Opnd Bl{pool.LY + I.kk_off, 1, k, 0, 1 << 30, k, k};
-  double* Ph = pool.Ph + I.a_off;
-  for (int tile = wi.y; tile < wi.z; ++tile) {
-    double acc[DmmaCfgKN::FM][DmmaCfgKN::FN][2];
-    zero_acc<DmmaCfgKN>(acc);
-    f64_tile_mainloop<DmmaCfgKN>(acc, At, Bl, tile * 64, 0, 0, k, smem);
+    f64_tile_mainloop<DmmaCfgKN>(acc, Aw, Bj, 0, 0, 0, k, smem);
     for_each_acc<DmmaCfgKN>(acc, [&](int r, int c, double v) {
-      const int gr = tile * 64 + r;
-      if (gr < k * m && c < k)
-        Ph[(long long)(gr / k) * kk + (gr % k) + (long long)c * k] = v;
+      if (r < k && c < k) T[r + (long long)c * k] = v;
     });
+    __syncthreads();
+    zero_acc<DmmaCfgKN>(acc);
+    f64_tile_mainloop<DmmaCfgKN>(acc, At, Bl, 0, 0, 0, k, smem);
+    double* Pj = pool.Ph + I.a_off + (long long)j * kk;
+    for_each_acc<DmmaCfgKN>(acc, [&](int r, int c, double v) {
+      if (r < k && c < k) Pj[r + (long long)c * k] = v;
+    });
+    __syncthreads();
   }
 }
 
@@ -1266,18 +1251,17 @@ struct Engine {
 
   // The Schur assembly on the FP64 tensor cores: three grouped DMMA products
   // (T = W·A, P̂ = T·L_Y, S = P̂P̂ᵀ), work items of about `g` flops, largest first.
-  DBuf<double> Tbuf;
+  DBuf<double> Tbuf;  // one k×k scratch per fused T·P̂ work item
+  bool dmma_attrs = false;
   void schur_dmma(const std::vector<int>& ids, double g) {
     const int n = (int)ids.size();
     if (n == 0) return;
-    if (!Tbuf.p) {
-      Tbuf.alloc(a_tot);
-      pool.T = Tbuf.p;
-      for (WorkKernel kf : {k_b_dmma_t, k_b_dmma_p})
-        SDPX_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)DmmaCfgKN::SMEM_BYTES));
+    if (!dmma_attrs) {
+      SDPX_CUDA(cudaFuncSetAttribute(k_b_dmma_tp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)DmmaCfgKN::SMEM_BYTES));
       SDPX_CUDA(cudaFuncSetAttribute(k_b_dmma_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)DmmaCfgKK::SMEM_BYTES));
+      dmma_attrs = true;
     }
     SDPX_CUDA(cudaStreamSynchronize(st));
     int* ha = static_cast<int*>(h_act.p);
@@ -1288,46 +1272,43 @@ struct Engine {
       return 4.0 * I.k * I.k * I.k * I.m + (double)I.k * I.k * I.m * I.m;
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
-    std::vector<int4> w1, w2, w3;
-    auto split = [&](std::vector<int4>& w, int q, int tiles, double flops) {
+    std::vector<int4> w1, w3;
+    auto split = [&](std::vector<int4>& w, int q, int units, double flops) {
       int parts = g > 0 ? (int)std::ceil(flops / g) : 1;
-      parts = std::max(1, std::min(parts, tiles));
+      parts = std::max(1, std::min(parts, units));
       for (int p = 0; p < parts; ++p)
-        w.push_back(make_int4(q, (int)((long long)tiles * p / parts),
-                              (int)((long long)tiles * (p + 1) / parts), 0));
+        w.push_back(make_int4(q, (int)((long long)units * p / parts),
+                              (int)((long long)units * (p + 1) / parts), 0));
     };
     for (int q = 0; q < n; ++q) ha[q] = ids[q];
     for (int q : order) {
       const Inst& I = inst[ids[q]];
-      const int ct = (I.k * I.m + 63) / 64;        // 64-column (or row) tiles of the k·m panel
       const int nt = (I.m + 63) / 64, tri = nt * (nt + 1) / 2;
-      const double pf = 2.0 * I.k * I.k * I.k * I.m;
-      split(w1, q, ct, pf);
-      split(w2, q, ct, pf);
+      split(w1, q, I.m, 4.0 * I.k * I.k * I.k * I.m);  // constraint ranges
       split(w3, q, tri, (double)I.k * I.k * I.m * I.m);
       schur_flops += 2.0 * I.k * I.k * I.k * I.m + (double)I.k * I.k * I.m * I.m;
     }
-    const size_t nw = w1.size() + w2.size() + w3.size();
+    if (Tbuf.n < w1.size() * (size_t)pool.kq) {
+      Tbuf.alloc(w1.size() * (size_t)pool.kq + w1.size() * (size_t)pool.kq / 4);
+      pool.T = Tbuf.p;
+    }
+    const size_t nw = w1.size() + w3.size();
     if (d_work.n < nw) d_work.alloc(nw + nw / 4);
     h_work.ensure(nw * sizeof(int4));
     int4* hw = static_cast<int4*>(h_work.p);
     std::copy(w1.begin(), w1.end(), hw);
-    std::copy(w2.begin(), w2.end(), hw + w1.size());
-    std::copy(w3.begin(), w3.end(), hw + w1.size() + w2.size());
+    std::copy(w3.begin(), w3.end(), hw + w1.size());
     SDPX_CUDA(cudaMemcpyAsync(d_act.p, ha, n * sizeof(int), cudaMemcpyHostToDevice, st));
     SDPX_CUDA(cudaMemcpyAsync(d_work.p, hw, nw * sizeof(int4), cudaMemcpyHostToDevice, st));
     SDPX_CUDA(cudaEventRecord(ev[0], st));
-    k_b_dmma_t<<<(int)w1.size(), DmmaCfgKN::NT, DmmaCfgKN::SMEM_BYTES, st>>>(pool, d_act.p,
-                                                                            d_work.p);
-    SDPX_LAUNCH_CHECK();
-    k_b_dmma_p<<<(int)w2.size(), DmmaCfgKN::NT, DmmaCfgKN::SMEM_BYTES, st>>>(
-        pool, d_act.p, d_work.p + w1.size());
+    k_b_dmma_tp<<<(int)w1.size(), DmmaCfgKN::NT, DmmaCfgKN::SMEM_BYTES, st>>>(pool, d_act.p,
+                                                                             d_work.p);
     SDPX_LAUNCH_CHECK();
     k_b_dmma_syrk<<<(int)w3.size(), DmmaCfgKK::NT, DmmaCfgKK::SMEM_BYTES, st>>>(
-        pool, d_act.p, d_work.p + w1.size() + w2.size());
+        pool, d_act.p, d_work.p + w1.size());
     SDPX_LAUNCH_CHECK();
     SDPX_CUDA(cudaEventRecord(ev[1], st));
-    launches += 3;
+    launches += 2;
     SDPX_CUDA(cudaEventSynchronize(ev[1]));
     float ms = 0;
     SDPX_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));

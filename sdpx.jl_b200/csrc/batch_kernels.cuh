@@ -34,7 +34,7 @@ struct Pool {
   const Inst* inst;
   const double* A;
   double* Ph;
-  double* T;  // W·A_j of every constraint (the DMMA Schur path)
+  double* T;  // k×k scratch per work item of the DMMA Schur path (T_j = W·A_j)
   const double* C;
   const double* c;
   double *X, *Y, *P, *R, *LX, *LY, *W, *dX, *dY, *Z, *Xb, *Yb;
