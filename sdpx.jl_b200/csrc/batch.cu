@@ -1125,6 +1125,17 @@ struct Engine {
       scale_p[i] = 1.0 + mc;
       scale_d[i] = 1.0 + mcc;
     }
+    {  // instances ranked by an estimate of their per-iteration work
+      std::vector<int> order(N);
+      std::iota(order.begin(), order.end(), 0);
+      auto w = [&](int i) {
+        const double k = inst[i].k, m = inst[i].m;
+        return 4.0 * k * k * k + 4.0 * m * k * k + m * m * k * k / 64.0 + m * m * m / 3.0;
+      };
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w(a) > w(b); });
+      work_rank.assign(N, 0);
+      for (int r = 0; r < N; ++r) work_rank[order[r]] = r;
+    }
     d_act.alloc(N);
     d_par.alloc((size_t)N * kNIn);
     d_res.alloc((size_t)N * oNOut);
@@ -1184,12 +1195,18 @@ struct Engine {
     // The staging buffers are reused by every launch: the copies queued from
     // them by the previous one must have run first.
     SDPX_CUDA(cudaStreamSynchronize(st));
+    // CTAs in decreasing order of the instance's work (largest first, so the
+    // last wave of a phase holds small instances); rows map back to `ids`.
+    lpt.resize(n);
+    std::iota(lpt.begin(), lpt.end(), 0);
+    std::stable_sort(lpt.begin(), lpt.end(),
+                     [&](int a, int b) { return work_rank[ids[a]] < work_rank[ids[b]]; });
     int* ha = static_cast<int*>(h_act.p);
     double* hp = static_cast<double*>(h_par.p);
     std::memset(hp, 0, (size_t)n * kNIn * sizeof(double));
     for (int q = 0; q < n; ++q) {
-      ha[q] = ids[q];
-      fill(ids[q], hp + (size_t)q * kNIn);
+      ha[q] = ids[lpt[q]];
+      fill(ids[lpt[q]], hp + (size_t)q * kNIn);
     }
     SDPX_CUDA(cudaMemcpyAsync(d_act.p, ha, n * sizeof(int), cudaMemcpyHostToDevice, st));
     SDPX_CUDA(cudaMemcpyAsync(d_par.p, hp, (size_t)n * kNIn * sizeof(double),
@@ -1201,8 +1218,15 @@ struct Engine {
     SDPX_CUDA(cudaMemcpyAsync(h_res.p, d_res.p, (size_t)n * oNOut * sizeof(double),
                               cudaMemcpyDeviceToHost, st));
     SDPX_CUDA(cudaStreamSynchronize(st));
-    return static_cast<const double*>(h_res.p);
+    const double* launched = static_cast<const double*>(h_res.p);
+    rows.resize((size_t)n * oNOut);
+    for (int q = 0; q < n; ++q)
+      std::memcpy(rows.data() + (size_t)lpt[q] * oNOut, launched + (size_t)q * oNOut,
+                  oNOut * sizeof(double));
+    return rows.data();
   }
+  std::vector<int> lpt, work_rank;  // launch order; rank of each instance by work
+  std::vector<double> rows;         // output rows in the caller's order
   const double* phase(PhaseKernel kf, const std::vector<int>& ids, size_t smem, bool read) {
     return phase(kf, ids, smem, [](int, double*) {}, read);
   }
