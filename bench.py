@@ -66,7 +66,7 @@ EQ_ROWS = 64
 # the gap tolerance becomes 1e-9/objective_scale, which the FP64 path (the CPU
 # restatement too) cannot reach on this shape (NumericalBreakdown near 2e-11).
 ADJ_WORKLOAD = dict(m=500, blocks=[200], lp=0, instances=64, A_count=10, tol=1e-9,
-                    scaling="none", refine=3)
+                    scaling="none", refine=32)
 # Structurally sparse SDP in the regime of SDPX's SparseCons path (the lattice
 # bootstrap shape its sparse engine was tuned on: 32 PSD blocks of order
 # 23–74, each coefficient storing 2–6 entries per block it touches).
@@ -450,7 +450,7 @@ def bench_adjoint(args, world, rank, local):
         out["cpu_adjoint_s"] = time.perf_counter() - t0
         out["cpu_kind"] = "port: the oracle's FP64 adjoint (NumPy/OpenBLAS, all host cores)"
         t0 = time.perf_counter()
-        gd = dd_adjoint(prob, r.x, r.X, r.Y, wx=v, WY=W, A_index=idx, refine=wl["refine"])
+        gd = dd_adjoint(prob, r.x, r.X, r.Y, wx=v, WY=W, A_index=idx, refine=4)
         out["cpu_float64x2_reference_s"] = time.perf_counter() - t0
 
         def rel(a, b):

@@ -219,15 +219,14 @@ int sdpx_b200_adjoint(sdpx_b200_handle* h, const double* wx, const double* wy, c
 /* The same gradient (no equality rows: n = 0) with the linear system solved
  * to double-double (Float64x2) accuracy: X⁻¹ by Newton–Schulz steps from the
  * FP64 inverse, every product of S·v = 𝒜ᵀ(X⁻¹ mat(𝒜v) Y) and of the seeds in
- * double-double, and λ refined refine_steps times on the FP64 factor with
- * double-double residuals (the low-precision factor / high-precision
- * residual scheme of `_solve_mixed_kkt_guarded!`,
- * src/kernels/mixed_precision_kkt.jl:1475-1586, one level up).  Near a
- * solution S is ill-conditioned and the single FP64 solve of
- * sdpx_b200_adjoint loses κ(S)·eps.  A step that does not reduce the
- * residual is rolled back and ends the refinement (when κ(S)·eps ≥ 1 the FP64
- * factor no longer contracts it).  residual (may be NULL) = ‖w − S·λ‖∞ /
- * ‖w‖∞ of the returned λ, in double-double. */
+ * double-double, and λ solved by up to refine_steps (≤ 64) conjugate-gradient
+ * steps in double-double preconditioned by the FP64 factor (the
+ * low-precision factor / high-precision residual scheme of
+ * `_solve_mixed_kkt_guarded!`, src/kernels/mixed_precision_kkt.jl:1475-1586,
+ * one level up; CG keeps converging when κ(S)·eps ≥ 1 near a solution, where
+ * plain refinement on the FP64 factor stops contracting).  The FP64 solve is
+ * returned when CG does not reduce the true residual.  residual (may be
+ * NULL) = ‖w − S·λ‖∞ / ‖w‖∞ of the returned λ, in double-double. */
 int sdpx_b200_adjoint_refined(sdpx_b200_handle* h, const double* wx, const double* WX,
                               const double* WY, double* grad_c, double* grad_C, int32_t nA,
                               const int32_t* A_index, double* grad_A, int32_t refine_steps,

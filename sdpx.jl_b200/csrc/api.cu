@@ -2591,6 +2591,7 @@ struct Handle {
   // (hi, lo) of stacked K-vectors and m-vectors.
   DBuf<double> ddXi_h, ddXi_l, ddT_h, ddT_l, ddU_h, ddU_l, ddV_h, ddV_l, ddD_h, ddD_l;
   DBuf<double> ddp_h, ddp_l, ddw_h, ddw_l, ddlam_h, ddlam_l, ddu_h, ddu_l, ddlb_h, ddlb_l;
+  DBuf<double> ddcg_ph, ddcg_pl, ddcg_qh, ddcg_ql;  // conjugate-gradient directions
   void dd_prepare_inverse();
   void dd_xinv_m_y(const double* Mh, const double* Ml, double* Zh, double* Zl);
   void dd_schur_apply(const double* vh, const double* vl, double* oh, double* ol);

@@ -146,6 +146,32 @@ __global__ void k_dd_diag_mul(int nd, long long od, const double* ah, const doub
   dd_store(ch, cl, od + j, dd_mul(dd_load(ah, al, od + j), dd_load(bh, bl, od + j)));
 }
 
+// ⟨a, b⟩ in double-double (a, b double-double vectors; a null low half reads
+// as 0), one CTA of 1024 threads; out[0], out[1] = hi, lo.
+__global__ void __launch_bounds__(1024) k_dd_dot(long long n, const double* ah, const double* al,
+                                                 const double* bh, const double* bl,
+                                                 double* out) {
+  __shared__ double red[64];
+  ddv s{0.0, 0.0};
+  for (long long i = threadIdx.x; i < n; i += blockDim.x)
+    s = dd_add(s, dd_mul(dd_load(ah, al, i), dd_load(bh, bl, i)));
+  for (int o = 16; o > 0; o >>= 1) s = dd_add(s, dd_shfl_xor(s, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[2 * w] = s.hi;
+    red[2 * w + 1] = s.lo;
+  }
+  __syncthreads();
+  if (w == 0) {
+    ddv t = lane < (int)(blockDim.x >> 5) ? ddv{red[2 * lane], red[2 * lane + 1]} : ddv{0.0, 0.0};
+    for (int o = 16; o > 0; o >>= 1) t = dd_add(t, dd_shfl_xor(t, o));
+    if (lane == 0) {
+      out[0] = t.hi;
+      out[1] = t.lo;
+    }
+  }
+}
+
 }  // namespace
 
 void dd_gemv_n(const double* A, long long K, int m, const double* vh, const double* vl,
@@ -207,6 +233,12 @@ void dd_diag_mul(int nd, long long od, const double* ah, const double* al, const
                  const double* bl, double* ch, double* cl, cudaStream_t st) {
   if (nd == 0) return;
   k_dd_diag_mul<<<ceil_div(nd, 256), 256, 0, st>>>(nd, od, ah, al, bh, bl, ch, cl);
+  SDPX_LAUNCH_CHECK();
+}
+
+void dd_dot(long long n, const double* ah, const double* al, const double* bh, const double* bl,
+            double* out, cudaStream_t st) {
+  k_dd_dot<<<1, 1024, 0, st>>>(n, ah, al, bh, bl, out);
   SDPX_LAUNCH_CHECK();
 }
 

@@ -21,6 +21,9 @@ void dd_gemm_blocks(const long long* doff, const int* dk, int nb, int kmax, cons
 // C = sa·A + sb·B elementwise (n entries; B may be NULL).
 void dd_axpby(long long n, double sa, const double* ah, const double* al, double sb,
               const double* bh, const double* bl, double* ch, double* cl, cudaStream_t st);
+// out[0], out[1] = ⟨a, b⟩ in double-double (device); null low halves read as 0.
+void dd_dot(long long n, const double* ah, const double* al, const double* bh, const double* bl,
+            double* out, cudaStream_t st);
 // C_b = I − A_b per dense block.
 void dd_eye_minus_blocks(const long long* doff, const int* dk, int nb, int kmax, const double* ah,
                          const double* al, double* ch, double* cl, cudaStream_t st);

@@ -211,11 +211,12 @@ def test_refined_adjoint_at_a_solution_matches_double_double(cuda):
 
 def test_refined_adjoint_residual_never_grows(cuda):
     """On the differentiable-SDP shape at 1e-9 solutions the double-double
-    refinement keeps its best λ: more steps never leave a larger residual."""
+    conjugate gradients never return a larger residual than the FP64 solve,
+    and 32 steps reach double-double accuracy."""
     from sdpx_b200 import SolverOptions
     from sdpx_b200.cuda_backend import CudaBackend
     opts = SolverOptions(scaling="none").with_tolerance(1e-9)
-    tested = 0
+    tested = reached = 0
     for inst in range(8):
         prob = G.sdpa_dense(m=500, blocks=[200], lp=0, seed=1000 + inst)
         rng = np.random.default_rng(inst)
@@ -229,8 +230,9 @@ def test_refined_adjoint_residual_never_grows(cuda):
             if not cb.factorize()["ok"]:
                 continue
             res = [cb.adjoint_refined(v, None, None, (0,), steps=s)["residual"]
-                   for s in (0, 3, 16)]
+                   for s in (0, 3, 32)]
         tested += 1
         assert all(np.isfinite(res)), res
-        assert res[1] <= res[0] and res[2] <= res[1], res
-    assert tested >= 4
+        assert res[1] <= res[0] and res[2] <= res[0], res
+        reached += res[2] <= 1e-20
+    assert tested >= 4 and reached >= tested - 1
