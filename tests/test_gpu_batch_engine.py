@@ -240,3 +240,26 @@ def test_eigenvalue_step_bounds_match_the_bisection(cuda_ok):
             rel(a.pObj, b.pObj) > 1e-7]
     assert len(diff) <= 1, diff
     assert sum(r.status.value == "Optimal" for r in eig) >= len(probs) - 1
+
+
+def test_batched_engine_at_its_size_limits(cuda_ok):
+    """The smallest and largest instances the engine takes (k = 3 with m = 1,
+    k = 64 with m = 256) mixed with ordinary ones, in both precisions, against
+    single-instance solves with the same options."""
+    from sdpx_b200 import generators as G, solve
+    from sdpx_b200.batch import BATCH_OPTIONS, BatchSolver, batch_options
+    probs = [G.sdpa_dense(m=1, blocks=[3], lp=0, seed=31),
+             G.sdpa_dense(m=256, blocks=[64], lp=0, seed=32),
+             G.sdpa_dense(m=6, blocks=[3], lp=0, seed=33),
+             G.sdpa_dense(m=200, blocks=[64], lp=0, seed=34)] + batch_instances(8, seed=35)
+    opts = batch_options(1e-8)
+    with BatchSolver(probs) as bs:
+        res = bs.optimize(opts)
+        dd = bs.optimize(batch_options(1e-10, precision="float64x2"), solutions=False)
+    for p, rb in zip(probs, res):
+        rs = solve(p, tolerance=1e-8, **BATCH_OPTIONS)
+        assert rb.status == rs.status, (p.k, p.m, rb.message, rs.message)
+        assert abs(rb.iterations - rs.iterations) <= 2
+        assert rel(rb.pObj, rs.pObj) <= 1e-7 and rel(rb.dObj, rs.dObj) <= 1e-7
+    assert all(r.status.value == "Optimal" for r in res)
+    assert all(r.status.value == "Optimal" and r.relative_gap <= 1e-10 for r in dd)
