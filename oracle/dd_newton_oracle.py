@@ -9,7 +9,7 @@ provider, ext/SDPXMultiFloatLinearAlgebraExt.jl:743-778):
 
 * residuals P = 𝒜x − X − C, d = c − 𝒜ᵀY, R = −XY (+μI) (src/step.jl:25-72);
 * X⁻¹ from the FP64 inverse by three Newton–Schulz steps Z ← sym(Z + Z(I − XZ));
-* S_ij = ⟨A_i, X⁻¹A_jY⟩, symmetrised (src/schur.jl:511-562 in the HKM form);
+* S_ij = ⟨A_i, X⁻¹A_jY⟩ for i ≥ j, mirrored (src/schur.jl:511-562 in the HKM form);
 * Cholesky of S with the regularisation retries of src/kkt.jl:1419-1445;
 * right-hand sides, corrector targets, direction blocks (src/step.jl:95-108,
   src/kernels/threaded.jl:574-663, 837-1067), the refinement residual
@@ -124,7 +124,9 @@ class DDNewtonBackend(O.OracleBackend):
         cols = [dd_matmul(dd_matmul(self.Xi, DD(self.Av[0][j].reshape(k, k, order="F"))), Yd)
                 .reshape(-1, order="F") for j in range(m)]
         G = DD(np.stack([g.hi for g in cols], 1), np.stack([g.lo for g in cols], 1))
-        self.Sdd = _sym(dd_matmul(DD(self.Av[0]), G))
+        full = dd_matmul(DD(self.Av[0]), G)           # S_ij = ⟨A_i, G_j⟩; the lower part
+        lo_h, lo_l = np.tril(full.hi), np.tril(full.lo)  # is kept and mirrored
+        self.Sdd = DD(lo_h + np.tril(lo_h, -1).T, lo_l + np.tril(lo_l, -1).T)
         self.S = np.tril(self.Sdd.to_float())
         return self.S
 

@@ -4,7 +4,7 @@
 // The iterate (x, X, Y) stays in FP64; the Newton system is formed and solved
 // in double-double: the block residuals P = 𝒜x − X − C, d = c − 𝒜ᵀY and
 // R = −XY (+μI), X⁻¹ refined from the FP64 inverse by Newton–Schulz steps
-// Z ← Z + Z(I − XZ), the Schur matrix S_ij = ⟨A_i, X⁻¹A_jY⟩ (symmetrised),
+// Z ← Z + Z(I − XZ), the Schur matrix S_ij = ⟨A_i, X⁻¹A_jY⟩ (i ≥ j, mirrored),
 // its Cholesky factor with the regularisation retries of the FP64 path, the
 // right-hand sides, the solves and refinement residuals ρ = r − S·dx, and the
 // direction blocks dX = 𝒜dx + P, dY = sym(X⁻¹(R − dX·Y)), rounded to FP64 for
@@ -180,9 +180,8 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // D3: the Schur columns j ∈ [lo, hi) of one work item: G_j = X⁻¹·A_j·Y
-// (double-double X⁻¹, FP64 A_j and Y) into the panel, then
-// S(i, j) = ⟨A_i, G_j⟩ for every i (one warp per i).  S is left
-// unsymmetrised; k_dd_factor symmetrises it.
+// (double-double X⁻¹, FP64 A_j and Y) into the panel, then the lower part
+// S(i, j) = ⟨A_i, G_j⟩, i ≥ j (one warp per i); k_dd_factor mirrors it.
 __global__ void k_dd_schur(Pool pool, const int* act, const int4* work) {
   const int4 wi = work[blockIdx.x];
   const Inst I = pool.inst[act[wi.x]];
@@ -222,7 +221,7 @@ __global__ void k_dd_schur(Pool pool, const int* act, const int4* work) {
       Gl[(long long)j * kk + e] = s.lo;
     }
     __syncthreads();
-    for (int i = warp; i < m; i += nw) {  // S(i, j) = ⟨A_i, G_j⟩
+    for (int i = j + warp; i < m; i += nw) {  // S(i, j) = ⟨A_i, G_j⟩, i ≥ j
       ddv s{0.0, 0.0};
       for (long long e = lane; e < kk; e += 32)
         s = dd_fma_d(s, {Gh[(long long)j * kk + e], Gl[(long long)j * kk + e]},
@@ -234,7 +233,7 @@ __global__ void k_dd_schur(Pool pool, const int* act, const int4* work) {
   }
 }
 
-// D4: S ← sym(S), then the double-double Cholesky of S with ≤ 6
+// D4: S's upper triangle ← its lower one, then the double-double Cholesky of S with ≤ 6
 // regularisation retries S_ii += δ·max(|S_ii|, 1), δ = √eps then ×10 (as the
 // FP64 path, src/kkt.jl:1419-1445); quality = min/max |L_jj|.
 __global__ void __launch_bounds__(kThreads)
@@ -246,22 +245,12 @@ __global__ void __launch_bounds__(kThreads)
   double* Lh = pool.LS + I.mm_off;
   double* Ll = pool.LSl + I.mm_off;
   const long long mm = (long long)m * m;
-  for (long long e = threadIdx.x; e < mm; e += blockDim.x) {  // lower ← (S + Sᵀ)/2
+  for (long long e = threadIdx.x; e < mm; e += blockDim.x) {  // upper ← lower
     const int r = (int)(e % m), c = (int)(e / m);
-    if (r > c) {
+    if (r < c) {
       const long long t = c + (long long)r * m;
-      const ddv s = dd_mul_d(dd_add({Sh[e], Sl[e]}, {Sh[t], Sl[t]}), 0.5);
-      Lh[e] = s.hi;  // staged in L: S's upper half is still being read
-      Ll[e] = s.lo;
-    }
-  }
-  __syncthreads();
-  for (long long e = threadIdx.x; e < mm; e += blockDim.x) {
-    const int r = (int)(e % m), c = (int)(e / m);
-    if (r > c) {
-      const long long t = c + (long long)r * m;
-      Sh[e] = Sh[t] = Lh[e];
-      Sl[e] = Sl[t] = Ll[e];
+      Sh[e] = Sh[t];
+      Sl[e] = Sl[t];
     }
   }
   __syncthreads();
