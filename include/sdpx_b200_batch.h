@@ -107,7 +107,8 @@ int sdpx_b200_batch_set_step_bounds(sdpx_b200_batch* b, int32_t mode);
 
 /* Launch shape of the Schur phase: threads per CTA (128, 256 or 512), the
  * SYRK tile (16 or 32; 512 threads need 32; tile 64 with 128 threads selects
- * the FP64 tensor-core (DMMA) products) and the Schur work per CTA in
+ * the FP64 tensor-core (DMMA) products, which tile each instance by 32 or 64
+ * as its k and m need) and the Schur work per CTA in
  * FLOPs (an instance's panel and SYRK are split over ceil(work / grain) CTAs;
  * grain ≤ 0: one CTA per instance). */
 int sdpx_b200_batch_set_schur_shape(sdpx_b200_batch* b, int32_t threads, int32_t tile,

@@ -252,15 +252,20 @@ __global__ void __launch_bounds__(NT) k_b_syrk(Pool pool, const int* act, const 
 
 // ---- B2 on the FP64 tensor cores (DMMA m8n8k4 tiles of gemm_f64.cuh) -----
 // Per instance P̂_j = W·A_j·L_Y (W = L_X⁻¹) for every constraint, then
-// S = P̂·P̂ᵀ over the lower 64×64 tiles (both triangles written); 4 warps per
-// CTA, work items {row, first, end} as for the scalar kernels.
+// S = P̂·P̂ᵀ over the lower tiles (both triangles written); 4 warps per CTA,
+// work items {row, first, end} as for the scalar kernels.  Each instance takes
+// the tile that pads least: 32×32 for T·P̂ when k ≤ 32 and for the SYRK when
+// m ≤ 64, else 64×64.
 using DmmaCfgKN = F64Cfg<64, 64, 2, 2, false, true>;  // A MN-contiguous, B K-contiguous
 using DmmaCfgKK = F64Cfg<64, 64, 2, 2, true, true>;   // both K-contiguous
+using DmmaCfgKN32 = F64Cfg<32, 32, 2, 2, false, true>;  // 32×32 tiles for small instances
+using DmmaCfgKK32 = F64Cfg<32, 32, 2, 2, true, true>;
 
 // T and P̂ fused per constraint: work item {row, first j, end j}; T_j = W·A_j
 // goes to this CTA's k×k scratch (pool.T + blockIdx.x·kq, reused for every j,
 // so it stays in L2), then P̂_j = T_j·L_Y.
-__global__ void __launch_bounds__(DmmaCfgKN::NT)
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT)
     k_b_dmma_tp(Pool pool, const int* act, const int4* work) {
   extern __shared__ __align__(16) double smem[];
   const int4 wi = work[blockIdx.x];
@@ -273,24 +278,25 @@ __global__ void __launch_bounds__(DmmaCfgKN::NT)
   const Opnd Bl{pool.LY + I.kk_off, 1, k, 0, 1 << 30, k, k};    // (q, c) at q + c·k
   for (int j = wi.y; j < wi.z; ++j) {
     const Opnd Bj{pool.A + I.a_off + (long long)j * kk, 1, k, 0, 1 << 30, k, k};  // (p, c)
-    double acc[DmmaCfgKN::FM][DmmaCfgKN::FN][2];
-    zero_acc<DmmaCfgKN>(acc);
-    f64_tile_mainloop<DmmaCfgKN>(acc, Aw, Bj, 0, 0, 0, k, smem);
-    for_each_acc<DmmaCfgKN>(acc, [&](int r, int c, double v) {
+    double acc[Cfg::FM][Cfg::FN][2];
+    zero_acc<Cfg>(acc);
+    f64_tile_mainloop<Cfg>(acc, Aw, Bj, 0, 0, 0, k, smem);
+    for_each_acc<Cfg>(acc, [&](int r, int c, double v) {
       if (r < k && c < k) T[r + (long long)c * k] = v;
     });
     __syncthreads();
-    zero_acc<DmmaCfgKN>(acc);
-    f64_tile_mainloop<DmmaCfgKN>(acc, At, Bl, 0, 0, 0, k, smem);
+    zero_acc<Cfg>(acc);
+    f64_tile_mainloop<Cfg>(acc, At, Bl, 0, 0, 0, k, smem);
     double* Pj = pool.Ph + I.a_off + (long long)j * kk;
-    for_each_acc<DmmaCfgKN>(acc, [&](int r, int c, double v) {
+    for_each_acc<Cfg>(acc, [&](int r, int c, double v) {
       if (r < k && c < k) Pj[r + (long long)c * k] = v;
     });
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(DmmaCfgKK::NT)
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT)
     k_b_dmma_syrk(Pool pool, const int* act, const int4* work) {
   extern __shared__ __align__(16) double smem[];
   const int4 wi = work[blockIdx.x];
@@ -302,11 +308,11 @@ __global__ void __launch_bounds__(DmmaCfgKK::NT)
   double* S = pool.S + I.mm_off;
   for (int q = wi.y; q < wi.z; ++q) {
     const int ti = tri_row(q), tj = q - ti * (ti + 1) / 2;
-    double acc[DmmaCfgKK::FM][DmmaCfgKK::FN][2];
-    zero_acc<DmmaCfgKK>(acc);
-    f64_tile_mainloop<DmmaCfgKK>(acc, Pp, Pp, ti * 64, tj * 64, 0, kk, smem);
-    for_each_acc<DmmaCfgKK>(acc, [&](int r, int c, double v) {
-      const int gi = ti * 64 + r, gj = tj * 64 + c;
+    double acc[Cfg::FM][Cfg::FN][2];
+    zero_acc<Cfg>(acc);
+    f64_tile_mainloop<Cfg>(acc, Pp, Pp, ti * Cfg::BM, tj * Cfg::BM, 0, kk, smem);
+    for_each_acc<Cfg>(acc, [&](int r, int c, double v) {
+      const int gi = ti * Cfg::BM + r, gj = tj * Cfg::BM + c;
       if (gi < m && gj < m && gi >= gj) {
         S[gi + (long long)gj * m] = v;
         S[gj + (long long)gi * m] = v;
@@ -1281,9 +1287,11 @@ struct Engine {
     const int n = (int)ids.size();
     if (n == 0) return;
     if (!dmma_attrs) {
-      SDPX_CUDA(cudaFuncSetAttribute(k_b_dmma_tp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      SDPX_CUDA(cudaFuncSetAttribute(k_b_dmma_tp<DmmaCfgKN>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)DmmaCfgKN::SMEM_BYTES));
-      SDPX_CUDA(cudaFuncSetAttribute(k_b_dmma_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      SDPX_CUDA(cudaFuncSetAttribute(k_b_dmma_syrk<DmmaCfgKK>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)DmmaCfgKK::SMEM_BYTES));
       dmma_attrs = true;
     }
@@ -1296,7 +1304,9 @@ struct Engine {
       return 4.0 * I.k * I.k * I.k * I.m + (double)I.k * I.k * I.m * I.m;
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
-    std::vector<int4> w1, w3;
+    // Per instance the tile that pads least: 32 for T·P̂ when k ≤ 32 (one k×k
+    // tile per constraint) and for the SYRK when m ≤ 64, else 64.
+    std::vector<int4> tp64, tp32, sy64, sy32;
     auto split = [&](std::vector<int4>& w, int q, int units, double flops) {
       int parts = g > 0 ? (int)std::ceil(flops / g) : 1;
       parts = std::max(1, std::min(parts, units));
@@ -1307,32 +1317,60 @@ struct Engine {
     for (int q = 0; q < n; ++q) ha[q] = ids[q];
     for (int q : order) {
       const Inst& I = inst[ids[q]];
-      const int nt = (I.m + 63) / 64, tri = nt * (nt + 1) / 2;
-      split(w1, q, I.m, 4.0 * I.k * I.k * I.k * I.m);  // constraint ranges
-      split(w3, q, tri, (double)I.k * I.k * I.m * I.m);
+      split(I.k <= 32 ? tp32 : tp64, q, I.m, 4.0 * I.k * I.k * I.k * I.m);
+      const int T = I.m <= 64 ? 32 : 64;
+      const int nt = (I.m + T - 1) / T, tri = nt * (nt + 1) / 2;
+      split(T == 32 ? sy32 : sy64, q, tri, (double)I.k * I.k * I.m * I.m);
       schur_flops += 2.0 * I.k * I.k * I.k * I.m + (double)I.k * I.k * I.m * I.m;
     }
-    if (Tbuf.n < w1.size() * (size_t)pool.kq) {
-      Tbuf.alloc(w1.size() * (size_t)pool.kq + w1.size() * (size_t)pool.kq / 4);
+    const size_t ntp = tp64.size() + tp32.size();
+    if (Tbuf.n < ntp * (size_t)pool.kq) {
+      Tbuf.alloc(ntp * (size_t)pool.kq + ntp * (size_t)pool.kq / 4);
       pool.T = Tbuf.p;
     }
-    const size_t nw = w1.size() + w3.size();
+    const size_t nw = ntp + sy64.size() + sy32.size();
     if (d_work.n < nw) d_work.alloc(nw + nw / 4);
     h_work.ensure(nw * sizeof(int4));
     int4* hw = static_cast<int4*>(h_work.p);
-    std::copy(w1.begin(), w1.end(), hw);
-    std::copy(w3.begin(), w3.end(), hw + w1.size());
+    size_t o = 0;
+    for (auto* w : {&tp64, &tp32, &sy64, &sy32}) {
+      std::copy(w->begin(), w->end(), hw + o);
+      o += w->size();
+    }
     SDPX_CUDA(cudaMemcpyAsync(d_act.p, ha, n * sizeof(int), cudaMemcpyHostToDevice, st));
     SDPX_CUDA(cudaMemcpyAsync(d_work.p, hw, nw * sizeof(int4), cudaMemcpyHostToDevice, st));
     SDPX_CUDA(cudaEventRecord(ev[0], st));
-    k_b_dmma_tp<<<(int)w1.size(), DmmaCfgKN::NT, DmmaCfgKN::SMEM_BYTES, st>>>(pool, d_act.p,
-                                                                             d_work.p);
-    SDPX_LAUNCH_CHECK();
-    k_b_dmma_syrk<<<(int)w3.size(), DmmaCfgKK::NT, DmmaCfgKK::SMEM_BYTES, st>>>(
-        pool, d_act.p, d_work.p + w1.size());
-    SDPX_LAUNCH_CHECK();
+    // The T·P̂ kernels index their scratch by blockIdx.x: the 32-tile launch
+    // takes the slots after the 64-tile one's.
+    Pool p32 = pool;
+    p32.T = pool.T + (long long)tp64.size() * pool.kq;
+    const int4* w = d_work.p;
+    if (!tp64.empty()) {
+      k_b_dmma_tp<DmmaCfgKN><<<(int)tp64.size(), DmmaCfgKN::NT, DmmaCfgKN::SMEM_BYTES, st>>>(
+          pool, d_act.p, w);
+      SDPX_LAUNCH_CHECK();
+    }
+    w += tp64.size();
+    if (!tp32.empty()) {
+      k_b_dmma_tp<DmmaCfgKN32><<<(int)tp32.size(), DmmaCfgKN32::NT, DmmaCfgKN32::SMEM_BYTES,
+                                 st>>>(p32, d_act.p, w);
+      SDPX_LAUNCH_CHECK();
+    }
+    w += tp32.size();
+    if (!sy64.empty()) {
+      k_b_dmma_syrk<DmmaCfgKK><<<(int)sy64.size(), DmmaCfgKK::NT, DmmaCfgKK::SMEM_BYTES, st>>>(
+          pool, d_act.p, w);
+      SDPX_LAUNCH_CHECK();
+    }
+    w += sy64.size();
+    if (!sy32.empty()) {
+      k_b_dmma_syrk<DmmaCfgKK32><<<(int)sy32.size(), DmmaCfgKK32::NT, DmmaCfgKK32::SMEM_BYTES,
+                                   st>>>(pool, d_act.p, w);
+      SDPX_LAUNCH_CHECK();
+    }
     SDPX_CUDA(cudaEventRecord(ev[1], st));
-    launches += 2;
+    launches += (tp64.empty() ? 0 : 1) + (tp32.empty() ? 0 : 1) + (sy64.empty() ? 0 : 1) +
+                (sy32.empty() ? 0 : 1);
     SDPX_CUDA(cudaEventSynchronize(ev[1]));
     float ms = 0;
     SDPX_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
