@@ -144,6 +144,23 @@ struct Handle {
     fold_sym(Kt, z, ap_lo.p, ap_up.p, kt_fold.p, st);
     gemv_t(Ap.p, Kt, m, kt_fold.p, alpha, base, beta, out, st);
   }
+  // The residuals P = 𝒜x − X − C and d = c − 𝒜ᵀY with every entry rounded
+  // once from compensated (Dot2) sums: near convergence they sit at the
+  // rounding floor, where the controller's centring test compares them, and
+  // this makes them independent of the device's summation order.
+  void primal_residual(const double* xv, double* out) {
+    if (!use_packed)
+      return gemv_n_acc(A.p, K, m, xv, X.p, Cst.p, out, gemv_part.p, gemv_chunks, st);
+    ensure_packed();
+    gemv_n_sym_acc(Ap.p, Kt, m, xv, ap_lo.p, ap_up.p, X.p, Cst.p, out, gemv_part.p, gemv_chunks,
+                   st);
+  }
+  void dual_residual(const double* Yv, double* out) {
+    if (!use_packed) return gemv_t_acc(A.p, K, m, Yv, -1.0, c.p, 1.0, out, st);
+    ensure_packed();
+    fold_sym(Kt, Yv, ap_lo.p, ap_up.p, kt_fold.p, st);
+    gemv_t_acc(Ap.p, Kt, m, kt_fold.p, -1.0, c.p, 1.0, out, st);
+  }
   void ensure_packed() {
     if (ap_ver == a_ver) return;
     pack_rows(A.p, K, m, ap_lo.p, Kt, Ap.p, st);
@@ -586,7 +603,7 @@ struct Handle {
     oz_err.alloc(1);
     oz_err.zero(st);
     gemv_chunks = std::max(1, std::min(16, m / 64));
-    gemv_part.alloc((size_t)gemv_chunks * std::max<long long>(K, m));
+    gemv_part.alloc((size_t)2 * gemv_chunks * std::max<long long>(K, m));  // Dot2 partials: 2×
     {
       std::vector<long long> lo, up;
       for (auto& b : dense)
@@ -932,11 +949,8 @@ struct Handle {
   void residuals(const double* mu, int use_affine, int factor, double* p_res, double* d_res,
                  int* ok) {
     PhaseScope ps(this, 0);
-    // P = 𝒜x − X − C
-    amul(x.p, tmpK.p);
-    axpbypcz(K, 1.0, tmpK.p, -1.0, X.p, -1.0, Cst.p, P.p, st);
-    // d = c − 𝒜ᵀ vec(Y)
-    atmul(Y.p, -1.0, c.p, 1.0, d.p);
+    primal_residual(x.p, P.p);  // P = 𝒜x − X − C
+    dual_residual(Y.p, d.p);    // d = c − 𝒜ᵀ vec(Y)
     clear_red(0, 3);
     if (n_eq) {
       // d −= B·y, p = b − Bᵀx (src/step.jl:41-51)
@@ -2088,9 +2102,8 @@ struct Handle {
     *dobj = dd;
   }
   void solution_residuals(double* pr, double* dr) {
-    amul(x.p, tmpK.p);
-    axpbypcz(K, 1.0, tmpK.p, -1.0, X.p, -1.0, Cst.p, tmpK2.p, st);
-    atmul(Y.p, -1.0, c.p, 1.0, work_m.p);
+    primal_residual(x.p, tmpK2.p);
+    dual_residual(Y.p, work_m.p);
     clear_red(0, 3);
     if (n_eq) {
       gemv_n(Beq.p, m, n_eq, yv.p, eq_tm.p, gemv_part.p, gemv_chunks, st);

@@ -5,8 +5,9 @@
 // TwoSum, Dekker's FastTwoSum, the exact product a·b = p + e with
 // e = fma(a, b, −p) — and the double-double sum and product of Hida, Li and
 // Bailey's QD library (accurate addition: both halves summed with TwoSum).
-// None of them contains a multiply that the compiler could contract into the
-// sums, so the results do not depend on FMA contraction.
+// The product's rounded part is an explicit __dmul_rn, so the compiler cannot
+// contract it into a following sum and the results do not depend on FMA
+// contraction.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -26,7 +27,7 @@ __device__ __forceinline__ ddv dd_fast_two_sum(double a, double b) {
   return {s, b - (s - a)};
 }
 __device__ __forceinline__ ddv dd_two_prod(double a, double b) {
-  const double p = a * b;
+  const double p = __dmul_rn(a, b);  // never contracted into a following sum
   return {p, __fma_rn(a, b, -p)};
 }
 __device__ __forceinline__ ddv dd_add(ddv a, ddv b) {

@@ -1,6 +1,7 @@
 // Memory-bound kernels over the stacked constraint matrix 𝒜 (K×m, column i =
 // vec(A_i) of every block, 1×1 blocks gathered at the end) and over stacked
 // block vectors (length K, same row offsets as 𝒜).
+#include "dd.cuh"
 #include "vec_kernels.h"
 
 namespace sdpx {
@@ -203,6 +204,207 @@ void gemv_t(const double* A, long long K, int m, const double* z, double alpha, 
     k_gemv_t2<<<m, 512, 0, st>>>(A, K, m, z, alpha, base, beta, out);
   else
     k_gemv_t<<<m, 512, 0, st>>>(A, K, m, z, alpha, base, beta, out);
+  SDPX_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------ compensated residuals ---
+// Dot2 of Ogita, Rump and Oishi ("Accurate sum and dot product", SIAM J. Sci.
+// Comput. 26(6), 2005): every term enters as its exact product p + e (FMA),
+// the running sum is advanced by TwoSum and the rounding errors (TwoSum's and
+// the products') collect in a second accumulator; partial accumulators merge
+// by TwoSum the same way, and the result s + c is rounded once.  The value is
+// as accurate as if computed in twice the working precision, so it does not
+// depend on the order of the terms.
+struct Dot2 {
+  double s, c;
+};
+__device__ __forceinline__ void dot2_fma(Dot2& a, double x, double y) {
+  const ddv p = dd_two_prod(x, y);
+  const ddv t = dd_two_sum(a.s, p.hi);
+  a.s = t.hi;
+  a.c += t.lo + p.lo;
+}
+__device__ __forceinline__ void dot2_add(Dot2& a, double v) {
+  const ddv t = dd_two_sum(a.s, v);
+  a.s = t.hi;
+  a.c += t.lo;
+}
+__device__ __forceinline__ void dot2_merge(Dot2& a, const Dot2& b) {
+  const ddv t = dd_two_sum(a.s, b.s);
+  a.s = t.hi;
+  a.c += t.lo + b.c;
+}
+
+// Partials of 𝒜·x over `chunks` column ranges as Dot2 pairs: sums at
+// part[ch·K + row], error terms at part[(chunks + ch)·K + row]; 128-bit loads
+// of the row pair (2q, 2q+1) when K is even and A 16-byte aligned.
+__global__ void k_gemv_n_part2_acc(const double* __restrict__ A, long long K, int m,
+                                   const double* __restrict__ x, int chunks,
+                                   double* __restrict__ part) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long K2 = K >> 1;
+  if (q >= K2) return;
+  const int ch = blockIdx.y;
+  const int per = (m + chunks - 1) / chunks;
+  const int i0 = ch * per, i1 = min(m, i0 + per);
+  const double2* p = reinterpret_cast<const double2*>(A) + q;
+  Dot2 a0{0, 0}, a1{0, 0}, b0{0, 0}, b1{0, 0};
+  int i = i0;
+  for (; i + 1 < i1; i += 2) {
+    const double2 u = __ldg(p + (long long)i * K2), v = __ldg(p + (long long)(i + 1) * K2);
+    const double x0 = x[i], x1 = x[i + 1];
+    dot2_fma(a0, u.x, x0);
+    dot2_fma(b0, u.y, x0);
+    dot2_fma(a1, v.x, x1);
+    dot2_fma(b1, v.y, x1);
+  }
+  if (i < i1) {
+    const double2 u = __ldg(p + (long long)i * K2);
+    dot2_fma(a0, u.x, x[i]);
+    dot2_fma(b0, u.y, x[i]);
+  }
+  dot2_merge(a0, a1);
+  dot2_merge(b0, b1);
+  reinterpret_cast<double2*>(part + (long long)ch * K)[q] = make_double2(a0.s, b0.s);
+  reinterpret_cast<double2*>(part + (long long)(chunks + ch) * K)[q] = make_double2(a0.c, b0.c);
+}
+__global__ void k_gemv_n_part_acc(const double* __restrict__ A, long long K, int m,
+                                  const double* __restrict__ x, int chunks,
+                                  double* __restrict__ part) {
+  const long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (row >= K) return;
+  const int ch = blockIdx.y;
+  const int per = (m + chunks - 1) / chunks;
+  const int i0 = ch * per, i1 = min(m, i0 + per);
+  Dot2 a0{0, 0}, a1{0, 0};
+  int i = i0;
+  for (; i + 1 < i1; i += 2) {
+    dot2_fma(a0, A[row + (long long)i * K], x[i]);
+    dot2_fma(a1, A[row + (long long)(i + 1) * K], x[i + 1]);
+  }
+  if (i < i1) dot2_fma(a0, A[row + (long long)i * K], x[i]);
+  dot2_merge(a0, a1);
+  part[(long long)ch * K + row] = a0.s;
+  part[(long long)(chunks + ch) * K + row] = a0.c;
+}
+
+// out[r] = Σ_chunks partials − X[r] − C[r] (X, C may be null), rounded once;
+// with lo/up (packed rows) the row's value goes to both stacked positions.
+__global__ void k_gemv_n_reduce_acc(const double* __restrict__ part, long long K, int chunks,
+                                    const double* __restrict__ X, const double* __restrict__ C,
+                                    const long long* __restrict__ lo,
+                                    const long long* __restrict__ up, double* __restrict__ out) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= K) return;
+  Dot2 a{0, 0};
+  for (int c = 0; c < chunks; ++c)
+    dot2_merge(a, Dot2{part[(long long)c * K + q], part[(long long)(chunks + c) * K + q]});
+  const long long r0 = lo ? lo[q] : q, r1 = up ? up[q] : q;
+  Dot2 b = a;
+  if (X) dot2_add(a, -X[r0]);
+  if (C) dot2_add(a, -C[r0]);
+  out[r0] = a.s + a.c;
+  if (r1 != r0) {
+    if (X) dot2_add(b, -X[r1]);
+    if (C) dot2_add(b, -C[r1]);
+    out[r1] = b.s + b.c;
+  }
+}
+
+static void gemv_n_partials_acc(const double* A, long long K, int m, const double* x, int chunks,
+                                double* part, cudaStream_t st) {
+  if ((K & 1) == 0 && aligned16(A) && aligned16(part)) {
+    dim3 g(ceil_div(K / 2, 256), chunks);
+    k_gemv_n_part2_acc<<<g, 256, 0, st>>>(A, K, m, x, chunks, part);
+  } else {
+    dim3 g(ceil_div(K, 256), chunks);
+    k_gemv_n_part_acc<<<g, 256, 0, st>>>(A, K, m, x, chunks, part);
+  }
+}
+
+void gemv_n_acc(const double* A, long long K, int m, const double* x, const double* X,
+                const double* C, double* out, double* part, int chunks, cudaStream_t st) {
+  if (K == 0) return;
+  gemv_n_partials_acc(A, K, m, x, chunks, part, st);
+  k_gemv_n_reduce_acc<<<ceil_div(K, 256), 256, 0, st>>>(part, K, chunks, X, C, nullptr, nullptr,
+                                                         out);
+  SDPX_LAUNCH_CHECK_N(2);
+}
+
+void gemv_n_sym_acc(const double* Ap, long long Kt, int m, const double* x, const long long* lo,
+                    const long long* up, const double* X, const double* C, double* out,
+                    double* part, int chunks, cudaStream_t st) {
+  if (Kt == 0) return;
+  gemv_n_partials_acc(Ap, Kt, m, x, chunks, part, st);
+  k_gemv_n_reduce_acc<<<ceil_div(Kt, 256), 256, 0, st>>>(part, Kt, chunks, X, C, lo, up, out);
+  SDPX_LAUNCH_CHECK_N(2);
+}
+
+// Block-wide merge of the Dot2 pairs (every thread receives the total).
+__device__ __forceinline__ Dot2 block_dot2(Dot2 a, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const Dot2 b{__shfl_xor_sync(0xffffffffu, a.s, o), __shfl_xor_sync(0xffffffffu, a.c, o)};
+    dot2_merge(a, b);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    red[w] = a.s;
+    red[32 + w] = a.c;
+  }
+  __syncthreads();
+  if (w == 0) {
+    a = lane < nw ? Dot2{red[lane], red[32 + lane]} : Dot2{0, 0};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const Dot2 b{__shfl_xor_sync(0xffffffffu, a.s, o), __shfl_xor_sync(0xffffffffu, a.c, o)};
+      dot2_merge(a, b);
+    }
+  }
+  return a;  // valid in thread 0
+}
+
+// out[i] = alpha·(A[:,i]·z) + beta·base[i] from one double-double value,
+// rounded once (one CTA per column; 128-bit loads when K is even and A, z
+// are 16-byte aligned).
+template <bool VEC>
+__global__ void k_gemv_t_acc(const double* __restrict__ A, long long K, int m,
+                             const double* __restrict__ z, double alpha,
+                             const double* __restrict__ base, double beta,
+                             double* __restrict__ out) {
+  __shared__ double red[64];
+  const int i = blockIdx.x;
+  Dot2 a0{0, 0}, a1{0, 0};
+  if (VEC) {
+    const long long K2 = K >> 1;
+    const double2* col = reinterpret_cast<const double2*>(A + (long long)i * K);
+    const double2* z2 = reinterpret_cast<const double2*>(z);
+    for (long long r = threadIdx.x; r < K2; r += blockDim.x) {
+      const double2 u = __ldg(col + r), v = __ldg(z2 + r);
+      dot2_fma(a0, u.x, v.x);
+      dot2_fma(a1, u.y, v.y);
+    }
+  } else {
+    const double* col = A + (long long)i * K;
+    for (long long r = threadIdx.x; r < K; r += blockDim.x) dot2_fma(a0, col[r], z[r]);
+  }
+  dot2_merge(a0, a1);
+  const Dot2 t = block_dot2(a0, red);
+  if (threadIdx.x == 0) {
+    ddv v = dd_mul_d(dd_two_sum(t.s, t.c), alpha);
+    if (base) v = dd_add(v, dd_two_prod(beta, base[i]));
+    out[i] = v.hi + v.lo;
+  }
+}
+
+void gemv_t_acc(const double* A, long long K, int m, const double* z, double alpha,
+                const double* base, double beta, double* out, cudaStream_t st) {
+  if (m == 0) return;
+  if ((K & 1) == 0 && aligned16(A) && aligned16(z))
+    k_gemv_t_acc<true><<<m, 512, 0, st>>>(A, K, m, z, alpha, base, beta, out);
+  else
+    k_gemv_t_acc<false><<<m, 512, 0, st>>>(A, K, m, z, alpha, base, beta, out);
   SDPX_LAUNCH_CHECK();
 }
 

@@ -19,6 +19,16 @@ void gemv_n(const double* A, long long K, int m, const double* x, double* out, d
             int chunks, cudaStream_t st);
 void gemv_t(const double* A, long long K, int m, const double* z, double alpha, const double* base,
             double beta, double* out, cudaStream_t st);
+// The same products as compensated (Dot2) sums rounded once, for the
+// residuals: out = 𝒜x − X − C (X, C may be null; part holds 2·chunks·K
+// doubles) and out = alpha·𝒜ᵀz + beta·base.
+void gemv_n_acc(const double* A, long long K, int m, const double* x, const double* X,
+                const double* C, double* out, double* part, int chunks, cudaStream_t st);
+void gemv_n_sym_acc(const double* Ap, long long Kt, int m, const double* x, const long long* lo,
+                    const long long* up, const double* X, const double* C, double* out,
+                    double* part, int chunks, cudaStream_t st);
+void gemv_t_acc(const double* A, long long K, int m, const double* z, double alpha,
+                const double* base, double beta, double* out, cudaStream_t st);
 // Lower-triangle copy of the constraint matrix (Kt kept rows per column):
 // pack_rows gathers it, gemv_n_sym writes Ap·x to both stacked positions
 // lo[q] and up[q] of every kept row, fold_sym folds a stacked vector onto the
