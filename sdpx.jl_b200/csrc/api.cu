@@ -228,6 +228,7 @@ struct Handle {
   // batched Cholesky workspace (dense blocks X, Y and line-search trials)
   DBuf<MatDesc<double>> d_descs;
   DBuf<int> d_info;
+  DBuf<unsigned> coop_bar;  // grid-barrier state of the single-launch Schur Cholesky
   DBuf<double> d_dmin, d_dmax;
   size_t desc_cap = 0;
   DBuf<double> trials;
@@ -1314,9 +1315,15 @@ struct Handle {
     int att = 0;
     while (true) {
       copy_reg(m, S.p, Sf.p, att == 0 ? 0.0 : reg, st);
-      ensure_descs(1);
-      h2d(d_descs.p, &md, sizeof(md));
-      potrf_batched<double, 64>(d_descs.p, 1, m, d_info.p, d_dmin.p, d_dmax.p, st);
+      if (potrf_single_pays<double, 64>(m)) {
+        if (coop_bar.n < 4) coop_bar.alloc(4);
+        potrf_single<double, 64>(Sf.p, m, m, d_info.p, d_dmin.p, d_dmax.p,
+                                 reinterpret_cast<CoopBar*>(coop_bar.p), true, st);
+      } else {
+        ensure_descs(1);
+        h2d(d_descs.p, &md, sizeof(md));
+        potrf_batched<double, 64>(d_descs.p, 1, m, d_info.p, d_dmin.p, d_dmax.p, st);
+      }
       info.resize(1);
       dmn.resize(1);
       dmx.resize(1);
@@ -1324,6 +1331,7 @@ struct Handle {
       d2h(dmn.data(), d_dmin.p, sizeof(double));
       d2h(dmx.data(), d_dmax.p, sizeof(double));
       sync();
+      if (info[0] < 0) throw CudaError("Schur Cholesky: a grid barrier timed out");
       if (info[0] == 0 || att >= 6) break;
       ++att;
       reg = (att == 1) ? kSqrtEps : reg * 10.0;

@@ -399,6 +399,441 @@ void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* d
   SDPX_LAUNCH_CHECK_N(launches);
 }
 
+// ---------------------------------------------------------------------------
+// One large matrix (the Schur factor): the whole right-looking factorization
+// in one cooperative launch of at most one CTA per SM, panels separated by
+// grid barriers instead of kernel boundaries.  Per panel j:
+//   A  every CTA loads the factored diagonal tile and solves its contiguous
+//      share of the rows below (X = B·L_jj⁻ᵀ in the operation order of
+//      k_potrf_trsm_rows, 16 threads per row);
+//   B  after a barrier, CTA 0 updates the next diagonal tile and factors it
+//      in shared memory at once (look-ahead: the factor's latency chain runs
+//      while the other CTAs update the remaining trailing lower tiles), with
+//      the arithmetic of k_potrf_diag, so the factor is bit-identical to the
+//      batched path's; tile updates are FP64 on DMMA m8n8k4 fragments, FP32
+//      on 4×4 register tiles;
+//   and a barrier before the next panel.  Matrix loads bypass L1 (__ldcg):
+//   other SMs wrote the data since this SM may last have cached it.  A pivot
+//   failure is published in the barrier state before the barrier, so every
+//   CTA reads it at the same panel and all leave together.
+//   Barrier waits are bounded (about a second); on a timeout the kernel sets
+//   info = −1 and every CTA returns.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned coop_ld(const unsigned* p) {
+  return *reinterpret_cast<const volatile unsigned*>(p);
+}
+
+__device__ bool coop_barrier(CoopBar* bar, unsigned nblocks, int* info) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned g = coop_ld(&bar->gen);
+    __threadfence();
+    if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (coop_ld(&bar->gen) == g) {
+        if (coop_ld(&bar->err) != 0u || ++spins > (1ull << 24)) {
+          atomicExch(&bar->err, 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (!ok || coop_ld(&bar->err) != 0u) {
+      ok = 0;
+      atomicExch(info, -1);
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Lower part of the h×w tile at (r0, c0) into shared T (column c at
+// T[c·LD + …]), zeros elsewhere up to NB×NB; `lower` masks r < c.
+template <class T, int NB>
+__device__ __forceinline__ void coop_load_tile(T* Ts, const T* a, int ld, int r0, int c0, int h, int w,
+                                               bool lower) {
+  constexpr int LD = NB + 1, PER = NB * NB / 256;
+  T v[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * 256, r = e % NB, c = e / NB;
+    v[k] = (r < h && c < w && (!lower || r >= c)) ? __ldcg(a + (size_t)(c0 + c) * ld + (r0 + r)) : T(0);
+  }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * 256, r = e % NB, c = e / NB;
+    Ts[c * LD + r] = v[k];
+  }
+}
+
+// Trailing tile (i, q) of panel j, FP32: 4×4 register tiles (k_potrf_update's
+// arithmetic).
+template <int NB>
+__device__ __forceinline__ void coop_update_tile(float* a, int ld, int n, int c0, int r0, int q0,
+                                                 bool diag, float* La, float* Lb) {
+  constexpr int LD = NB + 1, RB = NB / 16, TPR = NB / RB;
+  const int w = min(NB, n - c0), h = min(NB, n - r0), hq = min(NB, n - q0);
+  const int tr = threadIdx.x % TPR, tc = threadIdx.x / TPR;
+  float cur[RB][RB];
+#pragma unroll
+  for (int x = 0; x < RB; ++x)
+#pragma unroll
+    for (int y = 0; y < RB; ++y) {
+      const int r = tr + x * TPR, c = tc + y * TPR;
+      cur[x][y] = (r < h && c < hq) ? __ldcg(a + (size_t)(q0 + c) * ld + (r0 + r)) : 0.f;
+    }
+  __syncthreads();  // the previous tile's reads of La/Lb are done
+  coop_load_tile<float, NB>(La, a, ld, r0, c0, h, w, false);
+  coop_load_tile<float, NB>(Lb, a, ld, q0, c0, hq, w, false);
+  __syncthreads();
+  float acc[RB][RB] = {};
+  for (int p = 0; p < w; ++p) {
+    float av[RB], bv[RB];
+#pragma unroll
+    for (int x = 0; x < RB; ++x) av[x] = La[p * LD + tr + x * TPR];
+#pragma unroll
+    for (int y = 0; y < RB; ++y) bv[y] = Lb[p * LD + tc + y * TPR];
+#pragma unroll
+    for (int x = 0; x < RB; ++x)
+#pragma unroll
+      for (int y = 0; y < RB; ++y) acc[x][y] += av[x] * bv[y];
+  }
+#pragma unroll
+  for (int x = 0; x < RB; ++x)
+#pragma unroll
+    for (int y = 0; y < RB; ++y) {
+      const int r = tr + x * TPR, c = tc + y * TPR;
+      if (r < h && c < hq && (!diag || r >= c))
+        a[(size_t)(q0 + c) * ld + (r0 + r)] = cur[x][y] - acc[x][y];
+    }
+}
+
+// FP64: warp wp owns rows 8·wp … 8·wp+7 of the tile and all eight 8-column
+// fragments; K runs over the panel's columns in steps of 4 (zero-padded).
+template <int NB>
+__device__ __forceinline__ void coop_update_tile(double* a, int ld, int n, int c0, int r0, int q0,
+                                                 bool diag, double* La, double* Lb) {
+  static_assert(NB == 64, "the DMMA tile update covers 64×64 tiles with 8 warps");
+  constexpr int LD = NB + 1;
+  const int w = min(NB, n - c0), h = min(NB, n - r0), hq = min(NB, n - q0);
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int r = wp * 8 + g;
+  double cur[8][2];
+#pragma unroll
+  for (int fc = 0; fc < 8; ++fc)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int c = fc * 8 + 2 * t + e;
+      cur[fc][e] = (r < h && c < hq) ? __ldcg(a + (size_t)(q0 + c) * ld + (r0 + r)) : 0.0;
+    }
+  __syncthreads();
+  coop_load_tile<double, NB>(La, a, ld, r0, c0, h, w, false);
+  coop_load_tile<double, NB>(Lb, a, ld, q0, c0, hq, w, false);
+  __syncthreads();
+  double acc[8][2] = {};
+  for (int kk = 0; kk < w; kk += 4) {
+    const double av = La[(kk + t) * LD + r];
+#pragma unroll
+    for (int fc = 0; fc < 8; ++fc) dmma_8x8x4(acc[fc][0], acc[fc][1], av, Lb[(kk + t) * LD + fc * 8 + g]);
+  }
+#pragma unroll
+  for (int fc = 0; fc < 8; ++fc)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int c = fc * 8 + 2 * t + e;
+      if (r < h && c < hq && (!diag || r >= c))
+        a[(size_t)(q0 + c) * ld + (r0 + r)] = cur[fc][e] - acc[fc][e];
+    }
+}
+
+// The NB×NB diagonal tile (shared, ld LD, order w) factored by one CTA with
+// the arithmetic of factor_panel_smem — 8×8 block in registers (l_cc =
+// sqrt(a_cc), 1/l_cc scaling), rows below solved against it, rank-8 update of
+// the trailing columns, every element in increasing column order — so the
+// factor is bit-identical to the batched path's.  Only warp 0 runs the 8×8
+// block factor (every thread of factor_panel_smem repeats it, which saturates
+// the FP64 pipe); its result and the reciprocal pivots go to shared memory.
+// The trailing update takes two columns per step for two independent chains.
+template <class T, int NB>
+__device__ int factor_diag_tile(T* D, int LD, int w, T* sinv, int* sfail) {
+  __syncthreads();
+  for (int kb = 0; kb < w; kb += 8) {
+    const int kw = min(8, w - kb);
+    if (threadIdx.x < 32) {
+      T B[8][8], inv[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+          B[c][r] = (c < kw && r < kw && r >= c) ? D[(kb + c) * LD + kb + r] : T(0);
+      int fail = -1;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        inv[c] = T(0);
+        if (c < kw && fail < 0) {
+          const T piv = B[c][c];
+          if (!(piv > T(0))) {
+            fail = c;
+          } else {
+            const T lc = sqrt(piv);
+            inv[c] = T(1) / lc;
+            B[c][c] = lc;
+#pragma unroll
+            for (int r = c + 1; r < 8; ++r) B[c][r] *= inv[c];
+#pragma unroll
+            for (int q = c + 1; q < 8; ++q)
+#pragma unroll
+              for (int r = q; r < 8; ++r) B[q][r] -= B[c][r] * B[c][q];
+          }
+        }
+      }
+      __syncwarp();
+      if (threadIdx.x == 0) {
+        *sfail = fail;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          sinv[c] = inv[c];
+#pragma unroll
+          for (int r = 0; r < 8; ++r)
+            if (c < kw && r < kw && r >= c) D[(kb + c) * LD + kb + r] = B[c][r];
+        }
+      }
+    }
+    __syncthreads();
+    if (*sfail >= 0) return kb + *sfail;  // the same in every thread
+    // rows below the block: x = a · L_bb^{-T}
+    for (int r = kb + kw + threadIdx.x; r < w; r += blockDim.x) {
+      T x[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) x[c] = (c < kw) ? D[(kb + c) * LD + r] : T(0);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < kw) {
+          x[c] *= sinv[c];
+#pragma unroll
+          for (int q = c + 1; q < 8; ++q) x[q] -= x[c] * D[(kb + c) * LD + kb + q];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c < kw) D[(kb + c) * LD + r] = x[c];
+    }
+    __syncthreads();
+    {
+      const int r0 = kb + kw, nrow = w - r0;
+      const int slices = nrow > 0 ? max(1, (int)blockDim.x / nrow) : 1;
+      for (int idx = threadIdx.x; idx < nrow * slices; idx += blockDim.x) {
+        const int r = r0 + idx % nrow, sl = idx / nrow;
+        T x[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) x[c] = (c < kw) ? D[(kb + c) * LD + r] : T(0);
+        const int qe = min(w, r + 1);
+        int q = r0 + sl;
+        for (; q + slices < qe; q += 2 * slices) {
+          const int q2 = q + slices;
+          T a1 = D[q * LD + r], a2 = D[q2 * LD + r];
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c < kw) {
+              a1 -= x[c] * D[(kb + c) * LD + q];
+              a2 -= x[c] * D[(kb + c) * LD + q2];
+            }
+          D[q * LD + r] = a1;
+          D[q2 * LD + r] = a2;
+        }
+        if (q < qe) {
+          T a1 = D[q * LD + r];
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c < kw) a1 -= x[c] * D[(kb + c) * LD + q];
+          D[q * LD + r] = a1;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  return -1;
+}
+
+// Rows [r0, r1) of panel c0 solved against the factored diagonal tile D:
+// X = B·L⁻ᵀ with 16 threads per row, thread s owning columns s, s+16, s+32,
+// s+48; column c's value is finished by its owner (x_c ← x_c·(1/l_cc)) and
+// shuffled to the row's other threads, which subtract x_c·l_qc from their
+// columns q > c — the operation order of k_potrf_trsm_rows.
+template <class T, int NB>
+__device__ void coop_trsm_rows(T* a, int ld, int c0, int w, int r0, int r1, const T* D, int LD,
+                               const T* inv) {
+  static_assert(NB == 64, "16 threads × 4 columns per row");
+  const int s = threadIdx.x & 15, grp = threadIdx.x >> 4, ngrp = blockDim.x >> 4;
+  const unsigned gmask = 0xffffu << (threadIdx.x & 16);
+  for (int rb = r0; rb < r1; rb += ngrp) {  // uniform trip count within each warp
+    const int r = rb + grp;
+    const bool live = r < r1;
+    T x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int c = s + 16 * u;
+      x[u] = (live && c < w) ? __ldcg(a + (size_t)(c0 + c) * ld + r) : T(0);
+    }
+    for (int c = 0; c < w; ++c) {
+      const int owner = c & 15, uc = c >> 4;
+      T xc = T(0);
+      if (s == owner) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (u == uc) {
+            x[u] *= inv[c];
+            xc = x[u];
+          }
+      }
+      xc = __shfl_sync(gmask, xc, owner, 16);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int q = s + 16 * u;
+        if (q > c && q < w) x[u] -= xc * D[c * LD + q];
+      }
+    }
+    if (live)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int c = s + 16 * u;
+        if (c < w) a[(size_t)(c0 + c) * ld + r] = x[u];
+      }
+  }
+}
+
+// CTA 0: the diagonal tile at (c0, c0) (already updated) factored in its
+// shared memory D and written back; the failing pivot (1-based) goes to
+// bar->fail, the pivot range to lo/hi (thread 0).
+template <class T, int NB>
+__device__ void coop_factor_diag(T* a, int n, int ld, int c0, T* D, T* sinv8, int* sfail, CoopBar* bar,
+                                 T& lo, T& hi) {
+  constexpr int LD = NB + 1;
+  const int w = min(NB, n - c0);
+  __syncthreads();
+  coop_load_tile<T, NB>(D, a, ld, c0, c0, w, w, true);
+  const int fail = factor_diag_tile<T, NB>(D, LD, w, sinv8, sfail);
+  if (fail >= 0) {
+    if (threadIdx.x == 0) atomicExch(&bar->fail, (unsigned)(c0 + fail + 1));
+    return;
+  }
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    const int r = e % NB, c = e / NB;
+    if (r < w && c < w && r >= c) a[(size_t)(c0 + c) * ld + (c0 + r)] = D[c * LD + r];
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < w; ++c) {
+      const T v = fabs(D[c * LD + c]);
+      lo = fmin(lo, v);
+      hi = fmax(hi, v);
+    }
+}
+
+template <class T, int NB>
+__global__ void __launch_bounds__(256) k_potrf_coop(T* a, int n, int ld, int* info, T* dmin, T* dmax,
+                                                   CoopBar* bar, int zero_upper) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  constexpr int LD = NB + 1;
+  T* D = reinterpret_cast<T*>(raw);  // the diagonal tile; in updates, operand La
+  T* Lb = D + NB * LD;
+  __shared__ T inv[NB];
+  __shared__ T sinv8[8];
+  __shared__ int sfail;
+  const int nt = (n + NB - 1) / NB;
+  const unsigned G = gridDim.x;
+  T lo = T(INFINITY), hi = T(0);
+  if (blockIdx.x == 0) coop_factor_diag<T, NB>(a, n, ld, 0, D, sinv8, &sfail, bar, lo, hi);
+  if (nt > 1 && !coop_barrier(bar, G, info)) return;
+  for (int j = 0; j < nt; ++j) {
+    const int c0 = j * NB, w = min(NB, n - c0);
+    __syncthreads();  // CTA 0's own flag write is visible to all of its threads
+    const unsigned failed = coop_ld(&bar->fail);  // read after a barrier: the same in every CTA
+    if (failed != 0u) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        info[0] = (int)failed;
+        dmin[0] = lo;
+        dmax[0] = hi;
+      }
+      return;
+    }
+    if (j == nt - 1) break;
+    // A: the rows below against the factored diagonal tile
+    __syncthreads();
+    coop_load_tile<T, NB>(D, a, ld, c0, c0, w, w, true);
+    __syncthreads();
+    for (int c = threadIdx.x; c < w; c += blockDim.x) inv[c] = T(1) / D[c * LD + c];
+    __syncthreads();
+    const int rfirst = c0 + w, nrow = n - rfirst;
+    const int per = (nrow + (int)G - 1) / (int)G;
+    const int r0 = min(n, rfirst + (int)blockIdx.x * per), r1 = min(n, r0 + per);
+    coop_trsm_rows<T, NB>(a, ld, c0, w, r0, r1, D, LD, inv);
+    if (!coop_barrier(bar, G, info)) return;
+    // B: CTA 0 updates the next diagonal tile and factors it at once (the
+    // look-ahead), the other CTAs take the remaining trailing tiles
+    const int rem = nt - j - 1, ntile = rem * (rem + 1) / 2;
+    if (blockIdx.x == 0) {
+      coop_update_tile<NB>(a, ld, n, c0, (j + 1) * NB, (j + 1) * NB, true, D, Lb);
+      coop_factor_diag<T, NB>(a, n, ld, (j + 1) * NB, D, sinv8, &sfail, bar, lo, hi);
+    }
+    const int first = G > 1 ? (int)blockIdx.x - 1 : 1;
+    const int step = G > 1 ? (int)G - 1 : 1;
+    if (G == 1 || blockIdx.x > 0)
+      for (int u = 1 + (G > 1 ? first : 0); u < ntile; u += step) {
+        int ti = (int)((sqrt(8.0 * u + 1.0) - 1.0) * 0.5);
+        while ((ti + 1) * (ti + 2) / 2 <= u) ++ti;
+        while (ti * (ti + 1) / 2 > u) --ti;
+        const int tq = u - ti * (ti + 1) / 2;
+        const int i = j + 1 + ti, q = j + 1 + tq;
+        coop_update_tile<NB>(a, ld, n, c0, i * NB, q * NB, i == q, D, Lb);
+      }
+    if (!coop_barrier(bar, G, info)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    dmin[0] = lo;
+    dmax[0] = hi;
+  }
+  if (zero_upper) {  // strict upper triangle: a warp per column
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int c = blockIdx.x * nw + (threadIdx.x >> 5); c < n; c += G * nw)
+      for (int r = lane; r < c; r += 32) a[(size_t)c * ld + r] = T(0);
+  }
+}
+
+template <class T, int NB>
+void potrf_single(T* a, int n, int ld, int* info, T* dmin, T* dmax, CoopBar* bar, bool zero_upper,
+                  cudaStream_t st) {
+  if (n <= 0) return;
+  const size_t smem = 2 * sizeof(T) * NB * (NB + 1);
+  ensure_smem(k_potrf_coop<T, NB>, smem);
+  int dev = 0, sms = 0, per_sm = 0, coop = 0;
+  SDPX_CUDA(cudaGetDevice(&dev));
+  SDPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SDPX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  SDPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_potrf_coop<T, NB>, 256, smem));
+  if (!coop || per_sm < 1) throw CudaError("potrf_single: cooperative launch unavailable");
+  const int nt = ceil_div(n, NB);
+  const int grid = std::max(1, std::min(sms, nt * (nt - 1) / 2));
+  SDPX_CUDA(cudaMemsetAsync(bar, 0, sizeof(CoopBar), st));
+  SDPX_CUDA(cudaMemsetAsync(info, 0, sizeof(int), st));
+  int zu = zero_upper ? 1 : 0;
+  void* args[] = {&a, &n, &ld, &info, &dmin, &dmax, &bar, &zu};
+  SDPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_potrf_coop<T, NB>), dim3(grid),
+                                        dim3(256), args, smem, st));
+}
+template void potrf_single<double, 64>(double*, int, int, int*, double*, double*, CoopBar*, bool,
+                                       cudaStream_t);
+template void potrf_single<float, 64>(float*, int, int, int*, float*, float*, CoopBar*, bool,
+                                      cudaStream_t);
+
 template void potrf_batched<double, 32>(const MatDesc<double>*, int, int, int*, double*, double*,
                                         cudaStream_t, bool);
 template void potrf_batched<double, 48>(const MatDesc<double>*, int, int, int*, double*, double*,

@@ -22,6 +22,30 @@ template <class T, int NB>
 void potrf_batched(const MatDesc<T>* d_mats, int nmat, int nmax, int* info, T* dmin, T* dmax,
                    cudaStream_t st, bool zero_upper = true);
 
+// Grid-barrier state of one potrf_single call site (device memory, 16 bytes).
+struct CoopBar {
+  unsigned count, gen, err, fail;
+};
+
+// Lower Cholesky in place of one n×n matrix (leading dimension ld) in a single
+// cooperative launch, for orders above the whole-panel shared-memory size.
+// info[0] = 0 on success, the 1-based failing pivot, or −1 when a grid
+// barrier timed out (the call site's `bar` must not be shared by concurrent
+// calls).  dmin/dmax: min/max |L_ii|.
+template <class T, int NB>
+void potrf_single(T* a, int n, int ld, int* info, T* dmin, T* dmax, CoopBar* bar, bool zero_upper,
+                  cudaStream_t st);
+
+// Whether potrf_single is the faster path for one matrix of order n: FP64
+// orders above the whole-panel shared-memory size (measured on the B200 with
+// identical factors: 0.88 vs 0.93 ms at n = 1000, 1.78 vs 1.99 ms at 2000,
+// 3.09 vs 3.26 ms at 3000; below that size, and in FP32, the batched path is
+// as fast or faster).
+template <class T, int NB>
+inline bool potrf_single_pays(int n) {
+  return sizeof(T) == 8 && sizeof(T) * (size_t)(n | 1) * NB > 224 * 1024;
+}
+
 // W_b = L_b^{-1} for lower-triangular L_b (W zero-initialised by the caller).
 template <class T, int NB>
 void trinv_batched(const MatDesc<T>* d_L, const MatDesc<T>* d_W, int nmat, int nmax,

@@ -286,6 +286,7 @@ struct NormalHandle {
   std::vector<int> cone_dim;
   DBuf<long long> d_off;
   DBuf<int> d_dim, d_row, d_ok, d_info;
+  DBuf<unsigned> coop_bar;  // grid-barrier state of the single-launch Cholesky
   DBuf<double> B, Bh, coef, weights, D, Dinv, Dis, w, lam, eta, eta2, s, z, v, out;
   DBuf<double> Q, F, Finv_diag, partial, rhs, t, red, work, u, gemv_part;
   DBuf<double> dmin, dmax;
@@ -568,12 +569,11 @@ struct NormalHandle {
         info = 0;
         break;
       }
-      MatDesc<double> md{F.p, m, m};
-      h2d(descs.p, &md, sizeof(md));
-      potrf_batched<double, 64>(descs.p, 1, m, d_info.p, dmin.p, dmax.p, st);
+      factor_F();
       SDPX_CUDA(cudaEventRecord(ev[2], st));
       d2h(&info, d_info.p, sizeof(int));
       sync();
+      if (info < 0) throw CudaError("normal-matrix Cholesky: a grid barrier timed out");
       float a = 0.f, f = 0.f;
       SDPX_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
       SDPX_CUDA(cudaEventElapsedTime(&f, ev[1], ev[2]));
@@ -591,6 +591,20 @@ struct NormalHandle {
     sync();
     have_factor = true;
     return 0;
+  }
+
+  // Cholesky of the reduced matrix F in place: one cooperative launch above the
+  // whole-panel size, the batched panels below it (identical factors).
+  void factor_F() {
+    if (potrf_single_pays<double, 64>(m)) {
+      if (coop_bar.n < 4) coop_bar.alloc(4);
+      potrf_single<double, 64>(F.p, m, m, d_info.p, dmin.p, dmax.p,
+                               reinterpret_cast<CoopBar*>(coop_bar.p), true, st);
+      return;
+    }
+    MatDesc<double> md{F.p, m, m};
+    h2d(descs.p, &md, sizeof(md));
+    potrf_batched<double, 64>(descs.p, 1, m, d_info.p, dmin.p, dmax.p, st);
   }
 
   // One assembly + Cholesky attempt with LP weights already on the device
@@ -611,12 +625,11 @@ struct NormalHandle {
       have_factor = true;
       return 0;
     }
-    MatDesc<double> md{F.p, m, m};
-    h2d(descs.p, &md, sizeof(md));
-    potrf_batched<double, 64>(descs.p, 1, m, d_info.p, dmin.p, dmax.p, st);
+    factor_F();
     int info = 1;
     d2h(&info, d_info.p, sizeof(int));
     sync();
+    if (info < 0) throw CudaError("normal-matrix Cholesky: a grid barrier timed out");
     if (info != 0) return 1;
     factor_diag_inverses<double, 64>(F.p, m, m, Finv_diag.p, st);
     if (split) make_inverse();

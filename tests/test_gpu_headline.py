@@ -82,7 +82,8 @@ def chunked_case():
     dx, dX, dY = ob.get_direction()
     kappa = 1.0 / max(fo["quality"], 1e-300) ** 2
     return dict(prob=prob, it=(x, X, Y), S=S, rhs=rhs, dx=dx, dX=dX, dY=dY,
-                DIR=max(REL, 64 * 2.2e-16 * kappa))
+                DIR=max(REL, 64 * 2.2e-16 * kappa), quality=fo["quality"],
+                reg_attempts=fo["reg_attempts"])
 
 
 @pytest.mark.parametrize("engine", ["int8", "dmma"])
@@ -96,7 +97,9 @@ def test_chunked_fp64_schur_and_direction_match_oracle(cuda, chunked_case, engin
         be.schur_build()
         S = be.schur_matrix()
         assert rel(S, c["S"]) <= 1e-12
-        assert be.factorize()["ok"]
+        f = be.factorize()  # m = 600: the single-launch cooperative FP64 Cholesky
+        assert f["ok"] and f["reg_attempts"] == c["reg_attempts"]
+        assert abs(f["quality"] - c["quality"]) <= 1e-10
         be.predictor_rhs()
         assert rel(be.get_rhs(), c["rhs"]) <= REL
         be.solve_direction()
