@@ -216,6 +216,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 // rows of L_X⁻¹), 2 starts at the B tile (B rows are columns of L_Y, zero
 // above the diagonal).
 constexpr int PG_THREADS = 6 * 32;
+// Epilogue staging: per warp one plane's 32 rows × 32 columns (64 B a row,
+// padded to 80 B) after the barrier block.
+constexpr int EPI_ROW_BYTES = 80;
+constexpr int EPI_WARP_BYTES = 32 * EPI_ROW_BYTES;
+constexpr size_t PG_SMEM_BYTES = SNST * SSTAGE_BYTES + 1024 + 256 + 4 * EPI_WARP_BYTES;
 
 struct PGemmShared {
   uint64_t full[SNST], empty[SNST], tfull[2], tempty[2], mdone;
@@ -356,8 +361,12 @@ __global__ void __launch_bounds__(PG_THREADS, 1)
       umma::mbar_wait_bounded(&sh->mdone, 0, err);
     }
   } else {
-    // Epilogue: warps 0-3, TMEM lane quarter = warp, one output row per thread.
-    const int row = warp * 32 + lane;
+    // Epilogue: warps 0-3, TMEM lane quarter = warp, one accumulator row per
+    // thread.  Each 32-column slice is split into the three planes; a plane's
+    // 32 × 32 BF16 block goes through this warp's staging rows so that every
+    // store instruction writes eight whole 64-byte row segments (a quarter of
+    // the L2 write requests of one 16-byte store per row).
+    unsigned char* stage = smem + SNST * SSTAGE_BYTES + 256 + warp * EPI_WARP_BYTES;
     uint32_t j = 0;
     for (long long u = blockIdx.x; u < g.ntask; u += gridDim.x, ++j) {
       int r0, c0, kb, nk;
@@ -365,9 +374,14 @@ __global__ void __launch_bounds__(PG_THREADS, 1)
       const int b = j & 1;
       if (!pg_wait(&sh->tfull[b], (j >> 1) & 1, err, abort)) break;
       umma::fence_after_sync();
-      const int grow = r0 + row;
-      const bool live = grow < out.rows.extent;
-      const long long ro = live ? row_off(out.rows, grow) : 0;
+      long long ro[4];
+      bool live[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int grow = r0 + warp * 32 + k * 8 + (lane >> 2);
+        live[k] = grow < out.rows.extent;
+        ro[k] = live[k] ? row_off(out.rows, grow) : 0;
+      }
       const uint32_t acc0 = tmem + (uint32_t)(b * 256);
       for (int cb = 0; cb < TN; cb += 32) {
         float v[32];
@@ -382,19 +396,37 @@ __global__ void __launch_bounds__(PG_THREADS, 1)
           __syncwarp();
           if (lane == 0) umma::mbar_arrive(&sh->tempty[b]);
         }
-        if (!live) continue;
+        uint32_t pk[3][16];
 #pragma unroll
-        for (int q = 0; q < 32; q += 8) {
-          const int gcol = c0 + cb + q;
-          if (gcol >= out.col_extent) continue;
-          const long long co = (long long)(gcol / out.col_inner) * out.col_os +
-                               (long long)(gcol % out.col_inner);
-          __align__(16) __nv_bfloat16 h[3][8];
+        for (int e = 0; e < 16; ++e) {
+          __nv_bfloat16 x[3], y[3];
+          split3(v[2 * e], x[0], x[1], x[2]);
+          split3(v[2 * e + 1], y[0], y[1], y[2]);
 #pragma unroll
-          for (int e = 0; e < 8; ++e) split3(v[q + e], h[0][e], h[1][e], h[2][e]);
+          for (int p = 0; p < 3; ++p) {
+            __nv_bfloat162 t = __halves2bfloat162(x[p], y[p]);
+            pk[p][e] = *reinterpret_cast<uint32_t*>(&t);
+          }
+        }
+        const int gcol = c0 + cb + (lane & 3) * 8;
+        const bool col_ok = gcol < out.col_extent;
+        const long long co = (long long)(gcol / out.col_inner) * out.col_os +
+                             (long long)(gcol % out.col_inner);
 #pragma unroll
-          for (int p = 0; p < 3; ++p)
-            *reinterpret_cast<uint4*>(out.plane[p] + ro + co) = *reinterpret_cast<uint4*>(h[p]);
+        for (int p = 0; p < 3; ++p) {
+          __syncwarp();  // the previous plane's reads of the staging rows are done
+          uint4* mine = reinterpret_cast<uint4*>(stage + lane * EPI_ROW_BYTES);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            mine[q] = make_uint4(pk[p][4 * q], pk[p][4 * q + 1], pk[p][4 * q + 2], pk[p][4 * q + 3]);
+          __syncwarp();
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int rr = k * 8 + (lane >> 2);
+            if (live[k] && col_ok)
+              *reinterpret_cast<uint4*>(out.plane[p] + ro[k] + co) =
+                  *reinterpret_cast<const uint4*>(stage + rr * EPI_ROW_BYTES + (lane & 3) * 16);
+          }
         }
       }
     }
@@ -554,7 +586,7 @@ void split_gemm_planes(const Plane2D& A, const Plane2D& B, int Ktot, const OutMa
     encode_plane_map(&maps.a[p], A.plane[p], A.rows, Ktot, A.pitch);
     encode_plane_map(&maps.b[p], B.plane[p], B.rows, Ktot, B.pitch);
   }
-  ensure_smem(k_split_gemm_persistent, SSMEM_BYTES);
+  ensure_smem(k_split_gemm_persistent, PG_SMEM_BYTES);
   PGemmTiles g;
   g.ta = ceil_div(out.rows.extent, TM);
   g.tb = ceil_div(out.col_extent, TN);
@@ -566,7 +598,7 @@ void split_gemm_planes(const Plane2D& A, const Plane2D& B, int Ktot, const OutMa
   SDPX_CUDA(cudaGetDevice(&dev));
   SDPX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const long long grid = std::min<long long>(g.ntask, sms);
-  k_split_gemm_persistent<<<(unsigned)grid, PG_THREADS, SSMEM_BYTES, st>>>(maps, out, g, err);
+  k_split_gemm_persistent<<<(unsigned)grid, PG_THREADS, PG_SMEM_BYTES, st>>>(maps, out, g, err);
   SDPX_LAUNCH_CHECK();
 }
 
