@@ -436,17 +436,42 @@ __global__ void __launch_bounds__(PG_THREADS, 1)
   if (warp == 0) umma::tmem_dealloc(tmem, 512);
 }
 
-__global__ void k_reduce_partials(const float* partial, int ntri, int nchunk, int m, double* S) {
-  const int tri = blockIdx.x;
+// S tile (ti, tj) = Σ_chunks of the FP32 partial tiles, in FP64 and in chunk
+// order.  Four CTAs per tile, 32 rows each: every thread sums 16 elements of
+// the row-major partials (coalesced reads, the 16 loads of a chunk in flight
+// together), the 32 × 128 block is transposed through shared memory, and each
+// warp writes 32 consecutive rows of one column of the column-major S.
+__global__ void __launch_bounds__(256) k_reduce_partials(const float* partial, int ntri, int nchunk,
+                                                         int m, double* S) {
+  __shared__ double blk[TN][33];
+  const int tri = blockIdx.x >> 2, r0 = (blockIdx.x & 3) * 32;
   int ti, tj;
   tri_index(tri, ti, tj);
-  for (int e = threadIdx.x; e < TM * TN; e += blockDim.x) {
-    const int r = e / TN, c = e % TN;
-    const int gi = ti * TM + r, gj = tj * TN + c;
-    if (gi >= m || gj >= m) continue;
-    double s = 0.0;
-    for (int ch = 0; ch < nchunk; ++ch) s += (double)partial[((size_t)ch * ntri + tri) * TM * TN + e];
-    S[gi + (size_t)gj * m] = s;
+  constexpr int PER = 32 * TN / 256;
+  double acc[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) acc[k] = 0.0;
+  const size_t tile = (size_t)TM * TN;
+  const float* base = partial + (size_t)tri * tile + (size_t)r0 * TN;
+  for (int ch = 0; ch < nchunk; ++ch) {
+    const float* src = base + (size_t)ch * ntri * tile;
+    float v[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) v[k] = src[threadIdx.x + k * 256];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) acc[k] += (double)v[k];
+  }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * 256, r = e / TN, c = e % TN;
+    blk[c][r] = acc[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * 256, r = e & 31, c = e >> 5;
+    const int gi = ti * TM + r0 + r, gj = tj * TN + c;
+    if (gi < m && gj < m) S[gi + (size_t)gj * m] = blk[c][r];
   }
 }
 
@@ -617,7 +642,7 @@ void split_syrk(const Plane2D& P, int m, int Kp, const SplitSyrkPlan& plan, floa
   k_split_syrk_tma<<<units, NTHREADS, SSMEM_BYTES, st>>>(maps, plan.ntri, plan.kchunk, Kp, partial,
                                                         err);
   if (ev_end) SDPX_CUDA(cudaEventRecord(ev_end, st));
-  k_reduce_partials<<<plan.ntri, 256, 0, st>>>(partial, plan.ntri, plan.nchunk, m, S);
+  k_reduce_partials<<<plan.ntri * 4, 256, 0, st>>>(partial, plan.ntri, plan.nchunk, m, S);
   SDPX_LAUNCH_CHECK_N(2);
 }
 
