@@ -421,15 +421,39 @@ struct Handle {
     gemm_f64(a, akc, b, bkc, blk_out(out, blk.off, blk.k), alpha, beta, mode, false, st);
   }
 
+  // The same product on every dense block, C_b = alpha·op(A_b)·op(B_b) +
+  // beta·C_b (operands from opA(b), opB(b)), as one grouped launch per eight
+  // blocks: the blocks' products are independent and each tile is computed
+  // as blk_gemm computes it.
+  template <class FA, class FB>
+  void blk_gemm_all(FA opA, bool akc, FB opB, bool bkc, double* out, double alpha, double beta,
+                    int mode) {
+    GemmGroups g;
+    for (auto& b : dense) {
+      if (g.n == kGemmGroups) {
+        gemm_f64_grouped(g, akc, bkc, st);
+        g.n = 0;
+      }
+      g.A[g.n] = opA(b);
+      g.B[g.n] = opB(b);
+      g.C[g.n] = blk_out(out, b.off, b.k);
+      g.alpha[g.n] = alpha;
+      g.beta[g.n] = beta;
+      g.mode[g.n] = mode;
+      ++g.n;
+    }
+    gemm_f64_grouped(g, akc, bkc, st);
+  }
+
   // M ← X⁻¹·M for every dense block using W = L_X⁻¹ (Z = Wᵀ (W M)); M is read
   // from `in` and the result written to `out` (distinct from T2).
   void dense_cholsolve(const double* in, double* out) {
-    for (auto& b : dense) {
-      blk_gemm(blk_as_A(W.p, b.off, b.k), false, blk_as_B(in, b.off, b.k), true, T2.p, b, 1.0, 0.0,
-               KR_A_LOWER);
-      blk_gemm(blk_as_At(W.p, b.off, b.k), true, blk_as_B(T2.p, b.off, b.k), true, out, b, 1.0, 0.0,
-               KR_A_UPPER);
-    }
+    blk_gemm_all([&](const DenseBlk& b) { return blk_as_A(W.p, b.off, b.k); }, false,
+                 [&](const DenseBlk& b) { return blk_as_B(in, b.off, b.k); }, true, T2.p, 1.0, 0.0,
+                 KR_A_LOWER);
+    blk_gemm_all([&](const DenseBlk& b) { return blk_as_At(W.p, b.off, b.k); }, true,
+                 [&](const DenseBlk& b) { return blk_as_B(T2.p, b.off, b.k); }, true, out, 1.0, 0.0,
+                 KR_A_UPPER);
   }
 
   void ensure_descs(size_t n) {
@@ -964,9 +988,9 @@ struct Handle {
     absmax(m, d.p, red.p + 1, st);
     // R = −XY (+ μ I)
     h2d(mu_user.p, mu, L * sizeof(double));
-    for (auto& b : dense)
-      blk_gemm(blk_as_A(X.p, b.off, b.k), false, blk_as_B(Y.p, b.off, b.k), true, R.p, b, -1.0, 0.0,
-               KR_FULL);
+    blk_gemm_all([&](const DenseBlk& b) { return blk_as_A(X.p, b.off, b.k); }, false,
+                 [&](const DenseBlk& b) { return blk_as_B(Y.p, b.off, b.k); }, true, R.p, -1.0, 0.0,
+                 KR_FULL);
     if (!use_affine && !dense.empty()) {
       std::vector<double> shifts(dense.size());
       for (size_t b = 0; b < dense.size(); ++b) shifts[b] = mu[dense[b].user];
@@ -1183,9 +1207,10 @@ struct Handle {
     }
     if (!dense.empty()) {
       Xinv.alloc(K);
-      for (auto& b : dense)  // X⁻¹ = WᵀW with W = L_X⁻¹
-        blk_gemm(blk_as_At(W.p, b.off, b.k), true, blk_as_B(W.p, b.off, b.k), true, Xinv.p, b,
-                 1.0, 0.0, KR_FULL);
+      // X⁻¹ = WᵀW with W = L_X⁻¹
+      blk_gemm_all([&](const DenseBlk& b) { return blk_as_At(W.p, b.off, b.k); }, true,
+                   [&](const DenseBlk& b) { return blk_as_B(W.p, b.off, b.k); }, true, Xinv.p, 1.0,
+                   0.0, KR_FULL);
       for (size_t b = 0; b < dense.size(); ++b)
         sparse_schur_block(Y.p + dense[b].off, Xinv.p + dense[b].off, dense[b].k,
                            sp_ptr.p + sp_act_off[b], sp_lin.p, sp_val.p, sp_ids.p + sp_act_off[b],
@@ -1565,11 +1590,10 @@ struct Handle {
   // -------------------------------------------------------- right sides ---
   void rhs_from_R() {
     // Z = X⁻¹(P·Y − R); v = 𝒜ᵀ vec(Z); r = −(d + v)
-    for (auto& b : dense) {
-      d2d(T1.p + b.off, R.p + b.off, sizeof(double) * b.k * b.k);
-      blk_gemm(blk_as_A(P.p, b.off, b.k), false, blk_as_B(Y.p, b.off, b.k), true, T1.p, b, 1.0,
-               -1.0, KR_FULL);  // T1 = P·Y − R
-    }
+    for (auto& b : dense) d2d(T1.p + b.off, R.p + b.off, sizeof(double) * b.k * b.k);
+    blk_gemm_all([&](const DenseBlk& b) { return blk_as_A(P.p, b.off, b.k); }, false,
+                 [&](const DenseBlk& b) { return blk_as_B(Y.p, b.off, b.k); }, true, T1.p, 1.0,
+                 -1.0, KR_FULL);  // T1 = P·Y − R
     dense_cholsolve(T1.p, Z.p);
     diag_rhs_Z(nd, od, P.p, Y.p, R.p, LX.p, Z.p, st);
     atmul(Z.p, -1.0, d.p, -1.0, r.p);  // r = −v − d
@@ -1609,12 +1633,12 @@ struct Handle {
   }
   void build_corrector_R(const std::vector<double>& target) {
     // R = target·I − X·Y − dX·dY
-    for (auto& b : dense) {
-      blk_gemm(blk_as_A(X.p, b.off, b.k), false, blk_as_B(Y.p, b.off, b.k), true, R.p, b, -1.0, 0.0,
-               KR_FULL);
-      blk_gemm(blk_as_A(dX.p, b.off, b.k), false, blk_as_B(dY.p, b.off, b.k), true, R.p, b, -1.0,
-               1.0, KR_FULL);
-    }
+    blk_gemm_all([&](const DenseBlk& b) { return blk_as_A(X.p, b.off, b.k); }, false,
+                 [&](const DenseBlk& b) { return blk_as_B(Y.p, b.off, b.k); }, true, R.p, -1.0, 0.0,
+                 KR_FULL);
+    blk_gemm_all([&](const DenseBlk& b) { return blk_as_A(dX.p, b.off, b.k); }, false,
+                 [&](const DenseBlk& b) { return blk_as_B(dY.p, b.off, b.k); }, true, R.p, -1.0,
+                 1.0, KR_FULL);
     if (!dense.empty()) {
       std::vector<double> sh(dense.size());
       for (size_t b = 0; b < dense.size(); ++b) sh[b] = target[dense[b].user];
@@ -1640,11 +1664,10 @@ struct Handle {
     PhaseScope ps(this, 4);
     adx_current();
     axpbypcz(K, 1.0, adx.p, 1.0, P.p, 0.0, nullptr, dX.p, st);  // dX = 𝒜dx + P
-    for (auto& b : dense) {
-      d2d(T1.p + b.off, R.p + b.off, sizeof(double) * b.k * b.k);
-      blk_gemm(blk_as_A(dX.p, b.off, b.k), false, blk_as_B(Y.p, b.off, b.k), true, T1.p, b, -1.0,
-               1.0, KR_FULL);  // T1 = R − dX·Y
-    }
+    for (auto& b : dense) d2d(T1.p + b.off, R.p + b.off, sizeof(double) * b.k * b.k);
+    blk_gemm_all([&](const DenseBlk& b) { return blk_as_A(dX.p, b.off, b.k); }, false,
+                 [&](const DenseBlk& b) { return blk_as_B(Y.p, b.off, b.k); }, true, T1.p, -1.0,
+                 1.0, KR_FULL);  // T1 = R − dX·Y
     dense_cholsolve(T1.p, dY.p);
     if (!dense.empty()) symmetrize(d_doff.p, d_dk.p, (int)dense.size(), kmax, dY.p, st);
     diag_dY(nd, od, R.p, dX.p, Y.p, LX.p, dY.p, st);

@@ -41,6 +41,28 @@ __global__ void __launch_bounds__(Cfg::NT) k_gemm(Opnd A, Opnd B, OutDesc C, dou
   store_acc<Cfg>(acc, C, m0, n0, alpha, beta);
 }
 
+// Grouped products: CTA b belongs to the group whose tile range holds it
+// (first[g] ≤ b < first[g+1]); within a group the row tiles run fastest.
+struct GemmGroupsDev {
+  GemmGroups g;
+  int first[kGemmGroups + 1], tr[kGemmGroups];
+};
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT) k_gemm_grouped(const __grid_constant__ GemmGroupsDev d) {
+  extern __shared__ __align__(16) double smem[];
+  int q = 0;
+  while (q + 1 < d.g.n && (int)blockIdx.x >= d.first[q + 1]) ++q;
+  const int t = (int)blockIdx.x - d.first[q];
+  const int m0 = (t % d.tr[q]) * Cfg::BM, n0 = (t / d.tr[q]) * Cfg::BN;
+  const Opnd A = d.g.A[q], B = d.g.B[q];
+  int kb, ke;
+  k_limits(d.g.mode[q], A.k_extent, m0, n0, Cfg::BM, Cfg::BN, kb, ke);
+  double acc[Cfg::FM][Cfg::FN][2];
+  zero_acc<Cfg>(acc);
+  f64_tile_mainloop<Cfg>(acc, A, B, m0, n0, kb, ke, smem);
+  store_acc<Cfg>(acc, d.g.C[q], m0, n0, d.g.alpha[q], d.g.beta[q]);
+}
+
 // In-place  T ← T · L  for a lower-triangular L (k×k, explicit zeros above the
 // diagonal).  One CTA owns BM consecutive rows of T and sweeps the output
 // column tiles left to right; output tile [n0, n0+BN) reads only columns ≥ n0,
@@ -128,6 +150,43 @@ static void launch_gemm_cfg(const Opnd& A, const Opnd& B, const OutDesc& C, doub
   dim3 grid(rows_fast ? tr : tc, rows_fast ? tc : tr);
   k_gemm<Cfg><<<grid, Cfg::NT, Cfg::SMEM_BYTES, st>>>(A, B, C, alpha, beta, mode, rows_fast);
   SDPX_LAUNCH_CHECK();
+}
+
+template <class Cfg>
+static void launch_gemm_grouped(const GemmGroups& g, cudaStream_t st) {
+  ensure_smem(k_gemm_grouped<Cfg>, Cfg::SMEM_BYTES);
+  GemmGroupsDev d;
+  d.g = g;
+  int total = 0;
+  for (int q = 0; q < g.n; ++q) {
+    d.first[q] = total;
+    d.tr[q] = ceil_div(g.C[q].rows, Cfg::BM);
+    total += d.tr[q] * ceil_div(g.C[q].cols, Cfg::BN);
+  }
+  d.first[g.n] = total;
+  if (total == 0) return;
+  k_gemm_grouped<Cfg><<<total, Cfg::NT, Cfg::SMEM_BYTES, st>>>(d);
+  SDPX_LAUNCH_CHECK();
+}
+
+void gemm_f64_grouped(const GemmGroups& g, bool a_kcontig, bool b_kcontig, cudaStream_t st) {
+  if (g.n <= 0) return;
+  if (g.n > kGemmGroups) throw std::invalid_argument("gemm_f64_grouped: too many groups");
+  // the rule gemm_f64 applies to one product, applied to each of them: 32×32
+  // tiles when every product alone would take them
+  bool tiny = true;
+  for (int q = 0; q < g.n; ++q)
+    tiny = tiny && (long long)ceil_div(g.C[q].rows, 64) * ceil_div(g.C[q].cols, 64) < gemm_sm_count();
+  if (!tiny) {  // mixed shapes: one launch per product, as gemm_f64
+    for (int q = 0; q < g.n; ++q)
+      gemm_f64(g.A[q], a_kcontig, g.B[q], b_kcontig, g.C[q], g.alpha[q], g.beta[q], g.mode[q], false,
+               st);
+    return;
+  }
+  if (!a_kcontig && b_kcontig) return launch_gemm_grouped<CfgTnMK>(g, st);
+  if (a_kcontig && b_kcontig) return launch_gemm_grouped<CfgTnKK>(g, st);
+  if (!a_kcontig && !b_kcontig) return launch_gemm_grouped<CfgTnMM>(g, st);
+  return launch_gemm_grouped<CfgTnKM>(g, st);
 }
 
 void gemm_f64(const Opnd& A, bool a_kcontig, const Opnd& B, bool b_kcontig, const OutDesc& C,

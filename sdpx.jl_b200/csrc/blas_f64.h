@@ -12,6 +12,20 @@ namespace sdpx {
 void gemm_f64(const Opnd& A, bool a_kcontig, const Opnd& B, bool b_kcontig, const OutDesc& C,
               double alpha, double beta, int mode, bool big, cudaStream_t st);
 
+// Up to kGemmGroups independent products C_g = alpha_g·A_g·B_g + beta_g·C_g
+// (K range mode_g each, the same operand contiguity for all) in one launch:
+// the tiles of every product in one grid, each tile computed exactly as
+// gemm_f64 computes it (the same tile shape is chosen by the same rule).
+constexpr int kGemmGroups = 8;
+struct GemmGroups {
+  int n = 0;
+  Opnd A[kGemmGroups], B[kGemmGroups];
+  OutDesc C[kGemmGroups];
+  double alpha[kGemmGroups], beta[kGemmGroups];
+  int mode[kGemmGroups];
+};
+void gemm_f64_grouped(const GemmGroups& g, bool a_kcontig, bool b_kcontig, cudaStream_t st);
+
 // T ← T·L in place, L lower triangular with explicit zeros above the diagonal.
 void trmm_right_lower_inplace_f64(const Opnd& T, const Opnd& L, const OutDesc& C, cudaStream_t st);
 
