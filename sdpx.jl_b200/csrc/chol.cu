@@ -1098,19 +1098,39 @@ void trinv_recursive_f64(const double* L, int n, double* Linv, double* Dinv, dou
     d.cols = cols;
     return d;
   };
+  // The pairs of one doubling level are independent: their first products
+  // go out as grouped launches, then their second products.
   for (int g = 1; g < nt; g *= 2) {
+    GemmGroups first, second;
+    auto flush = [&]() {
+      gemm_f64_grouped(first, false, true, st);
+      gemm_f64_grouped(second, false, true, st);
+      first.n = second.n = 0;
+    };
     for (int i0 = 0; i0 < nt; i0 += 2 * g) {
       const int a0 = i0 * 64, a1 = std::min(n, (i0 + g) * 64);
       const int c0 = a1, c1 = std::min(n, (i0 + 2 * g) * 64);
       if (c0 >= n) continue;
       const int ra = a1 - a0, rc = c1 - c0;
+      if (first.n == kGemmGroups) flush();
       // T = B · A⁻¹   (B = L[c0:c1, a0:a1], A⁻¹ lower: k ≥ col)
-      gemm_f64(sub(L, c0, a0, rc, ra, false), false, sub(Linv, a0, a0, ra, ra, true), true,
-               out(tmp, c0, a0, rc, ra), 1.0, 0.0, KR_B_LOWER, false, st);
+      const int q = first.n++;
+      first.A[q] = sub(L, c0, a0, rc, ra, false);
+      first.B[q] = sub(Linv, a0, a0, ra, ra, true);
+      first.C[q] = out(tmp, c0, a0, rc, ra);
+      first.alpha[q] = 1.0;
+      first.beta[q] = 0.0;
+      first.mode[q] = KR_B_LOWER;
       // Linv[c0:c1, a0:a1] = −C⁻¹ · T   (C⁻¹ lower: k ≤ row)
-      gemm_f64(sub(Linv, c0, c0, rc, rc, false), false, sub(tmp, c0, a0, rc, ra, true), true,
-               out(Linv, c0, a0, rc, ra), -1.0, 0.0, KR_A_LOWER, false, st);
+      second.n++;
+      second.A[q] = sub(Linv, c0, c0, rc, rc, false);
+      second.B[q] = sub(tmp, c0, a0, rc, ra, true);
+      second.C[q] = out(Linv, c0, a0, rc, ra);
+      second.alpha[q] = -1.0;
+      second.beta[q] = 0.0;
+      second.mode[q] = KR_A_LOWER;
     }
+    flush();
   }
 }
 template void cholesky_solve<double, 64>(const double*, long long, int, const double*, double*,
