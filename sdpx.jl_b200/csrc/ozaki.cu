@@ -299,17 +299,42 @@ __global__ void __launch_bounds__(ONT, 1)
   if (warp == 0) umma::tmem_dealloc(tmem, 512);
 }
 
-__global__ void k_oz_reduce(const double* __restrict__ partial, const int2* __restrict__ pairs,
-                            int npairs, int nchunk, int m, double* __restrict__ S) {
-  const int pr = blockIdx.x;
+// S tile = Σ_chunks of the partial tiles, in chunk order, lower part only.
+// Four CTAs per tile, 32 rows each: coalesced reads of the row-major partials
+// (a thread's eight loads of a chunk in flight together), the 32 × 64 block
+// transposed through shared memory, each warp writing 32 consecutive rows of
+// one column of the column-major S.
+__global__ void __launch_bounds__(256) k_oz_reduce(const double* __restrict__ partial,
+                                                   const int2* __restrict__ pairs, int npairs,
+                                                   int nchunk, int m, double* __restrict__ S) {
+  __shared__ double blk[ON][33];
+  const int pr = blockIdx.x >> 2, r0 = (blockIdx.x & 3) * 32;
   const int2 tile = pairs[pr];
-  for (int e = threadIdx.x; e < OM * ON; e += blockDim.x) {
-    const int r = e / ON, c = e % ON;
-    const int gi = tile.x * OM + r, gj = tile.y * ON + c;
-    if (gi >= m || gj >= m || gi < gj) continue;
-    double s = 0.0;
-    for (int ch = 0; ch < nchunk; ++ch) s += partial[((size_t)ch * npairs + pr) * OM * ON + e];
-    S[gi + (size_t)gj * m] = s;
+  constexpr int PER = 32 * ON / 256;
+  double acc[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) acc[k] = 0.0;
+  const size_t tsz = (size_t)OM * ON;
+  const double* base = partial + (size_t)pr * tsz + (size_t)r0 * ON;
+  for (int ch = 0; ch < nchunk; ++ch) {
+    const double* src = base + (size_t)ch * npairs * tsz;
+    double v[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) v[k] = src[threadIdx.x + k * 256];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) acc[k] += v[k];
+  }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * 256, r = e / ON, c = e % ON;
+    blk[c][r] = acc[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * 256, r = e & 31, c = e >> 5;
+    const int gi = tile.x * OM + r0 + r, gj = tile.y * ON + c;
+    if (gi < m && gj < m && gi >= gj) S[gi + (size_t)gj * m] = blk[c][r];
   }
 }
 
@@ -682,7 +707,7 @@ void ozaki_syrk(const double* P, const OzakiPlan& plan, int8_t* digits, int* exp
   k_oz_syrk<<<units, ONT, OSMEM, st>>>(maps, d_pairs, plan.ntri, plan.kchunk, plan.Kp, exps, m,
                                        partial, err);
   if (ev_end) SDPX_CUDA(cudaEventRecord(ev_end, st));
-  k_oz_reduce<<<plan.ntri, 256, 0, st>>>(partial, d_pairs, plan.ntri, plan.nchunk, m, S);
+  k_oz_reduce<<<plan.ntri * 4, 256, 0, st>>>(partial, d_pairs, plan.ntri, plan.nchunk, m, S);
   SDPX_LAUNCH_CHECK_N(2);
 }
 
