@@ -71,6 +71,11 @@ int sdpx_b200_batch_optimize(sdpx_b200_batch* b, const sdpx_b200_solve_options* 
  * (k² column-major).  Any pointer may be NULL. */
 int sdpx_b200_batch_get_solution(sdpx_b200_batch* b, int32_t i, double* x, double* X, double* Y);
 
+/* Every instance's solution in one read-back: x receives Σ m_i doubles
+ * (instance i at Σ_{j<i} m_j), X and Y Σ k_i² doubles each (instance i's
+ * k_i² column-major entries at Σ_{j<i} k_j²).  Any pointer may be NULL. */
+int sdpx_b200_batch_get_solutions(sdpx_b200_batch* b, double* x, double* X, double* Y);
+
 /* Replaces instance i's current iterate with host x (m), X and Y (k²
  * column-major), e.g. to certify solutions computed elsewhere; NULL keeps
  * that part.  Certificates need every instance's x, X and Y set (or a solve). */

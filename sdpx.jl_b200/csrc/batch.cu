@@ -28,6 +28,7 @@
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/sdpx_b200_batch.h"
@@ -991,9 +992,12 @@ struct Pinned {
     SDPX_CUDA(cudaHostAlloc(&p, b, cudaHostAllocDefault));
     bytes = b;
   }
-  ~Pinned() {
+  void release() {
     if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
   }
+  ~Pinned() { release(); }
 };
 
 // The loop state of one instance (CoreLoop of driver_api.inc, one block).
@@ -1043,6 +1047,8 @@ struct Engine {
   DBuf<int4> d_work;
   DBuf<double> d_par, d_res;
   Pinned h_act, h_par, h_res, h_work;
+  Pinned h_stage[2];          // upload staging (create only)
+  cudaEvent_t ev_stage[2] = {nullptr, nullptr};
   Pool pool{};
   int schur_threads = 256, schur_tile = 32;
   // Affine fraction-to-boundary bounds: 0 the bisection of Cholesky trials
@@ -1061,6 +1067,8 @@ struct Engine {
     if (st) cudaStreamSynchronize(st);
     release_scope.begin();
     for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : ev_stage)
       if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
   }
@@ -1107,6 +1115,7 @@ struct Engine {
     SDPX_CUDA(cudaSetDevice(dev));
     SDPX_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     for (auto& e : ev) SDPX_CUDA(cudaEventCreate(&e));
+    for (auto& e : ev_stage) SDPX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     d_inst.alloc(N);
     A.alloc(a_tot);
     Ph.alloc(a_tot);
@@ -1116,15 +1125,14 @@ struct Engine {
     S.alloc(mm_tot);
     LS.alloc(mm_tot);
     SDPX_CUDA(cudaMemcpyAsync(d_inst.p, inst.data(), N * sizeof(Inst), cudaMemcpyHostToDevice, st));
+    upload_pooled(A.p, prob->Av, [&](int i) { return (long long)inst[i].k * inst[i].k * inst[i].m; });
+    upload_pooled(C.p, prob->C, [&](int i) { return (long long)inst[i].k * inst[i].k; });
+    upload_pooled(c.p, prob->c, [&](int i) { return (long long)inst[i].m; });
+    h_stage[0].release();  // the engine keeps no pinned staging after the upload
+    h_stage[1].release();
     for (int i = 0; i < N; ++i) {
       const Inst& I = inst[i];
       const long long kk = (long long)I.k * I.k;
-      SDPX_CUDA(cudaMemcpyAsync(A.p + I.a_off, prob->Av[i], kk * I.m * sizeof(double),
-                                cudaMemcpyHostToDevice, st));
-      SDPX_CUDA(cudaMemcpyAsync(C.p + I.kk_off, prob->C[i], kk * sizeof(double),
-                                cudaMemcpyHostToDevice, st));
-      SDPX_CUDA(cudaMemcpyAsync(c.p + I.m_off, prob->c[i], I.m * sizeof(double),
-                                cudaMemcpyHostToDevice, st));
       double mc = 0, mcc = 0;  // scale_p = 1 + ‖C‖max, scale_d = 1 + ‖c‖∞ (`data_norms`)
       for (long long e = 0; e < kk; ++e) mc = std::max(mc, std::fabs(prob->C[i][e]));
       for (int j = 0; j < I.m; ++j) mcc = std::max(mcc, std::fabs(prob->c[i][j]));
@@ -2134,6 +2142,69 @@ struct Engine {
     if (all) solved = true;
   }
 
+  // Host → device copy of one pooled array whose instance segments lie in
+  // input order (segment i of len(i) doubles from src[i]): consecutive
+  // instances are packed by a few host threads into one of two 64 MB pinned
+  // staging buffers, each buffer goes out as one asynchronous copy, and the
+  // other buffer is filled meanwhile — instead of one pageable copy per
+  // instance and array.
+  template <class Len>
+  void upload_pooled(double* dst, const double* const* src, Len len) {
+    constexpr size_t kStage = (size_t)8 << 20;  // doubles per staging buffer (64 MB)
+    Pinned& b0 = h_stage[0];
+    Pinned& b1 = h_stage[1];
+    b0.ensure(kStage * sizeof(double));
+    b1.ensure(kStage * sizeof(double));
+    const unsigned nthr = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    long long doff = 0;
+    int i = 0, which = 0;
+    bool pending[2] = {false, false};
+    while (i < N) {
+      // instances [i, j) that fit one buffer (a single instance always fits:
+      // at most 64²·256 doubles)
+      int j = i;
+      size_t fill = 0;
+      std::vector<size_t> at;
+      while (j < N && fill + (size_t)len(j) <= kStage) {
+        at.push_back(fill);
+        fill += (size_t)len(j);
+        ++j;
+      }
+      if (j == i) throw std::logic_error("upload_pooled: segment larger than the staging buffer");
+      if (pending[which]) SDPX_CUDA(cudaEventSynchronize(ev_stage[which]));
+      double* buf = static_cast<double*>((which ? b1 : b0).p);
+      auto pack = [&](unsigned t) {
+        for (int q = i + (int)t; q < j; q += (int)nthr)
+          std::memcpy(buf + at[q - i], src[q], (size_t)len(q) * sizeof(double));
+      };
+      std::vector<std::thread> pool;
+      for (unsigned t = 1; t < nthr && (int)t < j - i; ++t) pool.emplace_back(pack, t);
+      pack(0);
+      for (auto& th : pool) th.join();
+      SDPX_CUDA(cudaMemcpyAsync(dst + doff, buf, fill * sizeof(double), cudaMemcpyHostToDevice, st));
+      SDPX_CUDA(cudaEventRecord(ev_stage[which], st));
+      pending[which] = true;
+      doff += (long long)fill;
+      which ^= 1;
+      i = j;
+    }
+    SDPX_CUDA(cudaStreamSynchronize(st));  // the staging buffers are reused by the next array
+  }
+
+  // Every instance's x, X and Y in one read-back: the pooled arrays are laid
+  // out in input order (x_i at Σ_{j<i} m_j, X_i and Y_i at Σ_{j<i} k_j²).
+  void get_solutions(double* hx, double* hX, double* hY) {
+    long long mt = 0, kt = 0;
+    for (const Inst& I : inst) {
+      mt += I.m;
+      kt += (long long)I.k * I.k;
+    }
+    if (hx) SDPX_CUDA(cudaMemcpyAsync(hx, x.p, mt * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (hX) SDPX_CUDA(cudaMemcpyAsync(hX, X.p, kt * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (hY) SDPX_CUDA(cudaMemcpyAsync(hY, Y.p, kt * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SDPX_CUDA(cudaStreamSynchronize(st));
+  }
+
   void get_solution(int i, double* hx, double* hX, double* hY) {
     if (i < 0 || i >= N) throw std::invalid_argument("instance index out of range");
     const Inst& I = inst[i];
@@ -2238,6 +2309,10 @@ int sdpx_b200_batch_set_solution(sdpx_b200_batch* b, int32_t i, const double* x,
 
 int sdpx_b200_batch_get_solution(sdpx_b200_batch* b, int32_t i, double* x, double* X, double* Y) {
   BGUARD(b, b->e.get_solution(i, x, X, Y));
+}
+
+int sdpx_b200_batch_get_solutions(sdpx_b200_batch* b, double* x, double* X, double* Y) {
+  BGUARD(b, b->e.get_solutions(x, X, Y));
 }
 
 int sdpx_b200_batch_stats(sdpx_b200_batch* b, double* out8) {

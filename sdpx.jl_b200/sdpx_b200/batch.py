@@ -193,13 +193,19 @@ class BatchSolver:
         res = (SolveResult * n)()
         self._call("sdpx_b200_batch_optimize", C.byref(no), res)
         dp = C.POINTER(C.c_double)
+        mt = sum(p.m for p in self.problems)
+        kt = sum(p.k[0] * p.k[0] for p in self.problems)
+        xs, Xs, Ys = np.zeros(mt), np.zeros(kt), np.zeros(kt)
+        if solutions:  # one read-back of every instance's x, X, Y
+            self._call("sdpx_b200_batch_get_solutions", xs.ctypes.data_as(dp),
+                       Xs.ctypes.data_as(dp), Ys.ctypes.data_as(dp))
         out = []
+        mo = ko = 0
         for i, p in enumerate(self.problems):
             k = p.k[0]
-            x, X, Y = np.zeros(p.m), np.zeros(k * k), np.zeros(k * k)
-            if solutions:
-                self._call("sdpx_b200_batch_get_solution", i, x.ctypes.data_as(dp),
-                           X.ctypes.data_as(dp), Y.ctypes.data_as(dp))
+            x, X, Y = xs[mo:mo + p.m], Xs[ko:ko + k * k], Ys[ko:ko + k * k]
+            mo += p.m
+            ko += k * k
             r = res[i]
             out.append(SDPResult(
                 status=Status(STATUS_NAMES[r.status]), message=r.message.decode(errors="replace"),

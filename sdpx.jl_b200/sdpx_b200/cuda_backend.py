@@ -180,6 +180,7 @@ _SIGS = {
     "sdpx_b200_batch_create": [C.POINTER(BatchProblem), C.c_int, C.POINTER(C.c_void_p)],
     "sdpx_b200_batch_optimize": [C.c_void_p, C.POINTER(SolveOptions), C.POINTER(SolveResult)],
     "sdpx_b200_batch_get_solution": [C.c_void_p, C.c_int32, _dp, _dp, _dp],
+    "sdpx_b200_batch_get_solutions": [C.c_void_p, _dp, _dp, _dp],
     "sdpx_b200_batch_set_solution": [C.c_void_p, C.c_int32, _dp, _dp, _dp],
     "sdpx_b200_batch_certificate": [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int32,
                                     C.POINTER(CertificateResult)],

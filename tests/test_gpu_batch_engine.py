@@ -263,3 +263,22 @@ def test_batched_engine_at_its_size_limits(cuda_ok):
         assert rel(rb.pObj, rs.pObj) <= 1e-7 and rel(rb.dObj, rs.dObj) <= 1e-7
     assert all(r.status.value == "Optimal" for r in res)
     assert all(r.status.value == "Optimal" and r.relative_gap <= 1e-10 for r in dd)
+
+
+def test_bulk_solution_readback_equals_per_instance(cuda_ok):
+    """sdpx_b200_batch_get_solutions (one read-back, instances in input order)
+    returns exactly what sdpx_b200_batch_get_solution returns per instance."""
+    import ctypes as C
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = batch_instances(12, seed=5)
+    dp = C.POINTER(C.c_double)
+    with BatchSolver(probs) as bs:
+        res = bs.optimize(batch_options(1e-8), solutions=True)
+        for i, (p, r) in enumerate(zip(probs, res)):
+            k = p.k[0]
+            x, X, Y = np.zeros(p.m), np.zeros(k * k), np.zeros(k * k)
+            bs._call("sdpx_b200_batch_get_solution", i, x.ctypes.data_as(dp),
+                     X.ctypes.data_as(dp), Y.ctypes.data_as(dp))
+            assert np.array_equal(r.x, x)
+            assert np.array_equal(r.X[0], X.reshape(k, k).T)
+            assert np.array_equal(r.Y[0], Y.reshape(k, k).T)
