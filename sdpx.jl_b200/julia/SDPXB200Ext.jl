@@ -486,17 +486,25 @@ function optimize(b::B200Batch, tolerance::Float64; autotune::Bool=false,
     _bcheck(b, ccall((:sdpx_b200_batch_optimize, libsdpx), Cint,
                      (Ptr{Cvoid}, Ref{B200SolveOptions}, Ptr{B200SolveResult}), b.ptr, o, res),
             "optimize")
+    # every instance's (x, X, Y) in one read-back, concatenated in input order
+    mt = sum(d[2] for d in b.dims)
+    kt = sum(d[1]^2 for d in b.dims)
+    xs, Xs, Ys = zeros(mt), zeros(kt), zeros(kt)
+    _bcheck(b, ccall((:sdpx_b200_batch_get_solutions, libsdpx), Cint,
+                     (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                     b.ptr, xs, Xs, Ys), "get_solutions")
     out = Vector{Any}(undef, b.count)
+    mo = ko = 0
     for i in 1:b.count
         k, m = b.dims[i]
-        x, X, Y = zeros(m), zeros(k * k), zeros(k * k)
-        _bcheck(b, ccall((:sdpx_b200_batch_get_solution, libsdpx), Cint,
-                         (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
-                         b.ptr, Int32(i - 1), x, X, Y), "get_solution")
+        x = xs[mo+1:mo+m]
+        X = reshape(Xs[ko+1:ko+k*k], k, k)
+        Y = reshape(Ys[ko+1:ko+k*k], k, k)
+        mo += m
+        ko += k * k
         r = res[i]
         out[i] = (status=_STATUS[r.status], iterations=Int(r.iterations), x=x,
-                  X=reshape(X, k, k), Y=reshape(Y, k, k), pObj=r.p_obj, dObj=r.d_obj,
-                  pRes=r.p_res, dRes=r.d_res)
+                  X=X, Y=Y, pObj=r.p_obj, dObj=r.d_obj, pRes=r.p_res, dRes=r.d_res)
     end
     return out
 end
