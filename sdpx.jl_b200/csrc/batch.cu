@@ -2150,7 +2150,10 @@ struct Engine {
   // instance and array.
   template <class Len>
   void upload_pooled(double* dst, const double* const* src, Len len) {
-    constexpr size_t kStage = (size_t)8 << 20;  // doubles per staging buffer (64 MB)
+    size_t total = 0;
+    for (int q = 0; q < N; ++q) total += (size_t)len(q);
+    // doubles per staging buffer: 64 MB, or the whole array when smaller
+    const size_t kStage = std::min<size_t>((size_t)8 << 20, total);
     Pinned& b0 = h_stage[0];
     Pinned& b1 = h_stage[1];
     b0.ensure(kStage * sizeof(double));
