@@ -415,16 +415,11 @@ struct Handle {
     c.cols = kk;
     return c;
   }
-  // C_blk = alpha·op(A)·op(B) + beta·C_blk on block b (op given by descriptors)
-  void blk_gemm(const Opnd& a, bool akc, const Opnd& b, bool bkc, double* out, const DenseBlk& blk,
-                double alpha, double beta, int mode) {
-    gemm_f64(a, akc, b, bkc, blk_out(out, blk.off, blk.k), alpha, beta, mode, false, st);
-  }
 
   // The same product on every dense block, C_b = alpha·op(A_b)·op(B_b) +
   // beta·C_b (operands from opA(b), opB(b)), as one grouped launch per eight
   // blocks: the blocks' products are independent and each tile is computed
-  // as blk_gemm computes it.
+  // as gemm_f64 computes it for one block.
   template <class FA, class FB>
   void blk_gemm_all(FA opA, bool akc, FB opB, bool bkc, double* out, double alpha, double beta,
                     int mode) {
