@@ -96,6 +96,53 @@ def test_dense_gate_iteration_count_is_summation_order_sensitive():
     assert abs(a.iterations - b.iterations) <= 2
 
 
+def test_dense_gate_with_correctly_rounded_residuals_takes_the_reference_count():
+    """With P = 𝒜x − X − C and d = c − 𝒜ᵀY each rounded once from exact sums
+    (math.fsum of the exactly split products), the residuals no longer depend
+    on summation order, and the oracle takes the reference's recorded 9
+    iterations on the sdp_dense gate — the property the device's compensated
+    (Dot2) residual kernels rely on."""
+    import numpy as np
+    from sdpx_b200.driver import solve_with_backend
+    from oracle.sdpx_oracle import OracleBackend
+
+    def split(a):  # Veltkamp: a = hi + lo with 26-bit halves
+        c = 134217729.0 * a
+        hi = c - (c - a)
+        return hi, a - hi
+
+    def exact_products(u, v):  # u_i·v_i as exact sums of four products
+        uh, ul = split(np.asarray(u, dtype=np.float64))
+        vh, vl = split(np.asarray(v, dtype=np.float64))
+        return np.concatenate([uh * vh, uh * vl, ul * vh, ul * vl])
+
+    class CorrectlyRounded(OracleBackend):
+        def compute_residuals(self, mu, use_affine, factor):
+            r = super().compute_residuals(mu, use_affine, factor)
+            d = np.empty(self.m)
+            for i in range(self.m):
+                terms = [self.c[i]]
+                for l in range(len(self.k)):
+                    terms.extend((-exact_products(self.Av[l][i], self.Y[l].reshape(-1))).tolist())
+                d[i] = math.fsum(terms)
+            self.d = d
+            for l in range(len(self.k)):
+                A = self.Av[l]
+                Xv, Cv = self.X[l].reshape(-1), self.C[l].reshape(-1)
+                P = np.array([math.fsum(exact_products(self.x, A[:, e]).tolist() + [-Xv[e], -Cv[e]])
+                              for e in range(A.shape[1])])
+                self.P[l] = P.reshape(self.k[l], self.k[l])
+                self.block_norms[l] = float(np.max(np.abs(P)))
+            return float(np.max(self.block_norms)), float(np.max(np.abs(d))), r[2]
+
+    opts = SolverOptions().with_tolerance(GOLD["sdp_dense"]["tolerance"])
+    r = solve_with_backend(CorrectlyRounded(G.gate_dense()), opts)
+    assert r.status.value == GOLD["sdp_dense"]["status"]
+    assert r.iterations == GOLD["sdp_dense"]["iterations"]
+    base = GOLD["sdp_dense"]["objective"]
+    assert abs(r.pObj - base) / max(1.0, abs(base)) <= GOLD["compare"]["objective_rel"]
+
+
 # ---- equality rows (n > 0): test/correctness.jl:97-135, T6 pin :230-242 ----
 
 def _fixed():
