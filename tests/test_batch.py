@@ -93,3 +93,58 @@ def test_concurrent_batch_equals_single_solves():
         assert rb.iterations == rs.iterations
         assert rb.pObj == rs.pObj and rb.dObj == rs.dObj
     assert sum(r.status.value == "Optimal" for r in batch) >= 11
+
+
+def test_bulk_solutions_are_sliced_per_instance(monkeypatch):
+    """BatchSolver.optimize reads every solution with one
+    sdpx_b200_batch_get_solutions call and slices the concatenated arrays in
+    input order (x_i at Σ_{j<i} m_j, X_i and Y_i at Σ_{j<i} k_j², column-major):
+    checked against a stand-in for the library that writes position-tagged
+    values, so no device is needed."""
+    import sdpx_b200.cuda_backend as cb
+    from sdpx_b200.batch import BatchSolver, batch_options
+    probs = batch_instances(5, seed=1)
+    mt = sum(p.m for p in probs)
+    kt = sum(p.k[0] ** 2 for p in probs)
+    calls = []
+
+    class StandIn:
+        def sdpx_b200_batch_create(self, prob, device, h):
+            h._obj.value = 1
+            return 0
+
+        def sdpx_b200_batch_optimize(self, h, opts, res):
+            for i in range(len(probs)):
+                res[i].status = 1
+                res[i].iterations = i
+            return 0
+
+        def sdpx_b200_batch_get_solutions(self, h, x, X, Y):
+            calls.append("bulk")
+            np.ctypeslib.as_array(x, shape=(mt,))[:] = np.arange(mt)
+            np.ctypeslib.as_array(X, shape=(kt,))[:] = np.arange(kt) + 0.5
+            np.ctypeslib.as_array(Y, shape=(kt,))[:] = -np.arange(kt, dtype=np.float64)
+            return 0
+
+        def sdpx_b200_batch_destroy(self, h):
+            return None
+
+        def sdpx_b200_batch_last_error(self, h):
+            return b""
+
+    monkeypatch.setattr(cb, "load_library", lambda *a, **k: StandIn())
+    with BatchSolver(probs) as bs:
+        res = bs.optimize(batch_options(1e-8), solutions=True)
+        assert calls == ["bulk"]
+        mo = ko = 0
+        for i, (p, r) in enumerate(zip(probs, res)):
+            k = p.k[0]
+            assert r.status.value == "Optimal" and r.iterations == i
+            assert np.array_equal(r.x, np.arange(mo, mo + p.m))
+            X = (np.arange(ko, ko + k * k) + 0.5).reshape(k, k).T   # column-major → matrix
+            assert np.array_equal(r.X[0], X)
+            assert np.array_equal(r.Y[0], -np.arange(ko, ko + k * k, dtype=np.float64).reshape(k, k).T)
+            mo += p.m
+            ko += k * k
+        bare = bs.optimize(batch_options(1e-8), solutions=False)
+        assert calls == ["bulk"] and all(not r.x.any() for r in bare)
